@@ -1,0 +1,351 @@
+"""Benchmark of the frozen-flow ellipsoidal-particle step (particle-steps/s).
+
+Default workload: 512^3 FP32 frozen field, 16,777,216 polydisperse spheroids
+(AR log-uniform [0.2, 5], b log-normal(ln 1e-3, 0.3), St uniform [0.1, 10]),
+dt = 5e-4, collisions on, mixed-precision form, one CUDA-graph step per iteration.
+
+``python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]``
+
+* ours: W untimed steps, then K steps timed with CUDA events on the library's stream
+  (one captured graph of K steps with events around every phase), barrier and max over
+  ranks; N>1 runs independent replicas (one ensemble per GPU, no collective in the step).
+* reference: the CPU restatement of the reference algorithm (candidate pairs solved
+  with Levenberg-Marquardt without a prefilter, as the reference does) timed on the
+  host cores on a bounded sample with the workload's particle density and sizes.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c3_512cube_n16777216_fp32field")
+    ap.add_argument("--precision", default=None, choices=[None, "mixed", "fp64"])
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the FP64 comparison run")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# workload construction
+# ---------------------------------------------------------------------------
+def build_inputs(w, device, precision):
+    import torch
+    from gazpart_b200 import field, particles
+    setup = w.setup()
+    f = field.generate(w.grid, seed=w.field_seed, device=device)
+    st = particles.draw(w.spec, setup)
+    return setup, f, st
+
+
+def make_context(setup, f, st, precision, device):
+    import torch
+    from gazpart_b200 import api, particles
+    ctx = api.Context(setup, precision)
+    ctx.set_fields({k: f[k].contiguous() for k in api.FIELD_KEYS})
+    # initial velocities: u = u_f(x), omega = 1/2 omega_f in the body frame
+    xs = [torch.from_numpy(st[k]).to(device) for k in ("x", "y", "z")]
+    g = [ctx.interp_lag3(c, *xs).cpu().numpy() for c in range(6)]
+    st["u"], st["v"], st["w"] = g[0], g[1], g[2]
+    particles.body_half_vorticity(st, g[3], g[4], g[5])
+    ctx.upload(st)
+    return ctx
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class Clocks:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        except OSError:
+            pass
+        finally:
+            try:
+                os.unlink(self.path)
+            except OSError:
+                pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# measured peaks
+# ---------------------------------------------------------------------------
+def hbm_peak():
+    try:
+        d = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def reduce_max_ms(ms: float, dist, device) -> float:
+    """Job time of N replicas: the slowest rank's device time (max over ranks)."""
+    if dist is None:
+        return ms
+    import torch
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def advance_bytes_per_particle(components: int, field_bytes: int) -> int:
+    """Algorithmic bytes of one particle-step of the fused advance kernel.
+
+    Gather: 64 stencil points x C components x field word, positions read (24 B) and the
+    interpolated values (8 B each, as the reference stores them); plus the particle state
+    read and written (13 doubles each way) and the per-particle constants (6 doubles)."""
+    gather = 64 * components * field_bytes + 24 + 8 * components
+    return gather + 256
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the restatement of the reference algorithm on the host cores
+# ---------------------------------------------------------------------------
+def cpu_sample(w, scale: int, max_emaj: float):
+    """A periodic box of side L/scale with the workload's particle density and size
+    distribution; the collision box edge is taken from the full workload's largest
+    particle so each particle sees the same candidate count as in the full run."""
+    import torch
+    from gazpart_b200 import config, field, particles
+    import pyoracle as po
+    base = w.setup()
+    n_s = max(8, w.grid // scale)
+    L = base.lx / scale
+    setup = config.Setup(nx=n_s, ny=n_s, nz=n_s, lx=L, ly=L, lz=L, visc=base.visc, dtime=base.dtime)
+    spec = config.ParticleSpec(**{**w.spec.__dict__, "n": max(64, w.spec.n // scale ** 3), "seed": 77})
+    f = field.generate(n_s, lbox=L, seed=1, device="cpu")
+    refs = [field.reference_layout(f[k], "periodic" if k in ("u", "v", "w") else "zero").numpy().copy()
+            for k in field.COMPONENTS_6]
+    st = particles.draw(spec, setup)
+    uf = [po.interp_lag3(setup, refs[c], st["x"], st["y"], st["z"]) for c in range(6)]
+    st["u"], st["v"], st["w"] = uf[0].copy(), uf[1].copy(), uf[2].copy()
+    particles.body_half_vorticity(st, uf[3], uf[4], uf[5])
+    ens = po.Ensemble(setup, st)
+    g = po.OrcBoxGrid()
+    po.lib().orc_collision_initiation(po.C.byref(po.make_setup(setup)), po.C.c_double(max_emaj), po.C.byref(g))
+    return ens, refs, g
+
+
+def time_cpu(w, steps: int, threads: int, scale: int, max_emaj: float):
+    ens, refs, g = cpu_sample(w, scale, max_emaj)
+    t_adv = t_col = 0.0
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        rc = ens.advance(refs, nthreads=threads)
+        t1 = time.perf_counter()
+        res = ens.collide(prefilter=False, nthreads=threads, grid=g)
+        t2 = time.perf_counter()
+        t_adv += t1 - t0
+        t_col += t2 - t1
+        if rc or res["rc"]:
+            break
+    per_step = (t_adv + t_col) / steps
+    return {"value": ens.n / per_step, "n": ens.n, "steps": steps, "t_adv": t_adv / steps,
+            "t_col": t_col / steps, "candidates_per_step": res["n_candidates"], "nbox": g.nbox}
+
+
+def workload_max_emaj(w) -> float:
+    from gazpart_b200 import particles
+    st = particles.draw(w.spec, w.setup())
+    return float(st["emaj"].max())
+
+
+# ---------------------------------------------------------------------------
+def main():
+    args = parse()
+    from gazpart_b200 import config
+    w = config.WORKLOADS[args.workload]
+    precision = args.precision or ("mixed" if w.field_dtype == "f32" else "fp64")
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        threads = os.cpu_count() or 1
+        scale = 16 if w.grid >= 256 else 1
+        max_emaj = workload_max_emaj(w)
+        k = max(1, min(args.steps, 8))
+        if args.warmup:
+            time_cpu(w, 1, threads, scale, max_emaj)
+        r = time_cpu(w, k, threads, scale, max_emaj)
+        sample = (f"{r['n']} particles at the workload's density in a (L/{scale})^3 periodic box, "
+                  f"collision boxes sized from the full workload ({r['nbox']} boxes), "
+                  f"{r['candidates_per_step']} candidate pairs/step each solved by Levenberg-Marquardt "
+                  f"as the reference does; {k} steps timed")
+        line = {"impl": "reference", "metric": "particle-steps/s", "value": r["value"], "unit": "particle-steps/s",
+                "n_gpus": args.gpus, "steps": k, "warmup": args.warmup, "ms_per_step": 1e3 * (r["t_adv"] + r["t_col"]),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "config": {"workload": w.name, "precision": "fp64 (reference)"},
+                "cpu_baseline": {"value": r["value"], "unit": "particle-steps/s", "cores": threads,
+                                 "kind": "port", "sample": sample},
+                "e2e": {"value": r["value"], "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+    from gazpart_b200 import api
+    torch.cuda.set_device(local)
+    device = f"cuda:{local}"
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device(device))
+
+    setup, f, st = build_inputs(w, device, precision)
+    max_emaj = float(st["emaj"].max())
+    ctx = make_context(setup, f, st, precision, device)
+    n = ctx.n
+    ctx.step(args.warmup)
+    ctx.sync()
+    ctx.raise_status("warm-up")
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with Clocks(local) as clk:
+        total_ms, adv_ms, col_ms, kps = ctx.step_timed(args.steps)
+    clocks = clk.summary()
+    ctx.raise_status("timed steps")
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    total_ms = reduce_max_ms(total_ms, dist, device)
+    ms_per_step = total_ms / args.steps
+    value = n * world * args.steps / (total_ms / 1e3)
+
+    # roofline of the dominant kernel (the fused advance)
+    fbytes = 4 if precision == "mixed" else 8
+    bpp = advance_bytes_per_particle(6, fbytes)
+    peak, peak_kind = hbm_peak()
+    achieved = bpp * n / (adv_ms / 1e3) / 1e9
+    roofline = {"bound": "hbm", "kernel": "k_advance", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind,
+                "bytes_per_launch": bpp * n, "bytes_per_particle": bpp,
+                "advance_ms": adv_ms, "collision_ms": col_ms, "traffic": None}
+
+    # end to end through the C ABI with host buffers: H2D of the state, one step,
+    # D2H of the state, every step
+    pinned = {k: torch.empty(n, dtype=torch.float64, pin_memory=True).numpy() for k in api.STATE_KEYS}
+    ctx.download_into(pinned)
+    ctx.sync()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        ctx.put_state(pinned)
+        ctx.step(1)
+        ctx.download_into(pinned)
+    e2e_s = (time.perf_counter() - t0) / args.e2e_steps
+    ctx.raise_status("e2e steps")
+    bytes_state = 13 * 8 * n
+    e2e = {"value": n / e2e_s, "unit": "particle-steps/s", "h2d_bytes_per_step": bytes_state,
+           "d2h_bytes_per_step": bytes_state, "ms_per_step": 1e3 * e2e_s}
+
+    plain = None
+    if not args.no_plain and precision == "mixed":
+        ctx.close()
+        del ctx
+        torch.cuda.empty_cache()
+        st2 = build_inputs(w, device, "fp64")[2]
+        f64 = {k: v for k, v in f.items()}
+        pctx = make_context(setup, f64, st2, "fp64", device)
+        pctx.step(max(1, args.warmup))
+        pctx.sync()
+        tms, pa, pc, _ = pctx.step_timed(max(5, args.steps // 5))
+        pctx.raise_status("fp64 steps")
+        plain = {"value": n * max(5, args.steps // 5) / (tms / 1e3), "advance_ms": pa, "collision_ms": pc}
+        pctx.close()
+    else:
+        ctx.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        threads = os.cpu_count() or 1
+        scale = 16 if w.grid >= 256 else 1
+        r = time_cpu(w, 2, threads, scale, max_emaj)
+        cpu = {"value": r["value"], "unit": "particle-steps/s", "cores": threads, "kind": "port",
+               "sample": f"{r['n']} particles at the workload's density in a (L/{scale})^3 periodic box, "
+                         f"{r['candidates_per_step']} LM contact solves/step as the reference does, 2 steps"}
+
+    if rank == 0:
+        line = {"metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if precision == "fp64" else "f32/f64",
+                "data": "synthetic",
+                "config": {"workload": w.name, "precision": precision, "particles_per_gpu": n,
+                           "field": f"{w.grid}^3 x 6 {'f32' if fbytes == 4 else 'f64'}",
+                           "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (state+field > 5 GB)"},
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": kps * args.steps,
+                "kernels_per_step": kps, "clocks": clocks, "fp64_plain": plain}
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

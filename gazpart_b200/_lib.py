@@ -1,0 +1,134 @@
+"""ctypes binding of ``libgazpart_b200.so`` (the C ABI in ``include/gazpart_gpu.h``).
+
+The shared library is built in-tree (``gazpart_b200/csrc/Makefile``).  Loading fails
+loudly if it is missing: there is no CPU fallback for any entry point.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgazpart_b200.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "gazpart_gpu.h")
+
+GP_OK = 0
+ERRORS = {
+    1: "GP_ENAN_FORCE: NaN drag coefficient ('In Fluid force')",
+    2: "GP_ENAN_TORQUE: NaN angular velocity in FLUID_TORQUE_ELLIPSOID",
+    3: "GP_EENERGY: kinetic-energy balance violated in an impulse response",
+    4: "GP_ESINGULAR: matrix is numerically singular",
+    5: "GP_EPAIR_OVERFLOW: pair buffer full",
+    6: "GP_EOUT_OF_GRID: particle outside the box grid or stencil range",
+    7: "GP_ETIMEOUT: bounded loop or wait gave up",
+    8: "GP_ECUDA: CUDA runtime error",
+    9: "GP_EBADARG: invalid argument or unsupported configuration",
+    10: "GP_ENOMEM: device allocation refused",
+}
+PREC_FP64, PREC_MIXED = 0, 1
+LAYOUT_INTERIOR, LAYOUT_REFERENCE = 0, 1
+GHOST_PERIODIC, GHOST_ZERO = 0, 1
+
+
+class GPError(RuntimeError):
+    def __init__(self, code: int, where: str):
+        self.code = code
+        super().__init__(f"{where}: {ERRORS.get(code, code)}")
+
+
+class GPParams(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
+                ("lx", C.c_double), ("ly", C.c_double), ("lz", C.c_double),
+                ("visc", C.c_double), ("rhof", C.c_double), ("dtime", C.c_double),
+                ("gravity", C.c_double), ("ecp", C.c_double), ("mup", C.c_double),
+                ("ecw", C.c_double), ("muw", C.c_double),
+                ("periodicity", C.c_int32), ("wall_boundary", C.c_int32),
+                ("interp_scheme", C.c_int32), ("frozen_flow", C.c_int32),
+                ("precision", C.c_int32), ("store_fluid", C.c_int32),
+                ("max_particles", C.c_int64)]
+
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int32)
+_i64p = C.POINTER(C.c_int64)
+_vp = C.c_void_p
+_ctx = C.c_void_p
+
+# name -> argtypes (restype is int for all)
+SIGNATURES = {
+    "gp_ctx_create": [C.POINTER(GPParams), C.POINTER(_ctx)],
+    "gp_ctx_destroy": [_ctx],
+    "gp_status": [_ctx, _ip, _i64p],
+    "gp_clear_status": [_ctx],
+    "gp_sync": [_ctx],
+    "gp_set_class": [_ctx, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double],
+    "gp_set_field": [_ctx, C.c_int32, _vp, C.c_int32, C.c_int32, C.c_int32],
+    "gp_upload_state": [_ctx, C.c_int64, C.POINTER(_vp), C.POINTER(_vp), C.c_int32],
+    "gp_download_state": [_ctx, C.c_int64, C.POINTER(_vp), C.POINTER(_vp), C.c_int32],
+    "gp_put_state": [_ctx, C.c_int64, C.POINTER(_vp), C.c_int32],
+    "gp_step_timed": [_ctx, C.c_int32, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float),
+                      _ip],
+    "gp_adv_particle_ellp": [_ctx, C.c_int32],
+    "gp_collision": [_ctx, C.c_int32, C.c_double, _i64p, _i64p, _i64p],
+    "gp_step": [_ctx, C.c_int32],
+    "gp_collision_pairs": [_ctx, C.c_int64, _ip, _ip, _i64p],
+    "gp_collision_box_connectivity": [_ctx, _ip, _ip, _ip, _ip, _dp],
+    "gp_interp_lag3": [_ctx, C.c_int32, C.c_int64, _vp, _vp, _vp, _vp, C.c_int32],
+    "gp_frozen_interp_lag3": [_ctx, _dp, _dp, _dp, C.c_int32, C.c_int32, C.c_int32, _dp, C.c_int64,
+                              _dp, _dp, _dp, _dp],
+    "gp_fluid_force_ellipsoid": [_ctx, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double,
+                                 C.c_double, C.c_double, C.c_double, _dp, _dp, _dp],
+    "gp_fluid_force_ellipsoid_batch": [_ctx, C.c_int64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, C.c_int32],
+    "gp_fluid_torque_ellipsoid": [_ctx, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, _dp,
+                                  _dp, _dp, _dp, _dp, _dp],
+    "gp_fluid_torque_ellipsoid_batch": [_ctx, C.c_int64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                                        C.c_int32],
+    "gp_quaternion_integration": [_ctx, _dp, C.c_double, C.c_double, C.c_double, C.c_double],
+    "gp_quaternion_integration_batch": [_ctx, C.c_int64, _vp, _vp, C.c_double, C.c_int32],
+    "gp_euler_integration": [_ctx, C.c_int32, C.c_int32, _dp, _dp, _dp],
+    "gp_ellipsoid_contact_detection": [_ctx, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double,
+                                       C.c_double, _dp, C.c_double, C.c_double, C.c_double, _dp, _ip,
+                                       _dp, _dp, _dp],
+    "gp_ellipsoid_contact_detection_batch": [_ctx, C.c_int64, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                                             C.c_int32],
+    "gp_collision_response": [_ctx, C.c_int32, C.c_int32, _dp, _dp, _dp, _dp, _dp],
+}
+
+_lib = None
+
+
+def build(verbose: bool = False) -> None:
+    """Compile the CUDA library in-tree for sm_100a."""
+    cmd = ["make", "-C", os.path.join(HERE, "csrc"), "-j4"]
+    if not verbose:
+        cmd.insert(1, "-s")
+    subprocess.run(cmd, check=True)
+
+
+def lib():
+    """Load the library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with gazpart_b200._lib.build() "
+                               "(there is no CPU fallback)")
+        L = C.CDLL(LIB_PATH)
+        for name, args in SIGNATURES.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def check(rc: int, where: str) -> None:
+    if rc != GP_OK:
+        raise GPError(rc, where)
+
+
+def exported_symbols():
+    """Names declared in include/gazpart_gpu.h (parsed from the header)."""
+    import re
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"^int\s+(gp_\w+)\s*\(", text, flags=re.M)))

@@ -1,0 +1,445 @@
+// gp_advance.cuh -- fused ADV_PARTICLE_ELLP kernel body: 64-point Lagrange gather of
+// the six field components at x_n, RK2 predictor/corrector with the wall test and
+// rebound, periodic wrap.  Included by the FP64 (plain) and the mixed translation units.
+#pragma once
+#include "gp_device.cuh"
+
+namespace gp {
+
+// Internal field layout: [k: nz+4][j: ny+4][i: nx+3][c: ncomp].  Reference index
+// (I, J, K) with J, K in -1..N+2 (NGHTCELL=2 ghost planes) and I in 1..NX maps to
+// (I, J+1, K+1); x ghost columns 0, NX+1, NX+2 hold columns NX, 1, 2 so that the
+// periodic x wrap of interp_lag3.f90:132-154 reads four contiguous points.
+__device__ __forceinline__ int64_t field_point(const InstDev& I, int ix, int jy, int kz) {
+  return ((int64_t)(kz + 1) * (I.ny + 4) + (jy + 1)) * (int64_t)(I.nx + 3) + ix;
+}
+
+// Cubic Lagrange weights (interp_lag3.f90:196-211), FP64.
+__device__ __forceinline__ void lag3_w(double a, double f[4]) {
+  f[0] = -1. / 6. * (a - 2.) * (a - 1.) * a;
+  f[1] = 1. / 2. * (a - 2.) * (a - 1.) * (a + 1.);
+  f[2] = -1. / 2. * (a - 2.) * a * (a + 1.);
+  f[3] = 1. / 6. * (a - 1.) * a * (a + 1.);
+}
+__device__ __forceinline__ void lag3_wf(float a, float f[4]) {
+  f[0] = -1.f / 6.f * (a - 2.f) * (a - 1.f) * a;
+  f[1] = 0.5f * (a - 2.f) * (a - 1.f) * (a + 1.f);
+  f[2] = -0.5f * (a - 2.f) * a * (a + 1.f);
+  f[3] = 1.f / 6.f * (a - 1.f) * a * (a + 1.f);
+}
+
+struct Stencil {
+  int ix[4], j0, k0;
+  double alfa, beta, gama;
+  bool contiguous;
+};
+
+// Stencil nodes of interp_lag3.f90:124-190.  Returns false if the stencil leaves the
+// array (the reference would read out of bounds).
+__device__ __forceinline__ bool stencil(const InstDev& I, double x, double y, double z, Stencil& s) {
+  const double dxa = I.dx, dya = I.dy, dza = I.dz;   // XAIN(2)-XAIN(1) = DX
+  const double fx = x / dxa, fy = y / dya, fz = z / dza;
+  if (!(fx > -2.0 && fx < 2147483000.0 && fy > -2.0 && fy < 2147483000.0 && fz > -2.0 &&
+        fz < 2147483000.0))
+    return false;
+  const int i0 = (int)fx + 1, j0 = (int)fy + 1, k0 = (int)fz + 1;
+  if (i0 < 1 || i0 > I.nx || j0 < 0 || j0 > I.ny || k0 < 0 || k0 > I.nz) return false;
+  if (I.wall_boundary) {
+    const int iend = I.nx;
+    int ip1 = (i0 == iend) ? iend - 1 : i0 + 1;
+    int ip2 = (ip1 == iend) ? iend - 1 : ip1 + 1;
+    int im1 = (i0 == 1) ? 2 : i0 - 1;
+    s.ix[0] = im1; s.ix[1] = i0; s.ix[2] = ip1; s.ix[3] = ip2;
+    s.contiguous = (ip2 == i0 + 2) && (im1 == i0 - 1);
+  } else {
+    s.ix[0] = i0 - 1; s.ix[1] = i0; s.ix[2] = i0 + 1; s.ix[3] = i0 + 2;
+    s.contiguous = true;
+  }
+  s.j0 = j0;
+  s.k0 = k0;
+  // explicit IEEE roundings: identical offsets whether or not the translation unit
+  // contracts multiply-adds (the FP64 and mixed paths share this routine)
+  s.alfa = __ddiv_rn(__dsub_rn(x, __dmul_rn((double)(i0 - 1), I.dx)), dxa);
+  s.beta = __ddiv_rn(__dsub_rn(y, __dmul_rn(I.dy, (double)(j0 - 1))), dya);
+  s.gama = __ddiv_rn(__dsub_rn(z, __dmul_rn(I.dz, (double)(k0 - 1))), dza);
+  return true;
+}
+
+// FP64 gather of the six components with the reference's nesting z(y(x))
+// (interp_lag3.f90:220-288).
+__device__ __forceinline__ void gather6_fp64(const InstDev& I, const Stencil& s, double out[6]) {
+  const double* __restrict__ F = static_cast<const double*>(I.field);
+  double fx[4], fy[4], fz[4];
+  lag3_w(s.alfa, fx);
+  lag3_w(s.beta, fy);
+  lag3_w(s.gama, fz);
+  double zs[6];
+#pragma unroll
+  for (int kk = 0; kk < 4; ++kk) {
+    double ys[6];
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj) {
+      double xs[6];
+      const int64_t p0 = field_point(I, s.ix[0], s.j0 - 1 + jj, s.k0 - 1 + kk);
+      if (s.contiguous) {
+        const double2* row = reinterpret_cast<const double2*>(F + p0 * 6);
+        double v[24];
+#pragma unroll
+        for (int t = 0; t < 12; ++t) {
+          const double2 d = __ldg(row + t);
+          v[2 * t] = d.x;
+          v[2 * t + 1] = d.y;
+        }
+#pragma unroll
+        for (int c = 0; c < 6; ++c)
+          xs[c] = fx[0] * v[c] + fx[1] * v[6 + c] + fx[2] * v[12 + c] + fx[3] * v[18 + c];
+      } else {
+        double v[24];
+#pragma unroll
+        for (int ii = 0; ii < 4; ++ii) {
+          const int64_t pp = field_point(I, s.ix[ii], s.j0 - 1 + jj, s.k0 - 1 + kk);
+#pragma unroll
+          for (int c = 0; c < 6; ++c) v[6 * ii + c] = __ldg(F + pp * 6 + c);
+        }
+#pragma unroll
+        for (int c = 0; c < 6; ++c)
+          xs[c] = fx[0] * v[c] + fx[1] * v[6 + c] + fx[2] * v[12 + c] + fx[3] * v[18 + c];
+      }
+#pragma unroll
+      for (int c = 0; c < 6; ++c) ys[c] = (jj == 0) ? fy[0] * xs[c] : ys[c] + fy[jj] * xs[c];
+    }
+#pragma unroll
+    for (int c = 0; c < 6; ++c) zs[c] = (kk == 0) ? fz[0] * ys[c] : zs[c] + fz[kk] * ys[c];
+  }
+#pragma unroll
+  for (int c = 0; c < 6; ++c) out[c] = zs[c];
+}
+
+// FP32 field, FP32 weights, Kahan-compensated FP32 accumulation of the 64 products
+// w_x w_y w_z U.  Result returned in double.
+__device__ __forceinline__ void gather6_fp32(const InstDev& I, const Stencil& s, double out[6]) {
+  const float* __restrict__ F = static_cast<const float*>(I.field);
+  float fx[4], fy[4], fz[4];
+  lag3_wf((float)s.alfa, fx);
+  lag3_wf((float)s.beta, fy);
+  lag3_wf((float)s.gama, fz);
+  float sum[6], cmp[6];
+#pragma unroll
+  for (int c = 0; c < 6; ++c) { sum[c] = 0.f; cmp[c] = 0.f; }
+#pragma unroll
+  for (int kk = 0; kk < 4; ++kk) {
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj) {
+      const float wyz = fz[kk] * fy[jj];
+      const int64_t p0 = field_point(I, s.ix[0], s.j0 - 1 + jj, s.k0 - 1 + kk);
+      float v[24];
+      if (s.contiguous) {
+        const float2* row = reinterpret_cast<const float2*>(F + p0 * 6);
+#pragma unroll
+        for (int t = 0; t < 12; ++t) {
+          const float2 d = __ldg(row + t);
+          v[2 * t] = d.x;
+          v[2 * t + 1] = d.y;
+        }
+      } else {
+#pragma unroll
+        for (int ii = 0; ii < 4; ++ii) {
+          const int64_t pp = field_point(I, s.ix[ii], s.j0 - 1 + jj, s.k0 - 1 + kk);
+#pragma unroll
+          for (int c = 0; c < 6; ++c) v[6 * ii + c] = __ldg(F + pp * 6 + c);
+        }
+      }
+#pragma unroll
+      for (int ii = 0; ii < 4; ++ii) {
+        const float w = wyz * fx[ii];
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+          // Kahan step: sum += w*v with the lost low part carried in cmp
+          const float y = __fmaf_rn(w, v[6 * ii + c], -cmp[c]);
+          const float t = __fadd_rn(sum[c], y);
+          cmp[c] = __fsub_rn(__fsub_rn(t, sum[c]), y);
+          sum[c] = t;
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 6; ++c) out[c] = (double)sum[c] - (double)cmp[c];
+}
+
+// ---------------------------------------------------------------------------
+// Mixed-precision force and torque: relative velocities and frames in FP64, the
+// Zastawny correlation coefficients in FP32, forces assembled in FP64.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool fluid_force_mixed(const PartConst& pc, double visc, double up, double vp,
+                                                  double wp, double uf, double vf, double wf, const double r[9],
+                                                  double f[3]) {
+  double p[3] = {uf - up, vf - vp, wf - wp};
+  const double umag = sqrt(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]);
+  f[0] = f[1] = f[2] = 0.0;
+  if (umag == 0.0) return true;
+  // body frame: R^T p
+  const double b0 = r[0] * p[0] + r[1] * p[1] + r[2] * p[2];
+  const double b1 = r[3] * p[0] + r[4] * p[1] + r[5] * p[2];
+  const double b2 = r[6] * p[0] + r[7] * p[1] + r[8] * p[2];
+  const double syz = sqrt(b1 * b1 + b2 * b2);
+  const float rep = (float)((umag * pc.deq) / visc);
+  const float phi = fabsf(atanf((float)(syz / b0)));
+  float sphi, cphi;
+  sincosf(phi, &sphi, &cphi);
+  cphi = fmaxf(cphi, 0.f);   // float(pi/2) lies above pi/2: keep cos(phi) >= 0 as in FP64
+  const float lr = __log2f(rep);
+  const float cd0 = 18.12f * exp2f(-1.023f * lr) + 4.26f * exp2f(-0.384f * lr);
+  const float cd90 = 21.52f * exp2f(-0.990f * lr) + 2.86f * exp2f(-0.260f * lr);
+  const float cdrag = cd0 + (cd90 - cd0) * powf(sphi, 1.95f);
+  const float clift = (0.083f * exp2f(0.21f * lr) + 1.582f * exp2f(-0.851f * lr)) *
+                      powf(sphi, 1.842f - 0.802f * exp2f(-0.006f * lr)) *
+                      powf(cphi, 0.874f + 0.009f * exp2f(0.570f * lr));
+  const double kd = pc.cdrag * (double)cdrag * umag;
+  const double kl = pc.cdrag * (double)clift * (umag * umag);
+  double fb0 = kd * b0 + kl * (double)sphi * copysign(1.0, -b0);
+  double fb1 = kd * b1, fb2 = kd * b2;
+  if (syz != 0.0) {
+    fb1 += kl * (double)cphi * (b1 / syz);
+    fb2 += kl * (double)cphi * (b2 / syz);
+  }
+  f[0] = r[0] * fb0 + r[3] * fb1 + r[6] * fb2;
+  f[1] = r[1] * fb0 + r[4] * fb1 + r[7] * fb2;
+  f[2] = r[2] * fb0 + r[5] * fb1 + r[8] * fb2;
+  return !(cdrag != cdrag) && isfinite(f[0]) && isfinite(f[1]) && isfinite(f[2]);
+}
+
+__device__ __forceinline__ void fluid_torque_mixed(const PartConst& pc, double visc, double upn, double vpn,
+                                                   double wpn, double uf, double vf, double wf, double wx,
+                                                   double wy, double wz, double ox, double oy, double oz,
+                                                   const double r[9], double t[3]) {
+  const double p0 = uf - upn, p1 = vf - vpn, p2 = wf - wpn;
+  const double umag = sqrt(p0 * p0 + p1 * p1 + p2 * p2);
+  const double b0 = r[0] * p0 + r[1] * p1 + r[2] * p2;
+  const double b1 = r[3] * p0 + r[4] * p1 + r[5] * p2;
+  const double b2 = r[6] * p0 + r[7] * p1 + r[8] * p2;
+  const double syz = sqrt(b1 * b1 + b2 * b2);
+  const double c0 = r[0] * wx + r[1] * wy + r[2] * wz;
+  const double c1 = r[3] * wx + r[4] * wy + r[5] * wz;
+  const double c2 = r[6] * wx + r[7] * wy + r[8] * wz;
+  const double o0 = 0.5 * c0 - ox, o1 = 0.5 * c1 - oy, o2 = 0.5 * c2 - oz;
+  const double omag = sqrt(o0 * o0 + o1 * o1 + o2 * o2);
+  const double oyz = sqrt(o2 * o2 + o1 * o1);
+  t[0] = t[1] = t[2] = 0.0;
+  if (umag != 0.0 && syz != 0.0) {
+    const float rep = (float)((umag * pc.deq) / visc);
+    const float lr = __log2f(rep);
+    const float phi = fabsf(atanf((float)(syz / b0)));
+    float sphi, cphi;
+    sincosf(phi, &sphi, &cphi);
+    cphi = fmaxf(cphi, 0.f);
+    const float ctp = (0.935f * exp2f(-0.146f * lr) - 0.469f * exp2f(-0.145f * lr)) *
+                      powf(sphi, 0.116f + 0.748f * exp2f(0.041f * lr)) *
+                      powf(cphi, 0.221f + 0.657f * exp2f(0.044f * lr));
+    const double cp = pc.cpitch * (double)ctp * (umag * umag);
+    t[1] = cp * (fabs(b2) / syz) * copysign(1.0, b0 * b2);
+    t[2] = cp * (fabs(b1) / syz) * copysign(1.0, b0 * b1);
+  }
+  const double re_r = (omag * (pc.deq * pc.deq)) / visc;
+  if (re_r != 0.0) {
+    const float lr = __log2f((float)re_r);
+    const float ctr = 0.573f * exp2f(-0.154f * lr) + 116.61f / (float)re_r;
+    const float ctr2 = 1.244f * exp2f(0.239f * lr) + 378.12f * exp2f(-0.789f * lr);
+    const double k = pc.crot * pc.h5;
+    t[0] += (double)ctr * k * fabs(o0) * o0;
+    t[1] += (double)ctr2 * k * oyz * o1;
+    t[2] += (double)ctr2 * k * oyz * o2;
+  }
+}
+
+template <bool kMixed>
+struct Forces {
+  // F (lab frame, per unit mass) and T (body frame) for stage velocities.
+  __device__ __forceinline__ static bool eval(const PartConst& pc, double visc, const double u[3],
+                                              const double un[3], const double uf[3], const double wv[3],
+                                              double ox, double oy, double oz, const Quat& q, double f[3],
+                                              double t[3]) {
+    if (kMixed) {
+      double r[9];
+      rotmat(q, r);
+      const bool ok = fluid_force_mixed(pc, visc, u[0], u[1], u[2], uf[0], uf[1], uf[2], r, f);
+      fluid_torque_mixed(pc, visc, un[0], un[1], un[2], uf[0], uf[1], uf[2], wv[0], wv[1], wv[2], ox, oy, oz, r,
+                         t);
+      return ok;
+    } else {
+      double fd[3], fl[3], tp[3], tr[3];
+      const bool ok = fluid_force(pc, visc, u[0], u[1], u[2], uf[0], uf[1], uf[2], q, fd, fl);
+      fluid_torque(pc, visc, un[0], un[1], un[2], uf[0], uf[1], uf[2], wv[0], wv[1], wv[2], ox, oy, oz, q, tp, tr);
+      f[0] = fd[0] + fl[0]; f[1] = fd[1] + fl[1]; f[2] = fd[2] + fl[2];
+      t[0] = tp[0] + tr[0]; t[1] = tp[1] + tr[1]; t[2] = tp[2] + tr[2];
+      return ok;
+    }
+  }
+};
+
+__device__ __forceinline__ void k_omega(const double t[3], double ox, double oy, double oz, const PartConst& pc,
+                                        double k[3]) {
+  // adv_particle_new.f90:305-307
+  k[0] = (t[0] + oy * oz * (pc.ipyy - pc.ipzz)) / pc.ipxx;
+  k[1] = (t[1] + oz * ox * (pc.ipzz - pc.ipxx)) / pc.ipyy;
+  k[2] = (t[2] + ox * oy * (pc.ipxx - pc.ipyy)) / pc.ipzz;
+}
+
+__device__ __forceinline__ void renorm(Quat& q) {
+  const double n = sqrt(q.a * q.a + q.b * q.b + q.c * q.c + q.d * q.d);
+  const double inv = 1.0 / n;
+  q.a *= inv; q.b *= inv; q.c *= inv; q.d *= inv;
+}
+
+// One particle of adv_particle_new.f90:268-637.  State in/out in registers.
+// Returns 0 or an error code.
+template <bool kMixed>
+__device__ __forceinline__ int advance_particle(const InstDev& I, const PartConst& pc, const double uf[3],
+                                                const double wv[3], double X[3], double U[3], double O[3],
+                                                Quat& Q) {
+  const double dt = I.dtime;
+  const double rmax = fmax(pc.a, pc.b);
+  const double un[3] = {U[0], U[1], U[2]};
+  double f[3], t[3];
+  int err = 0;
+  if (!Forces<kMixed>::eval(pc, I.visc, un, un, uf, wv, O[0], O[1], O[2], Q, f, t)) err = GP_ENAN_FORCE;
+  if (O[0] != O[0] && !err) err = GP_ENAN_TORQUE;
+  const double k1x[3] = {U[0], U[1], U[2]};
+  const double k1u[3] = {f[0], f[1], f[2] + I.gravity};
+  double k1o[3];
+  k_omega(t, O[0], O[1], O[2], pc, k1o);
+  double xp1 = X[0] + dt * k1x[0], yp1 = X[1] + dt * k1x[1], zp1 = X[2] + dt * k1x[2];
+  double u1[3] = {U[0] + dt * k1u[0], U[1] + dt * k1u[1], U[2] + dt * k1u[2]};
+  double o1[3] = {O[0] + dt * k1o[0], O[1] + dt * k1o[1], O[2] + dt * k1o[2]};
+  Quat q1 = Q;
+  quaternion_integration(q1, o1[0], o1[1], o1[2], dt);
+  if (kMixed) renorm(q1);
+  double wn[3], arm[3], delta_x = 0.0;
+  bool isect;
+  int rc = wall_test(I.lx, pc, rmax, xp1, yp1, zp1, q1, wn, arm, delta_x, isect);
+  if (rc && !err) err = rc;
+  if (isect && u1[0] * wn[0] < 0.0) {
+    // rebound branch, adv_particle_new.f90:358-511
+    double ol[3] = {o1[0], o1[1], o1[2]};
+    rot_vec(q1, ol);
+    double vpc[3];
+    vpc[0] = u1[0] + (ol[1] * arm[2] - ol[2] * arm[1]);
+    vpc[1] = u1[1] + (ol[2] * arm[0] - ol[0] * arm[2]);
+    vpc[2] = u1[2] + (ol[0] * arm[1] - ol[1] * arm[0]);
+    xp1 = xp1 + delta_x;
+    const double delt = fabs(delta_x) / sqrt(vpc[0] * vpc[0] + vpc[1] * vpc[1] + vpc[2] * vpc[2]);
+    yp1 = X[1] + (dt - delt) * k1x[1];
+    zp1 = X[2] + (dt - delt) * k1x[2];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      u1[i] = U[i] + (dt - delt) * k1u[i];
+      o1[i] = O[i] + (dt - delt) * k1o[i];
+    }
+    q1 = Q;
+    quaternion_integration(q1, o1[0], o1[1], o1[2], dt - delt);
+    if (kMixed) renorm(q1);
+    rc = wall_rebound(I.ecw, I.muw, pc, u1[0], u1[1], u1[2], o1[0], o1[1], o1[2], q1, arm, wn);
+    if (rc && !err) err = rc;
+    if (!Forces<kMixed>::eval(pc, I.visc, u1, un, uf, wv, o1[0], o1[1], o1[2], q1, f, t) && !err) err = GP_ENAN_FORCE;
+    if (o1[0] != o1[0] && !err) err = GP_ENAN_TORQUE;
+    const double k2u[3] = {f[0], f[1], f[2] + I.gravity};
+    double k2o[3];
+    k_omega(t, o1[0], o1[1], o1[2], pc, k2o);
+    X[0] = xp1 + (delt) * u1[0];
+    X[1] = yp1 + (delt) * u1[1];
+    X[2] = zp1 + (delt) * u1[2];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      U[i] = u1[i] + (delt) * k2u[i];
+      O[i] = o1[i] + (delt) * k2o[i];
+    }
+    Q = q1;
+    quaternion_integration(Q, O[0], O[1], O[2], delt);
+    if (kMixed) renorm(Q);
+    return err;
+  }
+  // unbounced second stage, adv_particle_new.f90:513-637
+  if (!Forces<kMixed>::eval(pc, I.visc, u1, un, uf, wv, o1[0], o1[1], o1[2], q1, f, t) && !err) err = GP_ENAN_FORCE;
+  if (o1[0] != o1[0] && !err) err = GP_ENAN_TORQUE;
+  const double k2x[3] = {u1[0], u1[1], u1[2]};
+  const double k2u[3] = {f[0], f[1], f[2] + I.gravity};
+  double k2o[3];
+  k_omega(t, o1[0], o1[1], o1[2], pc, k2o);
+  const double xp2 = X[0] + 0.5 * dt * (k1x[0] + k2x[0]);
+  const double yp2 = X[1] + 0.5 * dt * (k1x[1] + k2x[1]);
+  const double zp2 = X[2] + 0.5 * dt * (k1x[2] + k2x[2]);
+  rc = wall_test(I.lx, pc, rmax, xp2, yp2, zp2, q1, wn, arm, delta_x, isect);
+  if (rc && !err) err = rc;
+  if (isect) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      X[i] = X[i] + dt * k1x[i];
+      U[i] = U[i] + dt * k1u[i];
+      O[i] = O[i] + dt * k1o[i];
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      X[i] = X[i] + 0.5 * dt * (k1x[i] + k2x[i]);
+      U[i] = U[i] + 0.5 * dt * (k1u[i] + k2u[i]);
+      O[i] = O[i] + 0.5 * dt * (k1o[i] + k2o[i]);
+    }
+  }
+  Q = q1;
+  quaternion_integration(Q, O[0], O[1], O[2], dt);
+  if (kMixed) renorm(Q);
+  return err;
+}
+
+__device__ __forceinline__ void load_pc(const PoolView& P, int64_t i, PartConst& pc) {
+  pc.a = P.pc[0][i]; pc.b = P.pc[1][i]; pc.deq = P.pc[2][i]; pc.cdrag = P.pc[3][i];
+  pc.cpitch = P.pc[4][i]; pc.crot = P.pc[5][i]; pc.h5 = P.pc[6][i];
+  pc.ipxx = P.pc[7][i]; pc.ipyy = P.pc[8][i]; pc.ipzz = P.pc[9][i];
+}
+
+// ADV_PARTICLE_ELLP over every particle of every instance, in place.
+template <bool kMixed>
+__global__ void __launch_bounds__(128) k_advance(const InstDev* __restrict__ insts, const PoolView* __restrict__ pv,
+                                                 int64_t n, double* const* __restrict__ fluid, Status* st) {
+  const PoolView P = *pv;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int inst = P.inst[i];
+    if (inst < 0) continue;   // empty slot
+    const InstDev& I = insts[inst];
+    double X[3] = {P.st[0][i], P.st[1][i], P.st[2][i]};
+    double U[3] = {P.st[3][i], P.st[4][i], P.st[5][i]};
+    Quat Q = {P.st[6][i], P.st[7][i], P.st[8][i], P.st[9][i]};
+    double O[3] = {P.st[10][i], P.st[11][i], P.st[12][i]};
+    PartConst pc;
+    load_pc(P, i, pc);
+    Stencil s;
+    double g[6];
+    if (!stencil(I, X[0], X[1], X[2], s)) {
+      set_error(st, GP_EOUT_OF_GRID, (long long)P.id[i]);
+      continue;
+    }
+    if (I.fprec == GP_PREC_MIXED) gather6_fp32(I, s, g); else gather6_fp64(I, s, g);
+    const double uf[3] = {g[0], g[1], g[2]}, wv[3] = {g[3], g[4], g[5]};
+    const int err = advance_particle<kMixed>(I, pc, uf, wv, X, U, O, Q);
+    if (err) set_error(st, err, (long long)P.id[i]);
+    // BOUNDARY_PARTICLE, boundary_particle.f90:50-59
+    if (I.periodicity) {
+      if (X[0] > I.lx) X[0] = X[0] - I.lx;
+      if (X[0] < 0.) X[0] = X[0] + I.lx;
+      if (X[1] > I.ly) X[1] = X[1] - I.ly;
+      if (X[1] < 0.) X[1] = X[1] + I.ly;
+      if (X[2] > I.lz) X[2] = X[2] - I.lz;
+      if (X[2] < 0.) X[2] = X[2] + I.lz;
+    }
+    P.st[0][i] = X[0]; P.st[1][i] = X[1]; P.st[2][i] = X[2];
+    P.st[3][i] = U[0]; P.st[4][i] = U[1]; P.st[5][i] = U[2];
+    P.st[6][i] = Q.a; P.st[7][i] = Q.b; P.st[8][i] = Q.c; P.st[9][i] = Q.d;
+    P.st[10][i] = O[0]; P.st[11][i] = O[1]; P.st[12][i] = O[2];
+    if (I.store_fluid && fluid != nullptr) {
+#pragma unroll
+      for (int c = 0; c < 6; ++c) fluid[c][i] = g[c];
+    }
+  }
+}
+
+}  // namespace gp

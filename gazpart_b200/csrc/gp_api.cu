@@ -1,0 +1,886 @@
+// gp_api.cu -- host side of the C ABI declared in include/gazpart_gpu.h.
+//
+// A context owns: one CUDA stream, the interpolation field (device layout, see
+// gp_advance.cuh), a structure-of-arrays particle pool, the ensemble table read by the
+// kernels, the collision search buffers, a device status word and a captured CUDA
+// graph of one step.  Host code here does set-up, bookkeeping and launches only; all
+// per-particle and per-pair arithmetic runs in the kernels.
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <utility>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/gazpart_gpu.h"
+#include "gp_launch.h"
+#include "gp_types.h"
+
+using namespace gp;
+
+#define GP_CK(call)                                                                               \
+  do {                                                                                            \
+    cudaError_t e_ = (call);                                                                      \
+    if (e_ != cudaSuccess) {                                                                      \
+      std::fprintf(stderr, "gazpart_b200: %s failed: %s (%s:%d)\n", #call, cudaGetErrorString(e_), \
+                   __FILE__, __LINE__);                                                           \
+      return e_ == cudaErrorMemoryAllocation ? GP_ENOMEM : GP_ECUDA;                              \
+    }                                                                                             \
+  } while (0)
+
+#define GP_TRY(expr)          \
+  do {                        \
+    int rc_ = (expr);         \
+    if (rc_ != GP_OK) return rc_; \
+  } while (0)
+
+namespace {
+
+template <typename T>
+int dalloc(T **p, size_t count) {
+  *p = nullptr;
+  if (count == 0) count = 1;
+  GP_CK(cudaMalloc(reinterpret_cast<void **>(p), count * sizeof(T)));
+  return GP_OK;
+}
+
+template <typename T>
+void dfree(T *&p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+// Per-particle constants of the force/torque routines, computed with the reference's
+// expressions on the host (fluid_force_ellipsoid.f90:59,70,119; fluid_torque_ellipsoid.f90:
+// 85,96,147,158).  Order: a b deq cdrag cpitch crot h5 ipxx ipyy ipzz.
+void part_const(double emaj, double apr, double rhop, double rhof, double ppi, double ipxx, double ipyy,
+                double ipzz, double out[kNConst]) {
+  const double pmass = rhop * (4.0 / 3.0) * ppi * std::pow(emaj, 3.0) / (apr * apr);
+  const double deq = (2.0 * emaj) / std::pow(apr, 2.0 / 3.0);
+  out[0] = emaj;
+  out[1] = emaj / apr;
+  out[2] = deq;
+  out[3] = (1.0 / 2.0) * (rhof / pmass) * (1.0 / 4.0) * (ppi * (deq * deq));
+  out[4] = (1.0 / 4.0) * (rhof / pmass) * (1.0 / 4.0) * ppi * (deq * deq * deq);
+  out[5] = 0.5 * rhof / pmass;
+  const double h = deq / 2.0, h2 = h * h;
+  out[6] = h2 * h2 * h;
+  out[7] = ipxx;
+  out[8] = ipyy;
+  out[9] = ipzz;
+}
+
+struct ClassProps {
+  double emaj, apr, rhop;
+};
+
+}  // namespace
+
+struct gp_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  gp_params prm{};
+  double ppi = 0.0;
+  // field
+  void *field = nullptr;
+  size_t field_bytes = 0;
+  double *stage = nullptr;
+  size_t stage_count = 0;
+  // ensemble table (one instance)
+  InstDev inst{};
+  InstDev *d_inst = nullptr;
+  bool grid_ready = false;
+  // pool
+  int64_t cap = 0, n = 0;
+  double *d_st[kNState] = {};
+  double *d_pc[kNConst] = {};
+  double *d_fluid[kNFluid] = {};
+  double **d_fluid_cols = nullptr;
+  int32_t *d_id = nullptr, *d_instof = nullptr;
+  PoolView *d_pv = nullptr;
+  // search
+  SearchArrays sa{};
+  int32_t *d_scan_tmp = nullptr;
+  int64_t ncells = 0, ncells_cap = 0;
+  PairRec *d_pairs = nullptr;
+  int64_t cap_pairs = 0;
+  CollRec *d_coll = nullptr;
+  int64_t cap_coll = 0;
+  unsigned long long *d_counters = nullptr;   // [0] npairs [1] ncoll [2] nacc
+  unsigned long long *d_best1 = nullptr, *d_best2 = nullptr;
+  int8_t *d_matched = nullptr, *d_state = nullptr;
+  int32_t *d_acc = nullptr;
+  Status *d_status = nullptr;
+  // scratch for per-routine calls
+  double *d_scratch = nullptr;
+  size_t scratch_count = 0;
+  std::map<std::pair<int, int>, ClassProps> classes;
+  // graph
+  cudaGraphExec_t graph = nullptr;
+  int grid = 148 * 4;
+};
+
+namespace {
+
+int ensure_scratch(gp_ctx *c, size_t count) {
+  if (c->scratch_count >= count) return GP_OK;
+  dfree(c->d_scratch);
+  c->scratch_count = 0;
+  GP_TRY(dalloc(&c->d_scratch, count));
+  c->scratch_count = count;
+  return GP_OK;
+}
+
+void drop_graph(gp_ctx *c) {
+  if (c->graph) cudaGraphExecDestroy(c->graph);
+  c->graph = nullptr;
+}
+
+int upload_inst(gp_ctx *c) {
+  GP_CK(cudaMemcpyAsync(c->d_inst, &c->inst, sizeof(InstDev), cudaMemcpyHostToDevice, c->stream));
+  return GP_OK;
+}
+
+int copy_in(gp_ctx *c, double *dst, const double *src, size_t count, int on_device) {
+  GP_CK(cudaMemcpyAsync(dst, src, count * sizeof(double), on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                        c->stream));
+  return GP_OK;
+}
+
+int class_props(gp_ctx *c, int ig, int idp, double pc[kNConst]) {
+  auto it = c->classes.find({ig, idp});
+  if (it == c->classes.end()) return GP_EBADARG;
+  const ClassProps &p = it->second;
+  // initiation_particle_position.f90:609-634
+  const double a = p.emaj, b = a / p.apr, cc = b;
+  const double ipxx = (b * b + cc * cc) / 5.0, ipyy = (a * a + cc * cc) / 5.0, ipzz = (a * a + b * b) / 5.0;
+  part_const(p.emaj, p.apr, p.rhop, c->prm.rhof, c->ppi, ipxx, ipyy, ipzz, pc);
+  return GP_OK;
+}
+
+void free_search(gp_ctx *c) {
+  dfree(c->sa.cell_count); dfree(c->sa.cell_start); dfree(c->sa.cell_fill);
+  dfree(c->d_scan_tmp);
+  c->ncells_cap = 0;
+}
+
+void free_pool(gp_ctx *c) {
+  for (auto &p : c->d_st) dfree(p);
+  for (auto &p : c->d_pc) dfree(p);
+  for (auto &p : c->d_fluid) dfree(p);
+  dfree(c->d_id); dfree(c->d_instof);
+  dfree(c->sa.cell_of); dfree(c->sa.sorted); dfree(c->sa.sx); dfree(c->sa.sy); dfree(c->sa.sz); dfree(c->sa.sr);
+  dfree(c->sa.sbox); dfree(c->sa.sinst); dfree(c->sa.sid);
+  dfree(c->d_best1); dfree(c->d_best2); dfree(c->d_matched);
+  dfree(c->d_pairs); dfree(c->d_coll); dfree(c->d_state); dfree(c->d_acc);
+  c->cap = 0;
+}
+
+int alloc_pool(gp_ctx *c, int64_t cap) {
+  free_pool(c);
+  for (auto &p : c->d_st) GP_TRY(dalloc(&p, cap));
+  for (auto &p : c->d_pc) GP_TRY(dalloc(&p, cap));
+  if (c->prm.store_fluid)
+    for (auto &p : c->d_fluid) GP_TRY(dalloc(&p, cap));
+  GP_TRY(dalloc(&c->d_id, cap));
+  GP_TRY(dalloc(&c->d_instof, cap));
+  GP_CK(cudaMemsetAsync(c->d_instof, 0xFF, cap * sizeof(int32_t), c->stream));   // -1: empty slot
+  SearchArrays &sa = c->sa;
+  GP_TRY(dalloc(&sa.cell_of, cap)); GP_TRY(dalloc(&sa.sorted, cap));
+  GP_TRY(dalloc(&sa.sx, cap)); GP_TRY(dalloc(&sa.sy, cap)); GP_TRY(dalloc(&sa.sz, cap)); GP_TRY(dalloc(&sa.sr, cap));
+  GP_TRY(dalloc(&sa.sbox, cap)); GP_TRY(dalloc(&sa.sinst, cap)); GP_TRY(dalloc(&sa.sid, cap));
+  GP_TRY(dalloc(&c->d_best1, cap)); GP_TRY(dalloc(&c->d_best2, cap)); GP_TRY(dalloc(&c->d_matched, cap));
+  GP_CK(cudaMemsetAsync(c->d_best1, 0xFF, cap * sizeof(unsigned long long), c->stream));
+  GP_CK(cudaMemsetAsync(c->d_best2, 0xFF, cap * sizeof(unsigned long long), c->stream));
+  GP_CK(cudaMemsetAsync(c->d_matched, 0, cap, c->stream));
+  c->cap_pairs = std::max<int64_t>(int64_t(1) << 20, cap);
+  c->cap_coll = std::max<int64_t>(int64_t(1) << 18, cap / 4);
+  GP_TRY(dalloc(&c->d_pairs, c->cap_pairs));
+  GP_TRY(dalloc(&c->d_coll, c->cap_coll));
+  GP_TRY(dalloc(&c->d_state, c->cap_coll));
+  GP_TRY(dalloc(&c->d_acc, c->cap_coll));
+  c->cap = cap;
+  PoolView pv;
+  for (int k = 0; k < kNState; ++k) pv.st[k] = c->d_st[k];
+  for (int k = 0; k < kNConst; ++k) pv.pc[k] = c->d_pc[k];
+  pv.id = c->d_id;
+  pv.inst = c->d_instof;
+  GP_CK(cudaMemcpyAsync(c->d_pv, &pv, sizeof(PoolView), cudaMemcpyHostToDevice, c->stream));
+  GP_CK(cudaMemcpyAsync(c->d_fluid_cols, c->d_fluid, sizeof(c->d_fluid), cudaMemcpyHostToDevice, c->stream));
+  return GP_OK;
+}
+
+// COLLISION_INITIATION (collision_initiation.f90:44-103, INIT_GRID=2, NPROC=1) and the
+// search grid.
+int setup_grids(gp_ctx *c, double max_emaj, double rmax) {
+  InstDev &I = c->inst;
+  const gp_params &p = c->prm;
+  const double zero_ref = 1.0e-33;
+  const double dpmax = 2.0 * max_emaj;
+  double dxbox = 2.0 * dpmax;
+  I.nxbox = (int32_t)(p.lx / dxbox);
+  if (I.nxbox < 3) return GP_EBADARG;
+  I.dxbox = p.lx / (double)I.nxbox;
+  I.xminbox = (double)(1 - 1) * I.dx;
+  I.yminbox = I.dy * (double)(1 - 1) - zero_ref;
+  const double ymaxbox = I.dy * (double)(p.ny - 1) + I.dy + zero_ref;
+  I.zminbox = I.dz * (double)(1 - 1) - zero_ref;
+  const double zmaxbox = I.dz * (double)(p.nz - 1) + I.dz + zero_ref;
+  I.nybox = (int32_t)((ymaxbox - I.yminbox) / I.dxbox);
+  I.nzbox = (int32_t)((zmaxbox - I.zminbox) / I.dxbox);
+  if (I.nybox < 3 || I.nzbox < 3) return GP_EBADARG;
+  if (I.nxbox >= (1 << 21) || I.nybox >= (1 << 21) || I.nzbox >= (1 << 21)) return GP_EBADARG;
+  I.dybox = (ymaxbox - I.yminbox) / (double)I.nybox;
+  I.dzbox = (zmaxbox - I.zminbox) / (double)I.nzbox;
+  // search grid: cell edge >= 2 rmax (1+1e-6), about two or more particles per cell
+  const double hmin = 2.0 * rmax * (1.0 + 1.0e-6);
+  const int64_t target = std::max<int64_t>(3, (int64_t)std::ceil(std::cbrt((double)std::max<int64_t>(c->n, 1) / 2.0)));
+  auto nf = [&](double L) {
+    int64_t m = (int64_t)std::floor(L / hmin);
+    return (int32_t)std::min<int64_t>(m, std::max<int64_t>(target, 3));
+  };
+  I.nfx = nf(p.lx); I.nfy = nf(p.ly); I.nfz = nf(p.lz);
+  if (I.nfx < 3 || I.nfy < 3 || I.nfz < 3) return GP_EBADARG;
+  I.hfx = p.lx / I.nfx; I.hfy = p.ly / I.nfy; I.hfz = p.lz / I.nfz;
+  I.rmax = rmax;
+  I.cell_begin = 0;
+  const int64_t ncells = (int64_t)I.nfx * I.nfy * I.nfz;
+  if (ncells >= (int64_t(1) << 31) - 2) return GP_EBADARG;
+  if (ncells > c->ncells_cap) {
+    free_search(c);
+    GP_TRY(dalloc(&c->sa.cell_count, ncells + 1));
+    GP_TRY(dalloc(&c->sa.cell_start, ncells + 1));
+    GP_TRY(dalloc(&c->sa.cell_fill, ncells + 1));
+    GP_TRY(dalloc(&c->d_scan_tmp, (size_t)scan_block_sums_size(ncells)));
+    c->ncells_cap = ncells;
+  }
+  c->ncells = ncells;
+  c->sa.ncells = ncells;
+  c->grid_ready = true;
+  return GP_OK;
+}
+
+int enqueue_advance(gp_ctx *c) {
+  if (c->prm.precision == GP_PREC_MIXED)
+    launch_advance_mixed(c->d_inst, c->d_pv, c->n, c->prm.store_fluid ? c->d_fluid_cols : nullptr, c->d_status,
+                         c->grid, c->stream);
+  else
+    launch_advance_fp64(c->d_inst, c->d_pv, c->n, c->prm.store_fluid ? c->d_fluid_cols : nullptr, c->d_status,
+                        c->grid, c->stream);
+  GP_CK(cudaGetLastError());
+  return GP_OK;
+}
+
+int enqueue_collision(gp_ctx *c) {
+  SearchArrays sa = c->sa;
+  GP_CK(cudaMemsetAsync(sa.cell_count, 0, (c->ncells + 1) * sizeof(int32_t), c->stream));
+  GP_CK(cudaMemsetAsync(sa.cell_fill, 0, (c->ncells + 1) * sizeof(int32_t), c->stream));
+  GP_CK(cudaMemsetAsync(c->d_counters, 0, 4 * sizeof(unsigned long long), c->stream));
+  launch_bin_count(c->d_inst, c->d_pv, c->n, sa, c->d_status, c->grid, c->stream);
+  launch_scan(sa.cell_count, sa.cell_start, c->ncells, c->d_scan_tmp, c->stream);
+  launch_bin_scatter(c->d_inst, c->d_pv, c->n, sa, c->d_status, c->grid, c->stream);
+  launch_search(c->d_inst, c->n, sa, c->d_pairs, c->d_counters + 0, c->cap_pairs, c->d_status, c->grid, c->stream);
+  launch_contact(c->d_inst, c->d_pv, c->d_pairs, c->d_counters + 0, c->cap_pairs, c->d_coll, c->d_counters + 1,
+                 c->cap_coll, c->d_status, c->grid, c->stream);
+  launch_match(c->d_coll, c->d_counters + 1, c->cap_coll, c->d_best1, c->d_best2, c->d_matched, c->d_state,
+               c->d_status, c->stream);
+  launch_response(c->d_inst, c->d_pv, c->d_coll, c->d_counters + 1, c->cap_coll, c->d_state, c->d_acc,
+                  c->d_counters + 2, c->d_status, c->grid, c->stream);
+  GP_CK(cudaGetLastError());
+  return GP_OK;
+}
+
+int read_status(gp_ctx *c, Status *h) {
+  GP_CK(cudaMemcpyAsync(h, c->d_status, sizeof(Status), cudaMemcpyDeviceToHost, c->stream));
+  GP_CK(cudaStreamSynchronize(c->stream));
+  return GP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gp_ctx_create(const gp_params *params, gp_ctx **out) {
+  if (!params || !out) return GP_EBADARG;
+  *out = nullptr;
+  const gp_params &p = *params;
+  if (p.nx < 4 || p.ny < 4 || p.nz < 4) return GP_EBADARG;
+  if (p.interp_scheme != 3) return GP_EBADARG;
+  if (p.frozen_flow != 2) return GP_EBADARG;
+  if (p.precision != GP_PREC_FP64 && p.precision != GP_PREC_MIXED) return GP_EBADARG;
+  if (!(p.lx > 0 && p.ly > 0 && p.lz > 0 && p.dtime > 0 && p.visc > 0)) return GP_EBADARG;
+  gp_ctx *c = new gp_ctx();
+  c->prm = p;
+  c->ppi = 4.0 * std::atan(1.0);   // init_run.f90:123
+  if (cudaGetDevice(&c->device) != cudaSuccess || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete c;
+    return GP_ECUDA;
+  }
+  InstDev &I = c->inst;
+  I.begin = 0;
+  I.count = 0;
+  I.nx = p.nx; I.ny = p.ny; I.nz = p.nz; I.ncomp = 6;
+  I.fprec = p.precision;
+  I.periodicity = p.periodicity ? 1 : 0;
+  I.wall_boundary = p.wall_boundary ? 1 : 0;
+  I.store_fluid = p.store_fluid ? 1 : 0;
+  I.lx = p.lx; I.ly = p.ly; I.lz = p.lz;
+  I.dx = p.lx / (double)(p.nx - 1);   // meshing.f90:43-45
+  I.dy = p.ly / (double)(p.ny - 1);
+  I.dz = p.lz / (double)(p.nz - 1);
+  I.visc = p.visc; I.dtime = p.dtime; I.gravity = p.gravity;
+  I.ecp = p.ecp; I.mup = p.mup; I.ecw = p.ecw; I.muw = p.muw;
+  const size_t elem = (p.precision == GP_PREC_MIXED) ? sizeof(float) : sizeof(double);
+  c->field_bytes = (size_t)(p.nx + 3) * (p.ny + 4) * (p.nz + 4) * 6 * elem;
+  int rc = GP_OK;
+  if (cudaMalloc(&c->field, c->field_bytes) != cudaSuccess || cudaMemset(c->field, 0, c->field_bytes) != cudaSuccess)
+    rc = GP_ENOMEM;
+  I.field = c->field;
+  if (!rc) rc = dalloc(&c->d_inst, 1);
+  if (!rc) rc = dalloc(&c->d_pv, 1);
+  if (!rc) rc = dalloc(&c->d_fluid_cols, kNFluid);
+  if (!rc) rc = dalloc(&c->d_counters, 4);
+  if (!rc) rc = dalloc(&c->d_status, 1);
+  if (!rc && cudaMemset(c->d_status, 0, sizeof(Status)) != cudaSuccess) rc = GP_ECUDA;
+  if (!rc) rc = upload_inst(c);
+  if (!rc && cudaStreamSynchronize(c->stream) != cudaSuccess) rc = GP_ECUDA;
+  if (rc) {
+    gp_ctx_destroy(c);
+    return rc;
+  }
+  if (p.max_particles > 0) {
+    rc = alloc_pool(c, p.max_particles);
+    if (rc) { gp_ctx_destroy(c); return rc; }
+  }
+  *out = c;
+  return GP_OK;
+}
+
+int gp_ctx_destroy(gp_ctx *c) {
+  if (!c) return GP_OK;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  drop_graph(c);
+  free_pool(c);
+  free_search(c);
+  if (c->field) cudaFree(c->field);
+  dfree(c->stage); dfree(c->d_inst); dfree(c->d_pv); dfree(c->d_fluid_cols); dfree(c->d_counters);
+  dfree(c->d_status); dfree(c->d_scratch);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return GP_OK;
+}
+
+int gp_status(gp_ctx *c, int32_t *code, int64_t *first_id) {
+  if (!c) return GP_EBADARG;
+  Status h;
+  GP_TRY(read_status(c, &h));
+  if (code) *code = h.code;
+  if (first_id) *first_id = h.first_id;
+  return GP_OK;
+}
+
+int gp_clear_status(gp_ctx *c) {
+  if (!c) return GP_EBADARG;
+  GP_CK(cudaMemsetAsync(c->d_status, 0, sizeof(Status), c->stream));
+  GP_CK(cudaStreamSynchronize(c->stream));
+  return GP_OK;
+}
+
+int gp_sync(gp_ctx *c) {
+  if (!c) return GP_EBADARG;
+  GP_CK(cudaStreamSynchronize(c->stream));
+  return GP_OK;
+}
+
+int gp_set_class(gp_ctx *c, int32_t ig, int32_t idp, double emaj, double apr, double rhop) {
+  if (!c || !(emaj > 0) || !(apr > 0) || !(rhop > 0)) return GP_EBADARG;
+  c->classes[{ig, idp}] = ClassProps{emaj, apr, rhop};
+  return GP_OK;
+}
+
+int gp_set_field(gp_ctx *c, int32_t comp, const double *src, int32_t src_layout, int32_t ghost_mode,
+                 int32_t on_device) {
+  if (!c || !src || comp < 0 || comp > 5) return GP_EBADARG;
+  if (src_layout != GP_LAYOUT_INTERIOR && src_layout != GP_LAYOUT_REFERENCE) return GP_EBADARG;
+  if (ghost_mode != GP_GHOST_PERIODIC && ghost_mode != GP_GHOST_ZERO) return GP_EBADARG;
+  const gp_params &p = c->prm;
+  const size_t count = (src_layout == GP_LAYOUT_REFERENCE) ? (size_t)p.nx * (p.ny + 4) * (p.nz + 4)
+                                                           : (size_t)p.nx * p.ny * p.nz;
+  const double *dsrc = src;
+  if (!on_device) {
+    if (c->stage_count < count) {
+      dfree(c->stage);
+      c->stage_count = 0;
+      GP_TRY(dalloc(&c->stage, count));
+      c->stage_count = count;
+    }
+    GP_CK(cudaMemcpyAsync(c->stage, src, count * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    dsrc = c->stage;
+  }
+  launch_field_layout(c->field, p.precision, p.nx, p.ny, p.nz, 6, comp, dsrc, src_layout, ghost_mode, c->stream);
+  GP_CK(cudaGetLastError());
+  GP_CK(cudaStreamSynchronize(c->stream));
+  return GP_OK;
+}
+
+int gp_upload_state(gp_ctx *c, int64_t n, const double *const *cols, const double *const *props, int32_t on_device) {
+  if (!c || !cols || !props || n <= 0 || n >= kMaxInstanceParticles) return GP_EBADARG;
+  // per-particle constants on the host (reference expressions, IEEE double)
+  std::vector<double> hp[GP_NPROP];
+  for (int k = 0; k < GP_NPROP; ++k) {
+    hp[k].resize(n);
+    if (on_device) {
+      GP_CK(cudaMemcpyAsync(hp[k].data(), props[k], n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    } else {
+      std::memcpy(hp[k].data(), props[k], n * sizeof(double));
+    }
+  }
+  GP_CK(cudaStreamSynchronize(c->stream));
+  std::vector<double> pcs((size_t)kNConst * n);
+  double max_emaj = 0.0, rmax = 0.0;
+  for (int64_t i = 0; i < n; ++i) {
+    double pc[kNConst];
+    const double emaj = hp[0][i], apr = hp[1][i], rhop = hp[2][i];
+    if (!(emaj > 0) || !(apr > 0) || !(rhop > 0)) return GP_EBADARG;
+    part_const(emaj, apr, rhop, c->prm.rhof, c->ppi, hp[3][i], hp[4][i], hp[5][i], pc);
+    for (int k = 0; k < kNConst; ++k) pcs[(size_t)k * n + i] = pc[k];
+    max_emaj = std::max(max_emaj, emaj);
+    rmax = std::max(rmax, std::max(pc[0], pc[1]));
+  }
+  drop_graph(c);
+  const int64_t want = std::max<int64_t>(n, c->prm.max_particles);
+  if (c->cap < want) GP_TRY(alloc_pool(c, want));
+  else GP_CK(cudaMemsetAsync(c->d_instof, 0xFF, c->cap * sizeof(int32_t), c->stream));
+  c->n = n;
+  double *stage_cols = nullptr, *stage_pc = nullptr;
+  GP_TRY(dalloc(&stage_cols, (size_t)kNState * n));
+  GP_TRY(dalloc(&stage_pc, (size_t)kNConst * n));
+  for (int k = 0; k < kNState; ++k) GP_TRY(copy_in(c, stage_cols + (size_t)k * n, cols[k], n, on_device));
+  GP_CK(cudaMemcpyAsync(stage_pc, pcs.data(), pcs.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  PoolView pv;
+  for (int k = 0; k < kNState; ++k) pv.st[k] = c->d_st[k];
+  for (int k = 0; k < kNConst; ++k) pv.pc[k] = c->d_pc[k];
+  pv.id = c->d_id;
+  pv.inst = c->d_instof;
+  launch_init_pool(pv, 0, n, 0, stage_cols, stage_pc, c->stream);
+  GP_CK(cudaGetLastError());
+  GP_CK(cudaStreamSynchronize(c->stream));
+  cudaFree(stage_cols);
+  cudaFree(stage_pc);
+  c->inst.count = n;
+  GP_TRY(setup_grids(c, max_emaj, rmax));
+  GP_TRY(upload_inst(c));
+  GP_CK(cudaStreamSynchronize(c->stream));
+  return GP_OK;
+}
+
+int gp_download_state(gp_ctx *c, int64_t n, double *const *cols, double *const *fluid, int32_t on_device) {
+  if (!c || !cols || n != c->n) return GP_EBADARG;
+  if (fluid && !c->prm.store_fluid) return GP_EBADARG;
+  double *tmp = nullptr;
+  const size_t per = (size_t)kNState + (fluid ? kNFluid : 0);
+  GP_TRY(dalloc(&tmp, per * n));
+  launch_gather_state(c->d_pv, c->n, 0, tmp, c->d_fluid_cols, fluid ? tmp + (size_t)kNState * n : nullptr, n,
+                      c->stream);
+  GP_CK(cudaGetLastError());
+  const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  for (int k = 0; k < kNState; ++k)
+    GP_CK(cudaMemcpyAsync(cols[k], tmp + (size_t)k * n, n * sizeof(double), kind, c->stream));
+  if (fluid)
+    for (int k = 0; k < kNFluid; ++k)
+      GP_CK(cudaMemcpyAsync(fluid[k], tmp + (size_t)(kNState + k) * n, n * sizeof(double), kind, c->stream));
+  GP_CK(cudaStreamSynchronize(c->stream));
+  cudaFree(tmp);
+  return GP_OK;
+}
+
+int gp_put_state(gp_ctx *c, int64_t n, const double *const *cols, int32_t on_device) {
+  if (!c || !cols || n != c->n) return GP_EBADARG;
+  GP_TRY(ensure_scratch(c, (size_t)kNState * n));
+  for (int k = 0; k < kNState; ++k) GP_TRY(copy_in(c, c->d_scratch + (size_t)k * n, cols[k], n, on_device));
+  launch_scatter_state(c->d_pv, c->n, 0, c->d_scratch, n, c->stream);
+  GP_CK(cudaGetLastError());
+  GP_CK(cudaStreamSynchronize(c->stream));
+  return GP_OK;
+}
+
+int gp_adv_particle_ellp(gp_ctx *c, int32_t /*ncycle*/) {
+  if (!c || c->n <= 0) return GP_EBADARG;
+  return enqueue_advance(c);
+}
+
+int gp_collision(gp_ctx *c, int32_t /*ncycle*/, double /*time*/, int64_t *n_near, int64_t *n_contact,
+                 int64_t *n_coll) {
+  if (!c || c->n <= 0 || !c->grid_ready) return GP_EBADARG;
+  GP_CK(cudaMemsetAsync(&c->d_status->n_near, 0, 5 * sizeof(unsigned long long), c->stream));
+  GP_TRY(enqueue_collision(c));
+  if (n_near || n_contact || n_coll) {
+    Status h;
+    GP_TRY(read_status(c, &h));
+    unsigned long long cnt[4];
+    GP_CK(cudaMemcpy(cnt, c->d_counters, sizeof(cnt), cudaMemcpyDeviceToHost));
+    if (n_near) *n_near = (int64_t)h.n_near;
+    if (n_contact) *n_contact = (int64_t)h.n_contact;
+    if (n_coll) *n_coll = (int64_t)cnt[1];
+    if (h.overflow) return GP_EPAIR_OVERFLOW;
+  }
+  return GP_OK;
+}
+
+int gp_step(gp_ctx *c, int32_t nsteps) {
+  if (!c || c->n <= 0 || !c->grid_ready || nsteps < 0) return GP_EBADARG;
+  if (!c->graph) {
+    cudaGraph_t g;
+    GP_CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = enqueue_advance(c);
+    if (!rc) rc = enqueue_collision(c);
+    cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    if (rc) return rc;
+    if (e != cudaSuccess) return GP_ECUDA;
+    e = cudaGraphInstantiate(&c->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) { c->graph = nullptr; return GP_ECUDA; }
+  }
+  for (int s = 0; s < nsteps; ++s) GP_CK(cudaGraphLaunch(c->graph, c->stream));
+  return GP_OK;
+}
+
+int gp_step_timed(gp_ctx *c, int32_t nsteps, float *total_ms, float *advance_ms_avg, float *collision_ms_avg,
+                  int32_t *kernels_per_step) {
+  if (!c || c->n <= 0 || !c->grid_ready || nsteps <= 0) return GP_EBADARG;
+  std::vector<cudaEvent_t> ev(2 * (size_t)nsteps + 1);
+  for (auto &e : ev) GP_CK(cudaEventCreate(&e));
+  cudaGraph_t g;
+  cudaGraphExec_t ge = nullptr;
+  GP_CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = GP_OK;
+  for (int s = 0; s < nsteps && !rc; ++s) {
+    if (cudaEventRecord(ev[2 * s], c->stream) != cudaSuccess) rc = GP_ECUDA;
+    if (!rc) rc = enqueue_advance(c);
+    if (!rc && cudaEventRecord(ev[2 * s + 1], c->stream) != cudaSuccess) rc = GP_ECUDA;
+    if (!rc) rc = enqueue_collision(c);
+  }
+  if (!rc && cudaEventRecord(ev[2 * nsteps], c->stream) != cudaSuccess) rc = GP_ECUDA;
+  cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+  if (!rc && e != cudaSuccess) rc = GP_ECUDA;
+  if (!rc && kernels_per_step) {
+    size_t nn = 0;
+    cudaGraphGetNodes(g, nullptr, &nn);
+    std::vector<cudaGraphNode_t> nodes(nn);
+    cudaGraphGetNodes(g, nodes.data(), &nn);
+    int nk = 0;
+    for (auto nd : nodes) {
+      cudaGraphNodeType t;
+      if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++nk;
+    }
+    *kernels_per_step = nk / nsteps;
+  }
+  if (!rc && cudaGraphInstantiate(&ge, g, 0) != cudaSuccess) rc = GP_ECUDA;
+  if (e == cudaSuccess) cudaGraphDestroy(g);
+  if (!rc && cudaGraphLaunch(ge, c->stream) != cudaSuccess) rc = GP_ECUDA;
+  if (!rc && cudaStreamSynchronize(c->stream) != cudaSuccess) rc = GP_ECUDA;
+  if (!rc) {
+    double adv = 0.0, col = 0.0;
+    float t = 0.f;
+    for (int s = 0; s < nsteps; ++s) {
+      cudaEventElapsedTime(&t, ev[2 * s], ev[2 * s + 1]);
+      adv += t;
+      cudaEventElapsedTime(&t, ev[2 * s + 1], ev[2 * s + 2]);
+      col += t;
+    }
+    cudaEventElapsedTime(&t, ev[0], ev[2 * nsteps]);
+    if (total_ms) *total_ms = t;
+    if (advance_ms_avg) *advance_ms_avg = (float)(adv / nsteps);
+    if (collision_ms_avg) *collision_ms_avg = (float)(col / nsteps);
+  }
+  if (ge) cudaGraphExecDestroy(ge);
+  for (auto &x : ev) cudaEventDestroy(x);
+  return rc;
+}
+
+int gp_collision_pairs(gp_ctx *c, int64_t cap, int32_t *home, int32_t *near, int64_t *count) {
+  if (!c) return GP_EBADARG;
+  unsigned long long cnt[4];
+  GP_CK(cudaStreamSynchronize(c->stream));
+  GP_CK(cudaMemcpy(cnt, c->d_counters, sizeof(cnt), cudaMemcpyDeviceToHost));
+  const int64_t nc = (int64_t)std::min<unsigned long long>(cnt[1], (unsigned long long)c->cap_coll);
+  std::vector<CollRec> recs(nc);
+  std::vector<int8_t> st(nc);
+  if (nc > 0) {
+    GP_CK(cudaMemcpy(recs.data(), c->d_coll, nc * sizeof(CollRec), cudaMemcpyDeviceToHost));
+    GP_CK(cudaMemcpy(st.data(), c->d_state, nc, cudaMemcpyDeviceToHost));
+  }
+  std::vector<std::pair<std::pair<unsigned long long, unsigned long long>, int64_t>> acc;
+  for (int64_t e = 0; e < nc; ++e)
+    if (st[e] == 1) acc.push_back({{recs[e].k1, recs[e].k2}, e});
+  std::sort(acc.begin(), acc.end());
+  if (count) *count = (int64_t)acc.size();
+  for (int64_t k = 0; k < (int64_t)acc.size() && k < cap; ++k) {
+    const unsigned long long k2 = acc[k].first.second;
+    if (home) home[k] = (int32_t)(k2 >> 34);
+    if (near) near[k] = (int32_t)(k2 & ((1ull << 30) - 1));
+  }
+  return GP_OK;
+}
+
+int gp_collision_box_connectivity(gp_ctx *c, int32_t *nbox, int32_t *ncon, int32_t *con, int32_t *grid_dims,
+                                  double *grid_geom) {
+  if (!c || !c->grid_ready) return GP_EBADARG;
+  const InstDev &I = c->inst;
+  const int64_t nb = (int64_t)I.nxbox * I.nybox * I.nzbox;
+  if (nbox) *nbox = (int32_t)nb;
+  if (grid_dims) { grid_dims[0] = I.nxbox; grid_dims[1] = I.nybox; grid_dims[2] = I.nzbox; }
+  if (grid_geom) {
+    grid_geom[0] = I.dxbox; grid_geom[1] = I.dybox; grid_geom[2] = I.dzbox;
+    grid_geom[3] = I.xminbox; grid_geom[4] = I.yminbox; grid_geom[5] = I.zminbox;
+  }
+  if (!ncon && !con) return GP_OK;
+  int32_t *dn = nullptr, *dc = nullptr;
+  GP_TRY(dalloc(&dn, nb));
+  GP_TRY(dalloc(&dc, nb * 27));
+  launch_connectivity(I.nxbox, I.nybox, I.nzbox, I.periodicity, dn, dc, c->stream);
+  GP_CK(cudaGetLastError());
+  if (ncon) GP_CK(cudaMemcpyAsync(ncon, dn, nb * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+  if (con) GP_CK(cudaMemcpyAsync(con, dc, nb * 27 * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+  GP_CK(cudaStreamSynchronize(c->stream));
+  cudaFree(dn);
+  cudaFree(dc);
+  return GP_OK;
+}
+
+// ---------------------------------------------------------------- drop-ins ----
+int gp_interp_lag3(gp_ctx *c, int32_t comp, int64_t nint, const double *xint, const double *yint, const double *zint,
+                   double *uint, int32_t on_device) {
+  if (!c || comp < 0 || comp > 5 || nint < 0) return GP_EBADARG;
+  if (nint == 0) return GP_OK;
+  const double *dx = xint, *dy = yint, *dz = zint;
+  double *dout = uint;
+  if (!on_device) {
+    GP_TRY(ensure_scratch(c, 4 * (size_t)nint));
+    double *s = c->d_scratch;
+    GP_TRY(copy_in(c, s, xint, nint, 0));
+    GP_TRY(copy_in(c, s + nint, yint, nint, 0));
+    GP_TRY(copy_in(c, s + 2 * nint, zint, nint, 0));
+    dx = s; dy = s + nint; dz = s + 2 * nint; dout = s + 3 * nint;
+  }
+  launch_interp(c->d_inst, comp, nint, dx, dy, dz, dout, c->d_status, c->stream);
+  GP_CK(cudaGetLastError());
+  if (!on_device) GP_CK(cudaMemcpyAsync(uint, dout, nint * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  GP_CK(cudaStreamSynchronize(c->stream));
+  return GP_OK;
+}
+
+int gp_frozen_interp_lag3(gp_ctx *c, const double *xain, const double *yain, const double *zain, int32_t nx,
+                          int32_t ny, int32_t nz, const double *uain, int64_t nint, const double *xint,
+                          const double *yint, const double *zint, double *uint) {
+  if (!c || nx < 3 || ny < 3 || nz < 3 || nint < 0) return GP_EBADARG;
+  if (nint == 0) return GP_OK;
+  const size_t nf = (size_t)nx * ny * nz;
+  GP_TRY(ensure_scratch(c, (size_t)nx + ny + nz + nf + 4 * (size_t)nint));
+  double *s = c->d_scratch;
+  double *dxa = s, *dya = dxa + nx, *dza = dya + ny, *du = dza + nz, *dxi = du + nf, *dyi = dxi + nint,
+         *dzi = dyi + nint, *dout = dzi + nint;
+  GP_TRY(copy_in(c, dxa, xain, nx, 0));
+  GP_TRY(copy_in(c, dya, yain, ny, 0));
+  GP_TRY(copy_in(c, dza, zain, nz, 0));
+  GP_TRY(copy_in(c, du, uain, nf, 0));
+  GP_TRY(copy_in(c, dxi, xint, nint, 0));
+  GP_TRY(copy_in(c, dyi, yint, nint, 0));
+  GP_TRY(copy_in(c, dzi, zint, nint, 0));
+  launch_frozen_interp(dxa, dya, dza, nx, ny, nz, du, nint, dxi, dyi, dzi, dout, c->d_status, c->stream);
+  GP_CK(cudaGetLastError());
+  GP_CK(cudaMemcpyAsync(uint, dout, nint * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  GP_CK(cudaStreamSynchronize(c->stream));
+  return GP_OK;
+}
+
+int gp_fluid_force_ellipsoid_batch(gp_ctx *c, int64_t n, const int32_t *ig, const int32_t *idp, const double *up,
+                                   const double *uf, const double *quat, double *fdrag, double *flift,
+                                   int32_t on_device) {
+  if (!c || n < 0 || !ig || !idp) return GP_EBADARG;
+  if (n == 0) return GP_OK;
+  std::vector<int32_t> hig(n), hidp(n);
+  if (on_device) {
+    GP_CK(cudaMemcpy(hig.data(), ig, n * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    GP_CK(cudaMemcpy(hidp.data(), idp, n * sizeof(int32_t), cudaMemcpyDeviceToHost));
+  } else {
+    std::memcpy(hig.data(), ig, n * sizeof(int32_t));
+    std::memcpy(hidp.data(), idp, n * sizeof(int32_t));
+  }
+  std::vector<double> pcs((size_t)kNConst * n);
+  for (int64_t i = 0; i < n; ++i) GP_TRY(class_props(c, hig[i], hidp[i], &pcs[(size_t)kNConst * i]));
+  GP_TRY(ensure_scratch(c, (size_t)n * (kNConst + 3 + 3 + 4 + 3 + 3)));
+  double *dpc = c->d_scratch, *dup = dpc + kNConst * n, *duf = dup + 3 * n, *dq = duf + 3 * n, *dfd = dq + 4 * n,
+         *dfl = dfd + 3 * n;
+  GP_CK(cudaMemcpyAsync(dpc, pcs.data(), pcs.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  GP_TRY(copy_in(c, dup, up, 3 * n, on_device));
+  GP_TRY(copy_in(c, duf, uf, 3 * n, on_device));
+  GP_TRY(copy_in(c, dq, quat, 4 * n, on_device));
+  launch_force_batch(n, dpc, c->prm.visc, dup, duf, dq, dfd, dfl, c->d_status, c->stream);
+  GP_CK(cudaGetLastError());
+  const cudaMemcpyKind k = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  GP_CK(cudaMemcpyAsync(fdrag, dfd, 3 * n * sizeof(double), k, c->stream));
+  GP_CK(cudaMemcpyAsync(flift, dfl, 3 * n * sizeof(double), k, c->stream));
+  GP_CK(cudaStreamSynchronize(c->stream));
+  return GP_OK;
+}
+
+int gp_fluid_force_ellipsoid(gp_ctx *c, int32_t ig, int32_t idp, double upart, double vpart, double wpart,
+                             double ufluid, double vfluid, double wfluid, const double quat[4], double fdrag[3],
+                             double flift[3]) {
+  const double up[3] = {upart, vpart, wpart}, uf[3] = {ufluid, vfluid, wfluid};
+  return gp_fluid_force_ellipsoid_batch(c, 1, &ig, &idp, up, uf, quat, fdrag, flift, 0);
+}
+
+int gp_fluid_torque_ellipsoid_batch(gp_ctx *c, int64_t n, const int32_t *ig, const int32_t *idp, const double *omega,
+                                    const double *quat, const double *part_up, const double *part_ufap,
+                                    const double *part_vort, double *tpitch, double *trot, int32_t on_device) {
+  if (!c || n < 0 || !ig || !idp) return GP_EBADARG;
+  if (n == 0) return GP_OK;
+  std::vector<int32_t> hig(n), hidp(n);
+  if (on_device) {
+    GP_CK(cudaMemcpy(hig.data(), ig, n * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    GP_CK(cudaMemcpy(hidp.data(), idp, n * sizeof(int32_t), cudaMemcpyDeviceToHost));
+  } else {
+    std::memcpy(hig.data(), ig, n * sizeof(int32_t));
+    std::memcpy(hidp.data(), idp, n * sizeof(int32_t));
+  }
+  std::vector<double> pcs((size_t)kNConst * n);
+  for (int64_t i = 0; i < n; ++i) GP_TRY(class_props(c, hig[i], hidp[i], &pcs[(size_t)kNConst * i]));
+  GP_TRY(ensure_scratch(c, (size_t)n * (kNConst + 3 + 4 + 3 + 3 + 3 + 3 + 3)));
+  double *dpc = c->d_scratch, *dom = dpc + kNConst * n, *dq = dom + 3 * n, *dup = dq + 4 * n, *duf = dup + 3 * n,
+         *dvo = duf + 3 * n, *dtp = dvo + 3 * n, *dtr = dtp + 3 * n;
+  GP_CK(cudaMemcpyAsync(dpc, pcs.data(), pcs.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  GP_TRY(copy_in(c, dom, omega, 3 * n, on_device));
+  GP_TRY(copy_in(c, dq, quat, 4 * n, on_device));
+  GP_TRY(copy_in(c, dup, part_up, 3 * n, on_device));
+  GP_TRY(copy_in(c, duf, part_ufap, 3 * n, on_device));
+  GP_TRY(copy_in(c, dvo, part_vort, 3 * n, on_device));
+  launch_torque_batch(n, dpc, c->prm.visc, dom, dq, dup, duf, dvo, dtp, dtr, c->d_status, c->stream);
+  GP_CK(cudaGetLastError());
+  const cudaMemcpyKind k = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  GP_CK(cudaMemcpyAsync(tpitch, dtp, 3 * n * sizeof(double), k, c->stream));
+  GP_CK(cudaMemcpyAsync(trot, dtr, 3 * n * sizeof(double), k, c->stream));
+  GP_CK(cudaStreamSynchronize(c->stream));
+  return GP_OK;
+}
+
+int gp_fluid_torque_ellipsoid(gp_ctx *c, int32_t ig, int32_t idp, double ox, double oy, double oz,
+                              const double quat[4], const double part_up[3], const double part_ufap[3],
+                              const double part_vort[3], double tpitch[3], double trot[3]) {
+  const double om[3] = {ox, oy, oz};
+  return gp_fluid_torque_ellipsoid_batch(c, 1, &ig, &idp, om, quat, part_up, part_ufap, part_vort, tpitch, trot, 0);
+}
+
+int gp_quaternion_integration_batch(gp_ctx *c, int64_t n, double *quat, const double *omega, double dt,
+                                    int32_t on_device) {
+  if (!c || n < 0) return GP_EBADARG;
+  if (n == 0) return GP_OK;
+  GP_TRY(ensure_scratch(c, (size_t)7 * n));
+  double *dq = c->d_scratch, *dom = dq + 4 * n;
+  GP_TRY(copy_in(c, dq, quat, 4 * n, on_device));
+  GP_TRY(copy_in(c, dom, omega, 3 * n, on_device));
+  launch_quat_batch(n, dq, dom, dt, c->stream);
+  GP_CK(cudaGetLastError());
+  GP_CK(cudaMemcpyAsync(quat, dq, 4 * n * sizeof(double), on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                        c->stream));
+  GP_CK(cudaStreamSynchronize(c->stream));
+  return GP_OK;
+}
+
+int gp_quaternion_integration(gp_ctx *c, double quat[4], double omgx, double omgy, double omgz, double dt) {
+  const double om[3] = {omgx, omgy, omgz};
+  return gp_quaternion_integration_batch(c, 1, quat, om, dt, 0);
+}
+
+int gp_euler_integration(gp_ctx *c, int32_t ig, int32_t idp, double *omgx, double *omgy, double *omgz) {
+  if (!c || !omgx || !omgy || !omgz) return GP_EBADARG;
+  double pc[kNConst];
+  GP_TRY(class_props(c, ig, idp, pc));
+  GP_TRY(ensure_scratch(c, 6));
+  const double h[6] = {pc[7], pc[8], pc[9], *omgx, *omgy, *omgz};
+  GP_CK(cudaMemcpyAsync(c->d_scratch, h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
+  launch_euler_batch(1, c->d_scratch, c->prm.dtime, c->d_scratch + 3, c->stream);
+  GP_CK(cudaGetLastError());
+  double o[3];
+  GP_CK(cudaMemcpyAsync(o, c->d_scratch + 3, sizeof(o), cudaMemcpyDeviceToHost, c->stream));
+  GP_CK(cudaStreamSynchronize(c->stream));
+  *omgx = o[0]; *omgy = o[1]; *omgz = o[2];
+  return GP_OK;
+}
+
+int gp_ellipsoid_contact_detection_batch(gp_ctx *c, int64_t n, const double *shapes, const double *centres,
+                                         const double *quats, int32_t *flag, double *ept1, double *ept2,
+                                         double *cnormal, int32_t on_device) {
+  if (!c || n < 0) return GP_EBADARG;
+  if (n == 0) return GP_OK;
+  // shapes come in as (emaj1, apr1, emaj2, apr2); the kernel takes semi-axes (a, a/apr)
+  std::vector<double> hs(4 * (size_t)n);
+  if (on_device) GP_CK(cudaMemcpy(hs.data(), shapes, hs.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  else std::memcpy(hs.data(), shapes, hs.size() * sizeof(double));
+  for (int64_t i = 0; i < n; ++i) {
+    hs[4 * i + 1] = hs[4 * i] / hs[4 * i + 1];
+    hs[4 * i + 3] = hs[4 * i + 2] / hs[4 * i + 3];
+  }
+  GP_TRY(ensure_scratch(c, (size_t)n * (4 + 6 + 8 + 9) + (size_t)n));
+  double *ds = c->d_scratch, *dc = ds + 4 * n, *dq = dc + 6 * n, *de1 = dq + 8 * n, *de2 = de1 + 3 * n,
+         *dcn = de2 + 3 * n;
+  int32_t *dflag = reinterpret_cast<int32_t *>(dcn + 3 * n);
+  GP_CK(cudaMemcpyAsync(ds, hs.data(), hs.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  GP_TRY(copy_in(c, dc, centres, 6 * n, on_device));
+  GP_TRY(copy_in(c, dq, quats, 8 * n, on_device));
+  launch_contact_batch(n, ds, dc, dq, dflag, de1, de2, dcn, c->stream);
+  GP_CK(cudaGetLastError());
+  const cudaMemcpyKind k = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  GP_CK(cudaMemcpyAsync(flag, dflag, n * sizeof(int32_t), k, c->stream));
+  GP_CK(cudaMemcpyAsync(ept1, de1, 3 * n * sizeof(double), k, c->stream));
+  GP_CK(cudaMemcpyAsync(ept2, de2, 3 * n * sizeof(double), k, c->stream));
+  GP_CK(cudaMemcpyAsync(cnormal, dcn, 3 * n * sizeof(double), k, c->stream));
+  GP_CK(cudaStreamSynchronize(c->stream));
+  return GP_OK;
+}
+
+int gp_ellipsoid_contact_detection(gp_ctx *c, int32_t ig, int32_t idp1, int32_t idp2, double ixp, double iyp,
+                                   double izp, const double iquat[4], double jxp, double jyp, double jzp,
+                                   const double jquat[4], int32_t *flag, double ept1[3], double ept2[3],
+                                   double cnormal[3]) {
+  if (!c) return GP_EBADARG;
+  auto a = c->classes.find({ig, idp1}), b = c->classes.find({ig, idp2});
+  if (a == c->classes.end() || b == c->classes.end()) return GP_EBADARG;
+  const double shapes[4] = {a->second.emaj, a->second.apr, b->second.emaj, b->second.apr};
+  const double centres[6] = {ixp, iyp, izp, jxp, jyp, jzp};
+  const double quats[8] = {iquat[0], iquat[1], iquat[2], iquat[3], jquat[0], jquat[1], jquat[2], jquat[3]};
+  return gp_ellipsoid_contact_detection_batch(c, 1, shapes, centres, quats, flag, ept1, ept2, cnormal, 0);
+}
+
+int gp_collision_response(gp_ctx *c, int32_t ig, int32_t idp, double part1[10], double part2[10],
+                          const double r_impact1[3], const double r_impact2[3], const double normal[3]) {
+  if (!c || !part1 || !part2) return GP_EBADARG;
+  double pc[kNConst];
+  GP_TRY(class_props(c, ig, idp, pc));
+  GP_TRY(ensure_scratch(c, 3 + 10 + 10 + 9));
+  double h[32];
+  h[0] = pc[7]; h[1] = pc[8]; h[2] = pc[9];
+  std::memcpy(h + 3, part1, 10 * sizeof(double));
+  std::memcpy(h + 13, part2, 10 * sizeof(double));
+  std::memcpy(h + 23, r_impact1, 3 * sizeof(double));
+  std::memcpy(h + 26, r_impact2, 3 * sizeof(double));
+  std::memcpy(h + 29, normal, 3 * sizeof(double));
+  double *d = c->d_scratch;
+  GP_CK(cudaMemcpyAsync(d, h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
+  GP_CK(cudaMemsetAsync(c->d_status, 0, sizeof(Status), c->stream));
+  launch_response_batch(1, c->prm.ecp, c->prm.mup, d, d + 3, d + 13, d + 23, d + 26, d + 29, c->d_status, c->stream);
+  GP_CK(cudaGetLastError());
+  GP_CK(cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  Status s;
+  GP_TRY(read_status(c, &s));
+  std::memcpy(part1, h + 3, 10 * sizeof(double));
+  std::memcpy(part2, h + 13, 10 * sizeof(double));
+  return s.code;
+}
+
+}  // extern "C"

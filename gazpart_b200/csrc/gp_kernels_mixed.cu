@@ -1,0 +1,16 @@
+// gp_kernels_mixed.cu -- mixed-precision ADV_PARTICLE_ELLP: FP32 field and stencil
+// weights with compensated FP32 sums, FP32 drag/lift/torque coefficients, FP64
+// integration and renormalised quaternions.  Compiled with FMA contraction.
+#include "gp_advance.cuh"
+#include "gp_launch.h"
+
+namespace gp {
+
+template __global__ void k_advance<true>(const InstDev *, const PoolView *, int64_t, double *const *, Status *);
+
+void launch_advance_mixed(const InstDev *insts, const PoolView *pv, int64_t n, double *const *fluid, Status *st,
+                          int grid, cudaStream_t s) {
+  k_advance<true><<<grid, 128, 0, s>>>(insts, pv, n, fluid, st);
+}
+
+}  // namespace gp

@@ -1,0 +1,65 @@
+// gp_launch.h -- host-side launchers of the device kernels (one per translation unit
+// so that the FP64 path can be compiled without FMA contraction).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "gp_types.h"
+
+namespace gp {
+
+// --- gp_kernels_fp64.cu (FP64 path, -fmad=false) ---
+void launch_advance_fp64(const InstDev *insts, const PoolView *pv, int64_t n, double *const *fluid, Status *st,
+                         int grid, cudaStream_t s);
+void launch_interp(const InstDev *inst, int comp, int64_t n, const double *x, const double *y, const double *z,
+                   double *out, Status *st, cudaStream_t s);
+void launch_frozen_interp(const double *xain, const double *yain, const double *zain, int nx, int ny, int nz,
+                          const double *uain, int64_t n, const double *x, const double *y, const double *z,
+                          double *out, Status *st, cudaStream_t s);
+void launch_contact(const InstDev *insts, const PoolView *pv, const PairRec *pairs, const unsigned long long *npairs,
+                    int64_t cap_pairs, CollRec *coll, unsigned long long *ncoll, int64_t cap_coll, Status *st,
+                    int grid, cudaStream_t s);
+void launch_response(const InstDev *insts, const PoolView *pv, const CollRec *coll, const unsigned long long *ncoll,
+                     int64_t cap_coll, const int8_t *state, int32_t *acc_list, unsigned long long *nacc, Status *st,
+                     int grid, cudaStream_t s);
+// per-routine drop-ins (n items; all pointers device)
+void launch_force_batch(int64_t n, const double *pcs /*n*10*/, double visc, const double *up,
+                        const double *uf, const double *quat, double *fdrag, double *flift, Status *st,
+                        cudaStream_t s);
+void launch_torque_batch(int64_t n, const double *pcs, double visc, const double *omega, const double *quat,
+                         const double *pup, const double *pufap, const double *pvort, double *tp, double *tr,
+                         Status *st, cudaStream_t s);
+void launch_quat_batch(int64_t n, double *quat, const double *omega, double dt, cudaStream_t s);
+void launch_euler_batch(int64_t n, const double *ip /*n*3*/, double dt, double *omega, cudaStream_t s);
+void launch_contact_batch(int64_t n, const double *shapes /*n*4: a1 b1 a2 b2*/, const double *centres,
+                          const double *quats, int32_t *flag, double *e1, double *e2, double *cn, cudaStream_t s);
+void launch_response_batch(int64_t n, double ecp, double mup, const double *ip /*n*3*/, double *p1 /*n*10*/,
+                           double *p2, const double *r1, const double *r2, const double *nrm, Status *st,
+                           cudaStream_t s);
+
+// --- gp_kernels_mixed.cu ---
+void launch_advance_mixed(const InstDev *insts, const PoolView *pv, int64_t n, double *const *fluid, Status *st,
+                          int grid, cudaStream_t s);
+
+// --- gp_search.cu ---
+void launch_bin_count(const InstDev *insts, const PoolView *pv, int64_t n, SearchArrays sa, Status *st, int grid,
+                      cudaStream_t s);
+void launch_scan(const int32_t *in, int32_t *out, int64_t n, int32_t *block_sums, cudaStream_t s);
+int64_t scan_block_sums_size(int64_t n);
+void launch_bin_scatter(const InstDev *insts, const PoolView *pv, int64_t n, SearchArrays sa, Status *st, int grid,
+                        cudaStream_t s);
+void launch_search(const InstDev *insts, int64_t n, SearchArrays sa, PairRec *pairs, unsigned long long *npairs,
+                   int64_t cap_pairs, Status *st, int grid, cudaStream_t s);
+void launch_match(const CollRec *coll, const unsigned long long *ncoll, int64_t cap_coll, unsigned long long *best1,
+                  unsigned long long *best2, int8_t *matched, int8_t *state, Status *st, cudaStream_t s);
+void launch_field_layout(void *dst, int prec, int nx, int ny, int nz, int ncomp, int comp, const double *src,
+                         int src_layout, int ghost_mode, cudaStream_t s);
+void launch_gather_state(const PoolView *pv, int64_t n, int inst, double *out /*13*count*/,
+                         double *const *fluid_cols, double *fluid_out /*6*count or null*/, int64_t count,
+                         cudaStream_t s);
+void launch_scatter_state(const PoolView *pv, int64_t n, int inst, const double *cols /*13*count*/,
+                          int64_t count, cudaStream_t s);
+void launch_init_pool(PoolView pv, int64_t begin, int64_t n, int inst, const double *cols /*13*n*/,
+                      const double *pcs /*10*n*/, cudaStream_t s);
+void launch_connectivity(int nxb, int nyb, int nzb, int periodicity, int32_t *ncon, int32_t *con, cudaStream_t s);
+
+}  // namespace gp

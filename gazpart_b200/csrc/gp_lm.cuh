@@ -1,0 +1,486 @@
+// gp_lm.cuh -- ellipsoid contact detection with a register-resident Levenberg-
+// Marquardt solve (FP64), one pair per thread.
+//
+// ellipsoid_contact_detection.f90:1-187 parametrises the common normal by two angles
+// and minimises the squared components of the gap between the two support points
+// with lmder1 (minpack_reduc.f90:652-757: ftol=xtol=sqrt(eps), gtol=0,
+// maxfev=100(n+1), mode=1, factor=100).  The solver below is the MINPACK
+// Levenberg-Marquardt method (Moré 1978; MINPACK-1 user guide, ANL-80-74: QR with
+// column pivoting, Levenberg-Marquardt parameter by the secular-equation iteration,
+// Givens-rotation least-squares update, trust-region step control) for the fixed size
+// n=2 variables, m=3 residuals; every loop bound is a compile-time constant.
+#pragma once
+#include <cfloat>
+#include <math_constants.h>
+
+#include "gp_device.cuh"
+
+namespace gp {
+
+// MINPACK's scaled Euclidean norm (minpack_reduc.f90:180-232): three accumulators
+// for tiny, mid-range and huge components.
+template <int N>
+__device__ __forceinline__ double lm_enorm(const double* x) {
+  constexpr double rdwarf = 3.834e-20, rgiant = 1.304e19;
+  double s1 = 0.0, s2 = 0.0, s3 = 0.0, x1max = 0.0, x3max = 0.0;
+  const double agiant = rgiant / (double)N;
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    const double xabs = fabs(x[i]);
+    if (xabs > rdwarf && xabs < agiant) {
+      s2 = s2 + xabs * xabs;
+    } else if (xabs <= rdwarf) {
+      if (xabs <= x3max) {
+        if (xabs != 0.0) { const double r = xabs / x3max; s3 = s3 + r * r; }
+      } else {
+        const double r = x3max / xabs;
+        s3 = 1.0 + s3 * (r * r);
+        x3max = xabs;
+      }
+    } else if (xabs <= x1max) {
+      const double r = xabs / x1max;
+      s1 = s1 + r * r;
+    } else {
+      const double r = x1max / xabs;
+      s1 = 1.0 + s1 * (r * r);
+      x1max = xabs;
+    }
+  }
+  if (s1 != 0.0) return x1max * sqrt(s1 + (s2 / x1max) / x1max);
+  if (s2 == 0.0) return x3max * sqrt(s3);
+  if (s2 >= x3max) return sqrt(s2 * (1.0 + (x3max / s2) * (x3max * s3)));
+  return sqrt(x3max * ((s2 / x3max) + (x3max * s3)));
+}
+
+struct ContactProb {
+  double e1[9], e2[9];   // R diag(a^2,b^2,b^2) R^T (calculate_ellipsoid_matrix.f90:33-72)
+  double b1[3], b2[3];
+};
+
+// Support points along +-c(x) (ellipsoid_pair_depth.f90:117-142).
+__device__ __forceinline__ void support_points(const ContactProb& P, const double x[2], double c1[3], double tmp1[3],
+                                               double tmp2[3], double& l1, double& l2, double pt1[3],
+                                               double pt2[3]) {
+  double s0, k0, s1, k1;
+  sincos(x[0], &s0, &k0);
+  sincos(x[1], &s1, &k1);
+  c1[0] = k0 * k1;
+  c1[1] = s0 * k1;
+  c1[2] = s1;
+  const double c2[3] = {-c1[0], -c1[1], -c1[2]};
+  matvec(P.e1, c1, tmp1);
+  matvec(P.e2, c2, tmp2);
+  l1 = sqrt(0.25 * (c1[0] * tmp1[0] + c1[1] * tmp1[1] + c1[2] * tmp1[2]));
+  l2 = sqrt(0.25 * (c2[0] * tmp2[0] + c2[1] * tmp2[1] + c2[2] * tmp2[2]));
+  const double f1 = 1.0 / (2.0 * l1), f2 = 1.0 / (2.0 * l2);
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    pt1[i] = f1 * tmp1[i] + P.b1[i];
+    pt2[i] = f2 * tmp2[i] + P.b2[i];
+  }
+}
+
+// fcn, iflag=1 (ellipsoid_contact_detection.f90:290-295)
+__device__ __forceinline__ void lm_fcn(const ContactProb& P, const double x[2], double fvec[3]) {
+  double c1[3], t1[3], t2[3], l1, l2, pt1[3], pt2[3];
+  support_points(P, x, c1, t1, t2, l1, l2, pt1, pt2);
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    const double d = pt1[i] - pt2[i];
+    fvec[i] = d * d;
+  }
+}
+
+__device__ __forceinline__ void grad_coeff(const double e[9], const double c[3], double l, double co[9]) {
+  double row[3];
+#pragma unroll
+  for (int j = 0; j < 3; ++j) row[j] = c[0] * e[3 * j] + c[1] * e[1 + 3 * j] + c[2] * e[2 + 3 * j];
+  double outer[9];
+#pragma unroll
+  for (int j = 0; j < 3; ++j)
+#pragma unroll
+    for (int i = 0; i < 3; ++i) outer[i + 3 * j] = c[i] * row[j];
+  double eo[9];
+  matmul(e, outer, eo);
+  const double s = 1.0 / (2.0 * l), t = 1.0 / (8.0 * pow(l, 3.0));
+#pragma unroll
+  for (int k = 0; k < 9; ++k) co[k] = s * e[k] - t * eo[k];
+}
+
+// fcn, iflag=2: analytic Jacobian (ellipsoid_contact_detection.f90:296-332), 3x2
+// column-major.
+__device__ __forceinline__ void lm_jac(const ContactProb& P, const double x[2], double fj[6]) {
+  double c1[3], t1[3], t2[3], l1, l2, pt1[3], pt2[3];
+  support_points(P, x, c1, t1, t2, l1, l2, pt1, pt2);
+  const double depth[3] = {pt1[0] - pt2[0], pt1[1] - pt2[1], pt1[2] - pt2[2]};
+  double s0, k0, s1, k1;
+  sincos(x[0], &s0, &k0);
+  sincos(x[1], &s1, &k1);
+  const double g[6] = {-s0 * k1, k0 * k1, 0.0, -k0 * s1, -s0 * s1, k1};
+  const double c2[3] = {-c1[0], -c1[1], -c1[2]};
+  double co1[9], co2[9];
+  grad_coeff(P.e1, c1, l1, co1);
+  grad_coeff(P.e2, c2, l2, co2);
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    const double gj[3] = {g[3 * j], g[3 * j + 1], g[3 * j + 2]};
+    const double ng[3] = {-gj[0], -gj[1], -gj[2]};
+    double gp1[3], gp2[3];
+    matvec(co1, gj, gp1);
+    matvec(co2, ng, gp2);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) fj[i + 3 * j] = 2.0 * (depth[i] * (gp1[i] - gp2[i]));
+  }
+}
+
+// QR with column pivoting (3x2), Householder vectors left in a.
+__device__ __forceinline__ void lm_qrfac(double a[6], int ipvt[2], double rdiag[2], double acnorm[2]) {
+  double wa[2];
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    acnorm[j] = lm_enorm<3>(a + 3 * j);
+    rdiag[j] = acnorm[j];
+    wa[j] = rdiag[j];
+    ipvt[j] = j;
+  }
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    int kmax = j;
+    if (j == 0 && rdiag[1] > rdiag[0]) kmax = 1;
+    if (kmax != j) {
+#pragma unroll
+      for (int i = 0; i < 3; ++i) { const double t = a[i]; a[i] = a[i + 3]; a[i + 3] = t; }
+      rdiag[1] = rdiag[0];
+      wa[1] = wa[0];
+      const int k = ipvt[0]; ipvt[0] = ipvt[1]; ipvt[1] = k;
+    }
+    double ajnorm = (j == 0) ? lm_enorm<3>(a) : lm_enorm<2>(a + 4);
+    if (ajnorm != 0.0) {
+      if (a[j + 3 * j] < 0.0) ajnorm = -ajnorm;
+#pragma unroll
+      for (int i = j; i < 3; ++i) a[i + 3 * j] = a[i + 3 * j] / ajnorm;
+      a[j + 3 * j] = a[j + 3 * j] + 1.0;
+      if (j == 0) {
+        double sum = 0.0;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) sum = sum + a[i] * a[i + 3];
+        const double temp = sum / a[0];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) a[i + 3] = a[i + 3] - temp * a[i];
+        if (rdiag[1] != 0.0) {
+          const double t2 = a[3] / rdiag[1];
+          const double f = 1.0 - t2 * t2;
+          rdiag[1] = rdiag[1] * sqrt(f > 0.0 ? f : 0.0);
+          const double r = rdiag[1] / wa[1];
+          if (0.05 * (r * r) <= DBL_EPSILON) {
+            rdiag[1] = lm_enorm<2>(a + 4);
+            wa[1] = rdiag[1];
+          }
+        }
+      }
+    }
+    rdiag[j] = -ajnorm;
+  }
+}
+
+__device__ __forceinline__ void lm_qrsolv(double r[6], const int ipvt[2], const double diag[2], const double qtb[2],
+                                          double x[2], double sdiag[2]) {
+  double wa[2];
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+#pragma unroll
+    for (int i = j; i < 2; ++i) r[i + 3 * j] = r[j + 3 * i];
+    x[j] = r[j + 3 * j];
+    wa[j] = qtb[j];
+  }
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    const int l = ipvt[j];
+    if (diag[l] != 0.0) {
+#pragma unroll
+      for (int k = j; k < 2; ++k) sdiag[k] = 0.0;
+      sdiag[j] = diag[l];
+      double qtbpj = 0.0;
+#pragma unroll
+      for (int k = j; k < 2; ++k) {
+        if (sdiag[k] == 0.0) continue;
+        double cs, sn;
+        if (fabs(r[k + 3 * k]) >= fabs(sdiag[k])) {
+          const double tn = sdiag[k] / r[k + 3 * k];
+          cs = 0.5 / sqrt(0.25 + 0.25 * (tn * tn));
+          sn = cs * tn;
+        } else {
+          const double ct = r[k + 3 * k] / sdiag[k];
+          sn = 0.5 / sqrt(0.25 + 0.25 * (ct * ct));
+          cs = sn * ct;
+        }
+        r[k + 3 * k] = cs * r[k + 3 * k] + sn * sdiag[k];
+        const double temp = cs * wa[k] + sn * qtbpj;
+        qtbpj = -sn * wa[k] + cs * qtbpj;
+        wa[k] = temp;
+        if (k == 0) {
+          const double t2 = cs * r[1] + sn * sdiag[1];
+          sdiag[1] = -sn * r[1] + cs * sdiag[1];
+          r[1] = t2;
+        }
+      }
+    }
+    sdiag[j] = r[j + 3 * j];
+    r[j + 3 * j] = x[j];
+  }
+  int nsing = 2;
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    if (sdiag[j] == 0.0 && nsing == 2) nsing = j;
+    if (nsing < 2) wa[j] = 0.0;
+  }
+  if (nsing >= 2) wa[1] = wa[1] / sdiag[1];
+  if (nsing >= 1) {
+    double sum = 0.0;
+    if (nsing >= 2) sum = sum + r[1] * wa[1];
+    wa[0] = (wa[0] - sum) / sdiag[0];
+  }
+  x[ipvt[0]] = wa[0];
+  x[ipvt[1]] = wa[1];
+}
+
+__device__ __forceinline__ void lm_lmpar(double r[6], const int ipvt[2], const double diag[2], const double qtb[2],
+                                         double delta, double& par, double x[2], double sdiag[2]) {
+  const double dwarf = DBL_MIN;
+  double wa1[2], wa2[2];
+  int nsing = 2;
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    wa1[j] = qtb[j];
+    if (r[j + 3 * j] == 0.0 && nsing == 2) nsing = j;
+    if (nsing < 2) wa1[j] = 0.0;
+  }
+  if (nsing >= 2) {
+    wa1[1] = wa1[1] / r[4];
+    wa1[0] = wa1[0] - r[3] * wa1[1];
+  }
+  if (nsing >= 1) wa1[0] = wa1[0] / r[0];
+  x[ipvt[0]] = wa1[0];
+  x[ipvt[1]] = wa1[1];
+  wa2[0] = diag[0] * x[0];
+  wa2[1] = diag[1] * x[1];
+  double dxnorm = lm_enorm<2>(wa2);
+  double fp = dxnorm - delta;
+  if (fp <= 0.1 * delta) {
+    par = 0.0;
+    return;
+  }
+  double parl = 0.0;
+  if (nsing >= 2) {
+#pragma unroll
+    for (int j = 0; j < 2; ++j) { const int l = ipvt[j]; wa1[j] = diag[l] * (wa2[l] / dxnorm); }
+    wa1[0] = (wa1[0] - 0.0) / r[0];
+    wa1[1] = (wa1[1] - (0.0 + r[3] * wa1[0])) / r[4];
+    const double temp = lm_enorm<2>(wa1);
+    parl = ((fp / delta) / temp) / temp;
+  }
+  {
+    const double s0 = 0.0 + r[0] * qtb[0];
+    const double s1 = (0.0 + r[3] * qtb[0]) + r[4] * qtb[1];
+    wa1[0] = s0 / diag[ipvt[0]];
+    wa1[1] = s1 / diag[ipvt[1]];
+  }
+  const double gnorm = lm_enorm<2>(wa1);
+  double paru = gnorm / delta;
+  if (paru == 0.0) paru = dwarf / (delta < 0.1 ? delta : 0.1);
+  double p = par;
+  p = (p > parl) ? p : parl;
+  p = (p < paru) ? p : paru;
+  if (p == 0.0) p = gnorm / dxnorm;
+  for (int iter = 1;; ++iter) {
+    if (p == 0.0) { const double t = 0.001 * paru; p = (dwarf > t) ? dwarf : t; }
+    const double sp = sqrt(p);
+    wa1[0] = sp * diag[0];
+    wa1[1] = sp * diag[1];
+    lm_qrsolv(r, ipvt, wa1, qtb, x, sdiag);
+    wa2[0] = diag[0] * x[0];
+    wa2[1] = diag[1] * x[1];
+    dxnorm = lm_enorm<2>(wa2);
+    const double told = fp;
+    fp = dxnorm - delta;
+    if (fabs(fp) <= 0.1 * delta || (parl == 0.0 && fp <= told && told < 0.0) || iter == 10) break;
+#pragma unroll
+    for (int j = 0; j < 2; ++j) { const int l = ipvt[j]; wa1[j] = diag[l] * (wa2[l] / dxnorm); }
+    wa1[0] = wa1[0] / sdiag[0];
+    wa1[1] = wa1[1] - r[1] * wa1[0];
+    wa1[1] = wa1[1] / sdiag[1];
+    const double temp = lm_enorm<2>(wa1);
+    const double parc = ((fp / delta) / temp) / temp;
+    if (fp > 0.0) parl = (parl > p) ? parl : p;
+    if (fp < 0.0) paru = (paru < p) ? paru : p;
+    const double t2 = p + parc;
+    p = (parl > t2) ? parl : t2;
+  }
+  par = p;
+}
+
+// lmder control flow; returns info (8 mapped to 4 as lmder1 does).
+__device__ __forceinline__ int lm_solve(const ContactProb& P, double x[2], double tol) {
+  constexpr int maxfev = 300;
+  const double ftol = tol, xtol = tol;
+  double fvec[3], fjac[6], diag[2] = {0.0, 0.0}, qtf[2], wa1[2], wa2[2], wa3[2], wa4[3];
+  int ipvt[2];
+  int info = 0;
+  double xnorm = 0.0, delta = 0.0, temp = 0.0;
+  lm_fcn(P, x, fvec);
+  int nfev = 1;
+  double fnorm = lm_enorm<3>(fvec);
+  double par = 0.0;
+  int iter = 1;
+  while (true) {
+    lm_jac(P, x, fjac);
+    lm_qrfac(fjac, ipvt, wa1, wa2);
+    if (iter == 1) {
+#pragma unroll
+      for (int j = 0; j < 2; ++j) { diag[j] = wa2[j]; if (wa2[j] == 0.0) diag[j] = 1.0; }
+      wa3[0] = diag[0] * x[0];
+      wa3[1] = diag[1] * x[1];
+      xnorm = lm_enorm<2>(wa3);
+      delta = 100.0 * xnorm;
+      if (delta == 0.0) delta = 100.0;
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) wa4[i] = fvec[i];
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      if (fjac[j + 3 * j] != 0.0) {
+        double sum = 0.0;
+#pragma unroll
+        for (int i = j; i < 3; ++i) sum = sum + fjac[i + 3 * j] * wa4[i];
+        const double t = -sum / fjac[j + 3 * j];
+#pragma unroll
+        for (int i = j; i < 3; ++i) wa4[i] = wa4[i] + fjac[i + 3 * j] * t;
+      }
+      fjac[j + 3 * j] = wa1[j];
+      qtf[j] = wa4[j];
+    }
+    double gnorm = 0.0;
+    if (fnorm != 0.0) {
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const int l = ipvt[j];
+        if (wa2[l] != 0.0) {
+          double sum = 0.0;
+#pragma unroll
+          for (int i = 0; i <= j; ++i) sum = sum + fjac[i + 3 * j] * (qtf[i] / fnorm);
+          const double g = fabs(sum / wa2[l]);
+          gnorm = (gnorm > g) ? gnorm : g;
+        }
+      }
+    }
+    if (gnorm <= 0.0) info = 4;
+    if (info != 0) break;
+    diag[0] = (diag[0] > wa2[0]) ? diag[0] : wa2[0];
+    diag[1] = (diag[1] > wa2[1]) ? diag[1] : wa2[1];
+    while (true) {
+      lm_lmpar(fjac, ipvt, diag, qtf, delta, par, wa1, wa2);
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        wa1[j] = -wa1[j];
+        wa2[j] = x[j] + wa1[j];
+        wa3[j] = diag[j] * wa1[j];
+      }
+      const double pnorm = lm_enorm<2>(wa3);
+      if (iter == 1) delta = (delta < pnorm) ? delta : pnorm;
+      lm_fcn(P, wa2, wa4);
+      ++nfev;
+      const double fnorm1 = lm_enorm<3>(wa4);
+      double actred = -1.0;
+      if (0.1 * fnorm1 < fnorm) { const double r = fnorm1 / fnorm; actred = 1.0 - r * r; }
+      wa3[0] = 0.0 + fjac[0] * wa1[ipvt[0]];
+      wa3[1] = 0.0;
+      {
+        const double t = wa1[ipvt[1]];
+        wa3[0] = wa3[0] + fjac[3] * t;
+        wa3[1] = wa3[1] + fjac[4] * t;
+      }
+      const double temp1 = lm_enorm<2>(wa3) / fnorm;
+      const double temp2 = (sqrt(par) * pnorm) / fnorm;
+      const double prered = temp1 * temp1 + (temp2 * temp2) / 0.5;
+      const double dirder = -(temp1 * temp1 + temp2 * temp2);
+      double ratio = 0.0;
+      if (prered != 0.0) ratio = actred / prered;
+      if (ratio <= 0.25) {
+        if (actred >= 0.0) temp = 0.5;
+        if (actred < 0.0) temp = 0.5 * dirder / (dirder + 0.5 * actred);
+        if (0.1 * fnorm1 >= fnorm || temp < 0.1) temp = 0.1;
+        const double m = (delta < pnorm / 0.1) ? delta : pnorm / 0.1;
+        delta = temp * m;
+        par = par / temp;
+      } else if (par == 0.0 || ratio >= 0.75) {
+        delta = pnorm / 0.5;
+        par = 0.5 * par;
+      }
+      if (ratio >= 1.0e-4) {
+#pragma unroll
+        for (int j = 0; j < 2; ++j) { x[j] = wa2[j]; wa2[j] = diag[j] * x[j]; }
+#pragma unroll
+        for (int i = 0; i < 3; ++i) fvec[i] = wa4[i];
+        xnorm = lm_enorm<2>(wa2);
+        fnorm = fnorm1;
+        ++iter;
+      }
+      if (fabs(actred) <= ftol && prered <= ftol && 0.5 * ratio <= 1.0) info = 1;
+      if (delta <= xtol * xnorm) info = 2;
+      if (fabs(actred) <= ftol && prered <= ftol && 0.5 * ratio <= 1.0 && info == 2) info = 3;
+      if (info != 0) return info;
+      if (nfev >= maxfev) info = 5;
+      if (fabs(actred) <= DBL_EPSILON && prered <= DBL_EPSILON && 0.5 * ratio <= 1.0) info = 6;
+      if (delta <= DBL_EPSILON * xnorm) info = 7;
+      if (gnorm <= DBL_EPSILON) info = 8;
+      if (info != 0) return info == 8 ? 4 : info;
+      if (ratio >= 1.0e-4) break;
+    }
+  }
+  return info;
+}
+
+// Margin function mod_particle_parallel.f90:145-201: v^T (R diag(1/a^2,1/b^2,1/b^2) R^T) v
+__device__ __forceinline__ double fmargin(double a, double b, const double pt[3], const double c[3], const Quat& q) {
+  double ell[9];
+  rot_diag(q, 1.0 / (a * a), 1.0 / (b * b), 1.0 / (b * b), ell);
+  const double v[3] = {pt[0] - c[0], pt[1] - c[1], pt[2] - c[2]};
+  double e_[3];
+  matvec(ell, v, e_);
+  return v[0] * e_[0] + v[1] * e_[1] + v[2] * e_[2];
+}
+
+// ellipsoid_contact_detection.f90:1-187.  A NaN starting angle (acos of a ratio just
+// above 1, :86-87) keeps every iterate NaN, so the reference reports no contact; that
+// result is returned without iterating.
+__device__ __forceinline__ bool contact_detection(double a1, double bb1, double a2, double bb2, const double c1[3],
+                                                  const Quat& q1, const double c2[3], const Quat& q2, double ept1[3],
+                                                  double ept2[3], double cn[3]) {
+  const double tol = 1.4901161193847656e-08;   // sqrt(epsilon(1.0_8))
+  double nrm[3] = {c1[0] - c2[0], c1[1] - c2[1], c1[2] - c2[2]};
+  const double c_norm = sqrt(nrm[0] * nrm[0] + nrm[1] * nrm[1] + nrm[2] * nrm[2]);
+  if (c_norm != 0.0) { nrm[0] = nrm[0] / c_norm; nrm[1] = nrm[1] / c_norm; nrm[2] = nrm[2] / c_norm; }
+  double x[2];
+  x[1] = asin(nrm[2]);
+  x[0] = acos(nrm[0] / cos(x[1]));
+  if (x[0] != x[0] || x[1] != x[1]) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i) { ept1[i] = CUDART_NAN; ept2[i] = CUDART_NAN; cn[i] = CUDART_NAN; }
+    return false;
+  }
+  ContactProb P;
+  rot_diag(q1, a1 * a1, bb1 * bb1, bb1 * bb1, P.e1);
+  rot_diag(q2, a2 * a2, bb2 * bb2, bb2 * bb2, P.e2);
+#pragma unroll
+  for (int i = 0; i < 3; ++i) { P.b1[i] = c1[i]; P.b2[i] = c2[i]; }
+  lm_solve(P, x, tol);
+  double cc[3], t1[3], t2[3], l1, l2, pt1[3], pt2[3];
+  support_points(P, x, cc, t1, t2, l1, l2, pt1, pt2);
+  const double d[3] = {pt1[0] - pt2[0], pt1[1] - pt2[1], pt1[2] - pt2[2]};
+  const double contact = d[0] * cc[0] + d[1] * cc[1] + d[2] * cc[2];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) { ept1[i] = pt1[i]; ept2[i] = pt2[i]; cn[i] = cc[i]; }
+  return (contact > 0) && (fmargin(a1, bb1, pt2, c1, q1) < 1.0) && (fmargin(a2, bb2, pt1, c2, q2) < 1.0);
+}
+
+}  // namespace gp

@@ -1,0 +1,555 @@
+// gp_search.cu -- binning, neighbour search, greedy matching and the data-movement
+// kernels of the collision step.
+#include <cooperative_groups.h>
+
+#include "gp_types.h"
+#include "gp_launch.h"
+
+namespace cg = cooperative_groups;
+
+namespace gp {
+
+// COLLISION on the device (collision.f90:7-200 with NPROC=1).
+//
+// The reference lists candidate pairs box by box (collision_detection_connectivity.f90:
+// 145-207): for each box IJK, for each particle NP1 of the box in ascending index,
+// first the later particles of the same box, then every particle of the 13 forward
+// neighbour boxes COLBOX(IJK)%CON(1..NCON) in order.  It then walks that list and lets
+// a pair collide only if neither particle has collided yet this step
+// (collision_interaction.f90:190-419).
+//
+// Device formulation (same result):
+//  1. particles are binned into a search grid whose cell edge is at least twice the
+//     largest bounding radius max(EMAJ, EMAJ/APR); a pair can only be in contact if
+//     its bounding spheres overlap (each contact point must lie inside the other body,
+//     ellipsoid_contact_detection.f90:125), so a half-stencil sweep over that grid
+//     finds every pair that could collide;
+//  2. for each such pair the reference's box ids decide whether the reference lists it
+//     at all and in which orientation, and give its position in the reference list as
+//     the key (IJK of HOME, index of HOME, stencil slot, index of NEAR);
+//  3. contacts and NVREL are evaluated for all of them on the pre-collision state (a
+//     pair is only ever evaluated while both its particles are unmodified);
+//  4. the lexicographically-first maximal matching of the colliding pairs under that key
+//     -- which is what the sequential COLOR walk produces -- is computed in parallel
+//     rounds (a pair is accepted when it holds the smallest key at both endpoints);
+//  5. COLLISION_RESPONSE is applied to the accepted pairs (disjoint, so race free).
+
+// Canonical slot of the 13 forward neighbour offsets in COLBOX order
+// (collision_box_connectivity.f90:127-312: boxes 9,12,15,17,18,20,21,22,23,24,25,26,27),
+// indexed by (dI+1)*9 + (dJ+1)*3 + (dK+1); 0 = not a forward offset.
+__constant__ int8_t c_fwd_slot[27] = {
+    // dI = -1: (dJ,dK) = (-1,-1) (-1,0) (-1,1) (0,-1) (0,0) (0,1) (1,-1) (1,0) (1,1)
+    0, 0, 0, 0, 0, 8, 0, 0, 11,
+    // dI = 0
+    0, 0, 6, 0, 0, 9, 0, 4, 12,
+    // dI = +1
+    0, 2, 7, 0, 3, 10, 1, 5, 13};
+
+__device__ __forceinline__ int wrap_delta(int d, int n, bool periodic) {
+  if (periodic) {
+    if (d == n - 1) return -1;
+    if (d == -(n - 1)) return 1;
+  }
+  return d;
+}
+
+
+// ---------------------------------------------------------------------------
+// 1. search-grid cell of every particle (counting pass)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int cell_coord(double v, double h, int n) {
+  const double f = v / h;
+  int c = (f >= 0.0) ? (f < (double)n ? (int)f : n - 1) : 0;
+  return c;
+}
+
+__global__ void k_bin_count(const InstDev *__restrict__ insts, const PoolView *__restrict__ pv, int64_t n,
+                            SearchArrays sa) {
+  const PoolView P = *pv;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int inst = P.inst[i];
+    if (inst < 0) { sa.cell_of[i] = -1; continue; }
+    const InstDev &I = insts[inst];
+    const int cx = cell_coord(P.st[0][i], I.hfx, I.nfx);
+    const int cy = cell_coord(P.st[1][i], I.hfy, I.nfy);
+    const int cz = cell_coord(P.st[2][i], I.hfz, I.nfz);
+    const int64_t c = I.cell_begin + ((int64_t)cz * I.nfy + cy) * I.nfx + cx;
+    sa.cell_of[i] = (int32_t)c;
+    atomicAdd(&sa.cell_count[c], 1);
+  }
+}
+
+void launch_bin_count(const InstDev *insts, const PoolView *pv, int64_t n, SearchArrays sa, Status *,
+                      int grid, cudaStream_t s) {
+  k_bin_count<<<grid, 256, 0, s>>>(insts, pv, n, sa);
+}
+
+// ---------------------------------------------------------------------------
+// 2. exclusive scan (three-level, 2048 elements per block)
+// ---------------------------------------------------------------------------
+constexpr int kScanThreads = 512, kScanPer = 4, kScanBlock = kScanThreads * kScanPer;
+
+__global__ void k_scan_block(const int32_t *__restrict__ in, int32_t *__restrict__ out, int64_t n,
+                             int32_t *__restrict__ sums) {
+  __shared__ int32_t warp_tot[kScanThreads / 32];
+  const int64_t base = (int64_t)blockIdx.x * kScanBlock + (int64_t)threadIdx.x * kScanPer;
+  int32_t v[kScanPer];
+  int32_t run = 0;
+#pragma unroll
+  for (int k = 0; k < kScanPer; ++k) {
+    const int64_t idx = base + k;
+    v[k] = (idx < n) ? in[idx] : 0;
+    const int32_t t = v[k];
+    v[k] = run;
+    run += t;
+  }
+  // inclusive warp scan of per-thread totals
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int32_t x = run;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) warp_tot[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    int32_t w = (lane < kScanThreads / 32) ? warp_tot[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int32_t y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    if (lane < kScanThreads / 32) warp_tot[lane] = w;
+  }
+  __syncthreads();
+  const int32_t excl = x - run + (wid > 0 ? warp_tot[wid - 1] : 0);
+#pragma unroll
+  for (int k = 0; k < kScanPer; ++k) {
+    const int64_t idx = base + k;
+    if (idx < n) out[idx] = v[k] + excl;
+  }
+  if (threadIdx.x == kScanThreads - 1 && sums != nullptr) sums[blockIdx.x] = excl + run;
+}
+
+__global__ void k_scan_add(int32_t *__restrict__ out, int64_t n, const int32_t *__restrict__ offs) {
+  const int64_t base = (int64_t)blockIdx.x * kScanBlock;
+  const int32_t o = offs[blockIdx.x];
+  for (int k = threadIdx.x; k < kScanBlock; k += blockDim.x) {
+    const int64_t idx = base + k;
+    if (idx < n) out[idx] += o;
+  }
+}
+
+static int64_t nblocks(int64_t n) { return (n + kScanBlock - 1) / kScanBlock; }
+
+int64_t scan_block_sums_size(int64_t n) {
+  // level-1 sums, level-2 sums (and their scans)
+  const int64_t b1 = nblocks(n + 1), b2 = nblocks(b1), b3 = nblocks(b2);
+  return 2 * (b1 + b2 + b3) + 16;
+}
+
+// out[0..n] = exclusive scan of in[0..n-1], out[n] = total.  in[n] must be readable
+// as zero (the caller allocates n+1 counters).
+void launch_scan(const int32_t *in, int32_t *out, int64_t n, int32_t *tmp, cudaStream_t s) {
+  const int64_t m = n + 1;
+  const int64_t b1 = nblocks(m), b2 = nblocks(b1), b3 = nblocks(b2);
+  int32_t *s1 = tmp, *s1x = s1 + b1, *s2 = s1x + b1, *s2x = s2 + b2, *s3 = s2x + b2;
+  k_scan_block<<<(unsigned)b1, kScanThreads, 0, s>>>(in, out, m, s1);
+  if (b1 > 1) {
+    k_scan_block<<<(unsigned)b2, kScanThreads, 0, s>>>(s1, s1x, b1, s2);
+    if (b2 > 1) {
+      k_scan_block<<<(unsigned)b3, kScanThreads, 0, s>>>(s2, s2x, b2, s3);   // b3 == 1 for n < 8.6e9
+      k_scan_add<<<(unsigned)b2, kScanThreads, 0, s>>>(s1x, b1, s2x);
+    }
+    k_scan_add<<<(unsigned)b1, kScanThreads, 0, s>>>(out, m, s1x);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 3. scatter into cell order + reference box ids (collision_detection_connectivity.f90:74-89)
+// ---------------------------------------------------------------------------
+__global__ void k_bin_scatter(const InstDev *__restrict__ insts, const PoolView *__restrict__ pv, int64_t n,
+                              SearchArrays sa, Status *st) {
+  const PoolView P = *pv;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t c = sa.cell_of[i];
+    if (c < 0) continue;
+    const int pos = sa.cell_start[c] + atomicAdd(&sa.cell_fill[c], 1);
+    const int inst = P.inst[i];
+    const InstDev &I = insts[inst];
+    const double x = P.st[0][i], y = P.st[1][i], z = P.st[2][i];
+    sa.sorted[pos] = (int32_t)i;
+    sa.sx[pos] = x;
+    sa.sy[pos] = y;
+    sa.sz[pos] = z;
+    sa.sr[pos] = fmax(P.pc[0][i], P.pc[1][i]);
+    sa.sinst[pos] = inst;
+    sa.sid[pos] = P.id[i];
+    const double fx = (x - I.xminbox) / I.dxbox, fy = (y - I.yminbox) / I.dybox, fz = (z - I.zminbox) / I.dzbox;
+    long long box = -1;
+    if (fx > -1.0 && fx < 2.0e9 && fy > -1.0 && fy < 2.0e9 && fz > -1.0 && fz < 2.0e9) {
+      const int i0 = (int)fx + 1, j0 = (int)fy + 1, k0 = (int)fz + 1;
+      if (i0 >= 1 && i0 <= I.nxbox && j0 >= 1 && j0 <= I.nybox && k0 >= 1 && k0 <= I.nzbox)
+        box = (long long)(i0 - 1) | ((long long)(j0 - 1) << 21) | ((long long)(k0 - 1) << 42);
+    }
+    if (box < 0) set_error(st, GP_EOUT_OF_GRID, (long long)P.id[i]);
+    sa.sbox[pos] = box;
+  }
+}
+
+void launch_bin_scatter(const InstDev *insts, const PoolView *pv, int64_t n, SearchArrays sa, Status *st, int grid,
+                        cudaStream_t s) {
+  k_bin_scatter<<<grid, 256, 0, s>>>(insts, pv, n, sa, st);
+}
+
+// ---------------------------------------------------------------------------
+// 4. half-stencil sweep of the search grid, reference adjacency and order key
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void emit_pair(PairRec *pairs, unsigned long long *npairs, int64_t cap, const PairRec &r,
+                                          Status *st) {
+  cg::coalesced_group g = cg::coalesced_threads();
+  unsigned long long base = 0;
+  if (g.thread_rank() == 0) base = atomicAdd(npairs, (unsigned long long)g.size());
+  base = g.shfl(base, 0);
+  const unsigned long long slot = base + g.thread_rank();
+  if ((int64_t)slot < cap) {
+    pairs[slot] = r;
+  } else {
+    atomicAdd(&st->overflow, 1ull);
+    set_error(st, GP_EPAIR_OVERFLOW, (long long)r.home);
+  }
+}
+
+// the 13 forward offsets (any half stencil of the search grid will do)
+__constant__ int8_t c_half[13][3] = {{1, 1, -1}, {1, -1, 0}, {1, 0, 0}, {0, 1, 0}, {1, 1, 0},
+                                     {0, -1, 1}, {1, -1, 1}, {-1, 0, 1}, {0, 0, 1}, {1, 0, 1},
+                                     {-1, 1, 1}, {0, 1, 1}, {1, 1, 1}};
+
+__global__ void __launch_bounds__(256) k_search(const InstDev *__restrict__ insts, int64_t n, SearchArrays sa,
+                                                PairRec *__restrict__ pairs, unsigned long long *npairs,
+                                                int64_t cap, Status *st) {
+  const int64_t nact = sa.cell_start[sa.ncells];
+  for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < nact; s += (int64_t)gridDim.x * blockDim.x) {
+    const int inst = sa.sinst[s];
+    const InstDev &I = insts[inst];
+    const double xp = sa.sx[s], yp = sa.sy[s], zp = sa.sz[s], rp = sa.sr[s];
+    const long long bp = sa.sbox[s];
+    const int pslot = sa.sorted[s];
+    const int32_t idp = sa.sid[s];
+    const int64_t lc = sa.cell_of[pslot] - I.cell_begin;
+    const int cx = (int)(lc % I.nfx), cy = (int)((lc / I.nfx) % I.nfy), cz = (int)(lc / ((int64_t)I.nfx * I.nfy));
+    const bool perx = I.periodicity != 0;
+    for (int o = -1; o < 13; ++o) {
+      int nx = cx, ny = cy, nz = cz;
+      if (o >= 0) {
+        nx += c_half[o][0];
+        ny += c_half[o][1];
+        nz += c_half[o][2];
+        if (nx < 0 || nx >= I.nfx) {
+          if (!perx) continue;
+          nx = (nx + I.nfx) % I.nfx;
+        }
+        ny = (ny + I.nfy) % I.nfy;
+        nz = (nz + I.nfz) % I.nfz;
+      }
+      const int64_t nc = I.cell_begin + ((int64_t)nz * I.nfy + ny) * I.nfx + nx;
+      int32_t q0 = sa.cell_start[nc];
+      const int32_t q1 = sa.cell_start[nc + 1];
+      if (o < 0) q0 = (int32_t)s + 1;
+      for (int32_t qs = q0; qs < q1; ++qs) {
+        double dx = sa.sx[qs] - xp, dy = sa.sy[qs] - yp, dz = sa.sz[qs] - zp;
+        if (perx && fabs(dx) > I.lx / 2) dx = dx - copysign(I.lx, dx);
+        if (fabs(dy) > I.ly / 2.) dy = dy - copysign(I.ly, dy);
+        if (fabs(dz) > I.lz / 2.) dz = dz - copysign(I.lz, dz);
+        const double rr = (rp + sa.sr[qs]) * (1.0 + 1e-9);
+        if (dx * dx + dy * dy + dz * dz > rr * rr) continue;
+        atomicAdd(&st->n_near, 1ull);
+        // reference adjacency of the two boxes (collision_box_connectivity.f90)
+        const long long bq = sa.sbox[qs];
+        if (bp < 0 || bq < 0) continue;   // already reported as out of grid
+        const int pi = (int)(bp & 0x1FFFFF), pj = (int)((bp >> 21) & 0x1FFFFF), pk = (int)(bp >> 42);
+        const int qi = (int)(bq & 0x1FFFFF), qj = (int)((bq >> 21) & 0x1FFFFF), qk = (int)(bq >> 42);
+        const int di = wrap_delta(qi - pi, I.nxbox, perx);
+        const int dj = wrap_delta(qj - pj, I.nybox, true);
+        const int dk = wrap_delta(qk - pk, I.nzbox, true);
+        if (di < -1 || di > 1 || dj < -1 || dj > 1 || dk < -1 || dk > 1) continue;
+        const int32_t idq = sa.sid[qs];
+        PairRec r;
+        int slot;
+        long long hb;
+        bool home_is_p;
+        if (di == 0 && dj == 0 && dk == 0) {
+          slot = 0;
+          home_is_p = idp < idq;
+          hb = bp;
+        } else {
+          const int idx = (di + 1) * 9 + (dj + 1) * 3 + (dk + 1);
+          slot = c_fwd_slot[idx];
+          if (slot > 0) {
+            home_is_p = true;
+            hb = bp;
+          } else {
+            slot = c_fwd_slot[26 - idx];
+            home_is_p = false;
+            hb = bq;
+          }
+        }
+        const int hi = (int)(hb & 0x1FFFFF), hj = (int)((hb >> 21) & 0x1FFFFF), hk = (int)(hb >> 42);
+        const unsigned long long ijk =
+            (unsigned long long)(hi + 1) + (unsigned long long)hj * I.nxbox + (unsigned long long)hk * I.nxbox * I.nybox;
+        const int32_t idh = home_is_p ? idp : idq, idn = home_is_p ? idq : idp;
+        r.home = home_is_p ? pslot : sa.sorted[qs];
+        r.near = home_is_p ? sa.sorted[qs] : pslot;
+        r.k1 = ijk;
+        r.k2 = ((unsigned long long)idh << 34) | ((unsigned long long)slot << 30) | (unsigned long long)idn;
+        emit_pair(pairs, npairs, cap, r, st);
+      }
+    }
+  }
+}
+
+void launch_search(const InstDev *insts, int64_t n, SearchArrays sa, PairRec *pairs, unsigned long long *npairs,
+                   int64_t cap_pairs, Status *st, int grid, cudaStream_t s) {
+  k_search<<<grid, 256, 0, s>>>(insts, n, sa, pairs, npairs, cap_pairs, st);
+}
+
+// ---------------------------------------------------------------------------
+// 5. lexicographically-first maximal matching of the colliding pairs
+//    (the outcome of the COLOR walk, collision_interaction.f90:190-207,397-398)
+// ---------------------------------------------------------------------------
+constexpr int kMatchThreads = 1024;
+
+__global__ void __launch_bounds__(kMatchThreads) k_match(const CollRec *__restrict__ coll,
+                                                         const unsigned long long *__restrict__ ncoll, int64_t cap,
+                                                         unsigned long long *best1, unsigned long long *best2,
+                                                         int8_t *matched, int8_t *state, Status *st) {
+  __shared__ int remaining_s[kMatchThreads / 32];
+  __shared__ int remaining;
+  const int64_t nc = (int64_t)min(*ncoll, (unsigned long long)cap);
+  const unsigned long long kMax = ~0ull;
+  for (int64_t e = threadIdx.x; e < nc; e += kMatchThreads) state[e] = 0;
+  __syncthreads();
+  bool done = (nc == 0);
+  int64_t round = 0;
+  while (!done) {
+    for (int64_t e = threadIdx.x; e < nc; e += kMatchThreads) {
+      if (state[e] != 0) continue;
+      const CollRec &r = coll[e];
+      atomicMin(&best1[r.home], r.k1);
+      atomicMin(&best1[r.near], r.k1);
+    }
+    __syncthreads();
+    for (int64_t e = threadIdx.x; e < nc; e += kMatchThreads) {
+      if (state[e] != 0) continue;
+      const CollRec &r = coll[e];
+      if (best1[r.home] == r.k1) atomicMin(&best2[r.home], r.k2);
+      if (best1[r.near] == r.k1) atomicMin(&best2[r.near], r.k2);
+    }
+    __syncthreads();
+    for (int64_t e = threadIdx.x; e < nc; e += kMatchThreads) {
+      if (state[e] != 0) continue;
+      const CollRec &r = coll[e];
+      if (best1[r.home] == r.k1 && best2[r.home] == r.k2 && best1[r.near] == r.k1 && best2[r.near] == r.k2) {
+        state[e] = 3;   // accepted in this round
+        matched[r.home] = 1;
+        matched[r.near] = 1;
+      }
+    }
+    __syncthreads();
+    for (int64_t e = threadIdx.x; e < nc; e += kMatchThreads) {
+      const int8_t sv = state[e];
+      if (sv != 0 && sv != 3) continue;
+      const CollRec &r = coll[e];
+      best1[r.home] = kMax; best1[r.near] = kMax;
+      best2[r.home] = kMax; best2[r.near] = kMax;
+    }
+    __syncthreads();
+    int cnt = 0;
+    for (int64_t e = threadIdx.x; e < nc; e += kMatchThreads) {
+      const int8_t sv = state[e];
+      if (sv == 3) { state[e] = 1; continue; }
+      if (sv != 0) continue;
+      const CollRec &r = coll[e];
+      if (matched[r.home] || matched[r.near]) state[e] = 2; else ++cnt;
+    }
+    cnt = __reduce_add_sync(0xffffffffu, cnt);
+    if ((threadIdx.x & 31) == 0) remaining_s[threadIdx.x >> 5] = cnt;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int t = 0;
+      for (int w = 0; w < kMatchThreads / 32; ++w) t += remaining_s[w];
+      remaining = t;
+    }
+    __syncthreads();
+    ++round;
+    done = (remaining == 0);
+    if (!done && round > nc + 1) {   // every round accepts at least one pair; cannot happen
+      if (threadIdx.x == 0) set_error(st, GP_ETIMEOUT, round);
+      done = true;
+    }
+  }
+  __syncthreads();
+  for (int64_t e = threadIdx.x; e < nc; e += kMatchThreads) {
+    const CollRec &r = coll[e];
+    matched[r.home] = 0;
+    matched[r.near] = 0;
+  }
+}
+
+void launch_match(const CollRec *coll, const unsigned long long *ncoll, int64_t cap_coll, unsigned long long *best1,
+                  unsigned long long *best2, int8_t *matched, int8_t *state, Status *st, cudaStream_t s) {
+  k_match<<<1, kMatchThreads, 0, s>>>(coll, ncoll, cap_coll, best1, best2, matched, state, st);
+}
+
+// ---------------------------------------------------------------------------
+// Data movement
+// ---------------------------------------------------------------------------
+// Internal field layout from a reference-layout or interior source (one component).
+template <typename T>
+__global__ void k_field_layout(T *__restrict__ dst, int nx, int ny, int nz, int ncomp, int comp,
+                               const double *__restrict__ src, int src_layout, int ghost_mode) {
+  const int64_t sx = nx + 3, sy = ny + 4, sz = nz + 4;
+  const int64_t total = sx * sy * sz;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const int ix = (int)(t % sx), jy = (int)((t / sx) % sy), kz = (int)(t / (sx * sy));
+    int i = ix;
+    if (ix == 0) i = nx;
+    else if (ix == nx + 1) i = 1;
+    else if (ix == nx + 2) i = 2;
+    const int j = jy - 1, k = kz - 1;   // reference indices, -1..N+2
+    double v;
+    if (src_layout == GP_LAYOUT_REFERENCE) {
+      v = src[(int64_t)(i - 1) + (int64_t)nx * ((int64_t)(j + 1) + (int64_t)(ny + 4) * (int64_t)(k + 1))];
+    } else {
+      const bool inside = (j >= 1 && j <= ny && k >= 1 && k <= nz);
+      if (!inside && ghost_mode == GP_GHOST_ZERO) {
+        v = 0.0;
+      } else {
+        const int jj = (j < 1) ? j + ny : (j > ny ? j - ny : j);
+        const int kk = (k < 1) ? k + nz : (k > nz ? k - nz : k);
+        v = src[(int64_t)(i - 1) + (int64_t)nx * ((int64_t)(jj - 1) + (int64_t)ny * (int64_t)(kk - 1))];
+      }
+    }
+    dst[t * ncomp + comp] = (T)v;
+  }
+}
+
+void launch_field_layout(void *dst, int prec, int nx, int ny, int nz, int ncomp, int comp, const double *src,
+                         int src_layout, int ghost_mode, cudaStream_t s) {
+  const int grid = 148 * 8;
+  if (prec == GP_PREC_MIXED)
+    k_field_layout<float><<<grid, 256, 0, s>>>(static_cast<float *>(dst), nx, ny, nz, ncomp, comp, src, src_layout,
+                                                ghost_mode);
+  else
+    k_field_layout<double><<<grid, 256, 0, s>>>(static_cast<double *>(dst), nx, ny, nz, ncomp, comp, src,
+                                                 src_layout, ghost_mode);
+}
+
+// Pool -> caller order for one instance: out[c*count + id] = state column c.
+__global__ void k_gather_state(const PoolView *__restrict__ pv, int64_t n, int inst, double *__restrict__ out,
+                               double *const *fluid, double *__restrict__ fout, int64_t count) {
+  const PoolView P = *pv;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    if (P.inst[i] != inst) continue;
+    const int64_t id = P.id[i];
+    if (id < 0 || id >= count) continue;
+#pragma unroll
+    for (int c = 0; c < kNState; ++c) out[c * count + id] = P.st[c][i];
+    if (fout != nullptr && fluid != nullptr) {
+#pragma unroll
+      for (int c = 0; c < kNFluid; ++c) fout[c * count + id] = fluid[c][i];
+    }
+  }
+}
+
+void launch_gather_state(const PoolView *pv, int64_t n, int inst, double *out, double *const *fluid_cols,
+                         double *fluid_out, int64_t count, cudaStream_t s) {
+  const int grid = 148 * 8;
+  k_gather_state<<<grid, 256, 0, s>>>(pv, n, inst, out, fluid_cols, fluid_out, count);
+}
+
+// caller order -> pool for one instance (state columns only)
+__global__ void k_scatter_state(const PoolView *__restrict__ pv, int64_t n, int inst, const double *__restrict__ cols,
+                                int64_t count) {
+  const PoolView P = *pv;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    if (P.inst[i] != inst) continue;
+    const int64_t id = P.id[i];
+    if (id < 0 || id >= count) continue;
+#pragma unroll
+    for (int c = 0; c < kNState; ++c) P.st[c][i] = cols[c * count + id];
+  }
+}
+
+void launch_scatter_state(const PoolView *pv, int64_t n, int inst, const double *cols, int64_t count,
+                          cudaStream_t s) {
+  k_scatter_state<<<148 * 8, 256, 0, s>>>(pv, n, inst, cols, count);
+}
+
+__global__ void k_init_pool(PoolView P, int64_t begin, int64_t n, int inst, const double *__restrict__ cols,
+                            const double *__restrict__ pcs) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = begin + k;
+#pragma unroll
+    for (int c = 0; c < kNState; ++c) P.st[c][i] = cols[c * n + k];
+#pragma unroll
+    for (int c = 0; c < kNConst; ++c) P.pc[c][i] = pcs[c * n + k];
+    P.id[i] = (int32_t)k;
+    P.inst[i] = inst;
+  }
+}
+
+void launch_init_pool(PoolView pv, int64_t begin, int64_t n, int inst, const double *cols, const double *pcs,
+                      cudaStream_t s) {
+  if (n <= 0) return;
+  k_init_pool<<<148 * 8, 256, 0, s>>>(pv, begin, n, inst, cols, pcs);
+}
+
+// COLLISION_BOX_CONNECTIVITY (collision_box_connectivity.f90:42-322), NPROC=1.
+__global__ void k_connectivity(int NXB, int NYB, int NZB, int periodicity, int32_t *ncon, int32_t *con) {
+  const int64_t nbox = (int64_t)NXB * NYB * NZB;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nbox; t += (int64_t)gridDim.x * blockDim.x) {
+    const int i0 = (int)(t % NXB) + 1, j0 = (int)((t / NXB) % NYB) + 1, k0 = (int)(t / ((int64_t)NXB * NYB)) + 1;
+    auto BOX = [&](int i, int j, int k) { return (int32_t)(i + (j - 1) * NXB + (k - 1) * NXB * NYB); };
+    int im1 = i0 - 1, ip1 = i0 + 1, jm1 = j0 - 1, jp1 = j0 + 1, km1 = k0 - 1, kp1 = k0 + 1;
+    if (im1 < 1 && periodicity) im1 = NXB;
+    if (ip1 > NXB && periodicity) ip1 = 1;
+    if (jm1 < 1) jm1 = NYB;
+    if (jp1 > NYB) jp1 = 1;
+    if (km1 < 1) km1 = NZB;
+    if (kp1 > NZB) kp1 = 1;
+    int32_t c[27];
+    int nn = 0;
+    if (km1 >= 1 && jp1 <= NYB && ip1 <= NXB) c[nn++] = BOX(ip1, jp1, km1);   // box 9
+    if (jm1 >= 1 && ip1 <= NXB) c[nn++] = BOX(ip1, jm1, k0);                  // box 12
+    if (ip1 <= NXB) c[nn++] = BOX(ip1, j0, k0);                                // box 15
+    if (jp1 <= NYB) {
+      c[nn++] = BOX(i0, jp1, k0);                                               // box 17
+      if (ip1 <= NXB) c[nn++] = BOX(ip1, jp1, k0);                             // box 18
+    }
+    if (kp1 <= NZB) {
+      if (jm1 >= 1) {
+        c[nn++] = BOX(i0, jm1, kp1);                                            // box 20
+        if (ip1 <= NXB) c[nn++] = BOX(ip1, jm1, kp1);                          // box 21
+      }
+      if (im1 >= 1) c[nn++] = BOX(im1, j0, kp1);                               // box 22
+      c[nn++] = BOX(i0, j0, kp1);                                               // box 23
+      if (ip1 <= NXB) c[nn++] = BOX(ip1, j0, kp1);                             // box 24
+      if (jp1 <= NYB) {
+        if (im1 >= 1) c[nn++] = BOX(im1, jp1, kp1);                            // box 25
+        c[nn++] = BOX(i0, jp1, kp1);                                            // box 26
+        if (ip1 <= NXB) c[nn++] = BOX(ip1, jp1, kp1);                          // box 27
+      }
+    }
+    const int64_t ijk = (i0 - 1) + (int64_t)(j0 - 1) * NXB + (int64_t)(k0 - 1) * NXB * NYB;
+    ncon[ijk] = nn;
+    for (int q = 0; q < 27; ++q) con[ijk * 27 + q] = (q < nn) ? c[q] : 0;
+  }
+}
+
+void launch_connectivity(int nxb, int nyb, int nzb, int periodicity, int32_t *ncon, int32_t *con, cudaStream_t s) {
+  k_connectivity<<<148 * 8, 128, 0, s>>>(nxb, nyb, nzb, periodicity, ncon, con);
+}
+
+}  // namespace gp

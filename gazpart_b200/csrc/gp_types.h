@@ -1,0 +1,89 @@
+// gp_types.h -- device-side data structures shared by the kernels and the host API.
+#pragma once
+#include <cstdint>
+
+#include "../../include/gazpart_gpu.h"
+
+namespace gp {
+
+// Per-ensemble record read by every kernel (one entry per instance; a single-ensemble
+// context has one).  Mirrors the module variables the reference routines read.
+struct InstDev {
+  // particle range in the pool
+  int64_t begin, count;
+  // field
+  const void *field;          // [z: nz+4][y: ny+4][x: nx+3][comp], float or double
+  int32_t nx, ny, nz, ncomp;  // interior sizes
+  int32_t fprec;              // GP_PREC_FP64 / GP_PREC_MIXED (float storage)
+  int32_t periodicity, wall_boundary, store_fluid;
+  double dx, dy, dz, lx, ly, lz;
+  double visc, dtime, gravity, ecp, mup, ecw, muw;
+  // collision box grid (collision_initiation.f90:44-103)
+  int32_t nxbox, nybox, nzbox, pad0;
+  double dxbox, dybox, dzbox, xminbox, yminbox, zminbox;
+  // search grid (cell edge >= 2 * largest bounding radius)
+  int32_t nfx, nfy, nfz, pad1;
+  double hfx, hfy, hfz, rmax;
+  int64_t cell_begin;         // first cell of this instance in the global cell arrays
+};
+
+// Double-buffered structure-of-arrays particle pool.  Column j of buffer b is
+// col[b][j]; kernels read the buffer `cur` through perm and write buffer cur^1.
+constexpr int kNState = 13;   // x y z u v w qa qb qc qd ox oy oz
+constexpr int kNConst = 10;   // a b deq cdrag cpitch crot h5 ipxx ipyy ipzz
+constexpr int kNFluid = 6;    // ufap vfap wfap vortx vorty vortz
+
+struct PoolView {
+  double *st[kNState];
+  double *pc[kNConst];
+  int32_t *id;      // index within the instance (caller order)
+  int32_t *inst;    // instance of the particle
+};
+
+// Device status word: first error code, the id that raised it, counters.
+struct Status {
+  int32_t code;
+  int32_t pad;
+  long long first_id;
+  unsigned long long n_near;      // candidate pairs within bounding distance
+  unsigned long long n_contact;   // pairs in contact
+  unsigned long long n_coll;      // colliding pairs (flag && NVREL < ZERO)
+  unsigned long long n_accept;    // accepted (responded) pairs
+  unsigned long long overflow;    // pairs dropped by a full buffer
+};
+
+__device__ inline void set_error(Status *s, int code, long long id) {
+  if (atomicCAS(&s->code, 0, code) == 0) s->first_id = id;
+}
+
+// A candidate pair in the pool: HOME/NEAR pool slots plus the reference order key
+// (IJK of HOME, index of HOME, stencil slot, index of NEAR), compared as (k1, k2).
+struct PairRec {
+  int32_t home, near;               // pool slots
+  unsigned long long k1;            // IJK (1-based box id of HOME)
+  unsigned long long k2;            // (id_home << 34) | (slot << 30) | id_near
+};
+constexpr int64_t kMaxInstanceParticles = (int64_t)1 << 30;
+
+// A colliding pair with what COLLISION_RESPONSE needs.
+struct CollRec {
+  int32_t home, near;
+  unsigned long long k1, k2;
+  double rx1[3], rx2[3], cn[3];
+};
+
+// Binned particles of the collision search grid (see gp_search.cu).
+struct SearchArrays {
+  int32_t *cell_count;   // per search cell (+1 zero sentinel)
+  int32_t *cell_start;   // exclusive scan, ncells+1
+  int32_t *cell_fill;
+  int32_t *cell_of;      // per pool slot
+  int32_t *sorted;       // pool slot of each sorted position
+  double *sx, *sy, *sz, *sr;
+  long long *sbox;       // packed box coords (I0-1) | (J0-1)<<21 | (K0-1)<<42, -1 if outside
+  int32_t *sinst;
+  int32_t *sid;          // index of the particle within its instance
+  int64_t ncells;
+};
+
+}  // namespace gp

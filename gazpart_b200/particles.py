@@ -4,7 +4,10 @@ The reference draws positions in ``[a, L-a]`` and orientations from a normalised
 uniform cube (``initiation_particle_position.f90:301-349``), then sets velocities from
 the fluid (``initiation_particle_velocity.f90:76-115``).  The benchmark ensembles use:
 
-* positions uniform in ``[0, L)^3``;
+* positions uniform in ``[r, L-r]^3`` with ``r`` the largest semi-axis (the
+  reference draws in ``[EMAJ, L-EMAJ]``, ``initiation_particle_position.f90:309-316``;
+  its wall test runs on the x planes even in periodic mode, so a particle must not
+  start across them);
 * orientations uniform on S^3 (Shoemake's subgroup algorithm);
 * shapes and Stokes numbers per :class:`~gazpart_b200.config.ParticleSpec`;
 * per-unit-mass inertia ``IPXX=(b^2+c^2)/5, IPYY=(a^2+c^2)/5, IPZZ=(a^2+b^2)/5``
@@ -33,9 +36,7 @@ def draw(spec: ParticleSpec, setup: Setup) -> Dict[str, np.ndarray]:
     rng = np.random.default_rng(spec.seed)
     n = spec.n
     out: Dict[str, np.ndarray] = {}
-    out["x"] = rng.random(n) * setup.lx
-    out["y"] = rng.random(n) * setup.ly
-    out["z"] = rng.random(n) * setup.lz
+    rx, ry, rz = rng.random(n), rng.random(n), rng.random(n)
     u1, u2, u3 = rng.random(n), rng.random(n), rng.random(n)
     s1, s2 = np.sqrt(1.0 - u1), np.sqrt(u1)
     out["qa"] = s2 * np.cos(2.0 * math.pi * u3)
@@ -67,6 +68,13 @@ def draw(spec: ParticleSpec, setup: Setup) -> Dict[str, np.ndarray]:
     if spec.st is not None and spec.ar is not None and spec.b is not None:
         # monodisperse: exactly the nominal density ratio
         rhop = np.full(n, spec.density_ratio * setup.rhof)
+    # positions as the reference draws them, XRAND*(L - 2 EMAJ) + EMAJ
+    # (initiation_particle_position.f90:309-316), with the largest semi-axis in place of
+    # EMAJ so that no particle starts across the x planes that the wall test watches
+    r = np.maximum(emaj, emaj / apr)
+    out["x"] = rx * (setup.lx - 2.0 * r) + r
+    out["y"] = ry * (setup.ly - 2.0 * r) + r
+    out["z"] = rz * (setup.lz - 2.0 * r) + r
     out["emaj"] = emaj
     out["apr"] = apr
     out["rhop"] = rhop

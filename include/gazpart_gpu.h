@@ -1,0 +1,228 @@
+/*
+ * gazpart_gpu.h -- C ABI of the B200 implementation of GAZPART's frozen-flow
+ * ellipsoidal-particle step (ADV_PARTICLE_ELLP followed by COLLISION).
+ *
+ * Every entry point replaces one Fortran routine of the reference; the routine and
+ * its file:line (relative to the reference's source/ directory) are given beside it.
+ * A Fortran driver binds these through ISO_C_BINDING interfaces with the reference's
+ * argument lists (scalars by VALUE, arrays by reference); the module-level inputs the
+ * reference reads implicitly (VISC, RHOF, DTIME, EMAJ_PART, ...) live in the context.
+ *
+ * Conventions
+ *  - All functions return an int status: GP_OK (0) or one of the GP_E* codes.  The
+ *    reference `stop`s where these report an error; a Fortran wrapper turns a nonzero
+ *    status into `error stop` with the reference's message.
+ *  - A context owns one CUDA stream on the current device and is not thread safe.
+ *    Calls that return host data synchronise the stream before returning.
+ *  - Arrays flagged `on_device` are device pointers on the context's device;
+ *    otherwise host pointers (pinned memory is fastest).
+ *  - Indices: IG (class) and IDP (sub-class) are 1-based as in the reference.
+ *  - Particle state columns, in this order (GP_NSTATE = 13):
+ *      x y z  u v w  qa qb qc qd  ox oy oz
+ *    (PARTTYPE XP..ZP, UP..WP, ELLQUAT%a..d, OMEGAX..Z; mod_particle_parallel.f90:17-47).
+ *  - Per-particle property columns (GP_NPROP = 6): emaj apr rhop ipxx ipyy ipzz
+ *    (EMAJ_PART, APR_PART, RHOP, IPXX..IPZZ of the particle's class; every particle
+ *    may carry its own values).
+ */
+#ifndef GAZPART_GPU_H
+#define GAZPART_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GP_NSTATE 13
+#define GP_NPROP 6
+#define GP_NFLUID 6
+
+/* status codes */
+enum {
+    GP_OK = 0,
+    GP_ENAN_FORCE = 1,      /* 'In Fluid force'           fluid_force_ellipsoid.f90:150-159 */
+    GP_ENAN_TORQUE = 2,     /* NaN angular velocity       fluid_torque_ellipsoid.f90:178-188 */
+    GP_EENERGY = 3,         /* kinetic-energy balance     collision_response.f90:408-436,
+                                                          wall_ellipsoid_rebound.f90:372-385 */
+    GP_ESINGULAR = 4,       /* 'Matrix is numerically singular!' invert_ndim3_matrix.f90:19-21 */
+    GP_EPAIR_OVERFLOW = 5,  /* candidate/contact buffer full (the reference has no check) */
+    GP_EOUT_OF_GRID = 6,    /* particle outside the box grid collision_detection_connectivity.f90:81-89,
+                               or outside the interpolation stencil range */
+    GP_ETIMEOUT = 7,        /* a bounded device loop or host wait gave up */
+    GP_ECUDA = 8,           /* CUDA runtime error */
+    GP_EBADARG = 9,         /* invalid argument / unsupported configuration */
+    GP_ENOMEM = 10          /* device allocation or HBM budget refused */
+};
+
+/* precision modes */
+enum {
+    GP_PREC_FP64 = 0,   /* plain path: FP64 field, FP64 everything */
+    GP_PREC_MIXED = 1   /* FP32 field and stencil weights with compensated FP32 sums,
+                           FP32 drag/lift/torque coefficients; FP64 integration,
+                           quaternion renormalisation and FP64 contact solve */
+};
+
+/* field source layouts for gp_set_field */
+enum {
+    GP_LAYOUT_INTERIOR = 0,   /* (NX, NY, NZ), x fastest */
+    GP_LAYOUT_REFERENCE = 1   /* (NX, NY+4, NZ+4) with ghost planes, x fastest
+                                 (allocate_arrays.f90:93-118, NGHTCELL=2) */
+};
+/* ghost-plane modes for GP_LAYOUT_INTERIOR sources */
+enum {
+    GP_GHOST_PERIODIC = 0,    /* FLUIDCOMM on one rank (MPI_structures.f90:84-132) */
+    GP_GHOST_ZERO = 1         /* never exchanged: the reference's vorticity arrays (main.f90:255-259) */
+};
+/* field components */
+enum { GP_U = 0, GP_V = 1, GP_W = 2, GP_VORTX = 3, GP_VORTY = 4, GP_VORTZ = 5 };
+
+/* Module-level inputs of the hot path (mod_param_phys.f90:14-113, mod_dns_dim.f90,
+ * collision variables mod_collision.f90:5-38, readparam.f90). */
+typedef struct {
+    int32_t nx, ny, nz;          /* NX, NY, NZ; DX = LXMAX/real(NX-1) (meshing.f90:43-45) */
+    double lx, ly, lz;           /* LXMAX, LYMAX, LZMAX */
+    double visc, rhof;           /* VISC, RHOF */
+    double dtime;                /* DTIME */
+    double gravity;              /* GRAVITY(IG) */
+    double ecp, mup;             /* ECP(IG), MUP(IG) */
+    double ecw, muw;             /* ECW, MUW */
+    int32_t periodicity;         /* PERIODICITY */
+    int32_t wall_boundary;       /* WALL_BOUNDARY (stencil x mirror) */
+    int32_t interp_scheme;       /* INTERP_SCHEME, must be 3 */
+    int32_t frozen_flow;         /* FROZEN_FLOW: 2 = interpolate a frozen field */
+    int32_t precision;           /* GP_PREC_FP64 or GP_PREC_MIXED */
+    int32_t store_fluid;         /* 1: write the interpolated field at each particle
+                                    (PART%UFAP..VORTZAP) every step */
+    int64_t max_particles;       /* particle capacity of the context (0: set by upload) */
+} gp_params;
+
+typedef struct gp_ctx gp_ctx;
+
+/* ---------------------------------------------------------------- context ---- */
+/* Allocates a context bound to the current CUDA device with one ensemble (class) and
+ * one field slot described by *params.  Replaces the set-up that INIT_RUN/MESHING/
+ * ALLOCATE_ARRAYS/COLLISION_INITIATION perform for the hot path (main.f90:125-340). */
+int gp_ctx_create(const gp_params *params, gp_ctx **out);
+int gp_ctx_destroy(gp_ctx *ctx);
+/* First error recorded on the device since the last gp_clear_status: code and the
+ * particle (or pair home) index that raised it. */
+int gp_status(gp_ctx *ctx, int32_t *code, int64_t *first_id);
+int gp_clear_status(gp_ctx *ctx);
+int gp_sync(gp_ctx *ctx);
+
+/* Class table used by the per-routine entry points that take IG/IDP:
+ * EMAJ_PART(IG,IDP), APR_PART(IG), RHOP(IG,IDP); IPXX..IPZZ follow
+ * initiation_particle_position.f90:609-634. */
+int gp_set_class(gp_ctx *ctx, int32_t ig, int32_t idp, double emaj, double apr, double rhop);
+
+/* Load one field component (UFLU, VFLU, WFLU, VORTICITY_X..Z;
+ * mod_fluid_variable.f90:11-24) into the device layout. */
+int gp_set_field(gp_ctx *ctx, int32_t comp, const double *src, int32_t src_layout,
+                 int32_t ghost_mode, int32_t on_device);
+
+/* Particle state (PART(1:N, IG)) in / out.  cols: GP_NSTATE column pointers;
+ * props: GP_NPROP column pointers.  Download returns the caller's original order. */
+int gp_upload_state(gp_ctx *ctx, int64_t n, const double *const *cols,
+                    const double *const *props, int32_t on_device);
+int gp_download_state(gp_ctx *ctx, int64_t n, double *const *cols, double *const *fluid,
+                      int32_t on_device);
+
+/* Replace the state columns of the resident particles (properties unchanged), caller
+ * order.  The drop-in form of handing PART back to the device after host-side edits. */
+int gp_put_state(gp_ctx *ctx, int64_t n, const double *const *cols, int32_t on_device);
+
+/* ---------------------------------------------------------------- hot path ---- */
+/* ADV_PARTICLE_ELLP(NCYCLE)  adv_particle_new.f90:7-704: interpolation of the six
+ * fields at x_n, RK2 predictor/corrector with wall handling, BOUNDARY_PARTICLE's
+ * periodic wrap (boundary_particle.f90:45-62).  State stays on the device. */
+int gp_adv_particle_ellp(gp_ctx *ctx, int32_t ncycle);
+/* COLLISION(NCYCLE, TIME)  collision.f90:7-200 with NPROC=1: detection
+ * (collision_detection_connectivity.f90) and greedy interaction in list order
+ * (collision_interaction.f90:190-419).  Optional counters: candidate pairs within
+ * bounding distance, contacts, collisions (any may be NULL). */
+int gp_collision(gp_ctx *ctx, int32_t ncycle, double time, int64_t *n_near,
+                 int64_t *n_contact, int64_t *n_coll);
+/* nsteps x (ADV_PARTICLE_ELLP + COLLISION) replayed from a captured CUDA graph. */
+int gp_step(gp_ctx *ctx, int32_t nsteps);
+/* nsteps steps with CUDA events recorded on the context's stream around every
+ * phase; returns the total and, per step on average, the ADV_PARTICLE_ELLP kernel and
+ * the collision phase durations in milliseconds, and the number of kernels one step
+ * launches (counted from the captured graph).  Any output pointer may be NULL. */
+int gp_step_timed(gp_ctx *ctx, int32_t nsteps, float *total_ms, float *advance_ms_avg,
+                  float *collision_ms_avg, int32_t *kernels_per_step);
+/* Last step's accepted collisions as (home, near) original indices, in acceptance
+ * (list) order; *count receives the total even if it exceeds cap. */
+int gp_collision_pairs(gp_ctx *ctx, int64_t cap, int32_t *home, int32_t *near, int64_t *count);
+
+/* COLLISION_BOX_CONNECTIVITY  collision_box_connectivity.f90:7-384 for the context's
+ * box grid (COLLISION_INITIATION, collision_initiation.f90:44-103).  ncon: NBOX,
+ * con: NBOX*27 (1-based box ids, zero-padded) host arrays; either may be NULL.
+ * grid_out (optional, 3 ints + 6 doubles): NXBOX NYBOX NZBOX, DXBOX DYBOX DZBOX,
+ * XMINBOX YMINBOX ZMINBOX. */
+int gp_collision_box_connectivity(gp_ctx *ctx, int32_t *nbox, int32_t *ncon, int32_t *con,
+                                  int32_t *grid_dims, double *grid_geom);
+
+/* ------------------------------------------------------ per-routine drop-ins ---- */
+/* INTERP_LAG3(XAIN,YAIN,ZAIN,UAIN,NINT,XINT,YINT,ZINT,UINT)  interp_lag3.f90:11-298
+ * on the context's field component `comp` (the mesh is the context's). */
+int gp_interp_lag3(gp_ctx *ctx, int32_t comp, int64_t nint, const double *xint,
+                   const double *yint, const double *zint, double *uint, int32_t on_device);
+/* FROZEN_INTERP_LAG3(XAIN,YAIN,ZAIN,NX,NY,NZ,UAIN,NINT,XINT,YINT,ZINT,UINT)
+ * frozen_interp_lag3.f90:11-274 (mirror boundaries).  Host arrays. */
+int gp_frozen_interp_lag3(gp_ctx *ctx, const double *xain, const double *yain,
+                          const double *zain, int32_t nx, int32_t ny, int32_t nz,
+                          const double *uain, int64_t nint, const double *xint,
+                          const double *yint, const double *zint, double *uint);
+/* FLUID_FORCE_ELLIPSOID(IG,IDP,UPART,VPART,WPART,UFLUID,VFLUID,WFLUID,quat,FDRAG,FLIFT)
+ * fluid_force_ellipsoid.f90:1-161 */
+int gp_fluid_force_ellipsoid(gp_ctx *ctx, int32_t ig, int32_t idp, double upart, double vpart,
+                             double wpart, double ufluid, double vfluid, double wfluid,
+                             const double quat[4], double fdrag[3], double flift[3]);
+/* batched form: n particles, arrays of length n (quat n*4, outputs n*3, row major) */
+int gp_fluid_force_ellipsoid_batch(gp_ctx *ctx, int64_t n, const int32_t *ig, const int32_t *idp,
+                                   const double *up, const double *uf, const double *quat,
+                                   double *fdrag, double *flift, int32_t on_device);
+/* FLUID_TORQUE_ELLIPSOID(I,IG,IDP,OX,OY,OZ,QUAT,TORQUE_PITCHING,TORQUE_ROTATION)
+ * fluid_torque_ellipsoid.f90:1-190.  The reference reads PART(I,IG)%UP..WP,
+ * %UFAP..WFAP and %VORTXAP..VORTZAP from its module; they are passed explicitly. */
+int gp_fluid_torque_ellipsoid(gp_ctx *ctx, int32_t ig, int32_t idp, double ox, double oy,
+                              double oz, const double quat[4], const double part_up[3],
+                              const double part_ufap[3], const double part_vort[3],
+                              double tpitch[3], double trot[3]);
+int gp_fluid_torque_ellipsoid_batch(gp_ctx *ctx, int64_t n, const int32_t *ig,
+                                    const int32_t *idp, const double *omega, const double *quat,
+                                    const double *part_up, const double *part_ufap,
+                                    const double *part_vort, double *tpitch, double *trot,
+                                    int32_t on_device);
+/* QUATERNION_INTEGRATION(qp_n, omgx, omgy, omgz, dt)  adv_quaternion.f90:1-117 */
+int gp_quaternion_integration(gp_ctx *ctx, double quat[4], double omgx, double omgy,
+                              double omgz, double dt);
+int gp_quaternion_integration_batch(gp_ctx *ctx, int64_t n, double *quat, const double *omega,
+                                    double dt, int32_t on_device);
+/* EULER_INTEGRATION(IG, IDP, omgx, omgy, omgz)  adv_angular_velocity.f90:1-168 */
+int gp_euler_integration(gp_ctx *ctx, int32_t ig, int32_t idp, double *omgx, double *omgy,
+                         double *omgz);
+/* ellipsoid_contact_detection(IG,IDP1,IDP2,IXP,IYP,IZP,IQUAT,JXP,JYP,JZP,JQUAT,
+ * flag,EPT1,EPT2,cnormal)  ellipsoid_contact_detection.f90:1-187 (lmder1 inside). */
+int gp_ellipsoid_contact_detection(gp_ctx *ctx, int32_t ig, int32_t idp1, int32_t idp2,
+                                   double ixp, double iyp, double izp, const double iquat[4],
+                                   double jxp, double jyp, double jzp, const double jquat[4],
+                                   int32_t *flag, double ept1[3], double ept2[3],
+                                   double cnormal[3]);
+/* batched form with explicit shapes: per pair emaj1 apr1 emaj2 apr2 (n*4), centres
+ * (n*6: b1,b2), quaternions (n*8: q1,q2).  Outputs flag n, ept1/ept2/cnormal n*3. */
+int gp_ellipsoid_contact_detection_batch(gp_ctx *ctx, int64_t n, const double *shapes,
+                                         const double *centres, const double *quats,
+                                         int32_t *flag, double *ept1, double *ept2,
+                                         double *cnormal, int32_t on_device);
+/* COLLISION_RESPONSE(IG,IDP,part1,part2,R_impact1,R_impact2,normal)
+ * collision_response.f90:1-437.  partK: 10 doubles in/out (UP VP WP, OMEGAX..Z,
+ * ELLQUAT a..d); inertia of class (IG,IDP) for both bodies as in the reference. */
+int gp_collision_response(gp_ctx *ctx, int32_t ig, int32_t idp, double part1[10],
+                          double part2[10], const double r_impact1[3],
+                          const double r_impact2[3], const double normal[3]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GAZPART_GPU_H */

@@ -1,0 +1,125 @@
+"""Host-side logic that needs no GPU: the C ABI library's exports, the workload
+conventions, the field generator, the particle initialiser and the replica timing
+reduction across ranks (gloo, two processes)."""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch
+
+from gazpart_b200 import _lib, config, field, particles
+
+
+def test_library_exports_every_declared_symbol():
+    names = _lib.exported_symbols()
+    assert len(names) >= 25
+    L = C.CDLL(_lib.LIB_PATH)
+    for n in names:
+        assert hasattr(L, n), n
+    # the ctypes table binds exactly the declared entry points
+    assert sorted(_lib.SIGNATURES) == names
+
+
+def test_params_struct_matches_header_layout():
+    # gp_params: 3 int32, 11 doubles, 6 int32, 1 int64 with natural alignment
+    assert C.sizeof(_lib.GPParams) == 3 * 4 + 4 + 11 * 8 + 6 * 4 + 8
+    assert _lib.GPParams.max_particles.offset % 8 == 0
+
+
+def test_workload_conventions():
+    w = config.C1
+    s = w.setup()
+    t = config.integral_time()
+    assert abs(t - math.sqrt(2 * math.pi) / 4) < 1e-15
+    st = particles.draw(w.spec, s)
+    assert np.all(st["rhop"] == 1000.0)
+    deq = (2 * st["emaj"]) / st["apr"] ** (2 / 3)
+    tau = (st["rhop"] / s.rhof) * deq ** 2 / (18 * s.visc)
+    assert np.allclose(tau / t, 1.0)          # St = 1
+    c3 = config.C3.spec
+    small = config.ParticleSpec(**{**c3.__dict__, "n": 20000})
+    st3 = particles.draw(small, config.C3.setup())
+    deq3 = (2 * st3["emaj"]) / st3["apr"] ** (2 / 3)
+    st_num = (st3["rhop"] / 1.0) * deq3 ** 2 / (18 * config.C3.setup().visc) / t
+    assert st_num.min() >= 0.1 - 1e-9 and st_num.max() <= 10 + 1e-9
+    assert (st3["apr"] < 1).any() and (st3["apr"] > 1).any()
+
+
+def test_particles_drawn_inside_and_unit_quaternions():
+    s = config.Setup(nx=32, ny=32, nz=32)
+    spec = config.ParticleSpec(n=5000, ar_range=(0.2, 5.0), b=0.01, st=1.0, seed=3)
+    st = particles.draw(spec, s)
+    r = np.maximum(st["emaj"], st["emaj"] / st["apr"])
+    for k, L in (("x", s.lx), ("y", s.ly), ("z", s.lz)):
+        assert np.all(st[k] >= r) and np.all(st[k] <= L - r)
+    qn = st["qa"] ** 2 + st["qb"] ** 2 + st["qc"] ** 2 + st["qd"] ** 2
+    assert np.allclose(qn, 1.0)
+    assert np.allclose(st["ipyy"], st["ipzz"])
+    again = particles.draw(spec, s)
+    assert all(np.array_equal(st[k], again[k]) for k in st)
+
+
+def test_field_is_solenoidal_with_the_target_energy():
+    n = 32
+    f = field.generate(n, seed=0, device="cpu")
+    e = 0.5 * sum(float((f[k] ** 2).mean()) for k in ("u", "v", "w"))
+    assert abs(e - 1.5) < 1e-12
+    period = n * (2 * math.pi / (n - 1))
+    k = torch.fft.fftfreq(n, d=period / n, dtype=torch.float64) * 2 * math.pi
+    kz, ky, kx = k.view(n, 1, 1), k.view(1, n, 1), k.view(1, 1, n)
+    div = torch.fft.ifftn(1j * (kx * torch.fft.fftn(f["u"]) + ky * torch.fft.fftn(f["v"]) + kz * torch.fft.fftn(f["w"]))).real
+    assert float(div.abs().max()) < 1e-10
+    g = field.generate(n, seed=0, device="cpu")
+    assert torch.equal(g["vortz"], f["vortz"])
+
+
+def test_reference_layout_ghosts():
+    rng = np.random.default_rng(0)
+    a = torch.from_numpy(rng.normal(size=(5, 6, 7)))
+    per = field.reference_layout(a, "periodic")
+    zer = field.reference_layout(a, "zero")
+    assert per.shape == (9, 10, 7)
+    # J = 0 ghost plane (index 1) holds interior J = NY (index 5 of the interior)
+    assert torch.equal(per[2:7, 1, :], a[:, 5, :])
+    assert torch.equal(per[0, 2:8, :], a[3, :, :])
+    assert torch.equal(zer[2:7, 2:8, :], a) and float(zer[0].abs().sum()) == 0.0
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+def _rank_main(rank, world, port, out):
+    import torch.distributed as dist
+    from bench import reduce_max_ms
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    local = [12.5, 20.0][rank]
+    out[rank] = reduce_max_ms(local, dist, "cpu")
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_replica_timing_reduction_two_ranks():
+    """bench.py --gpus N runs one replica per rank; the job time is the max over ranks."""
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    mgr = ctx.Manager()
+    out = mgr.dict()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_main, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+        assert p.exitcode == 0
+    assert out[0] == 20.0 and out[1] == 20.0
