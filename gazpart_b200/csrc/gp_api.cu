@@ -559,12 +559,16 @@ int gp_step_timed(gp_ctx *c, int32_t nsteps, float *total_ms, float *advance_ms_
   GP_CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
   int rc = GP_OK;
   for (int s = 0; s < nsteps && !rc; ++s) {
-    if (cudaEventRecord(ev[2 * s], c->stream) != cudaSuccess) rc = GP_ECUDA;
+    // external records: real timestamp nodes in the graph (a plain record inside a
+    // capture only orders work)
+    if (cudaEventRecordWithFlags(ev[2 * s], c->stream, cudaEventRecordExternal) != cudaSuccess) rc = GP_ECUDA;
     if (!rc) rc = enqueue_advance(c);
-    if (!rc && cudaEventRecord(ev[2 * s + 1], c->stream) != cudaSuccess) rc = GP_ECUDA;
+    if (!rc && cudaEventRecordWithFlags(ev[2 * s + 1], c->stream, cudaEventRecordExternal) != cudaSuccess)
+      rc = GP_ECUDA;
     if (!rc) rc = enqueue_collision(c);
   }
-  if (!rc && cudaEventRecord(ev[2 * nsteps], c->stream) != cudaSuccess) rc = GP_ECUDA;
+  if (!rc && cudaEventRecordWithFlags(ev[2 * nsteps], c->stream, cudaEventRecordExternal) != cudaSuccess)
+    rc = GP_ECUDA;
   cudaError_t e = cudaStreamEndCapture(c->stream, &g);
   if (!rc && e != cudaSuccess) rc = GP_ECUDA;
   if (!rc && kernels_per_step) {
@@ -586,13 +590,13 @@ int gp_step_timed(gp_ctx *c, int32_t nsteps, float *total_ms, float *advance_ms_
   if (!rc) {
     double adv = 0.0, col = 0.0;
     float t = 0.f;
-    for (int s = 0; s < nsteps; ++s) {
-      cudaEventElapsedTime(&t, ev[2 * s], ev[2 * s + 1]);
+    for (int s = 0; s < nsteps && !rc; ++s) {
+      if (cudaEventElapsedTime(&t, ev[2 * s], ev[2 * s + 1]) != cudaSuccess) rc = GP_ECUDA;
       adv += t;
-      cudaEventElapsedTime(&t, ev[2 * s + 1], ev[2 * s + 2]);
+      if (cudaEventElapsedTime(&t, ev[2 * s + 1], ev[2 * s + 2]) != cudaSuccess) rc = GP_ECUDA;
       col += t;
     }
-    cudaEventElapsedTime(&t, ev[0], ev[2 * nsteps]);
+    if (cudaEventElapsedTime(&t, ev[0], ev[2 * nsteps]) != cudaSuccess) rc = GP_ECUDA;
     if (total_ms) *total_ms = t;
     if (advance_ms_avg) *advance_ms_avg = (float)(adv / nsteps);
     if (collision_ms_avg) *collision_ms_avg = (float)(col / nsteps);

@@ -52,6 +52,116 @@ __device__ __forceinline__ double lm_enorm(const double* x) {
   return sqrt(x3max * ((s2 / x3max) + (x3max * s3)));
 }
 
+// Trigonometric functions of the contact solve.  The reference calls libm's
+// sin/cos/asin/acos there; the kernels and the CPU checker use these functions
+// (same constants, same operation order, compiled without contraction) so that their
+// Levenberg-Marquardt iterates agree bit for bit.  Method: Cody-Waite reduction by
+// pi/2 split into three parts and Taylor polynomials on [-pi/4, pi/4]; asin by its
+// Taylor series on |x| <= 1/2 and pi/2 - 2 asin(sqrt((1-x)/2)) above.  The solve
+// resolves its angles only to xtol = sqrt(eps), far above one-ulp differences.
+#define CT_QUAL __host__ __device__ __forceinline__
+CT_QUAL double ct_poly_sin(double z) {
+  double p = 1.9572941063391263e-20;
+  p = p * z + -8.22063524662433e-18;
+  p = p * z + 2.8114572543455206e-15;
+  p = p * z + -7.647163731819816e-13;
+  p = p * z + 1.6059043836821613e-10;
+  p = p * z + -2.505210838544172e-08;
+  p = p * z + 2.7557319223985893e-06;
+  p = p * z + -0.0001984126984126984;
+  p = p * z + 0.008333333333333333;
+  p = p * z + -0.16666666666666666;
+  return p;
+}
+
+CT_QUAL double ct_poly_cos(double z) {
+  double p = 4.110317623312165e-19;
+  p = p * z + -1.5619206968586225e-16;
+  p = p * z + 4.779477332387385e-14;
+  p = p * z + -1.1470745597729725e-11;
+  p = p * z + 2.08767569878681e-09;
+  p = p * z + -2.755731922398589e-07;
+  p = p * z + 2.48015873015873e-05;
+  p = p * z + -0.001388888888888889;
+  p = p * z + 0.041666666666666664;
+  return p;
+}
+
+/* sin and cos of x: Cody-Waite reduction by pi/2 = P1 + P2 + P3 (33 + 33 + 53 bits, so
+ * k*P1 and k*P2 are exact for |k| < 2^20), Taylor polynomials on [-pi/4, pi/4]. */
+CT_QUAL void ct_sincos(double x, double *s, double *c) {
+  if (!(fabs(x) < 1.0e9)) {
+    *s = x - x + (0.0 / 0.0 + x * 0.0);
+    *c = *s;
+    return;
+  }
+  const double k = rint(x * 0.6366197723675814);
+  const double r = ((x - k * 1.5707963267341256) - k * 6.077100506303966e-11) - k * 2.0222662487959506e-21;
+  const double z = r * r;
+  const double sn = r + r * z * ct_poly_sin(z);
+  const double cs = 1.0 + z * (-0.5 + z * ct_poly_cos(z));
+  switch ((long long)k & 3) {
+    case 0: *s = sn; *c = cs; break;
+    case 1: *s = cs; *c = -sn; break;
+    case 2: *s = -sn; *c = -cs; break;
+    default: *s = -cs; *c = sn; break;
+  }
+}
+
+CT_QUAL double ct_cos(double x) {
+  double s, c;
+  ct_sincos(x, &s, &c);
+  return c;
+}
+
+/* asin on |x| <= 1/2 by its Taylor series x + sum_k C(2k,k)/(4^k (2k+1)) x^(2k+1) */
+CT_QUAL double ct_asin_small(double x) {
+  const double z = x * x;
+  double p = 0.0020776610325181676;
+  p = p * z + 0.0022014739737101384;
+  p = p * z + 0.002338091892111975;
+  p = p * z + 0.0024894486782468836;
+  p = p * z + 0.00265787063820729;
+  p = p * z + 0.002846178401108942;
+  p = p * z + 0.0030578216492580306;
+  p = p * z + 0.003297059503473485;
+  p = p * z + 0.0035692053938259347;
+  p = p * z + 0.003880964558837669;
+  p = p * z + 0.004240907093679363;
+  p = p * z + 0.004660143486915096;
+  p = p * z + 0.005153309682319905;
+  p = p * z + 0.005740037670841924;
+  p = p * z + 0.006447210311889649;
+  p = p * z + 0.0073125258735988454;
+  p = p * z + 0.008390335809616815;
+  p = p * z + 0.009761609529194078;
+  p = p * z + 0.011551800896139705;
+  p = p * z + 0.01396484375;
+  p = p * z + 0.017352764423076924;
+  p = p * z + 0.022372159090909092;
+  p = p * z + 0.030381944444444444;
+  p = p * z + 0.044642857142857144;
+  p = p * z + 0.075;
+  p = p * z + 0.16666666666666666;
+  return x + x * z * p;
+}
+
+/* asin(x) = pi/2 - 2 asin(sqrt((1-|x|)/2)) for |x| > 1/2; NaN outside [-1, 1] */
+CT_QUAL double ct_asin(double x) {
+  const double ax = fabs(x);
+  if (!(ax <= 1.0)) return (x - x) / (x - x) + x;
+  double r;
+  if (ax <= 0.5) {
+    r = ct_asin_small(ax);
+  } else {
+    const double t = sqrt((1.0 - ax) * 0.5);
+    r = (1.5707963267948966 - 2.0 * ct_asin_small(t)) + 6.123233995736766e-17;
+  }
+  return copysign(r, x);
+}
+
+CT_QUAL double ct_acos(double x) { return (1.5707963267948966 - ct_asin(x)) + 6.123233995736766e-17; }
+
 struct ContactProb {
   double e1[9], e2[9];   // R diag(a^2,b^2,b^2) R^T (calculate_ellipsoid_matrix.f90:33-72)
   double b1[3], b2[3];
@@ -62,8 +172,8 @@ __device__ __forceinline__ void support_points(const ContactProb& P, const doubl
                                                double tmp2[3], double& l1, double& l2, double pt1[3],
                                                double pt2[3]) {
   double s0, k0, s1, k1;
-  sincos(x[0], &s0, &k0);
-  sincos(x[1], &s1, &k1);
+  ct_sincos(x[0], &s0, &k0);
+  ct_sincos(x[1], &s1, &k1);
   c1[0] = k0 * k1;
   c1[1] = s0 * k1;
   c1[2] = s1;
@@ -102,7 +212,7 @@ __device__ __forceinline__ void grad_coeff(const double e[9], const double c[3],
     for (int i = 0; i < 3; ++i) outer[i + 3 * j] = c[i] * row[j];
   double eo[9];
   matmul(e, outer, eo);
-  const double s = 1.0 / (2.0 * l), t = 1.0 / (8.0 * pow(l, 3.0));
+  const double s = 1.0 / (2.0 * l), t = 1.0 / (8.0 * (l * l * l));   // lambda**3.0
 #pragma unroll
   for (int k = 0; k < 9; ++k) co[k] = s * e[k] - t * eo[k];
 }
@@ -114,8 +224,8 @@ __device__ __forceinline__ void lm_jac(const ContactProb& P, const double x[2], 
   support_points(P, x, c1, t1, t2, l1, l2, pt1, pt2);
   const double depth[3] = {pt1[0] - pt2[0], pt1[1] - pt2[1], pt1[2] - pt2[2]};
   double s0, k0, s1, k1;
-  sincos(x[0], &s0, &k0);
-  sincos(x[1], &s1, &k1);
+  ct_sincos(x[0], &s0, &k0);
+  ct_sincos(x[1], &s1, &k1);
   const double g[6] = {-s0 * k1, k0 * k1, 0.0, -k0 * s1, -s0 * s1, k1};
   const double c2[3] = {-c1[0], -c1[1], -c1[2]};
   double co1[9], co2[9];
@@ -461,8 +571,8 @@ __device__ __forceinline__ bool contact_detection(double a1, double bb1, double 
   const double c_norm = sqrt(nrm[0] * nrm[0] + nrm[1] * nrm[1] + nrm[2] * nrm[2]);
   if (c_norm != 0.0) { nrm[0] = nrm[0] / c_norm; nrm[1] = nrm[1] / c_norm; nrm[2] = nrm[2] / c_norm; }
   double x[2];
-  x[1] = asin(nrm[2]);
-  x[0] = acos(nrm[0] / cos(x[1]));
+  x[1] = ct_asin(nrm[2]);
+  x[0] = ct_acos(nrm[0] / ct_cos(x[1]));
   if (x[0] != x[0] || x[1] != x[1]) {
 #pragma unroll
     for (int i = 0; i < 3; ++i) { ept1[i] = CUDART_NAN; ept2[i] = CUDART_NAN; cn[i] = CUDART_NAN; }
