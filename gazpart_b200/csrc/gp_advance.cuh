@@ -2,6 +2,8 @@
 // the six field components at x_n, RK2 predictor/corrector with the wall test and
 // rebound, periodic wrap.  Included by the FP64 (plain) and the mixed translation units.
 #pragma once
+#include <math_constants.h>
+
 #include "gp_device.cuh"
 
 namespace gp {
@@ -171,7 +173,7 @@ __device__ __forceinline__ void gather6_fp32(const InstDev& I, const Stencil& s,
 // Mixed-precision force and torque: relative velocities and frames in FP64, the
 // Zastawny correlation coefficients in FP32, forces assembled in FP64.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ bool fluid_force_mixed(const PartConst& pc, double visc, double up, double vp,
+static __device__ __noinline__ bool fluid_force_mixed(const PartConst& pc, double visc, double up, double vp,
                                                   double wp, double uf, double vf, double wf, const double r[9],
                                                   double f[3]) {
   double p[3] = {uf - up, vf - vp, wf - wp};
@@ -209,7 +211,7 @@ __device__ __forceinline__ bool fluid_force_mixed(const PartConst& pc, double vi
   return !(cdrag != cdrag) && isfinite(f[0]) && isfinite(f[1]) && isfinite(f[2]);
 }
 
-__device__ __forceinline__ void fluid_torque_mixed(const PartConst& pc, double visc, double upn, double vpn,
+static __device__ __noinline__ void fluid_torque_mixed(const PartConst& pc, double visc, double upn, double vpn,
                                                    double wpn, double uf, double vf, double wf, double wx,
                                                    double wy, double wz, double ox, double oy, double oz,
                                                    const double r[9], double t[3]) {
@@ -255,7 +257,7 @@ __device__ __forceinline__ void fluid_torque_mixed(const PartConst& pc, double v
 template <bool kMixed>
 struct Forces {
   // F (lab frame, per unit mass) and T (body frame) for stage velocities.
-  __device__ __forceinline__ static bool eval(const PartConst& pc, double visc, const double u[3],
+  __device__ __noinline__ static bool eval(const PartConst& pc, double visc, const double u[3],
                                               const double un[3], const double uf[3], const double wv[3],
                                               double ox, double oy, double oz, const Quat& q, double f[3],
                                               double t[3]) {
@@ -397,32 +399,63 @@ __device__ __forceinline__ void load_pc(const PoolView& P, int64_t i, PartConst&
   pc.ipxx = P.pc[7][i]; pc.ipyy = P.pc[8][i]; pc.ipzz = P.pc[9][i];
 }
 
-// ADV_PARTICLE_ELLP over every particle of every instance, in place.
-template <bool kMixed>
-__global__ void __launch_bounds__(128) k_advance(const InstDev* __restrict__ insts, const PoolView* __restrict__ pv,
-                                                 int64_t n, double* const* __restrict__ fluid, Status* st) {
-  const PoolView P = *pv;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const int inst = P.inst[i];
-    if (inst < 0) continue;   // empty slot
-    const InstDev& I = insts[inst];
-    double X[3] = {P.st[0][i], P.st[1][i], P.st[2][i]};
-    double U[3] = {P.st[3][i], P.st[4][i], P.st[5][i]};
-    Quat Q = {P.st[6][i], P.st[7][i], P.st[8][i], P.st[9][i]};
-    double O[3] = {P.st[10][i], P.st[11][i], P.st[12][i]};
-    PartConst pc;
-    load_pc(P, i, pc);
-    Stencil s;
-    double g[6];
-    if (!stencil(I, X[0], X[1], X[2], s)) {
-      set_error(st, GP_EOUT_OF_GRID, (long long)P.id[i]);
-      continue;
+// ADV_PARTICLE_ELLP, first half: particle perm[j] of the source buffer is moved to slot
+// j of the destination buffer (so that the pool follows the search-grid cell order of
+// the last binning and neighbouring stencils are gathered together) and the six field
+// components are interpolated at its position x_n (adv_particle_new.f90:139-206).  Any
+// permutation is correct: every particle carries its properties, id and instance.
+static __global__ void __launch_bounds__(256) k_gather_move(const InstDev* __restrict__ insts,
+                                                               const PoolView* __restrict__ src_pv,
+                                                               const PoolView* __restrict__ dst_pv,
+                                                               const int32_t* __restrict__ perm, int64_t n,
+                                                               double* const* __restrict__ fluid, Status* st) {
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = perm[j];
+    const int inst = src_pv->inst[i];
+    dst_pv->inst[j] = inst;
+    dst_pv->id[j] = src_pv->id[i];
+    // one column pointer pair live at a time keeps the register count low
+#pragma unroll 1
+    for (int c = 0; c < kNState; ++c) dst_pv->st[c][j] = src_pv->st[c][i];
+#pragma unroll 1
+    for (int c = 0; c < kNConst; ++c) dst_pv->pc[c][j] = src_pv->pc[c][i];
+    double g[6] = {CUDART_NAN, CUDART_NAN, CUDART_NAN, CUDART_NAN, CUDART_NAN, CUDART_NAN};
+    if (inst >= 0) {
+      const InstDev& I = insts[inst];
+      Stencil s;
+      if (stencil(I, src_pv->st[0][i], src_pv->st[1][i], src_pv->st[2][i], s)) {
+        if (I.fprec == GP_PREC_MIXED) gather6_fp32(I, s, g); else gather6_fp64(I, s, g);
+      } else {
+        set_error(st, GP_EOUT_OF_GRID, (long long)src_pv->id[i]);
+      }
     }
-    if (I.fprec == GP_PREC_MIXED) gather6_fp32(I, s, g); else gather6_fp64(I, s, g);
-    const double uf[3] = {g[0], g[1], g[2]}, wv[3] = {g[3], g[4], g[5]};
+#pragma unroll
+    for (int c = 0; c < 6; ++c) fluid[c][j] = g[c];
+  }
+}
+
+// ADV_PARTICLE_ELLP, second half, in place on the (now cell-ordered) buffer: the RK2
+// predictor/corrector with wall handling (adv_particle_new.f90:268-637) and
+// BOUNDARY_PARTICLE's periodic wrap (boundary_particle.f90:50-59).
+template <bool kMixed>
+__global__ void __launch_bounds__(128) k_integrate(const InstDev* __restrict__ insts, const PoolView* __restrict__ pv,
+                                                   int64_t n, const double* const* __restrict__ fluid, Status* st) {
+  const PoolView P = *pv;
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
+    const int inst = P.inst[j];
+    if (inst < 0) continue;
+    const InstDev& I = insts[inst];
+    const double uf[3] = {fluid[0][j], fluid[1][j], fluid[2][j]};
+    const double wv[3] = {fluid[3][j], fluid[4][j], fluid[5][j]};
+    if (uf[0] != uf[0] && wv[0] != wv[0]) continue;   // stencil out of range, reported by the gather
+    double X[3] = {P.st[0][j], P.st[1][j], P.st[2][j]};
+    double U[3] = {P.st[3][j], P.st[4][j], P.st[5][j]};
+    Quat Q = {P.st[6][j], P.st[7][j], P.st[8][j], P.st[9][j]};
+    double O[3] = {P.st[10][j], P.st[11][j], P.st[12][j]};
+    PartConst pc;
+    load_pc(P, j, pc);
     const int err = advance_particle<kMixed>(I, pc, uf, wv, X, U, O, Q);
-    if (err) set_error(st, err, (long long)P.id[i]);
-    // BOUNDARY_PARTICLE, boundary_particle.f90:50-59
+    if (err) set_error(st, err, (long long)P.id[j]);
     if (I.periodicity) {
       if (X[0] > I.lx) X[0] = X[0] - I.lx;
       if (X[0] < 0.) X[0] = X[0] + I.lx;
@@ -431,15 +464,18 @@ __global__ void __launch_bounds__(128) k_advance(const InstDev* __restrict__ ins
       if (X[2] > I.lz) X[2] = X[2] - I.lz;
       if (X[2] < 0.) X[2] = X[2] + I.lz;
     }
-    P.st[0][i] = X[0]; P.st[1][i] = X[1]; P.st[2][i] = X[2];
-    P.st[3][i] = U[0]; P.st[4][i] = U[1]; P.st[5][i] = U[2];
-    P.st[6][i] = Q.a; P.st[7][i] = Q.b; P.st[8][i] = Q.c; P.st[9][i] = Q.d;
-    P.st[10][i] = O[0]; P.st[11][i] = O[1]; P.st[12][i] = O[2];
-    if (I.store_fluid && fluid != nullptr) {
-#pragma unroll
-      for (int c = 0; c < 6; ++c) fluid[c][i] = g[c];
-    }
+    P.st[0][j] = X[0]; P.st[1][j] = X[1]; P.st[2][j] = X[2];
+    P.st[3][j] = U[0]; P.st[4][j] = U[1]; P.st[5][j] = U[2];
+    P.st[6][j] = Q.a; P.st[7][j] = Q.b; P.st[8][j] = Q.c; P.st[9][j] = Q.d;
+    P.st[10][j] = O[0]; P.st[11][j] = O[1]; P.st[12][j] = O[2];
   }
+}
+
+// After an advance the destination buffer becomes the current one.
+static __global__ void k_swap_pool(PoolView* a, PoolView* b) {
+  const PoolView t = *a;
+  *a = *b;
+  *b = t;
 }
 
 }  // namespace gp

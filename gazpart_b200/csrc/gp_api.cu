@@ -96,12 +96,14 @@ struct gp_ctx {
   bool grid_ready = false;
   // pool
   int64_t cap = 0, n = 0;
-  double *d_st[kNState] = {};
-  double *d_pc[kNConst] = {};
+  // two buffers: the advance reads one and writes the other in cell order
+  double *d_st[2][kNState] = {};
+  double *d_pc[2][kNConst] = {};
   double *d_fluid[kNFluid] = {};
   double **d_fluid_cols = nullptr;
-  int32_t *d_id = nullptr, *d_instof = nullptr;
-  PoolView *d_pv = nullptr;
+  int32_t *d_id[2] = {}, *d_instof[2] = {};
+  PoolView *d_pv = nullptr;       // current buffer
+  PoolView *d_pv_alt = nullptr;   // the other one
   // search
   SearchArrays sa{};
   int32_t *d_scan_tmp = nullptr;
@@ -110,7 +112,7 @@ struct gp_ctx {
   int64_t cap_pairs = 0;
   CollRec *d_coll = nullptr;
   int64_t cap_coll = 0;
-  unsigned long long *d_counters = nullptr;   // [0] npairs [1] ncoll [2] nacc
+  unsigned long long *d_counters = nullptr;   // [0] npairs [1] ncoll [2] nacc [3] contact queue
   unsigned long long *d_best1 = nullptr, *d_best2 = nullptr;
   int8_t *d_matched = nullptr, *d_state = nullptr;
   int32_t *d_acc = nullptr;
@@ -169,12 +171,16 @@ void free_search(gp_ctx *c) {
 }
 
 void free_pool(gp_ctx *c) {
-  for (auto &p : c->d_st) dfree(p);
-  for (auto &p : c->d_pc) dfree(p);
+  for (int b = 0; b < 2; ++b) {
+    for (auto &p : c->d_st[b]) dfree(p);
+    for (auto &p : c->d_pc[b]) dfree(p);
+    dfree(c->d_id[b]);
+    dfree(c->d_instof[b]);
+  }
   for (auto &p : c->d_fluid) dfree(p);
-  dfree(c->d_id); dfree(c->d_instof);
   dfree(c->sa.cell_of); dfree(c->sa.sorted); dfree(c->sa.sx); dfree(c->sa.sy); dfree(c->sa.sz); dfree(c->sa.sr);
   dfree(c->sa.sbox); dfree(c->sa.sinst); dfree(c->sa.sid);
+  dfree(c->sa.spk); dfree(c->sa.sex); dfree(c->sa.sey); dfree(c->sa.sez); dfree(c->sa.sa2); dfree(c->sa.sb2);
   dfree(c->d_best1); dfree(c->d_best2); dfree(c->d_matched);
   dfree(c->d_pairs); dfree(c->d_coll); dfree(c->d_state); dfree(c->d_acc);
   c->cap = 0;
@@ -182,17 +188,20 @@ void free_pool(gp_ctx *c) {
 
 int alloc_pool(gp_ctx *c, int64_t cap) {
   free_pool(c);
-  for (auto &p : c->d_st) GP_TRY(dalloc(&p, cap));
-  for (auto &p : c->d_pc) GP_TRY(dalloc(&p, cap));
-  if (c->prm.store_fluid)
-    for (auto &p : c->d_fluid) GP_TRY(dalloc(&p, cap));
-  GP_TRY(dalloc(&c->d_id, cap));
-  GP_TRY(dalloc(&c->d_instof, cap));
-  GP_CK(cudaMemsetAsync(c->d_instof, 0xFF, cap * sizeof(int32_t), c->stream));   // -1: empty slot
+  for (int b = 0; b < 2; ++b) {
+    for (auto &p : c->d_st[b]) GP_TRY(dalloc(&p, cap));
+    for (auto &p : c->d_pc[b]) GP_TRY(dalloc(&p, cap));
+    GP_TRY(dalloc(&c->d_id[b], cap));
+    GP_TRY(dalloc(&c->d_instof[b], cap));
+    GP_CK(cudaMemsetAsync(c->d_instof[b], 0xFF, cap * sizeof(int32_t), c->stream));   // -1: empty slot
+  }
+  for (auto &p : c->d_fluid) GP_TRY(dalloc(&p, cap));   // interpolated field at each particle
   SearchArrays &sa = c->sa;
   GP_TRY(dalloc(&sa.cell_of, cap)); GP_TRY(dalloc(&sa.sorted, cap));
   GP_TRY(dalloc(&sa.sx, cap)); GP_TRY(dalloc(&sa.sy, cap)); GP_TRY(dalloc(&sa.sz, cap)); GP_TRY(dalloc(&sa.sr, cap));
   GP_TRY(dalloc(&sa.sbox, cap)); GP_TRY(dalloc(&sa.sinst, cap)); GP_TRY(dalloc(&sa.sid, cap));
+  GP_TRY(dalloc(&sa.spk, cap)); GP_TRY(dalloc(&sa.sex, cap)); GP_TRY(dalloc(&sa.sey, cap)); GP_TRY(dalloc(&sa.sez, cap));
+  GP_TRY(dalloc(&sa.sa2, cap)); GP_TRY(dalloc(&sa.sb2, cap));
   GP_TRY(dalloc(&c->d_best1, cap)); GP_TRY(dalloc(&c->d_best2, cap)); GP_TRY(dalloc(&c->d_matched, cap));
   GP_CK(cudaMemsetAsync(c->d_best1, 0xFF, cap * sizeof(unsigned long long), c->stream));
   GP_CK(cudaMemsetAsync(c->d_best2, 0xFF, cap * sizeof(unsigned long long), c->stream));
@@ -204,12 +213,16 @@ int alloc_pool(gp_ctx *c, int64_t cap) {
   GP_TRY(dalloc(&c->d_state, c->cap_coll));
   GP_TRY(dalloc(&c->d_acc, c->cap_coll));
   c->cap = cap;
-  PoolView pv;
-  for (int k = 0; k < kNState; ++k) pv.st[k] = c->d_st[k];
-  for (int k = 0; k < kNConst; ++k) pv.pc[k] = c->d_pc[k];
-  pv.id = c->d_id;
-  pv.inst = c->d_instof;
-  GP_CK(cudaMemcpyAsync(c->d_pv, &pv, sizeof(PoolView), cudaMemcpyHostToDevice, c->stream));
+  PoolView pv[2];
+  for (int b = 0; b < 2; ++b) {
+    for (int k = 0; k < kNState; ++k) pv[b].st[k] = c->d_st[b][k];
+    for (int k = 0; k < kNConst; ++k) pv[b].pc[k] = c->d_pc[b][k];
+    pv[b].id = c->d_id[b];
+    pv[b].inst = c->d_instof[b];
+  }
+  GP_CK(cudaMemcpyAsync(c->d_pv, &pv[0], sizeof(PoolView), cudaMemcpyHostToDevice, c->stream));
+  GP_CK(cudaMemcpyAsync(c->d_pv_alt, &pv[1], sizeof(PoolView), cudaMemcpyHostToDevice, c->stream));
+  GP_CK(cudaStreamSynchronize(c->stream));
   GP_CK(cudaMemcpyAsync(c->d_fluid_cols, c->d_fluid, sizeof(c->d_fluid), cudaMemcpyHostToDevice, c->stream));
   return GP_OK;
 }
@@ -266,10 +279,10 @@ int setup_grids(gp_ctx *c, double max_emaj, double rmax) {
 
 int enqueue_advance(gp_ctx *c) {
   if (c->prm.precision == GP_PREC_MIXED)
-    launch_advance_mixed(c->d_inst, c->d_pv, c->n, c->prm.store_fluid ? c->d_fluid_cols : nullptr, c->d_status,
+    launch_advance_mixed(c->d_inst, c->d_pv, c->d_pv_alt, c->sa.sorted, c->n, c->d_fluid_cols, c->d_status,
                          c->grid, c->stream);
   else
-    launch_advance_fp64(c->d_inst, c->d_pv, c->n, c->prm.store_fluid ? c->d_fluid_cols : nullptr, c->d_status,
+    launch_advance_fp64(c->d_inst, c->d_pv, c->d_pv_alt, c->sa.sorted, c->n, c->d_fluid_cols, c->d_status,
                         c->grid, c->stream);
   GP_CK(cudaGetLastError());
   return GP_OK;
@@ -285,7 +298,7 @@ int enqueue_collision(gp_ctx *c) {
   launch_bin_scatter(c->d_inst, c->d_pv, c->n, sa, c->d_status, c->grid, c->stream);
   launch_search(c->d_inst, c->n, sa, c->d_pairs, c->d_counters + 0, c->cap_pairs, c->d_status, c->grid, c->stream);
   launch_contact(c->d_inst, c->d_pv, c->d_pairs, c->d_counters + 0, c->cap_pairs, c->d_coll, c->d_counters + 1,
-                 c->cap_coll, c->d_status, c->grid, c->stream);
+                 c->cap_coll, c->d_counters + 3, c->d_status, 148 * 4, c->stream);
   launch_match(c->d_coll, c->d_counters + 1, c->cap_coll, c->d_best1, c->d_best2, c->d_matched, c->d_state,
                c->d_status, c->stream);
   launch_response(c->d_inst, c->d_pv, c->d_coll, c->d_counters + 1, c->cap_coll, c->d_state, c->d_acc,
@@ -342,6 +355,7 @@ int gp_ctx_create(const gp_params *params, gp_ctx **out) {
   I.field = c->field;
   if (!rc) rc = dalloc(&c->d_inst, 1);
   if (!rc) rc = dalloc(&c->d_pv, 1);
+  if (!rc) rc = dalloc(&c->d_pv_alt, 1);
   if (!rc) rc = dalloc(&c->d_fluid_cols, kNFluid);
   if (!rc) rc = dalloc(&c->d_counters, 4);
   if (!rc) rc = dalloc(&c->d_status, 1);
@@ -367,7 +381,8 @@ int gp_ctx_destroy(gp_ctx *c) {
   free_pool(c);
   free_search(c);
   if (c->field) cudaFree(c->field);
-  dfree(c->stage); dfree(c->d_inst); dfree(c->d_pv); dfree(c->d_fluid_cols); dfree(c->d_counters);
+  dfree(c->stage); dfree(c->d_inst); dfree(c->d_pv); dfree(c->d_pv_alt); dfree(c->d_fluid_cols);
+  dfree(c->d_counters);
   dfree(c->d_status); dfree(c->d_scratch);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -454,19 +469,16 @@ int gp_upload_state(gp_ctx *c, int64_t n, const double *const *cols, const doubl
   drop_graph(c);
   const int64_t want = std::max<int64_t>(n, c->prm.max_particles);
   if (c->cap < want) GP_TRY(alloc_pool(c, want));
-  else GP_CK(cudaMemsetAsync(c->d_instof, 0xFF, c->cap * sizeof(int32_t), c->stream));
+  else
+    for (int b = 0; b < 2; ++b) GP_CK(cudaMemsetAsync(c->d_instof[b], 0xFF, c->cap * sizeof(int32_t), c->stream));
   c->n = n;
   double *stage_cols = nullptr, *stage_pc = nullptr;
   GP_TRY(dalloc(&stage_cols, (size_t)kNState * n));
   GP_TRY(dalloc(&stage_pc, (size_t)kNConst * n));
   for (int k = 0; k < kNState; ++k) GP_TRY(copy_in(c, stage_cols + (size_t)k * n, cols[k], n, on_device));
   GP_CK(cudaMemcpyAsync(stage_pc, pcs.data(), pcs.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-  PoolView pv;
-  for (int k = 0; k < kNState; ++k) pv.st[k] = c->d_st[k];
-  for (int k = 0; k < kNConst; ++k) pv.pc[k] = c->d_pc[k];
-  pv.id = c->d_id;
-  pv.inst = c->d_instof;
-  launch_init_pool(pv, 0, n, 0, stage_cols, stage_pc, c->stream);
+  launch_init_pool(c->d_pv, 0, n, 0, stage_cols, stage_pc, c->stream);
+  launch_iota(c->sa.sorted, n, c->stream);   // the first advance keeps the upload order
   GP_CK(cudaGetLastError());
   GP_CK(cudaStreamSynchronize(c->stream));
   cudaFree(stage_cols);

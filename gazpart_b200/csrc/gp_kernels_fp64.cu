@@ -10,11 +10,14 @@
 
 namespace gp {
 
-template __global__ void k_advance<false>(const InstDev *, const PoolView *, int64_t, double *const *, Status *);
+template __global__ void k_integrate<false>(const InstDev *, const PoolView *, int64_t, const double *const *, Status *);
 
-void launch_advance_fp64(const InstDev *insts, const PoolView *pv, int64_t n, double *const *fluid, Status *st,
+void launch_advance_fp64(const InstDev *insts, PoolView *pv, PoolView *pv_alt, const int32_t *perm, int64_t n,
+                         double *const *fluid, Status *st,
                          int grid, cudaStream_t s) {
-  k_advance<false><<<grid, 128, 0, s>>>(insts, pv, n, fluid, st);
+  k_gather_move<<<148 * 8, 256, 0, s>>>(insts, pv, pv_alt, perm, n, fluid, st);
+  k_swap_pool<<<1, 1, 0, s>>>(pv, pv_alt);
+  k_integrate<false><<<grid, 128, 0, s>>>(insts, pv, n, fluid, st);
 }
 
 // INTERP_LAG3 (interp_lag3.f90:11-298) for one component at arbitrary points.
@@ -102,40 +105,81 @@ void launch_frozen_interp(const double *xain, const double *yain, const double *
   k_frozen_interp<<<grid, 256, 0, s>>>(xain, yain, zain, nx, ny, nz, uain, n, x, y, z, out, st);
 }
 
-// collision_interaction.f90:216-348 for each candidate pair: minimum image, contact,
-// contact-point velocities, NVREL.  Colliding pairs (flag && NVREL < ZERO) are appended.
-__global__ void __launch_bounds__(128) k_contact(const InstDev *__restrict__ insts, const PoolView *__restrict__ pv,
-                                                 const PairRec *__restrict__ pairs,
-                                                 const unsigned long long *__restrict__ npairs, int64_t cap_pairs,
-                                                 CollRec *__restrict__ coll, unsigned long long *ncoll,
-                                                 int64_t cap_coll, Status *st) {
+// collision_interaction.f90:216-348 for every candidate pair: minimum image, contact
+// (ellipsoid_contact_detection), contact-point velocities, NVREL.  Colliding pairs
+// (flag && NVREL < ZERO) are appended.  Persistent warps with lane refill: a lane whose
+// Levenberg-Marquardt solve has returned finishes its pair and takes the next one from
+// a global queue, so warps do not idle on their slowest pair.
+__global__ void __launch_bounds__(128, 4) k_contact(const InstDev *__restrict__ insts,
+                                                    const PoolView *__restrict__ pv,
+                                                    const PairRec *__restrict__ pairs,
+                                                    const unsigned long long *__restrict__ npairs, int64_t cap_pairs,
+                                                    CollRec *__restrict__ coll, unsigned long long *ncoll,
+                                                    int64_t cap_coll, unsigned long long *queue, Status *st) {
   const PoolView P = *pv;
   const int64_t np = (int64_t)min(*npairs, (unsigned long long)cap_pairs);
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < np; e += (int64_t)gridDim.x * blockDim.x) {
+  const unsigned lane = threadIdx.x & 31u;
+  constexpr unsigned kFull = 0xffffffffu;
+  bool active = false, exhausted = false;
+  int64_t e = 0;
+  ContactProb CP;
+  LmState S;
+  Quat q1, q2;
+  double a1 = 0, b1 = 0, a2 = 0, b2 = 0;
+  for (;;) {
+    if (!exhausted) {
+      const unsigned want = __ballot_sync(kFull, !active);
+      if (want) {
+        const int leader = __ffs(want) - 1;
+        unsigned long long base = 0;
+        if ((int)lane == leader) base = atomicAdd(queue, (unsigned long long)__popc(want));
+        base = __shfl_sync(kFull, base, leader);
+        if ((int64_t)base >= np) {
+          exhausted = true;
+        } else if (!active) {
+          e = (int64_t)base + __popc(want & ((1u << lane) - 1u));
+          if (e < np) {
+            const PairRec pr = pairs[e];
+            const int i1 = pr.home, i2 = pr.near;
+            const InstDev &I = insts[P.inst[i1]];
+            const double x1 = P.st[0][i1], y1 = P.st[1][i1], z1 = P.st[2][i1];
+            double vkx = P.st[0][i2] - x1, vky = P.st[1][i2] - y1, vkz = P.st[2][i2] - z1;
+            if ((fabs(vkx) > I.lx / 2) && I.periodicity) vkx = vkx - copysign(I.lx, vkx);
+            if (fabs(vky) > I.ly / 2.) vky = vky - copysign(I.ly, vky);
+            if (fabs(vkz) > I.lz / 2.) vkz = vkz - copysign(I.lz, vkz);
+            const double c1[3] = {x1, y1, z1};
+            const double c2[3] = {x1 + vkx, y1 + vky, z1 + vkz};
+            q1 = {P.st[6][i1], P.st[7][i1], P.st[8][i1], P.st[9][i1]};
+            q2 = {P.st[6][i2], P.st[7][i2], P.st[8][i2], P.st[9][i2]};
+            a1 = P.pc[0][i1]; b1 = P.pc[1][i1]; a2 = P.pc[0][i2]; b2 = P.pc[1][i2];
+            if (contact_setup(a1, b1, a2, b2, c1, q1, c2, q2, CP, S.x)) {
+              lm_begin(CP, S);
+              active = true;
+            }
+          }
+        }
+      }
+    }
+    if (!__any_sync(kFull, active)) {
+      if (exhausted) break;
+      continue;
+    }
+    if (!active) continue;
+    if (lm_step(CP, S, kContactTol) == 0) continue;
+    active = false;
+    double ept1[3], ept2[3], cn[3];
+    if (!contact_finish(a1, b1, a2, b2, q1, q2, CP, S.x, ept1, ept2, cn)) continue;
+    atomicAdd(&st->n_contact, 1ull);
     const PairRec pr = pairs[e];
     const int i1 = pr.home, i2 = pr.near;
-    const InstDev &I = insts[P.inst[i1]];
-    const double x1 = P.st[0][i1], y1 = P.st[1][i1], z1 = P.st[2][i1];
-    double vkx = P.st[0][i2] - x1, vky = P.st[1][i2] - y1, vkz = P.st[2][i2] - z1;
-    if ((fabs(vkx) > I.lx / 2) && I.periodicity) vkx = vkx - copysign(I.lx, vkx);
-    if (fabs(vky) > I.ly / 2.) vky = vky - copysign(I.ly, vky);
-    if (fabs(vkz) > I.lz / 2.) vkz = vkz - copysign(I.lz, vkz);
-    const double b1[3] = {x1, y1, z1};
-    const double b2[3] = {x1 + vkx, y1 + vky, z1 + vkz};
-    const Quat q1 = {P.st[6][i1], P.st[7][i1], P.st[8][i1], P.st[9][i1]};
-    const Quat q2 = {P.st[6][i2], P.st[7][i2], P.st[8][i2], P.st[9][i2]};
-    double ept1[3], ept2[3], cn[3];
-    const bool flag = contact_detection(P.pc[0][i1], P.pc[1][i1], P.pc[0][i2], P.pc[1][i2], b1, q1, b2, q2, ept1,
-                                        ept2, cn);
-    if (!flag) continue;
-    atomicAdd(&st->n_contact, 1ull);
+    const double x1 = CP.b1[0], y1 = CP.b1[1], z1 = CP.b1[2];
     double rx1[3] = {(ept1[0] - x1), (ept1[1] - y1), (ept1[2] - z1)};
     double om1[3] = {P.st[10][i1], P.st[11][i1], P.st[12][i1]};
     rot_vec(q1, om1);
     const double up1 = P.st[3][i1] + (om1[1] * rx1[2] - om1[2] * rx1[1]);
     const double vp1 = P.st[4][i1] + (om1[2] * rx1[0] - om1[0] * rx1[2]);
     const double wp1 = P.st[5][i1] + (om1[0] * rx1[1] - om1[1] * rx1[0]);
-    double rx2[3] = {(ept2[0] - (x1 + vkx)), (ept2[1] - (y1 + vky)), (ept2[2] - (z1 + vkz))};
+    double rx2[3] = {(ept2[0] - CP.b2[0]), (ept2[1] - CP.b2[1]), (ept2[2] - CP.b2[2])};
     double om2[3] = {P.st[10][i2], P.st[11][i2], P.st[12][i2]};
     rot_vec(q2, om2);
     const double up2 = P.st[3][i2] + (om2[1] * rx2[2] - om2[2] * rx2[1]);
@@ -158,9 +202,9 @@ __global__ void __launch_bounds__(128) k_contact(const InstDev *__restrict__ ins
 }
 
 void launch_contact(const InstDev *insts, const PoolView *pv, const PairRec *pairs, const unsigned long long *npairs,
-                    int64_t cap_pairs, CollRec *coll, unsigned long long *ncoll, int64_t cap_coll, Status *st,
-                    int grid, cudaStream_t s) {
-  k_contact<<<grid, 128, 0, s>>>(insts, pv, pairs, npairs, cap_pairs, coll, ncoll, cap_coll, st);
+                    int64_t cap_pairs, CollRec *coll, unsigned long long *ncoll, int64_t cap_coll,
+                    unsigned long long *queue, Status *st, int grid, cudaStream_t s) {
+  k_contact<<<grid, 128, 0, s>>>(insts, pv, pairs, npairs, cap_pairs, coll, ncoll, cap_coll, queue, st);
 }
 
 // COLLISION_RESPONSE (collision_response.f90) for the accepted pairs; each particle is
@@ -255,7 +299,7 @@ __global__ void k_euler_batch(int64_t n, const double *ip, double dt, double *om
   }
 }
 
-__global__ void k_contact_batch(int64_t n, const double *shapes, const double *centres, const double *quats,
+__global__ void __launch_bounds__(128, 4) k_contact_batch(int64_t n, const double *shapes, const double *centres, const double *quats,
                                 int32_t *flag, double *e1, double *e2, double *cn) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const double *s = shapes + 4 * i, *c = centres + 6 * i, *q = quats + 8 * i;

@@ -6,11 +6,14 @@
 
 namespace gp {
 
-template __global__ void k_advance<true>(const InstDev *, const PoolView *, int64_t, double *const *, Status *);
+template __global__ void k_integrate<true>(const InstDev *, const PoolView *, int64_t, const double *const *, Status *);
 
-void launch_advance_mixed(const InstDev *insts, const PoolView *pv, int64_t n, double *const *fluid, Status *st,
+void launch_advance_mixed(const InstDev *insts, PoolView *pv, PoolView *pv_alt, const int32_t *perm, int64_t n,
+                         double *const *fluid, Status *st,
                           int grid, cudaStream_t s) {
-  k_advance<true><<<grid, 128, 0, s>>>(insts, pv, n, fluid, st);
+  k_gather_move<<<148 * 8, 256, 0, s>>>(insts, pv, pv_alt, perm, n, fluid, st);
+  k_swap_pool<<<1, 1, 0, s>>>(pv, pv_alt);
+  k_integrate<true><<<grid, 128, 0, s>>>(insts, pv, n, fluid, st);
 }
 
 }  // namespace gp

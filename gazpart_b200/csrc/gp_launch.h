@@ -8,16 +8,18 @@
 namespace gp {
 
 // --- gp_kernels_fp64.cu (FP64 path, -fmad=false) ---
-void launch_advance_fp64(const InstDev *insts, const PoolView *pv, int64_t n, double *const *fluid, Status *st,
-                         int grid, cudaStream_t s);
+// ADV_PARTICLE_ELLP: advances particle perm[j] of *pv into slot j of *pv_alt, then swaps
+// the two views (so *pv is current afterwards).
+void launch_advance_fp64(const InstDev *insts, PoolView *pv, PoolView *pv_alt, const int32_t *perm, int64_t n,
+                         double *const *fluid, Status *st, int grid, cudaStream_t s);
 void launch_interp(const InstDev *inst, int comp, int64_t n, const double *x, const double *y, const double *z,
                    double *out, Status *st, cudaStream_t s);
 void launch_frozen_interp(const double *xain, const double *yain, const double *zain, int nx, int ny, int nz,
                           const double *uain, int64_t n, const double *x, const double *y, const double *z,
                           double *out, Status *st, cudaStream_t s);
 void launch_contact(const InstDev *insts, const PoolView *pv, const PairRec *pairs, const unsigned long long *npairs,
-                    int64_t cap_pairs, CollRec *coll, unsigned long long *ncoll, int64_t cap_coll, Status *st,
-                    int grid, cudaStream_t s);
+                    int64_t cap_pairs, CollRec *coll, unsigned long long *ncoll, int64_t cap_coll,
+                    unsigned long long *queue, Status *st, int grid, cudaStream_t s);
 void launch_response(const InstDev *insts, const PoolView *pv, const CollRec *coll, const unsigned long long *ncoll,
                      int64_t cap_coll, const int8_t *state, int32_t *acc_list, unsigned long long *nacc, Status *st,
                      int grid, cudaStream_t s);
@@ -37,8 +39,9 @@ void launch_response_batch(int64_t n, double ecp, double mup, const double *ip /
                            cudaStream_t s);
 
 // --- gp_kernels_mixed.cu ---
-void launch_advance_mixed(const InstDev *insts, const PoolView *pv, int64_t n, double *const *fluid, Status *st,
-                          int grid, cudaStream_t s);
+void launch_advance_mixed(const InstDev *insts, PoolView *pv, PoolView *pv_alt, const int32_t *perm, int64_t n,
+                          double *const *fluid, Status *st, int grid, cudaStream_t s);
+void launch_iota(int32_t *a, int64_t n, cudaStream_t s);
 
 // --- gp_search.cu ---
 void launch_bin_count(const InstDev *insts, const PoolView *pv, int64_t n, SearchArrays sa, Status *st, int grid,
@@ -58,7 +61,7 @@ void launch_gather_state(const PoolView *pv, int64_t n, int inst, double *out /*
                          cudaStream_t s);
 void launch_scatter_state(const PoolView *pv, int64_t n, int inst, const double *cols /*13*count*/,
                           int64_t count, cudaStream_t s);
-void launch_init_pool(PoolView pv, int64_t begin, int64_t n, int inst, const double *cols /*13*n*/,
+void launch_init_pool(const PoolView *pv, int64_t begin, int64_t n, int inst, const double *cols /*13*n*/,
                       const double *pcs /*10*n*/, cudaStream_t s);
 void launch_connectivity(int nxb, int nyb, int nzb, int periodicity, int32_t *ncon, int32_t *con, cudaStream_t s);
 

@@ -89,7 +89,7 @@ CT_QUAL double ct_poly_cos(double z) {
 
 /* sin and cos of x: Cody-Waite reduction by pi/2 = P1 + P2 + P3 (33 + 33 + 53 bits, so
  * k*P1 and k*P2 are exact for |k| < 2^20), Taylor polynomials on [-pi/4, pi/4]. */
-CT_QUAL void ct_sincos(double x, double *s, double *c) {
+inline __host__ __device__ __noinline__ void ct_sincos(double x, double *s, double *c) {
   if (!(fabs(x) < 1.0e9)) {
     *s = x - x + (0.0 / 0.0 + x * 0.0);
     *c = *s;
@@ -168,7 +168,7 @@ struct ContactProb {
 };
 
 // Support points along +-c(x) (ellipsoid_pair_depth.f90:117-142).
-__device__ __forceinline__ void support_points(const ContactProb& P, const double x[2], double c1[3], double tmp1[3],
+static __device__ __noinline__ void support_points(const ContactProb& P, const double x[2], double c1[3], double tmp1[3],
                                                double tmp2[3], double& l1, double& l2, double pt1[3],
                                                double pt2[3]) {
   double s0, k0, s1, k1;
@@ -191,7 +191,7 @@ __device__ __forceinline__ void support_points(const ContactProb& P, const doubl
 }
 
 // fcn, iflag=1 (ellipsoid_contact_detection.f90:290-295)
-__device__ __forceinline__ void lm_fcn(const ContactProb& P, const double x[2], double fvec[3]) {
+static __device__ __noinline__ void lm_fcn(const ContactProb& P, const double x[2], double fvec[3]) {
   double c1[3], t1[3], t2[3], l1, l2, pt1[3], pt2[3];
   support_points(P, x, c1, t1, t2, l1, l2, pt1, pt2);
 #pragma unroll
@@ -201,7 +201,7 @@ __device__ __forceinline__ void lm_fcn(const ContactProb& P, const double x[2], 
   }
 }
 
-__device__ __forceinline__ void grad_coeff(const double e[9], const double c[3], double l, double co[9]) {
+static __device__ __noinline__ void grad_coeff(const double e[9], const double c[3], double l, double co[9]) {
   double row[3];
 #pragma unroll
   for (int j = 0; j < 3; ++j) row[j] = c[0] * e[3 * j] + c[1] * e[1 + 3 * j] + c[2] * e[2 + 3 * j];
@@ -219,7 +219,7 @@ __device__ __forceinline__ void grad_coeff(const double e[9], const double c[3],
 
 // fcn, iflag=2: analytic Jacobian (ellipsoid_contact_detection.f90:296-332), 3x2
 // column-major.
-__device__ __forceinline__ void lm_jac(const ContactProb& P, const double x[2], double fj[6]) {
+static __device__ __noinline__ void lm_jac(const ContactProb& P, const double x[2], double fj[6]) {
   double c1[3], t1[3], t2[3], l1, l2, pt1[3], pt2[3];
   support_points(P, x, c1, t1, t2, l1, l2, pt1, pt2);
   const double depth[3] = {pt1[0] - pt2[0], pt1[1] - pt2[1], pt1[2] - pt2[2]};
@@ -244,7 +244,7 @@ __device__ __forceinline__ void lm_jac(const ContactProb& P, const double x[2], 
 }
 
 // QR with column pivoting (3x2), Householder vectors left in a.
-__device__ __forceinline__ void lm_qrfac(double a[6], int ipvt[2], double rdiag[2], double acnorm[2]) {
+static __device__ __noinline__ void lm_qrfac(double a[6], int ipvt[2], double rdiag[2], double acnorm[2]) {
   double wa[2];
 #pragma unroll
   for (int j = 0; j < 2; ++j) {
@@ -293,7 +293,7 @@ __device__ __forceinline__ void lm_qrfac(double a[6], int ipvt[2], double rdiag[
   }
 }
 
-__device__ __forceinline__ void lm_qrsolv(double r[6], const int ipvt[2], const double diag[2], const double qtb[2],
+static __device__ __noinline__ void lm_qrsolv(double r[6], const int ipvt[2], const double diag[2], const double qtb[2],
                                           double x[2], double sdiag[2]) {
   double wa[2];
 #pragma unroll
@@ -354,7 +354,7 @@ __device__ __forceinline__ void lm_qrsolv(double r[6], const int ipvt[2], const 
   x[ipvt[1]] = wa[1];
 }
 
-__device__ __forceinline__ void lm_lmpar(double r[6], const int ipvt[2], const double diag[2], const double qtb[2],
+static __device__ __noinline__ void lm_lmpar(double r[6], const int ipvt[2], const double diag[2], const double qtb[2],
                                          double delta, double& par, double x[2], double sdiag[2]) {
   const double dwarf = DBL_MIN;
   double wa1[2], wa2[2];
@@ -429,129 +429,151 @@ __device__ __forceinline__ void lm_lmpar(double r[6], const int ipvt[2], const d
   par = p;
 }
 
-// lmder control flow; returns info (8 mapped to 4 as lmder1 does).
-__device__ __forceinline__ int lm_solve(const ContactProb& P, double x[2], double tol) {
+// lmder (minpack_reduc.f90:243-640) as a resumable state machine: lm_begin evaluates
+// the residual at the starting point; each lm_step runs, when the previous trial was
+// accepted (or at the start), the Jacobian/QR block of lmder's outer loop, then one
+// trial step of its inner loop, and returns 0 to continue or lmder's info code (8
+// mapped to 4 as lmder1 does) when lmder would return.  The sequence of operations per
+// pair is lmder's; the split lets a warp refill a lane with a new pair as soon as its
+// pair converges.
+struct LmState {
+  double x[2], fvec[3], fjac[6], diag[2], qtf[2];
+  double fnorm, xnorm, delta, par, temp, gnorm;
+  int ipvt[2];
+  int nfev, iter;
+  bool need_jac;
+};
+
+static __device__ __noinline__ void lm_begin(const ContactProb& P, LmState& S) {
+  lm_fcn(P, S.x, S.fvec);
+  S.nfev = 1;
+  S.fnorm = lm_enorm<3>(S.fvec);
+  S.par = 0.0;
+  S.iter = 1;
+  S.xnorm = 0.0;
+  S.delta = 0.0;
+  S.temp = 0.0;
+  S.gnorm = 0.0;
+  S.diag[0] = S.diag[1] = 0.0;
+  S.ipvt[0] = 0;
+  S.ipvt[1] = 1;
+  S.need_jac = true;
+}
+
+static __device__ __noinline__ int lm_step(const ContactProb& P, LmState& S, double tol) {
   constexpr int maxfev = 300;
   const double ftol = tol, xtol = tol;
-  double fvec[3], fjac[6], diag[2] = {0.0, 0.0}, qtf[2], wa1[2], wa2[2], wa3[2], wa4[3];
-  int ipvt[2];
-  int info = 0;
-  double xnorm = 0.0, delta = 0.0, temp = 0.0;
-  lm_fcn(P, x, fvec);
-  int nfev = 1;
-  double fnorm = lm_enorm<3>(fvec);
-  double par = 0.0;
-  int iter = 1;
-  while (true) {
-    lm_jac(P, x, fjac);
-    lm_qrfac(fjac, ipvt, wa1, wa2);
-    if (iter == 1) {
+  double wa1[2], wa2[2], wa3[2], wa4[3];
+  if (S.need_jac) {
+    lm_jac(P, S.x, S.fjac);
+    lm_qrfac(S.fjac, S.ipvt, wa1, wa2);
+    if (S.iter == 1) {
 #pragma unroll
-      for (int j = 0; j < 2; ++j) { diag[j] = wa2[j]; if (wa2[j] == 0.0) diag[j] = 1.0; }
-      wa3[0] = diag[0] * x[0];
-      wa3[1] = diag[1] * x[1];
-      xnorm = lm_enorm<2>(wa3);
-      delta = 100.0 * xnorm;
-      if (delta == 0.0) delta = 100.0;
+      for (int j = 0; j < 2; ++j) { S.diag[j] = wa2[j]; if (wa2[j] == 0.0) S.diag[j] = 1.0; }
+      wa3[0] = S.diag[0] * S.x[0];
+      wa3[1] = S.diag[1] * S.x[1];
+      S.xnorm = lm_enorm<2>(wa3);
+      S.delta = 100.0 * S.xnorm;
+      if (S.delta == 0.0) S.delta = 100.0;
     }
 #pragma unroll
-    for (int i = 0; i < 3; ++i) wa4[i] = fvec[i];
+    for (int i = 0; i < 3; ++i) wa4[i] = S.fvec[i];
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
-      if (fjac[j + 3 * j] != 0.0) {
+      if (S.fjac[j + 3 * j] != 0.0) {
         double sum = 0.0;
 #pragma unroll
-        for (int i = j; i < 3; ++i) sum = sum + fjac[i + 3 * j] * wa4[i];
-        const double t = -sum / fjac[j + 3 * j];
+        for (int i = j; i < 3; ++i) sum = sum + S.fjac[i + 3 * j] * wa4[i];
+        const double t = -sum / S.fjac[j + 3 * j];
 #pragma unroll
-        for (int i = j; i < 3; ++i) wa4[i] = wa4[i] + fjac[i + 3 * j] * t;
+        for (int i = j; i < 3; ++i) wa4[i] = wa4[i] + S.fjac[i + 3 * j] * t;
       }
-      fjac[j + 3 * j] = wa1[j];
-      qtf[j] = wa4[j];
+      S.fjac[j + 3 * j] = wa1[j];
+      S.qtf[j] = wa4[j];
     }
     double gnorm = 0.0;
-    if (fnorm != 0.0) {
+    if (S.fnorm != 0.0) {
 #pragma unroll
       for (int j = 0; j < 2; ++j) {
-        const int l = ipvt[j];
-        if (wa2[l] != 0.0) {
+        const double acn = (S.ipvt[j] == 0) ? wa2[0] : wa2[1];
+        if (acn != 0.0) {
           double sum = 0.0;
 #pragma unroll
-          for (int i = 0; i <= j; ++i) sum = sum + fjac[i + 3 * j] * (qtf[i] / fnorm);
-          const double g = fabs(sum / wa2[l]);
+          for (int i = 0; i <= j; ++i) sum = sum + S.fjac[i + 3 * j] * (S.qtf[i] / S.fnorm);
+          const double g = fabs(sum / acn);
           gnorm = (gnorm > g) ? gnorm : g;
         }
       }
     }
-    if (gnorm <= 0.0) info = 4;
-    if (info != 0) break;
-    diag[0] = (diag[0] > wa2[0]) ? diag[0] : wa2[0];
-    diag[1] = (diag[1] > wa2[1]) ? diag[1] : wa2[1];
-    while (true) {
-      lm_lmpar(fjac, ipvt, diag, qtf, delta, par, wa1, wa2);
-#pragma unroll
-      for (int j = 0; j < 2; ++j) {
-        wa1[j] = -wa1[j];
-        wa2[j] = x[j] + wa1[j];
-        wa3[j] = diag[j] * wa1[j];
-      }
-      const double pnorm = lm_enorm<2>(wa3);
-      if (iter == 1) delta = (delta < pnorm) ? delta : pnorm;
-      lm_fcn(P, wa2, wa4);
-      ++nfev;
-      const double fnorm1 = lm_enorm<3>(wa4);
-      double actred = -1.0;
-      if (0.1 * fnorm1 < fnorm) { const double r = fnorm1 / fnorm; actred = 1.0 - r * r; }
-      wa3[0] = 0.0 + fjac[0] * wa1[ipvt[0]];
-      wa3[1] = 0.0;
-      {
-        const double t = wa1[ipvt[1]];
-        wa3[0] = wa3[0] + fjac[3] * t;
-        wa3[1] = wa3[1] + fjac[4] * t;
-      }
-      const double temp1 = lm_enorm<2>(wa3) / fnorm;
-      const double temp2 = (sqrt(par) * pnorm) / fnorm;
-      const double prered = temp1 * temp1 + (temp2 * temp2) / 0.5;
-      const double dirder = -(temp1 * temp1 + temp2 * temp2);
-      double ratio = 0.0;
-      if (prered != 0.0) ratio = actred / prered;
-      if (ratio <= 0.25) {
-        if (actred >= 0.0) temp = 0.5;
-        if (actred < 0.0) temp = 0.5 * dirder / (dirder + 0.5 * actred);
-        if (0.1 * fnorm1 >= fnorm || temp < 0.1) temp = 0.1;
-        const double m = (delta < pnorm / 0.1) ? delta : pnorm / 0.1;
-        delta = temp * m;
-        par = par / temp;
-      } else if (par == 0.0 || ratio >= 0.75) {
-        delta = pnorm / 0.5;
-        par = 0.5 * par;
-      }
-      if (ratio >= 1.0e-4) {
-#pragma unroll
-        for (int j = 0; j < 2; ++j) { x[j] = wa2[j]; wa2[j] = diag[j] * x[j]; }
-#pragma unroll
-        for (int i = 0; i < 3; ++i) fvec[i] = wa4[i];
-        xnorm = lm_enorm<2>(wa2);
-        fnorm = fnorm1;
-        ++iter;
-      }
-      if (fabs(actred) <= ftol && prered <= ftol && 0.5 * ratio <= 1.0) info = 1;
-      if (delta <= xtol * xnorm) info = 2;
-      if (fabs(actred) <= ftol && prered <= ftol && 0.5 * ratio <= 1.0 && info == 2) info = 3;
-      if (info != 0) return info;
-      if (nfev >= maxfev) info = 5;
-      if (fabs(actred) <= DBL_EPSILON && prered <= DBL_EPSILON && 0.5 * ratio <= 1.0) info = 6;
-      if (delta <= DBL_EPSILON * xnorm) info = 7;
-      if (gnorm <= DBL_EPSILON) info = 8;
-      if (info != 0) return info == 8 ? 4 : info;
-      if (ratio >= 1.0e-4) break;
-    }
+    S.gnorm = gnorm;
+    if (gnorm <= 0.0) return 4;
+    S.diag[0] = (S.diag[0] > wa2[0]) ? S.diag[0] : wa2[0];
+    S.diag[1] = (S.diag[1] > wa2[1]) ? S.diag[1] : wa2[1];
+    S.need_jac = false;
   }
-  return info;
+  // one trial step (the body of lmder's inner loop)
+  lm_lmpar(S.fjac, S.ipvt, S.diag, S.qtf, S.delta, S.par, wa1, wa2);
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    wa1[j] = -wa1[j];
+    wa2[j] = S.x[j] + wa1[j];
+    wa3[j] = S.diag[j] * wa1[j];
+  }
+  const double pnorm = lm_enorm<2>(wa3);
+  if (S.iter == 1) S.delta = (S.delta < pnorm) ? S.delta : pnorm;
+  lm_fcn(P, wa2, wa4);
+  ++S.nfev;
+  const double fnorm1 = lm_enorm<3>(wa4);
+  double actred = -1.0;
+  if (0.1 * fnorm1 < S.fnorm) { const double r = fnorm1 / S.fnorm; actred = 1.0 - r * r; }
+  const double p0 = (S.ipvt[0] == 0) ? wa1[0] : wa1[1];
+  const double p1 = (S.ipvt[1] == 0) ? wa1[0] : wa1[1];
+  wa3[0] = 0.0 + S.fjac[0] * p0;
+  wa3[1] = 0.0;
+  wa3[0] = wa3[0] + S.fjac[3] * p1;
+  wa3[1] = wa3[1] + S.fjac[4] * p1;
+  const double temp1 = lm_enorm<2>(wa3) / S.fnorm;
+  const double temp2 = (sqrt(S.par) * pnorm) / S.fnorm;
+  const double prered = temp1 * temp1 + (temp2 * temp2) / 0.5;
+  const double dirder = -(temp1 * temp1 + temp2 * temp2);
+  double ratio = 0.0;
+  if (prered != 0.0) ratio = actred / prered;
+  if (ratio <= 0.25) {
+    if (actred >= 0.0) S.temp = 0.5;
+    if (actred < 0.0) S.temp = 0.5 * dirder / (dirder + 0.5 * actred);
+    if (0.1 * fnorm1 >= S.fnorm || S.temp < 0.1) S.temp = 0.1;
+    const double m = (S.delta < pnorm / 0.1) ? S.delta : pnorm / 0.1;
+    S.delta = S.temp * m;
+    S.par = S.par / S.temp;
+  } else if (S.par == 0.0 || ratio >= 0.75) {
+    S.delta = pnorm / 0.5;
+    S.par = 0.5 * S.par;
+  }
+  if (ratio >= 1.0e-4) {
+#pragma unroll
+    for (int j = 0; j < 2; ++j) { S.x[j] = wa2[j]; wa2[j] = S.diag[j] * S.x[j]; }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) S.fvec[i] = wa4[i];
+    S.xnorm = lm_enorm<2>(wa2);
+    S.fnorm = fnorm1;
+    ++S.iter;
+  }
+  int info = 0;
+  if (fabs(actred) <= ftol && prered <= ftol && 0.5 * ratio <= 1.0) info = 1;
+  if (S.delta <= xtol * S.xnorm) info = 2;
+  if (fabs(actred) <= ftol && prered <= ftol && 0.5 * ratio <= 1.0 && info == 2) info = 3;
+  if (info != 0) return info;
+  if (S.nfev >= maxfev) info = 5;
+  if (fabs(actred) <= DBL_EPSILON && prered <= DBL_EPSILON && 0.5 * ratio <= 1.0) info = 6;
+  if (S.delta <= DBL_EPSILON * S.xnorm) info = 7;
+  if (S.gnorm <= DBL_EPSILON) info = 8;
+  if (info != 0) return info == 8 ? 4 : info;
+  if (ratio >= 1.0e-4) S.need_jac = true;
+  return 0;
 }
 
 // Margin function mod_particle_parallel.f90:145-201: v^T (R diag(1/a^2,1/b^2,1/b^2) R^T) v
-__device__ __forceinline__ double fmargin(double a, double b, const double pt[3], const double c[3], const Quat& q) {
+static __device__ __noinline__ double fmargin(double a, double b, const double pt[3], const double c[3], const Quat& q) {
   double ell[9];
   rot_diag(q, 1.0 / (a * a), 1.0 / (b * b), 1.0 / (b * b), ell);
   const double v[3] = {pt[0] - c[0], pt[1] - c[1], pt[2] - c[2]};
@@ -560,37 +582,55 @@ __device__ __forceinline__ double fmargin(double a, double b, const double pt[3]
   return v[0] * e_[0] + v[1] * e_[1] + v[2] * e_[2];
 }
 
-// ellipsoid_contact_detection.f90:1-187.  A NaN starting angle (acos of a ratio just
-// above 1, :86-87) keeps every iterate NaN, so the reference reports no contact; that
-// result is returned without iterating.
-__device__ __forceinline__ bool contact_detection(double a1, double bb1, double a2, double bb2, const double c1[3],
-                                                  const Quat& q1, const double c2[3], const Quat& q2, double ept1[3],
-                                                  double ept2[3], double cn[3]) {
-  const double tol = 1.4901161193847656e-08;   // sqrt(epsilon(1.0_8))
+// Set-up of ellipsoid_contact_detection.f90:72-95: the two rotated ellipsoid matrices
+// and the starting angles from the centre line (:77-87).  Returns false when a starting
+// angle is NaN (acos of a ratio just above 1): every iterate would stay NaN and the
+// reference reports no contact, so the caller skips the solve.
+static __device__ __noinline__ bool contact_setup(double a1, double bb1, double a2, double bb2, const double c1[3],
+                                                  const Quat& q1, const double c2[3], const Quat& q2, ContactProb& P,
+                                                  double x[2]) {
   double nrm[3] = {c1[0] - c2[0], c1[1] - c2[1], c1[2] - c2[2]};
   const double c_norm = sqrt(nrm[0] * nrm[0] + nrm[1] * nrm[1] + nrm[2] * nrm[2]);
   if (c_norm != 0.0) { nrm[0] = nrm[0] / c_norm; nrm[1] = nrm[1] / c_norm; nrm[2] = nrm[2] / c_norm; }
-  double x[2];
   x[1] = ct_asin(nrm[2]);
   x[0] = ct_acos(nrm[0] / ct_cos(x[1]));
-  if (x[0] != x[0] || x[1] != x[1]) {
-#pragma unroll
-    for (int i = 0; i < 3; ++i) { ept1[i] = CUDART_NAN; ept2[i] = CUDART_NAN; cn[i] = CUDART_NAN; }
-    return false;
-  }
-  ContactProb P;
   rot_diag(q1, a1 * a1, bb1 * bb1, bb1 * bb1, P.e1);
   rot_diag(q2, a2 * a2, bb2 * bb2, bb2 * bb2, P.e2);
 #pragma unroll
   for (int i = 0; i < 3; ++i) { P.b1[i] = c1[i]; P.b2[i] = c2[i]; }
-  lm_solve(P, x, tol);
+  return !(x[0] != x[0] || x[1] != x[1]);
+}
+
+// pair_depth at the solution and the contact test (ellipsoid_contact_detection.f90:104-179)
+static __device__ __noinline__ bool contact_finish(double a1, double bb1, double a2, double bb2, const Quat& q1,
+                                                   const Quat& q2, const ContactProb& P, const double x[2],
+                                                   double ept1[3], double ept2[3], double cn[3]) {
   double cc[3], t1[3], t2[3], l1, l2, pt1[3], pt2[3];
   support_points(P, x, cc, t1, t2, l1, l2, pt1, pt2);
   const double d[3] = {pt1[0] - pt2[0], pt1[1] - pt2[1], pt1[2] - pt2[2]};
   const double contact = d[0] * cc[0] + d[1] * cc[1] + d[2] * cc[2];
 #pragma unroll
   for (int i = 0; i < 3; ++i) { ept1[i] = pt1[i]; ept2[i] = pt2[i]; cn[i] = cc[i]; }
-  return (contact > 0) && (fmargin(a1, bb1, pt2, c1, q1) < 1.0) && (fmargin(a2, bb2, pt1, c2, q2) < 1.0);
+  return (contact > 0) && (fmargin(a1, bb1, pt2, P.b1, q1) < 1.0) && (fmargin(a2, bb2, pt1, P.b2, q2) < 1.0);
+}
+
+constexpr double kContactTol = 1.4901161193847656e-08;   // sqrt(epsilon(1.0_8))
+
+// ellipsoid_contact_detection.f90:1-187 for one pair, start to finish.
+static __device__ __noinline__ bool contact_detection(double a1, double bb1, double a2, double bb2,
+                                                      const double c1[3], const Quat& q1, const double c2[3],
+                                                      const Quat& q2, double ept1[3], double ept2[3], double cn[3]) {
+  ContactProb P;
+  LmState S;
+  if (!contact_setup(a1, bb1, a2, bb2, c1, q1, c2, q2, P, S.x)) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i) { ept1[i] = CUDART_NAN; ept2[i] = CUDART_NAN; cn[i] = CUDART_NAN; }
+    return false;
+  }
+  lm_begin(P, S);
+  while (lm_step(P, S, kContactTol) == 0) {
+  }
+  return contact_finish(a1, bb1, a2, bb2, q1, q2, P, S.x, ept1, ept2, cn);
 }
 
 }  // namespace gp

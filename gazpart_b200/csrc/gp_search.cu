@@ -66,16 +66,26 @@ __device__ __forceinline__ int cell_coord(double v, double h, int n) {
 __global__ void k_bin_count(const InstDev *__restrict__ insts, const PoolView *__restrict__ pv, int64_t n,
                             SearchArrays sa) {
   const PoolView P = *pv;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const int inst = P.inst[i];
-    if (inst < 0) { sa.cell_of[i] = -1; continue; }
-    const InstDev &I = insts[inst];
-    const int cx = cell_coord(P.st[0][i], I.hfx, I.nfx);
-    const int cy = cell_coord(P.st[1][i], I.hfy, I.nfy);
-    const int cz = cell_coord(P.st[2][i], I.hfz, I.nfz);
-    const int64_t c = I.cell_begin + ((int64_t)cz * I.nfy + cy) * I.nfx + cx;
-    sa.cell_of[i] = (int32_t)c;
-    atomicAdd(&sa.cell_count[c], 1);
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t nround = (n + stride - 1) / stride * stride;   // whole warps stay in the loop
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nround; i += stride) {
+    int32_t c = -1;
+    if (i < n) {
+      const int inst = P.inst[i];
+      if (inst >= 0) {
+        const InstDev &I = insts[inst];
+        const int cx = cell_coord(P.st[0][i], I.hfx, I.nfx);
+        const int cy = cell_coord(P.st[1][i], I.hfy, I.nfy);
+        const int cz = cell_coord(P.st[2][i], I.hfz, I.nfz);
+        c = (int32_t)(I.cell_begin + ((int64_t)cz * I.nfy + cy) * I.nfx + cx);
+      }
+      sa.cell_of[i] = c;
+    }
+    // particles are kept in cell order, so neighbouring lanes usually share a cell:
+    // one atomic per cell per warp
+    const unsigned peers = __match_any_sync(0xffffffffu, c);
+    const int leader = __ffs(peers) - 1;
+    if (c >= 0 && (int)(threadIdx.x & 31) == leader) atomicAdd(&sa.cell_count[c], __popc(peers));
   }
 }
 
@@ -172,10 +182,18 @@ void launch_scan(const int32_t *in, int32_t *out, int64_t n, int32_t *tmp, cudaS
 __global__ void k_bin_scatter(const InstDev *__restrict__ insts, const PoolView *__restrict__ pv, int64_t n,
                               SearchArrays sa, Status *st) {
   const PoolView P = *pv;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const int32_t c = sa.cell_of[i];
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t nround = (n + stride - 1) / stride * stride;
+  const int lane = threadIdx.x & 31;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nround; i += stride) {
+    const int32_t c = (i < n) ? sa.cell_of[i] : -1;
+    const unsigned peers = __match_any_sync(0xffffffffu, c);
+    const int leader = __ffs(peers) - 1;
+    int base = 0;
+    if (c >= 0 && lane == leader) base = atomicAdd(&sa.cell_fill[c], __popc(peers));
+    base = __shfl_sync(0xffffffffu, base, leader);
     if (c < 0) continue;
-    const int pos = sa.cell_start[c] + atomicAdd(&sa.cell_fill[c], 1);
+    const int pos = sa.cell_start[c] + base + __popc(peers & ((1u << lane) - 1u));
     const int inst = P.inst[i];
     const InstDev &I = insts[inst];
     const double x = P.st[0][i], y = P.st[1][i], z = P.st[2][i];
@@ -183,7 +201,17 @@ __global__ void k_bin_scatter(const InstDev *__restrict__ insts, const PoolView 
     sa.sx[pos] = x;
     sa.sy[pos] = y;
     sa.sz[pos] = z;
-    sa.sr[pos] = fmax(P.pc[0][i], P.pc[1][i]);
+    const double ea = P.pc[0][i], eb = P.pc[1][i];
+    sa.sr[pos] = fmax(ea, eb);
+    sa.spk[pos] = make_float4((float)x, (float)y, (float)z, (float)fmax(ea, eb));
+    sa.sa2[pos] = ea * ea;
+    sa.sb2[pos] = eb * eb;
+    {
+      const double q0 = P.st[6][i], q1 = P.st[7][i], q2 = P.st[8][i], q3 = P.st[9][i];
+      sa.sex[pos] = 1.0 - 2.0 * (q2 * q2 + q3 * q3);
+      sa.sey[pos] = 2.0 * (q1 * q2 + q0 * q3);
+      sa.sez[pos] = 2.0 * (q1 * q3 - q0 * q2);
+    }
     sa.sinst[pos] = inst;
     sa.sid[pos] = P.id[i];
     const double fx = (x - I.xminbox) / I.dxbox, fy = (y - I.yminbox) / I.dybox, fz = (z - I.zminbox) / I.dzbox;
@@ -240,6 +268,8 @@ __global__ void __launch_bounds__(256) k_search(const InstDev *__restrict__ inst
     const int64_t lc = sa.cell_of[pslot] - I.cell_begin;
     const int cx = (int)(lc % I.nfx), cy = (int)((lc / I.nfx) % I.nfy), cz = (int)(lc / ((int64_t)I.nfx * I.nfy));
     const bool perx = I.periodicity != 0;
+    const float xpf = (float)xp, ypf = (float)yp, zpf = (float)zp, rpf = (float)rp;
+    const float lxf = (float)I.lx, lyf = (float)I.ly, lzf = (float)I.lz;
     for (int o = -1; o < 13; ++o) {
       int nx = cx, ny = cy, nz = cz;
       if (o >= 0) {
@@ -258,12 +288,36 @@ __global__ void __launch_bounds__(256) k_search(const InstDev *__restrict__ inst
       const int32_t q1 = sa.cell_start[nc + 1];
       if (o < 0) q0 = (int32_t)s + 1;
       for (int32_t qs = q0; qs < q1; ++qs) {
+        // conservative float test: |float - double| distance error < 2e-6, slack 1e-5
+        {
+          const float4 c = sa.spk[qs];
+          float fx = c.x - xpf, fy = c.y - ypf, fz = c.z - zpf;
+          if (perx && fabsf(fx) > 0.5f * lxf) fx = fx - copysignf(lxf, fx);
+          if (fabsf(fy) > 0.5f * lyf) fy = fy - copysignf(lyf, fy);
+          if (fabsf(fz) > 0.5f * lzf) fz = fz - copysignf(lzf, fz);
+          const float rf = rpf + c.w + 1.0e-5f;
+          if (fx * fx + fy * fy + fz * fz > rf * rf) continue;
+        }
         double dx = sa.sx[qs] - xp, dy = sa.sy[qs] - yp, dz = sa.sz[qs] - zp;
         if (perx && fabs(dx) > I.lx / 2) dx = dx - copysign(I.lx, dx);
         if (fabs(dy) > I.ly / 2.) dy = dy - copysign(I.ly, dy);
         if (fabs(dz) > I.lz / 2.) dz = dz - copysign(I.lz, dz);
         const double rr = (rp + sa.sr[qs]) * (1.0 + 1e-9);
-        if (dx * dx + dy * dy + dz * dz > rr * rr) continue;
+        const double d2 = dx * dx + dy * dy + dz * dz;
+        if (d2 > rr * rr) continue;
+        // Support-function test along the centre line: for unit d, the extent of a
+        // spheroid is h(d) = sqrt(b^2 + (a^2-b^2)(e.d)^2).  If h_p + h_q < |d| the two
+        // bodies are disjoint, so no contact point can lie inside the other body
+        // (ellipsoid_contact_detection.f90:125) and the reference cannot flag the pair.
+        if (d2 > 0.0) {
+          const double dist = sqrt(d2), inv = 1.0 / dist;
+          const double ux = dx * inv, uy = dy * inv, uz = dz * inv;
+          const double cp = sa.sex[s] * ux + sa.sey[s] * uy + sa.sez[s] * uz;
+          const double cq = sa.sex[qs] * ux + sa.sey[qs] * uy + sa.sez[qs] * uz;
+          const double hp = sqrt(fmax(sa.sb2[s] + (sa.sa2[s] - sa.sb2[s]) * cp * cp, 0.0));
+          const double hq = sqrt(fmax(sa.sb2[qs] + (sa.sa2[qs] - sa.sb2[qs]) * cq * cq, 0.0));
+          if (hp + hq < dist * (1.0 - 1e-9)) continue;
+        }
         atomicAdd(&st->n_near, 1ull);
         // reference adjacency of the two boxes (collision_box_connectivity.f90)
         const long long bq = sa.sbox[qs];
@@ -487,8 +541,9 @@ void launch_scatter_state(const PoolView *pv, int64_t n, int inst, const double 
   k_scatter_state<<<148 * 8, 256, 0, s>>>(pv, n, inst, cols, count);
 }
 
-__global__ void k_init_pool(PoolView P, int64_t begin, int64_t n, int inst, const double *__restrict__ cols,
-                            const double *__restrict__ pcs) {
+__global__ void k_init_pool(const PoolView *__restrict__ pv, int64_t begin, int64_t n, int inst,
+                            const double *__restrict__ cols, const double *__restrict__ pcs) {
+  const PoolView P = *pv;
   for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
     const int64_t i = begin + k;
 #pragma unroll
@@ -500,10 +555,19 @@ __global__ void k_init_pool(PoolView P, int64_t begin, int64_t n, int inst, cons
   }
 }
 
-void launch_init_pool(PoolView pv, int64_t begin, int64_t n, int inst, const double *cols, const double *pcs,
+void launch_init_pool(const PoolView *pv, int64_t begin, int64_t n, int inst, const double *cols, const double *pcs,
                       cudaStream_t s) {
   if (n <= 0) return;
   k_init_pool<<<148 * 8, 256, 0, s>>>(pv, begin, n, inst, cols, pcs);
+}
+
+__global__ void k_iota(int32_t *a, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    a[i] = (int32_t)i;
+}
+
+void launch_iota(int32_t *a, int64_t n, cudaStream_t s) {
+  if (n > 0) k_iota<<<148 * 8, 256, 0, s>>>(a, n);
 }
 
 // COLLISION_BOX_CONNECTIVITY (collision_box_connectivity.f90:42-322), NPROC=1.

@@ -80,6 +80,9 @@ struct SearchArrays {
   int32_t *cell_of;      // per pool slot
   int32_t *sorted;       // pool slot of each sorted position
   double *sx, *sy, *sz, *sr;
+  float4 *spk;           // (x, y, z, r) in float for the conservative first test
+  double *sex, *sey, *sez;   // symmetry axis in the lab frame (first column of R(q))
+  double *sa2, *sb2;         // squared semi-axes along / across the axis
   long long *sbox;       // packed box coords (I0-1) | (J0-1)<<21 | (K0-1)<<42, -1 if outside
   int32_t *sinst;
   int32_t *sid;          // index of the particle within its instance
