@@ -92,6 +92,8 @@ SIGNATURES = {
                                        _dp, _dp, _dp],
     "gp_ellipsoid_contact_detection_batch": [_ctx, C.c_int64, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                                              C.c_int32],
+    "gp_ellipsoid_contact_detection_batch_noalloc": [C.c_int64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, C.c_int32,
+                                                     _vp],
     "gp_collision_response": [_ctx, C.c_int32, C.c_int32, _dp, _dp, _dp, _dp, _dp],
 }
 

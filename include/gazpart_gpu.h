@@ -215,6 +215,25 @@ int gp_ellipsoid_contact_detection_batch(gp_ctx *ctx, int64_t n, const double *s
                                          const double *centres, const double *quats,
                                          int32_t *flag, double *ept1, double *ept2,
                                          double *cnormal, int32_t on_device);
+/* No counterpart in the reference.  The batched contact detection above for callers
+ * that cannot allocate device memory (a loop running under another library's stream
+ * capture, a pool that has filled HBM, a real-time loop that cannot take the device
+ * synchronisation of cudaFree).  Same arguments and results as
+ * gp_ellipsoid_contact_detection_batch, without a context; `stream` is a cudaStream_t
+ * (NULL: the default stream) on the current device.  It calls no allocator: inputs and
+ * results pass through one static device array of GP_NOALLOC_MAX_PAIRS pairs
+ * (220 bytes per pair), and n above that returns GP_EBADARG without doing any work.
+ * The array is shared by all calls on a device and keeps the last call's contents;
+ * calls that can overlap on the GPU race on it and must be ordered by the caller.
+ * The first call on each device looks up the array with that device current and may
+ * load this library's device code: make it before any stream capture starts.
+ * Synchronises `stream` before returning. */
+#define GP_NOALLOC_MAX_PAIRS 32768
+int gp_ellipsoid_contact_detection_batch_noalloc(int64_t n, const double *shapes,
+                                                 const double *centres, const double *quats,
+                                                 int32_t *flag, double *ept1, double *ept2,
+                                                 double *cnormal, int32_t on_device,
+                                                 void *stream);
 /* COLLISION_RESPONSE(IG,IDP,part1,part2,R_impact1,R_impact2,normal)
  * collision_response.f90:1-437.  partK: 10 doubles in/out (UP VP WP, OMEGAX..Z,
  * ELLQUAT a..d); inertia of class (IG,IDP) for both bodies as in the reference. */
