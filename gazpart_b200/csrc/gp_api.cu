@@ -124,6 +124,7 @@ struct gp_ctx {
   // graph
   cudaGraphExec_t graph = nullptr;
   int grid = 148 * 4;
+  int contact_grid = 148 * 4;   // persistent k_contact grid (resident blocks)
 };
 
 namespace {
@@ -298,7 +299,7 @@ int enqueue_collision(gp_ctx *c) {
   launch_bin_scatter(c->d_inst, c->d_pv, c->n, sa, c->d_status, c->grid, c->stream);
   launch_search(c->d_inst, c->n, sa, c->d_pairs, c->d_counters + 0, c->cap_pairs, c->d_status, c->grid, c->stream);
   launch_contact(c->d_inst, c->d_pv, c->d_pairs, c->d_counters + 0, c->cap_pairs, c->d_coll, c->d_counters + 1,
-                 c->cap_coll, c->d_counters + 3, c->d_status, 148 * 4, c->stream);
+                 c->cap_coll, c->d_counters + 3, c->d_status, c->contact_grid, c->stream);
   launch_match(c->d_coll, c->d_counters + 1, c->cap_coll, c->d_best1, c->d_best2, c->d_matched, c->d_state,
                c->d_status, c->stream);
   launch_response(c->d_inst, c->d_pv, c->d_coll, c->d_counters + 1, c->cap_coll, c->d_state, c->d_acc,
@@ -362,6 +363,10 @@ int gp_ctx_create(const gp_params *params, gp_ctx **out) {
   if (!rc && cudaMemset(c->d_status, 0, sizeof(Status)) != cudaSuccess) rc = GP_ECUDA;
   if (!rc) rc = upload_inst(c);
   if (!rc && cudaStreamSynchronize(c->stream) != cudaSuccess) rc = GP_ECUDA;
+  if (!rc) {
+    const int cg = contact_grid_blocks();
+    if (cg > 0) c->contact_grid = cg;
+  }
   if (rc) {
     gp_ctx_destroy(c);
     return rc;

@@ -110,7 +110,13 @@ void launch_frozen_interp(const double *xain, const double *yain, const double *
 // (flag && NVREL < ZERO) are appended.  Persistent warps with lane refill: a lane whose
 // Levenberg-Marquardt solve has returned finishes its pair and takes the next one from
 // a global queue, so warps do not idle on their slowest pair.
-__global__ void __launch_bounds__(128, 4) k_contact(const InstDev *__restrict__ insts,
+#ifdef GP_LM_INLINE
+#define GP_CONTACT_MIN_BLOCKS 2
+#else
+#define GP_CONTACT_MIN_BLOCKS 4
+#endif
+
+__global__ void __launch_bounds__(128, GP_CONTACT_MIN_BLOCKS) k_contact(const InstDev *__restrict__ insts,
                                                     const PoolView *__restrict__ pv,
                                                     const PairRec *__restrict__ pairs,
                                                     const unsigned long long *__restrict__ npairs, int64_t cap_pairs,
@@ -199,6 +205,17 @@ __global__ void __launch_bounds__(128, 4) k_contact(const InstDev *__restrict__ 
     for (int i = 0; i < 3; ++i) { r.rx1[i] = rx1[i]; r.rx2[i] = rx2[i]; r.cn[i] = cn[i]; }
     coll[slot] = r;
   }
+}
+
+// Persistent grid for k_contact: as many blocks as can be resident at once on the
+// current device (looked up once, at context creation, outside any stream capture).
+int contact_grid_blocks() {
+  int per_sm = 0, dev = 0, sms = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_contact, 128, 0) != cudaSuccess ||
+      cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || per_sm <= 0)
+    return 0;
+  return per_sm * sms;
 }
 
 void launch_contact(const InstDev *insts, const PoolView *pv, const PairRec *pairs, const unsigned long long *npairs,
@@ -299,7 +316,7 @@ __global__ void k_euler_batch(int64_t n, const double *ip, double dt, double *om
   }
 }
 
-__global__ void __launch_bounds__(128, 4) k_contact_batch(int64_t n, const double *shapes, const double *centres, const double *quats,
+__global__ void __launch_bounds__(128, GP_CONTACT_MIN_BLOCKS) k_contact_batch(int64_t n, const double *shapes, const double *centres, const double *quats,
                                 int32_t *flag, double *e1, double *e2, double *cn) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const double *s = shapes + 4 * i, *c = centres + 6 * i, *q = quats + 8 * i;

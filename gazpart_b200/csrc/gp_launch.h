@@ -17,6 +17,7 @@ void launch_interp(const InstDev *inst, int comp, int64_t n, const double *x, co
 void launch_frozen_interp(const double *xain, const double *yain, const double *zain, int nx, int ny, int nz,
                           const double *uain, int64_t n, const double *x, const double *y, const double *z,
                           double *out, Status *st, cudaStream_t s);
+int contact_grid_blocks();
 void launch_contact(const InstDev *insts, const PoolView *pv, const PairRec *pairs, const unsigned long long *npairs,
                     int64_t cap_pairs, CollRec *coll, unsigned long long *ncoll, int64_t cap_coll,
                     unsigned long long *queue, Status *st, int grid, cudaStream_t s);

@@ -17,6 +17,15 @@
 
 namespace gp {
 
+// Linkage of the solver's building blocks.  Out-of-line calls keep the register count
+// of the pair-search and batch kernels low; GP_LM_INLINE folds the whole solve into
+// its caller, which shortens the dependent-latency chain of one iteration.
+#ifdef GP_LM_INLINE
+#define GP_LM_FN static __device__ __forceinline__
+#else
+#define GP_LM_FN static __device__ __noinline__
+#endif
+
 // MINPACK's scaled Euclidean norm (minpack_reduc.f90:180-232): three accumulators
 // for tiny, mid-range and huge components.
 template <int N>
@@ -89,7 +98,12 @@ CT_QUAL double ct_poly_cos(double z) {
 
 /* sin and cos of x: Cody-Waite reduction by pi/2 = P1 + P2 + P3 (33 + 33 + 53 bits, so
  * k*P1 and k*P2 are exact for |k| < 2^20), Taylor polynomials on [-pi/4, pi/4]. */
-inline __host__ __device__ __noinline__ void ct_sincos(double x, double *s, double *c) {
+#ifdef GP_LM_INLINE
+#define CT_SINCOS_QUAL CT_QUAL
+#else
+#define CT_SINCOS_QUAL inline __host__ __device__ __noinline__
+#endif
+CT_SINCOS_QUAL void ct_sincos(double x, double *s, double *c) {
   if (!(fabs(x) < 1.0e9)) {
     *s = x - x + (0.0 / 0.0 + x * 0.0);
     *c = *s;
@@ -168,7 +182,7 @@ struct ContactProb {
 };
 
 // Support points along +-c(x) (ellipsoid_pair_depth.f90:117-142).
-static __device__ __noinline__ void support_points(const ContactProb& P, const double x[2], double c1[3], double tmp1[3],
+GP_LM_FN void support_points(const ContactProb& P, const double x[2], double c1[3], double tmp1[3],
                                                double tmp2[3], double& l1, double& l2, double pt1[3],
                                                double pt2[3]) {
   double s0, k0, s1, k1;
@@ -191,7 +205,7 @@ static __device__ __noinline__ void support_points(const ContactProb& P, const d
 }
 
 // fcn, iflag=1 (ellipsoid_contact_detection.f90:290-295)
-static __device__ __noinline__ void lm_fcn(const ContactProb& P, const double x[2], double fvec[3]) {
+GP_LM_FN void lm_fcn(const ContactProb& P, const double x[2], double fvec[3]) {
   double c1[3], t1[3], t2[3], l1, l2, pt1[3], pt2[3];
   support_points(P, x, c1, t1, t2, l1, l2, pt1, pt2);
 #pragma unroll
@@ -201,7 +215,7 @@ static __device__ __noinline__ void lm_fcn(const ContactProb& P, const double x[
   }
 }
 
-static __device__ __noinline__ void grad_coeff(const double e[9], const double c[3], double l, double co[9]) {
+GP_LM_FN void grad_coeff(const double e[9], const double c[3], double l, double co[9]) {
   double row[3];
 #pragma unroll
   for (int j = 0; j < 3; ++j) row[j] = c[0] * e[3 * j] + c[1] * e[1 + 3 * j] + c[2] * e[2 + 3 * j];
@@ -219,7 +233,7 @@ static __device__ __noinline__ void grad_coeff(const double e[9], const double c
 
 // fcn, iflag=2: analytic Jacobian (ellipsoid_contact_detection.f90:296-332), 3x2
 // column-major.
-static __device__ __noinline__ void lm_jac(const ContactProb& P, const double x[2], double fj[6]) {
+GP_LM_FN void lm_jac(const ContactProb& P, const double x[2], double fj[6]) {
   double c1[3], t1[3], t2[3], l1, l2, pt1[3], pt2[3];
   support_points(P, x, c1, t1, t2, l1, l2, pt1, pt2);
   const double depth[3] = {pt1[0] - pt2[0], pt1[1] - pt2[1], pt1[2] - pt2[2]};
@@ -244,7 +258,7 @@ static __device__ __noinline__ void lm_jac(const ContactProb& P, const double x[
 }
 
 // QR with column pivoting (3x2), Householder vectors left in a.
-static __device__ __noinline__ void lm_qrfac(double a[6], int ipvt[2], double rdiag[2], double acnorm[2]) {
+GP_LM_FN void lm_qrfac(double a[6], int ipvt[2], double rdiag[2], double acnorm[2]) {
   double wa[2];
 #pragma unroll
   for (int j = 0; j < 2; ++j) {
@@ -293,7 +307,7 @@ static __device__ __noinline__ void lm_qrfac(double a[6], int ipvt[2], double rd
   }
 }
 
-static __device__ __noinline__ void lm_qrsolv(double r[6], const int ipvt[2], const double diag[2], const double qtb[2],
+GP_LM_FN void lm_qrsolv(double r[6], const int ipvt[2], const double diag[2], const double qtb[2],
                                           double x[2], double sdiag[2]) {
   double wa[2];
 #pragma unroll
@@ -354,7 +368,7 @@ static __device__ __noinline__ void lm_qrsolv(double r[6], const int ipvt[2], co
   x[ipvt[1]] = wa[1];
 }
 
-static __device__ __noinline__ void lm_lmpar(double r[6], const int ipvt[2], const double diag[2], const double qtb[2],
+GP_LM_FN void lm_lmpar(double r[6], const int ipvt[2], const double diag[2], const double qtb[2],
                                          double delta, double& par, double x[2], double sdiag[2]) {
   const double dwarf = DBL_MIN;
   double wa1[2], wa2[2];
@@ -444,7 +458,7 @@ struct LmState {
   bool need_jac;
 };
 
-static __device__ __noinline__ void lm_begin(const ContactProb& P, LmState& S) {
+GP_LM_FN void lm_begin(const ContactProb& P, LmState& S) {
   lm_fcn(P, S.x, S.fvec);
   S.nfev = 1;
   S.fnorm = lm_enorm<3>(S.fvec);
@@ -460,7 +474,7 @@ static __device__ __noinline__ void lm_begin(const ContactProb& P, LmState& S) {
   S.need_jac = true;
 }
 
-static __device__ __noinline__ int lm_step(const ContactProb& P, LmState& S, double tol) {
+GP_LM_FN int lm_step(const ContactProb& P, LmState& S, double tol) {
   constexpr int maxfev = 300;
   const double ftol = tol, xtol = tol;
   double wa1[2], wa2[2], wa3[2], wa4[3];
@@ -573,7 +587,7 @@ static __device__ __noinline__ int lm_step(const ContactProb& P, LmState& S, dou
 }
 
 // Margin function mod_particle_parallel.f90:145-201: v^T (R diag(1/a^2,1/b^2,1/b^2) R^T) v
-static __device__ __noinline__ double fmargin(double a, double b, const double pt[3], const double c[3], const Quat& q) {
+GP_LM_FN double fmargin(double a, double b, const double pt[3], const double c[3], const Quat& q) {
   double ell[9];
   rot_diag(q, 1.0 / (a * a), 1.0 / (b * b), 1.0 / (b * b), ell);
   const double v[3] = {pt[0] - c[0], pt[1] - c[1], pt[2] - c[2]};
@@ -586,7 +600,7 @@ static __device__ __noinline__ double fmargin(double a, double b, const double p
 // and the starting angles from the centre line (:77-87).  Returns false when a starting
 // angle is NaN (acos of a ratio just above 1): every iterate would stay NaN and the
 // reference reports no contact, so the caller skips the solve.
-static __device__ __noinline__ bool contact_setup(double a1, double bb1, double a2, double bb2, const double c1[3],
+GP_LM_FN bool contact_setup(double a1, double bb1, double a2, double bb2, const double c1[3],
                                                   const Quat& q1, const double c2[3], const Quat& q2, ContactProb& P,
                                                   double x[2]) {
   double nrm[3] = {c1[0] - c2[0], c1[1] - c2[1], c1[2] - c2[2]};
@@ -602,7 +616,7 @@ static __device__ __noinline__ bool contact_setup(double a1, double bb1, double 
 }
 
 // pair_depth at the solution and the contact test (ellipsoid_contact_detection.f90:104-179)
-static __device__ __noinline__ bool contact_finish(double a1, double bb1, double a2, double bb2, const Quat& q1,
+GP_LM_FN bool contact_finish(double a1, double bb1, double a2, double bb2, const Quat& q1,
                                                    const Quat& q2, const ContactProb& P, const double x[2],
                                                    double ept1[3], double ept2[3], double cn[3]) {
   double cc[3], t1[3], t2[3], l1, l2, pt1[3], pt2[3];
@@ -617,7 +631,7 @@ static __device__ __noinline__ bool contact_finish(double a1, double bb1, double
 constexpr double kContactTol = 1.4901161193847656e-08;   // sqrt(epsilon(1.0_8))
 
 // ellipsoid_contact_detection.f90:1-187 for one pair, start to finish.
-static __device__ __noinline__ bool contact_detection(double a1, double bb1, double a2, double bb2,
+GP_LM_FN bool contact_detection(double a1, double bb1, double a2, double bb2,
                                                       const double c1[3], const Quat& q1, const double c2[3],
                                                       const Quat& q2, double ept1[3], double ept2[3], double cn[3]) {
   ContactProb P;
