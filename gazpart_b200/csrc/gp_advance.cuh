@@ -8,10 +8,12 @@
 
 namespace gp {
 
-// Internal field layout: [k: nz+4][j: ny+4][i: nx+3][c: ncomp].  Reference index
-// (I, J, K) with J, K in -1..N+2 (NGHTCELL=2 ghost planes) and I in 1..NX maps to
-// (I, J+1, K+1); x ghost columns 0, NX+1, NX+2 hold columns NX, 1, 2 so that the
-// periodic x wrap of interp_lag3.f90:132-154 reads four contiguous points.
+// Internal field layout: [k: nz+4][j: ny+4][i: nx+3][c: kFieldStride].  Reference
+// index (I, J, K) with J, K in -1..N+2 (NGHTCELL=2 ghost planes) and I in 1..NX maps
+// to (I, J+1, K+1); x ghost columns 0, NX+1, NX+2 hold columns NX, 1, 2 so that the
+// periodic x wrap of interp_lag3.f90:132-154 reads four contiguous points.  The six
+// components of a point are padded to eight, so a point is one 32-byte sector (FP32)
+// and a stencil row of four points is 128 contiguous, aligned bytes.
 __device__ __forceinline__ int64_t field_point(const InstDev& I, int ix, int jy, int kz) {
   return ((int64_t)(kz + 1) * (I.ny + 4) + (jy + 1)) * (int64_t)(I.nx + 3) + ix;
 }
@@ -84,14 +86,16 @@ __device__ __forceinline__ void gather6_fp64(const InstDev& I, const Stencil& s,
       double xs[6];
       const int64_t p0 = field_point(I, s.ix[0], s.j0 - 1 + jj, s.k0 - 1 + kk);
       if (s.contiguous) {
-        const double2* row = reinterpret_cast<const double2*>(F + p0 * 6);
+        const double2* row = reinterpret_cast<const double2*>(F + p0 * kFieldStride);
         double v[24];
 #pragma unroll
-        for (int t = 0; t < 12; ++t) {
-          const double2 d = __ldg(row + t);
-          v[2 * t] = d.x;
-          v[2 * t + 1] = d.y;
-        }
+        for (int ii = 0; ii < 4; ++ii)
+#pragma unroll
+          for (int t = 0; t < 3; ++t) {
+            const double2 d = __ldg(row + ii * (kFieldStride / 2) + t);
+            v[6 * ii + 2 * t] = d.x;
+            v[6 * ii + 2 * t + 1] = d.y;
+          }
 #pragma unroll
         for (int c = 0; c < 6; ++c)
           xs[c] = fx[0] * v[c] + fx[1] * v[6 + c] + fx[2] * v[12 + c] + fx[3] * v[18 + c];
@@ -101,7 +105,7 @@ __device__ __forceinline__ void gather6_fp64(const InstDev& I, const Stencil& s,
         for (int ii = 0; ii < 4; ++ii) {
           const int64_t pp = field_point(I, s.ix[ii], s.j0 - 1 + jj, s.k0 - 1 + kk);
 #pragma unroll
-          for (int c = 0; c < 6; ++c) v[6 * ii + c] = __ldg(F + pp * 6 + c);
+          for (int c = 0; c < 6; ++c) v[6 * ii + c] = __ldg(F + pp * kFieldStride + c);
         }
 #pragma unroll
         for (int c = 0; c < 6; ++c)
@@ -136,19 +140,20 @@ __device__ __forceinline__ void gather6_fp32(const InstDev& I, const Stencil& s,
       const int64_t p0 = field_point(I, s.ix[0], s.j0 - 1 + jj, s.k0 - 1 + kk);
       float v[24];
       if (s.contiguous) {
-        const float2* row = reinterpret_cast<const float2*>(F + p0 * 6);
+        const float4* row = reinterpret_cast<const float4*>(F + p0 * kFieldStride);
 #pragma unroll
-        for (int t = 0; t < 12; ++t) {
-          const float2 d = __ldg(row + t);
-          v[2 * t] = d.x;
-          v[2 * t + 1] = d.y;
+        for (int ii = 0; ii < 4; ++ii) {
+          const float4 d = __ldg(row + 2 * ii);
+          const float2 e = __ldg(reinterpret_cast<const float2*>(row + 2 * ii + 1));
+          v[6 * ii + 0] = d.x; v[6 * ii + 1] = d.y; v[6 * ii + 2] = d.z; v[6 * ii + 3] = d.w;
+          v[6 * ii + 4] = e.x; v[6 * ii + 5] = e.y;
         }
       } else {
 #pragma unroll
         for (int ii = 0; ii < 4; ++ii) {
           const int64_t pp = field_point(I, s.ix[ii], s.j0 - 1 + jj, s.k0 - 1 + kk);
 #pragma unroll
-          for (int c = 0; c < 6; ++c) v[6 * ii + c] = __ldg(F + pp * 6 + c);
+          for (int c = 0; c < 6; ++c) v[6 * ii + c] = __ldg(F + pp * kFieldStride + c);
         }
       }
 #pragma unroll
@@ -399,46 +404,146 @@ __device__ __forceinline__ void load_pc(const PoolView& P, int64_t i, PartConst&
   pc.ipxx = P.pc[7][i]; pc.ipyy = P.pc[8][i]; pc.ipzz = P.pc[9][i];
 }
 
+// Kahan step: sum += w*v with the lost low part carried in cmp.
+__device__ __forceinline__ void kahan_fma(float& sum, float& cmp, float w, float v) {
+  const float y = __fmaf_rn(w, v, -cmp);
+  const float t = __fadd_rn(sum, y);
+  cmp = __fsub_rn(__fsub_rn(t, sum), y);
+  sum = t;
+}
+
+__device__ __forceinline__ float pick4(const float f[4], int k) {
+  return k == 0 ? f[0] : (k == 1 ? f[1] : (k == 2 ? f[2] : f[3]));
+}
+
+// Warp-cooperative FP32 gather for the 32 particles of one warp.  Eight lanes serve one
+// particle: lane t of the group loads float4 (t & 1) of point (t >> 1) of each of the 16
+// stencil rows (one aligned 128-byte row per group and load instruction, instead of 32
+// scattered 8-byte loads), accumulates w_x w_y w_z U with Kahan-compensated FP32 sums,
+// and the four x points are then summed in double across the group.  mode: 0 no gather,
+// 1 cooperative (contiguous row), 2 left to the lane itself.
+__device__ __forceinline__ void gather_warp_fp32(const InstDev* __restrict__ insts, int mode, int inst,
+                                                 int64_t b, float al, float be, float ga, int64_t j0,
+                                                 double* const* __restrict__ fluid) {
+  constexpr unsigned kFull = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int t = lane & 7, k = t >> 1, half = t & 1;
+#pragma unroll 1
+  for (int g = 0; g < 8; ++g) {
+    const int o = g * 4 + (lane >> 3);
+    const int mo = __shfl_sync(kFull, mode, o);
+    const int io = __shfl_sync(kFull, inst, o);
+    const long long bo = __shfl_sync(kFull, (long long)b, o);
+    const float alo = __shfl_sync(kFull, al, o), beo = __shfl_sync(kFull, be, o), gao = __shfl_sync(kFull, ga, o);
+    float4 sum = make_float4(0.f, 0.f, 0.f, 0.f), cmp = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (mo == 1) {
+      const InstDev& I = insts[io];
+      const float* __restrict__ F = static_cast<const float*>(I.field);
+      const int64_t sy = I.nx + 3, sz = (int64_t)(I.ny + 4) * sy;
+      float fx[4], fy[4], fz[4];
+      lag3_wf(alo, fx);
+      lag3_wf(beo, fy);
+      lag3_wf(gao, fz);
+      const float wx = pick4(fx, k);
+      const float* __restrict__ p = F + (bo + k) * kFieldStride + 4 * half;
+#pragma unroll
+      for (int kk = 0; kk < 4; ++kk)
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj) {
+          const float4 v = __ldg(reinterpret_cast<const float4*>(p + (kk * sz + jj * sy) * kFieldStride));
+          const float w = (fz[kk] * fy[jj]) * wx;
+          kahan_fma(sum.x, cmp.x, w, v.x);
+          kahan_fma(sum.y, cmp.y, w, v.y);
+          kahan_fma(sum.z, cmp.z, w, v.z);
+          kahan_fma(sum.w, cmp.w, w, v.w);
+        }
+    }
+    double d0 = (double)sum.x - (double)cmp.x, d1 = (double)sum.y - (double)cmp.y;
+    double d2 = (double)sum.z - (double)cmp.z, d3 = (double)sum.w - (double)cmp.w;
+#pragma unroll
+    for (int m = 2; m <= 4; m <<= 1) {
+      d0 += __shfl_xor_sync(kFull, d0, m);
+      d1 += __shfl_xor_sync(kFull, d1, m);
+      d2 += __shfl_xor_sync(kFull, d2, m);
+      d3 += __shfl_xor_sync(kFull, d3, m);
+    }
+    if (mo == 1 && t < 2) {
+      const int64_t jo = j0 + o;
+      if (half == 0) {
+        fluid[0][jo] = d0; fluid[1][jo] = d1; fluid[2][jo] = d2; fluid[3][jo] = d3;
+      } else {
+        fluid[4][jo] = d0; fluid[5][jo] = d1;
+      }
+    }
+  }
+}
+
 // ADV_PARTICLE_ELLP, first half: particle perm[j] of the source buffer is moved to slot
 // j of the destination buffer (so that the pool follows the search-grid cell order of
 // the last binning and neighbouring stencils are gathered together) and the six field
 // components are interpolated at its position x_n (adv_particle_new.f90:139-206).  Any
 // permutation is correct: every particle carries its properties, id and instance.
-static __global__ void __launch_bounds__(256) k_gather_move(const InstDev* __restrict__ insts,
-                                                               const PoolView* __restrict__ src_pv,
-                                                               const PoolView* __restrict__ dst_pv,
-                                                               const int32_t* __restrict__ perm, int64_t n,
-                                                               double* const* __restrict__ fluid, Status* st) {
-  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t i = perm[j];
-    const int inst = src_pv->inst[i];
-    dst_pv->inst[j] = inst;
-    dst_pv->id[j] = src_pv->id[i];
-    // one column pointer pair live at a time keeps the register count low
+// kMixed: every instance holds an FP32 field (warp-cooperative gather); otherwise FP64
+// fields, gathered per lane in the reference's summation order.
+template <bool kMixed>
+__global__ void __launch_bounds__(256) k_gather_move(const InstDev* __restrict__ insts,
+                                                     const PoolView* __restrict__ src_pv,
+                                                     const PoolView* __restrict__ dst_pv,
+                                                     const int32_t* __restrict__ perm, int64_t n,
+                                                     double* const* __restrict__ fluid, Status* st) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w * 32 < n; w += nwarps) {
+    const int64_t j = w * 32 + lane;
+    int inst = -1;
+    int64_t i = 0;
+    if (j < n) {
+      i = perm[j];
+      inst = src_pv->inst[i];
+      dst_pv->inst[j] = inst;
+      dst_pv->id[j] = src_pv->id[i];
+      // one column pointer pair live at a time keeps the register count low
 #pragma unroll 1
-    for (int c = 0; c < kNState; ++c) dst_pv->st[c][j] = src_pv->st[c][i];
+      for (int c = 0; c < kNState; ++c) dst_pv->st[c][j] = src_pv->st[c][i];
 #pragma unroll 1
-    for (int c = 0; c < kNConst; ++c) dst_pv->pc[c][j] = src_pv->pc[c][i];
-    double g[6] = {CUDART_NAN, CUDART_NAN, CUDART_NAN, CUDART_NAN, CUDART_NAN, CUDART_NAN};
+      for (int c = 0; c < kNConst; ++c) dst_pv->pc[c][j] = src_pv->pc[c][i];
+    }
+    int mode = 0;
+    Stencil s;
     if (inst >= 0) {
       const InstDev& I = insts[inst];
-      Stencil s;
       if (stencil(I, src_pv->st[0][i], src_pv->st[1][i], src_pv->st[2][i], s)) {
-        if (I.fprec == GP_PREC_MIXED) gather6_fp32(I, s, g); else gather6_fp64(I, s, g);
+        mode = (kMixed && s.contiguous) ? 1 : 2;
       } else {
         set_error(st, GP_EOUT_OF_GRID, (long long)src_pv->id[i]);
       }
     }
+    if (j < n && mode == 0) {
 #pragma unroll
-    for (int c = 0; c < 6; ++c) fluid[c][j] = g[c];
+      for (int c = 0; c < 6; ++c) fluid[c][j] = CUDART_NAN;
+    }
+    if (kMixed) {
+      const int64_t b = (mode == 1) ? field_point(insts[inst], s.ix[0], s.j0 - 1, s.k0 - 1) : 0;
+      gather_warp_fp32(insts, mode, inst, b, (float)s.alfa, (float)s.beta, (float)s.gama, w * 32, fluid);
+    }
+    if (mode == 2) {
+      const InstDev& I = insts[inst];
+      double g[6];
+      if (kMixed) gather6_fp32(I, s, g); else gather6_fp64(I, s, g);
+#pragma unroll
+      for (int c = 0; c < 6; ++c) fluid[c][j] = g[c];
+    }
   }
 }
 
 // ADV_PARTICLE_ELLP, second half, in place on the (now cell-ordered) buffer: the RK2
 // predictor/corrector with wall handling (adv_particle_new.f90:268-637) and
 // BOUNDARY_PARTICLE's periodic wrap (boundary_particle.f90:50-59).
+#ifndef GP_INTEGRATE_MIN_BLOCKS
+#define GP_INTEGRATE_MIN_BLOCKS 1
+#endif
 template <bool kMixed>
-__global__ void __launch_bounds__(128) k_integrate(const InstDev* __restrict__ insts, const PoolView* __restrict__ pv,
+__global__ void __launch_bounds__(128, GP_INTEGRATE_MIN_BLOCKS) k_integrate(const InstDev* __restrict__ insts, const PoolView* __restrict__ pv,
                                                    int64_t n, const double* const* __restrict__ fluid, Status* st) {
   const PoolView P = *pv;
   for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {

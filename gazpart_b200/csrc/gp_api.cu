@@ -230,7 +230,7 @@ int alloc_pool(gp_ctx *c, int64_t cap) {
 
 // COLLISION_INITIATION (collision_initiation.f90:44-103, INIT_GRID=2, NPROC=1) and the
 // search grid.
-int setup_grids(gp_ctx *c, double max_emaj, double rmax) {
+int setup_grids(gp_ctx *c, double max_emaj, double rmax, double rsmall) {
   InstDev &I = c->inst;
   const gp_params &p = c->prm;
   const double zero_ref = 1.0e-33;
@@ -250,8 +250,9 @@ int setup_grids(gp_ctx *c, double max_emaj, double rmax) {
   if (I.nxbox >= (1 << 21) || I.nybox >= (1 << 21) || I.nzbox >= (1 << 21)) return GP_EBADARG;
   I.dybox = (ymaxbox - I.yminbox) / (double)I.nybox;
   I.dzbox = (zmaxbox - I.zminbox) / (double)I.nzbox;
-  // search grid: cell edge >= 2 rmax (1+1e-6), about two or more particles per cell
-  const double hmin = 2.0 * rmax * (1.0 + 1.0e-6);
+  // search grid: about two particles per cell, cell edge >= 2 rsmall (1+1e-6) so that
+  // all but the largest bounding radii fit the one-cell half stencil
+  const double hmin = 2.0 * rsmall * (1.0 + 1.0e-6);
   const int64_t target = std::max<int64_t>(3, (int64_t)std::ceil(std::cbrt((double)std::max<int64_t>(c->n, 1) / 2.0)));
   auto nf = [&](double L) {
     int64_t m = (int64_t)std::floor(L / hmin);
@@ -261,6 +262,7 @@ int setup_grids(gp_ctx *c, double max_emaj, double rmax) {
   if (I.nfx < 3 || I.nfy < 3 || I.nfz < 3) return GP_EBADARG;
   I.hfx = p.lx / I.nfx; I.hfy = p.ly / I.nfy; I.hfz = p.lz / I.nfz;
   I.rmax = rmax;
+  I.rcut = 0.5 * std::min(I.hfx, std::min(I.hfy, I.hfz)) / (1.0 + 1.0e-6);
   I.cell_begin = 0;
   const int64_t ncells = (int64_t)I.nfx * I.nfy * I.nfz;
   if (ncells >= (int64_t(1) << 31) - 2) return GP_EBADARG;
@@ -349,7 +351,7 @@ int gp_ctx_create(const gp_params *params, gp_ctx **out) {
   I.visc = p.visc; I.dtime = p.dtime; I.gravity = p.gravity;
   I.ecp = p.ecp; I.mup = p.mup; I.ecw = p.ecw; I.muw = p.muw;
   const size_t elem = (p.precision == GP_PREC_MIXED) ? sizeof(float) : sizeof(double);
-  c->field_bytes = (size_t)(p.nx + 3) * (p.ny + 4) * (p.nz + 4) * 6 * elem;
+  c->field_bytes = (size_t)(p.nx + 3) * (p.ny + 4) * (p.nz + 4) * kFieldStride * elem;
   int rc = GP_OK;
   if (cudaMalloc(&c->field, c->field_bytes) != cudaSuccess || cudaMemset(c->field, 0, c->field_bytes) != cudaSuccess)
     rc = GP_ENOMEM;
@@ -441,7 +443,8 @@ int gp_set_field(gp_ctx *c, int32_t comp, const double *src, int32_t src_layout,
     GP_CK(cudaMemcpyAsync(c->stage, src, count * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     dsrc = c->stage;
   }
-  launch_field_layout(c->field, p.precision, p.nx, p.ny, p.nz, 6, comp, dsrc, src_layout, ghost_mode, c->stream);
+  launch_field_layout(c->field, p.precision, p.nx, p.ny, p.nz, kFieldStride, comp, dsrc, src_layout, ghost_mode,
+                      c->stream);
   GP_CK(cudaGetLastError());
   GP_CK(cudaStreamSynchronize(c->stream));
   return GP_OK;
@@ -462,6 +465,7 @@ int gp_upload_state(gp_ctx *c, int64_t n, const double *const *cols, const doubl
   GP_CK(cudaStreamSynchronize(c->stream));
   std::vector<double> pcs((size_t)kNConst * n);
   double max_emaj = 0.0, rmax = 0.0;
+  std::vector<double> radii(n);
   for (int64_t i = 0; i < n; ++i) {
     double pc[kNConst];
     const double emaj = hp[0][i], apr = hp[1][i], rhop = hp[2][i];
@@ -470,7 +474,13 @@ int gp_upload_state(gp_ctx *c, int64_t n, const double *const *cols, const doubl
     for (int k = 0; k < kNConst; ++k) pcs[(size_t)k * n + i] = pc[k];
     max_emaj = std::max(max_emaj, emaj);
     rmax = std::max(rmax, std::max(pc[0], pc[1]));
+    radii[i] = std::max(pc[0], pc[1]);
   }
+  // the search grid is sized for all but the largest 0.1% of bounding radii
+  const int64_t qi = std::min<int64_t>(n - 1, (int64_t)(0.999 * (double)n));
+  std::nth_element(radii.begin(), radii.begin() + qi, radii.end());
+  const double rsmall = radii[qi];
+  std::vector<double>().swap(radii);
   drop_graph(c);
   const int64_t want = std::max<int64_t>(n, c->prm.max_particles);
   if (c->cap < want) GP_TRY(alloc_pool(c, want));
@@ -489,7 +499,7 @@ int gp_upload_state(gp_ctx *c, int64_t n, const double *const *cols, const doubl
   cudaFree(stage_cols);
   cudaFree(stage_pc);
   c->inst.count = n;
-  GP_TRY(setup_grids(c, max_emaj, rmax));
+  GP_TRY(setup_grids(c, max_emaj, rmax, rsmall));
   GP_TRY(upload_inst(c));
   GP_CK(cudaStreamSynchronize(c->stream));
   return GP_OK;

@@ -8,6 +8,10 @@
 #include "gp_lm.cuh"
 #include "gp_launch.h"
 
+#ifndef GP_GATHER_BLOCKS_PER_SM
+#define GP_GATHER_BLOCKS_PER_SM 8
+#endif
+
 namespace gp {
 
 template __global__ void k_integrate<false>(const InstDev *, const PoolView *, int64_t, const double *const *, Status *);
@@ -15,7 +19,7 @@ template __global__ void k_integrate<false>(const InstDev *, const PoolView *, i
 void launch_advance_fp64(const InstDev *insts, PoolView *pv, PoolView *pv_alt, const int32_t *perm, int64_t n,
                          double *const *fluid, Status *st,
                          int grid, cudaStream_t s) {
-  k_gather_move<<<148 * 8, 256, 0, s>>>(insts, pv, pv_alt, perm, n, fluid, st);
+  k_gather_move<false><<<148 * GP_GATHER_BLOCKS_PER_SM, 256, 0, s>>>(insts, pv, pv_alt, perm, n, fluid, st);
   k_swap_pool<<<1, 1, 0, s>>>(pv, pv_alt);
   k_integrate<false><<<grid, 128, 0, s>>>(insts, pv, n, fluid, st);
 }

@@ -4,6 +4,10 @@
 #include "gp_advance.cuh"
 #include "gp_launch.h"
 
+#ifndef GP_GATHER_BLOCKS_PER_SM
+#define GP_GATHER_BLOCKS_PER_SM 8
+#endif
+
 namespace gp {
 
 template __global__ void k_integrate<true>(const InstDev *, const PoolView *, int64_t, const double *const *, Status *);
@@ -11,7 +15,7 @@ template __global__ void k_integrate<true>(const InstDev *, const PoolView *, in
 void launch_advance_mixed(const InstDev *insts, PoolView *pv, PoolView *pv_alt, const int32_t *perm, int64_t n,
                          double *const *fluid, Status *st,
                           int grid, cudaStream_t s) {
-  k_gather_move<<<148 * 8, 256, 0, s>>>(insts, pv, pv_alt, perm, n, fluid, st);
+  k_gather_move<true><<<148 * GP_GATHER_BLOCKS_PER_SM, 256, 0, s>>>(insts, pv, pv_alt, perm, n, fluid, st);
   k_swap_pool<<<1, 1, 0, s>>>(pv, pv_alt);
   k_integrate<true><<<grid, 128, 0, s>>>(insts, pv, n, fluid, st);
 }

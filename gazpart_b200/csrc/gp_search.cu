@@ -203,7 +203,9 @@ __global__ void k_bin_scatter(const InstDev *__restrict__ insts, const PoolView 
     sa.sz[pos] = z;
     const double ea = P.pc[0][i], eb = P.pc[1][i];
     sa.sr[pos] = fmax(ea, eb);
-    sa.spk[pos] = make_float4((float)x, (float)y, (float)z, (float)fmax(ea, eb));
+    // w carries the bounding radius, negated for particles above the small-particle cut
+    const double rb = fmax(ea, eb);
+    sa.spk[pos] = make_float4((float)x, (float)y, (float)z, rb > I.rcut ? -(float)rb : (float)rb);
     sa.sa2[pos] = ea * ea;
     sa.sb2[pos] = eb * eb;
     {
@@ -249,115 +251,194 @@ __device__ __forceinline__ void emit_pair(PairRec *pairs, unsigned long long *np
   }
 }
 
-// the 13 forward offsets (any half stencil of the search grid will do)
-__constant__ int8_t c_half[13][3] = {{1, 1, -1}, {1, -1, 0}, {1, 0, 0}, {0, 1, 0}, {1, 1, 0},
-                                     {0, -1, 1}, {1, -1, 1}, {-1, 0, 1}, {0, 0, 1}, {1, 0, 1},
-                                     {-1, 1, 1}, {0, 1, 1}, {1, 1, 1}};
+// One candidate (s, qs) of the sweep: conservative float test, FP64 bounding-sphere
+// test, centre-line separation test, reference box adjacency, then emission with the
+// reference's ordering keys.
+struct SearchHome {
+  double xp, yp, zp, rp;
+  float xpf, ypf, zpf, rpf, lxf, lyf, lzf;
+  long long bp;
+  int32_t s, pslot, idp;
+  bool perx;
+};
 
+// kLarge: the home particle is above the cut and sweeps a full stencil; it takes every
+// small candidate and the large ones that follow it in sorted order.  Otherwise the home
+// particle is small, sweeps the half stencil and leaves large candidates to them.
+template <bool kLarge>
+__device__ __forceinline__ void search_candidate(const InstDev &I, const SearchArrays &sa, const SearchHome &h,
+                                                 int32_t qs, PairRec *pairs, unsigned long long *npairs,
+                                                 int64_t cap, Status *st) {
+  // conservative float test: |float - double| distance error < 2e-6, slack 1e-5
+  {
+    const float4 c = sa.spk[qs];
+    if (c.w < 0.f && (!kLarge || qs <= h.s)) return;
+    float fx = c.x - h.xpf, fy = c.y - h.ypf, fz = c.z - h.zpf;
+    if (h.perx && fabsf(fx) > 0.5f * h.lxf) fx = fx - copysignf(h.lxf, fx);
+    if (fabsf(fy) > 0.5f * h.lyf) fy = fy - copysignf(h.lyf, fy);
+    if (fabsf(fz) > 0.5f * h.lzf) fz = fz - copysignf(h.lzf, fz);
+    const float rf = h.rpf + fabsf(c.w) + 1.0e-5f;
+    if (fx * fx + fy * fy + fz * fz > rf * rf) return;
+  }
+  double dx = sa.sx[qs] - h.xp, dy = sa.sy[qs] - h.yp, dz = sa.sz[qs] - h.zp;
+  if (h.perx && fabs(dx) > I.lx / 2) dx = dx - copysign(I.lx, dx);
+  if (fabs(dy) > I.ly / 2.) dy = dy - copysign(I.ly, dy);
+  if (fabs(dz) > I.lz / 2.) dz = dz - copysign(I.lz, dz);
+  const double rr = (h.rp + sa.sr[qs]) * (1.0 + 1e-9);
+  const double d2 = dx * dx + dy * dy + dz * dz;
+  if (d2 > rr * rr) return;
+  // Support-function test along the centre line: for unit d, the extent of a
+  // spheroid is h(d) = sqrt(b^2 + (a^2-b^2)(e.d)^2).  If h_p + h_q < |d| the two
+  // bodies are disjoint, so no contact point can lie inside the other body
+  // (ellipsoid_contact_detection.f90:125) and the reference cannot flag the pair.
+  if (d2 > 0.0) {
+    const double dist = sqrt(d2), inv = 1.0 / dist;
+    const double ux = dx * inv, uy = dy * inv, uz = dz * inv;
+    const double cp = sa.sex[h.s] * ux + sa.sey[h.s] * uy + sa.sez[h.s] * uz;
+    const double cq = sa.sex[qs] * ux + sa.sey[qs] * uy + sa.sez[qs] * uz;
+    const double hp = sqrt(fmax(sa.sb2[h.s] + (sa.sa2[h.s] - sa.sb2[h.s]) * cp * cp, 0.0));
+    const double hq = sqrt(fmax(sa.sb2[qs] + (sa.sa2[qs] - sa.sb2[qs]) * cq * cq, 0.0));
+    if (hp + hq < dist * (1.0 - 1e-9)) return;
+  }
+  atomicAdd(&st->n_near, 1ull);
+  // reference adjacency of the two boxes (collision_box_connectivity.f90)
+  const long long bp = h.bp, bq = sa.sbox[qs];
+  if (bp < 0 || bq < 0) return;   // already reported as out of grid
+  const int pi = (int)(bp & 0x1FFFFF), pj = (int)((bp >> 21) & 0x1FFFFF), pk = (int)(bp >> 42);
+  const int qi = (int)(bq & 0x1FFFFF), qj = (int)((bq >> 21) & 0x1FFFFF), qk = (int)(bq >> 42);
+  const int di = wrap_delta(qi - pi, I.nxbox, h.perx);
+  const int dj = wrap_delta(qj - pj, I.nybox, true);
+  const int dk = wrap_delta(qk - pk, I.nzbox, true);
+  if (di < -1 || di > 1 || dj < -1 || dj > 1 || dk < -1 || dk > 1) return;
+  const int32_t idq = sa.sid[qs];
+  PairRec r;
+  int slot;
+  long long hb;
+  bool home_is_p;
+  if (di == 0 && dj == 0 && dk == 0) {
+    slot = 0;
+    home_is_p = h.idp < idq;
+    hb = bp;
+  } else {
+    const int idx = (di + 1) * 9 + (dj + 1) * 3 + (dk + 1);
+    slot = c_fwd_slot[idx];
+    if (slot > 0) {
+      home_is_p = true;
+      hb = bp;
+    } else {
+      slot = c_fwd_slot[26 - idx];
+      home_is_p = false;
+      hb = bq;
+    }
+  }
+  const int hi = (int)(hb & 0x1FFFFF), hj = (int)((hb >> 21) & 0x1FFFFF), hk = (int)(hb >> 42);
+  const unsigned long long ijk =
+      (unsigned long long)(hi + 1) + (unsigned long long)hj * I.nxbox + (unsigned long long)hk * I.nxbox * I.nybox;
+  const int32_t idh = home_is_p ? h.idp : idq, idn = home_is_p ? idq : h.idp;
+  r.home = home_is_p ? h.pslot : sa.sorted[qs];
+  r.near = home_is_p ? sa.sorted[qs] : h.pslot;
+  r.k1 = ijk;
+  r.k2 = ((unsigned long long)idh << 34) | ((unsigned long long)slot << 30) | (unsigned long long)idn;
+  emit_pair(pairs, npairs, cap, r, st);
+}
+
+__device__ __forceinline__ int wrap_cell(int c, int n) { return c < 0 ? c + n : (c >= n ? c - n : c); }
+
+// Cells [lo, hi] of one x-row as at most two contiguous ranges of sorted particles
+// (periodic x wraps, otherwise the row is clipped).  lo >= -nfx and hi < 2 nfx.
+struct RowRanges {
+  int32_t a0, a1, b0, b1;
+};
+__device__ __forceinline__ RowRanges row_ranges(const SearchArrays &sa, int64_t base, int nfx, int lo, int hi,
+                                                bool perx) {
+  RowRanges r = {0, 0, 0, 0};
+  if (hi - lo + 1 >= nfx && perx) {
+    r.a0 = sa.cell_start[base];
+    r.a1 = sa.cell_start[base + nfx];
+    return r;
+  }
+  if (lo < 0) {
+    if (perx) { r.b0 = sa.cell_start[base + nfx + lo]; r.b1 = sa.cell_start[base + nfx]; }
+    lo = 0;
+  }
+  if (hi >= nfx) {
+    if (perx) { r.b0 = sa.cell_start[base]; r.b1 = sa.cell_start[base + hi - nfx + 1]; }
+    hi = nfx - 1;
+  }
+  if (lo <= hi) {
+    r.a0 = sa.cell_start[base + lo];
+    r.a1 = sa.cell_start[base + hi + 1];
+  }
+  return r;
+}
+
+// Pair search over the search grid.  The cell edge is at least twice the cut radius,
+// so two small particles (bounding radius <= cut) can only meet in the same or an
+// adjacent cell; a small particle sweeps the half stencil of its cell: the 13 forward
+// neighbours that follow it in (z, y, x) order, (cx+1, cy, cz), the three cells
+// cx-1..cx+1 of row (cy+1, cz) and the nine of layer cz+1.  Cells are numbered
+// x-fastest, so these are five x-rows, each one or two contiguous ranges of sorted
+// particles; the home cell is swept from the next sorted particle on.  A large particle
+// (radius above the cut, rare) sweeps every cell within its radius plus the largest
+// radius.  Every pair is visited exactly once.
 __global__ void __launch_bounds__(256) k_search(const InstDev *__restrict__ insts, int64_t n, SearchArrays sa,
                                                 PairRec *__restrict__ pairs, unsigned long long *npairs,
                                                 int64_t cap, Status *st) {
   const int64_t nact = sa.cell_start[sa.ncells];
   for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < nact; s += (int64_t)gridDim.x * blockDim.x) {
-    const int inst = sa.sinst[s];
-    const InstDev &I = insts[inst];
-    const double xp = sa.sx[s], yp = sa.sy[s], zp = sa.sz[s], rp = sa.sr[s];
-    const long long bp = sa.sbox[s];
-    const int pslot = sa.sorted[s];
-    const int32_t idp = sa.sid[s];
-    const int64_t lc = sa.cell_of[pslot] - I.cell_begin;
-    const int cx = (int)(lc % I.nfx), cy = (int)((lc / I.nfx) % I.nfy), cz = (int)(lc / ((int64_t)I.nfx * I.nfy));
-    const bool perx = I.periodicity != 0;
-    const float xpf = (float)xp, ypf = (float)yp, zpf = (float)zp, rpf = (float)rp;
-    const float lxf = (float)I.lx, lyf = (float)I.ly, lzf = (float)I.lz;
-    for (int o = -1; o < 13; ++o) {
-      int nx = cx, ny = cy, nz = cz;
-      if (o >= 0) {
-        nx += c_half[o][0];
-        ny += c_half[o][1];
-        nz += c_half[o][2];
-        if (nx < 0 || nx >= I.nfx) {
-          if (!perx) continue;
-          nx = (nx + I.nfx) % I.nfx;
-        }
-        ny = (ny + I.nfy) % I.nfy;
-        nz = (nz + I.nfz) % I.nfz;
-      }
-      const int64_t nc = I.cell_begin + ((int64_t)nz * I.nfy + ny) * I.nfx + nx;
-      int32_t q0 = sa.cell_start[nc];
-      const int32_t q1 = sa.cell_start[nc + 1];
-      if (o < 0) q0 = (int32_t)s + 1;
-      for (int32_t qs = q0; qs < q1; ++qs) {
-        // conservative float test: |float - double| distance error < 2e-6, slack 1e-5
-        {
-          const float4 c = sa.spk[qs];
-          float fx = c.x - xpf, fy = c.y - ypf, fz = c.z - zpf;
-          if (perx && fabsf(fx) > 0.5f * lxf) fx = fx - copysignf(lxf, fx);
-          if (fabsf(fy) > 0.5f * lyf) fy = fy - copysignf(lyf, fy);
-          if (fabsf(fz) > 0.5f * lzf) fz = fz - copysignf(lzf, fz);
-          const float rf = rpf + c.w + 1.0e-5f;
-          if (fx * fx + fy * fy + fz * fz > rf * rf) continue;
-        }
-        double dx = sa.sx[qs] - xp, dy = sa.sy[qs] - yp, dz = sa.sz[qs] - zp;
-        if (perx && fabs(dx) > I.lx / 2) dx = dx - copysign(I.lx, dx);
-        if (fabs(dy) > I.ly / 2.) dy = dy - copysign(I.ly, dy);
-        if (fabs(dz) > I.lz / 2.) dz = dz - copysign(I.lz, dz);
-        const double rr = (rp + sa.sr[qs]) * (1.0 + 1e-9);
-        const double d2 = dx * dx + dy * dy + dz * dz;
-        if (d2 > rr * rr) continue;
-        // Support-function test along the centre line: for unit d, the extent of a
-        // spheroid is h(d) = sqrt(b^2 + (a^2-b^2)(e.d)^2).  If h_p + h_q < |d| the two
-        // bodies are disjoint, so no contact point can lie inside the other body
-        // (ellipsoid_contact_detection.f90:125) and the reference cannot flag the pair.
-        if (d2 > 0.0) {
-          const double dist = sqrt(d2), inv = 1.0 / dist;
-          const double ux = dx * inv, uy = dy * inv, uz = dz * inv;
-          const double cp = sa.sex[s] * ux + sa.sey[s] * uy + sa.sez[s] * uz;
-          const double cq = sa.sex[qs] * ux + sa.sey[qs] * uy + sa.sez[qs] * uz;
-          const double hp = sqrt(fmax(sa.sb2[s] + (sa.sa2[s] - sa.sb2[s]) * cp * cp, 0.0));
-          const double hq = sqrt(fmax(sa.sb2[qs] + (sa.sa2[qs] - sa.sb2[qs]) * cq * cq, 0.0));
-          if (hp + hq < dist * (1.0 - 1e-9)) continue;
-        }
-        atomicAdd(&st->n_near, 1ull);
-        // reference adjacency of the two boxes (collision_box_connectivity.f90)
-        const long long bq = sa.sbox[qs];
-        if (bp < 0 || bq < 0) continue;   // already reported as out of grid
-        const int pi = (int)(bp & 0x1FFFFF), pj = (int)((bp >> 21) & 0x1FFFFF), pk = (int)(bp >> 42);
-        const int qi = (int)(bq & 0x1FFFFF), qj = (int)((bq >> 21) & 0x1FFFFF), qk = (int)(bq >> 42);
-        const int di = wrap_delta(qi - pi, I.nxbox, perx);
-        const int dj = wrap_delta(qj - pj, I.nybox, true);
-        const int dk = wrap_delta(qk - pk, I.nzbox, true);
-        if (di < -1 || di > 1 || dj < -1 || dj > 1 || dk < -1 || dk > 1) continue;
-        const int32_t idq = sa.sid[qs];
-        PairRec r;
-        int slot;
-        long long hb;
-        bool home_is_p;
-        if (di == 0 && dj == 0 && dk == 0) {
-          slot = 0;
-          home_is_p = idp < idq;
-          hb = bp;
+    const InstDev &I = insts[sa.sinst[s]];
+    SearchHome h;
+    h.s = (int32_t)s;
+    h.xp = sa.sx[s]; h.yp = sa.sy[s]; h.zp = sa.sz[s]; h.rp = sa.sr[s];
+    h.bp = sa.sbox[s];
+    h.pslot = sa.sorted[s];
+    h.idp = sa.sid[s];
+    h.perx = I.periodicity != 0;
+    h.xpf = (float)h.xp; h.ypf = (float)h.yp; h.zpf = (float)h.zp; h.rpf = (float)h.rp;
+    h.lxf = (float)I.lx; h.lyf = (float)I.ly; h.lzf = (float)I.lz;
+    const int nfx = I.nfx, nfy = I.nfy, nfz = I.nfz;
+    // the binning pass's own cell of this particle (same inputs, same function)
+    const int cx = cell_coord(h.xp, I.hfx, nfx), cy = cell_coord(h.yp, I.hfy, nfy), cz = cell_coord(h.zp, I.hfz, nfz);
+    const int64_t lc = ((int64_t)cz * nfy + cy) * nfx + cx;
+    if (sa.spk[s].w >= 0.f) {
+      for (int r = 0; r < 5; ++r) {
+        int ry = cy, rz = cz, lo = cx - 1, hi = cx + 1;
+        if (r == 0) {
+          lo = hi = cx + 1;                    // the rest of the home cell is swept below
+        } else if (r == 1) {
+          ry = wrap_cell(cy + 1, nfy);
         } else {
-          const int idx = (di + 1) * 9 + (dj + 1) * 3 + (dk + 1);
-          slot = c_fwd_slot[idx];
-          if (slot > 0) {
-            home_is_p = true;
-            hb = bp;
-          } else {
-            slot = c_fwd_slot[26 - idx];
-            home_is_p = false;
-            hb = bq;
-          }
+          rz = wrap_cell(cz + 1, nfz);
+          ry = wrap_cell(cy + (r - 3), nfy);
         }
-        const int hi = (int)(hb & 0x1FFFFF), hj = (int)((hb >> 21) & 0x1FFFFF), hk = (int)(hb >> 42);
-        const unsigned long long ijk =
-            (unsigned long long)(hi + 1) + (unsigned long long)hj * I.nxbox + (unsigned long long)hk * I.nxbox * I.nybox;
-        const int32_t idh = home_is_p ? idp : idq, idn = home_is_p ? idq : idp;
-        r.home = home_is_p ? pslot : sa.sorted[qs];
-        r.near = home_is_p ? sa.sorted[qs] : pslot;
-        r.k1 = ijk;
-        r.k2 = ((unsigned long long)idh << 34) | ((unsigned long long)slot << 30) | (unsigned long long)idn;
-        emit_pair(pairs, npairs, cap, r, st);
+        const int64_t base = I.cell_begin + ((int64_t)rz * nfy + ry) * nfx;
+        RowRanges rr = row_ranges(sa, base, nfx, lo, hi, h.perx);
+        if (r == 0) {
+          // home cell from s+1, contiguous with cell cx+1 when that is not wrapped
+          if (rr.a1 == 0 && rr.a0 == 0) rr.a1 = sa.cell_start[I.cell_begin + lc + 1];
+          rr.a0 = (int32_t)s + 1;
+        }
+        for (int32_t qs = rr.a0; qs < rr.a1; ++qs) search_candidate<false>(I, sa, h, qs, pairs, npairs, cap, st);
+        for (int32_t qs = rr.b0; qs < rr.b1; ++qs) search_candidate<false>(I, sa, h, qs, pairs, npairs, cap, st);
+      }
+    } else {
+      const double reach = (h.rp + I.rmax) * (1.0 + 1.0e-6);
+      const int rx = (int)ceil(reach / I.hfx), ry = (int)ceil(reach / I.hfy), rz = (int)ceil(reach / I.hfz);
+      const bool ally = 2 * ry + 1 >= nfy, allz = 2 * rz + 1 >= nfz;
+      const int y0 = ally ? 0 : cy - ry, y1 = ally ? nfy - 1 : cy + ry;
+      const int z0 = allz ? 0 : cz - rz, z1 = allz ? nfz - 1 : cz + rz;
+      const int lo = (2 * rx + 1 >= nfx) ? 0 : cx - rx, hi = (2 * rx + 1 >= nfx) ? nfx - 1 : cx + rx;
+      for (int zz = z0; zz <= z1; ++zz) {
+        const int wz = wrap_cell(zz, nfz);
+        for (int yy = y0; yy <= y1; ++yy) {
+          const int wy = wrap_cell(yy, nfy);
+          const int64_t base = I.cell_begin + ((int64_t)wz * nfy + wy) * nfx;
+          const RowRanges rr = row_ranges(sa, base, nfx, lo, hi, h.perx || (2 * rx + 1 >= nfx));
+          for (int32_t qs = rr.a0; qs < rr.a1; ++qs)
+            if (qs != s) search_candidate<true>(I, sa, h, qs, pairs, npairs, cap, st);
+          for (int32_t qs = rr.b0; qs < rr.b1; ++qs)
+            if (qs != s) search_candidate<true>(I, sa, h, qs, pairs, npairs, cap, st);
+        }
       }
     }
   }

@@ -24,6 +24,7 @@ struct InstDev {
   // search grid (cell edge >= 2 * largest bounding radius)
   int32_t nfx, nfy, nfz, pad1;
   double hfx, hfy, hfz, rmax;
+  double rcut;                // particles with a larger bounding radius search a wider stencil
   int64_t cell_begin;         // first cell of this instance in the global cell arrays
 };
 
@@ -32,6 +33,7 @@ struct InstDev {
 constexpr int kNState = 13;   // x y z u v w qa qb qc qd ox oy oz
 constexpr int kNConst = 10;   // a b deq cdrag cpitch crot h5 ipxx ipyy ipzz
 constexpr int kNFluid = 6;    // ufap vfap wfap vortx vorty vortz
+constexpr int kFieldStride = 8; // field slots per grid point: the six components, padded
 
 struct PoolView {
   double *st[kNState];

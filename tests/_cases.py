@@ -43,11 +43,21 @@ def case(name: str):
         f = field.generate(48, seed=9, device="cpu")
         spec = config.ParticleSpec(n=8000, ar_range=(0.2, 5.0), b_lognormal=(np.log(0.01), 0.3),
                                    st_uniform=(0.1, 10.0), seed=4)
+    elif name == "bimodal":
+        # 20000 small spheroids and a dozen large ones (0.06%): the large ones exceed the
+        # search grid's one-cell reach and take the wide-stencil path
+        setup = config.Setup(nx=48, ny=48, nz=48, visc=0.05, dtime=1e-3)
+        f = field.generate(48, seed=13, device="cpu")
+        spec = config.ParticleSpec(n=20000, ar_range=(0.5, 2.0), b=0.02, st=1.0, seed=21)
+        big = config.ParticleSpec(n=12, ar_range=(0.4, 3.0), b=0.08, st=1.0, seed=22)
     else:
         raise KeyError(name)
     fn = {k: v.numpy().copy() for k, v in f.items()}
     refs = field_refs(f)
     st = init_state(setup, spec, f, refs)
+    if name == "bimodal":
+        st_big = init_state(setup, big, f, refs)
+        st = {k: np.concatenate([st[k], st_big[k]]) for k in st}
     return setup, fn, refs, st
 
 

@@ -56,7 +56,7 @@ def test_one_step_advance():
         assert np.array_equal(got[k], ens.a[k]), k
 
 
-@pytest.mark.parametrize("name", ["dense", "poly", "c1"])
+@pytest.mark.parametrize("name", ["dense", "poly", "c1", "bimodal"])
 def test_collision_pairs_bit_exact(name):
     """Same pre-collision state -> identical accepted pairs in identical order."""
     setup, fn, refs, st = case(name)
@@ -72,6 +72,8 @@ def test_collision_pairs_bit_exact(name):
         got = ctx.download()
     assert cnt["n_contact"] == par["n_contacts"]
     assert home.size == res["n_coll"]
+    if name == "bimodal":   # the large particles (the last 12) take part in collisions
+        assert np.any(home >= ens.n - 12) or np.any(near >= ens.n - 12)
     assert np.array_equal(home, res["home"]) and np.array_equal(near, res["near"])
     assert rel_err(got, ens.a, api.STATE_KEYS) < REL_TOL
 
