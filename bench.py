@@ -48,12 +48,29 @@ def parse():
 # ---------------------------------------------------------------------------
 # workload construction
 # ---------------------------------------------------------------------------
-def build_inputs(w, device, precision):
+def x_margin_for(w, steps: int) -> float:
+    """Distance from the x planes at which the run's particles start.
+
+    The reference tests every particle against the planes x = 0 and x = L even in a
+    periodic box (adv_particle_new.f90:331-336,555-560) and rebounds the ones that reach
+    them.  At dt = 5e-4 the spin such a rebound gives a slender spheroid (about 7e3 rad/s
+    about its axis) makes the explicit RK2 update of the angular velocity grow about
+    five-fold per step until the drag coefficient is NaN and the run stops ('In Fluid
+    force'); the FP64 path, which follows the reference bit for bit, stops on the same
+    particle at the same step.  So the benchmark keeps every particle further from the
+    x planes than a particle moving at 6 u' (beyond the fluid's largest velocity
+    component) travels in the steps of the run."""
+    return min(w.setup().lx / 4.0, 1.1 * 6.0 * w.dtime * steps)
+
+
+def build_inputs(w, device, precision, steps: int = 0):
+    import dataclasses
     import torch
     from gazpart_b200 import field, particles
     setup = w.setup()
     f = field.generate(w.grid, seed=w.field_seed, device=device)
-    st = particles.draw(w.spec, setup)
+    spec = dataclasses.replace(w.spec, x_margin=x_margin_for(w, steps)) if steps else w.spec
+    st = particles.draw(spec, setup)
     return setup, f, st
 
 
@@ -149,14 +166,19 @@ def reduce_max_ms(ms: float, dist, device) -> float:
     return float(t.item())
 
 
-def advance_bytes_per_particle(components: int, field_bytes: int) -> int:
-    """Algorithmic bytes of one particle-step of the fused advance kernel.
+def gather_bytes_per_particle(components: int, field_bytes: int) -> int:
+    """Algorithmic bytes of one particle in the stencil-gather kernel (k_gather_move):
+    64 stencil points x C components x field word, the position read (24 B) and the C
+    interpolated values written (8 B each, as the reference stores them).  No credit is
+    taken for stencil reuse between particles; the reordering copy of the particle
+    record that the kernel also performs is not algorithmic and is not counted."""
+    return 64 * components * field_bytes + 24 + 8 * components
 
-    Gather: 64 stencil points x C components x field word, positions read (24 B) and the
-    interpolated values (8 B each, as the reference stores them); plus the particle state
-    read and written (13 doubles each way) and the per-particle constants (6 doubles)."""
-    gather = 64 * components * field_bytes + 24 + 8 * components
-    return gather + 256
+
+# DRAM bytes (read + write) per particle of one k_gather_move launch, from ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum) on the steady-state step; the file
+# under profiles/ named in the value gives the command and the capture.
+GATHER_TRAFFIC = {}
 
 
 # ---------------------------------------------------------------------------
@@ -228,7 +250,7 @@ def main():
         threads = os.cpu_count() or 1
         scale = 16 if w.grid >= 256 else 1
         max_emaj = workload_max_emaj(w)
-        k = max(1, min(args.steps, 8))
+        k = max(1, min(args.steps, 4))
         if args.warmup:
             time_cpu(w, 1, threads, scale, max_emaj)
         r = time_cpu(w, k, threads, scale, max_emaj)
@@ -257,7 +279,8 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device(device))
 
-    setup, f, st = build_inputs(w, device, precision)
+    run_steps = args.warmup + args.steps + args.e2e_steps
+    setup, f, st = build_inputs(w, device, precision, run_steps)
     max_emaj = float(st["emaj"].max())
     ctx = make_context(setup, f, st, precision, device)
     n = ctx.n
@@ -268,7 +291,9 @@ def main():
         dist.barrier()
     torch.cuda.synchronize()
     with Clocks(local) as clk:
-        total_ms, adv_ms, col_ms, kps = ctx.step_timed(args.steps)
+        total_ms, phases, kps = ctx.step_timed(args.steps)
+    adv_ms = phases["gather"] + phases["integrate"]
+    col_ms = sum(phases.values()) - adv_ms
     clocks = clk.summary()
     ctx.raise_status("timed steps")
     torch.cuda.synchronize()
@@ -278,15 +303,17 @@ def main():
     ms_per_step = total_ms / args.steps
     value = n * world * args.steps / (total_ms / 1e3)
 
-    # roofline of the dominant kernel (the fused advance)
+    # roofline of the HBM-bound kernel of the step: the stencil gather (the phase
+    # timestamps around it bracket that one kernel on the library's stream)
     fbytes = 4 if precision == "mixed" else 8
-    bpp = advance_bytes_per_particle(6, fbytes)
+    bpp = gather_bytes_per_particle(6, fbytes)
     peak, peak_kind = hbm_peak()
-    achieved = bpp * n / (adv_ms / 1e3) / 1e9
-    roofline = {"bound": "hbm", "kernel": "k_advance", "achieved": achieved, "peak": peak, "unit": "GB/s",
+    achieved = bpp * n / (phases["gather"] / 1e3) / 1e9
+    tr = GATHER_TRAFFIC.get((w.name, precision))
+    roofline = {"bound": "hbm", "kernel": "k_gather_move", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": peak_kind,
-                "bytes_per_launch": bpp * n, "bytes_per_particle": bpp,
-                "advance_ms": adv_ms, "collision_ms": col_ms, "traffic": None}
+                "bytes_per_launch": bpp * n, "bytes_per_particle": bpp, "kernel_ms": phases["gather"],
+                "traffic": None if tr is None else tr[0] * n, "traffic_source": None if tr is None else tr[1]}
 
     # end to end through the C ABI with host buffers: H2D of the state, one step,
     # D2H of the state, every step
@@ -309,14 +336,14 @@ def main():
         ctx.close()
         del ctx
         torch.cuda.empty_cache()
-        st2 = build_inputs(w, device, "fp64")[2]
+        st2 = build_inputs(w, device, "fp64", run_steps)[2]
         f64 = {k: v for k, v in f.items()}
         pctx = make_context(setup, f64, st2, "fp64", device)
         pctx.step(max(1, args.warmup))
         pctx.sync()
-        tms, pa, pc, _ = pctx.step_timed(max(5, args.steps // 5))
+        tms, pph, _ = pctx.step_timed(max(5, args.steps // 5))
         pctx.raise_status("fp64 steps")
-        plain = {"value": n * max(5, args.steps // 5) / (tms / 1e3), "advance_ms": pa, "collision_ms": pc}
+        plain = {"value": n * max(5, args.steps // 5) / (tms / 1e3), "phase_ms": pph}
         pctx.close()
     else:
         ctx.close()
@@ -338,9 +365,11 @@ def main():
                 "data": "synthetic",
                 "config": {"workload": w.name, "precision": precision, "particles_per_gpu": n,
                            "field": f"{w.grid}^3 x 6 {'f32' if fbytes == 4 else 'f64'}",
-                           "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (state+field > 5 GB)"},
+                           "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (state+field > 5 GB)",
+                           "x_margin": x_margin_for(w, run_steps)},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": kps * args.steps,
-                "kernels_per_step": kps, "clocks": clocks, "fp64_plain": plain}
+                "kernels_per_step": kps, "phase_ms": phases, "advance_ms": adv_ms, "collision_ms": col_ms,
+                "clocks": clocks, "fp64_plain": plain}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

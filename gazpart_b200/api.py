@@ -165,13 +165,14 @@ class Context:
         check(_lib.lib().gp_download_state(self._h, self.n, cols, None, 0), "gp_download_state")
 
     def step_timed(self, nsteps: int):
-        """Run nsteps with device events around each phase.
+        """Run nsteps as one graph with device timestamps between the phases.
 
-        Returns (total_ms, advance_ms per step, collision_ms per step, kernels per step)."""
-        t, a, c, k = C.c_float(), C.c_float(), C.c_float(), C.c_int32()
-        check(_lib.lib().gp_step_timed(self._h, nsteps, C.byref(t), C.byref(a), C.byref(c), C.byref(k)),
-              "gp_step_timed")
-        return t.value, a.value, c.value, k.value
+        Returns (total_ms, {phase: ms per step}, kernels per step); the phases are
+        _lib.PHASES (gather, integrate, bin, search, contact, response)."""
+        t, k = C.c_float(), C.c_int32()
+        ph = (C.c_float * len(_lib.PHASES))()
+        check(_lib.lib().gp_step_timed(self._h, nsteps, C.byref(t), ph, C.byref(k)), "gp_step_timed")
+        return t.value, dict(zip(_lib.PHASES, (float(v) for v in ph))), k.value
 
     def download(self, fluid: bool = False) -> Dict[str, np.ndarray]:
         out = {k: np.empty(self.n) for k in STATE_KEYS}

@@ -88,6 +88,9 @@ class ParticleSpec:
     st_loguniform: Optional[Tuple[float, float]] = None
     density_ratio: float = 1000.0
     seed: int = 1
+    # distance kept between the particles and the x = 0 and x = L planes at t = 0 (at
+    # least the particle's own largest semi-axis)
+    x_margin: float = 0.0
 
     def reference_shape(self) -> Tuple[float, float]:
         """(AR, b) of the median particle, used to fix the viscosity."""

@@ -83,6 +83,8 @@ struct ClassProps {
 struct gp_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
+  // phase boundaries recorded while a timed step is captured (null otherwise)
+  cudaEvent_t *marks = nullptr;
   gp_params prm{};
   double ppi = 0.0;
   // field
@@ -280,15 +282,24 @@ int setup_grids(gp_ctx *c, double max_emaj, double rmax, double rsmall) {
   return GP_OK;
 }
 
+// Records the boundary after phase `phase` of a timed step (an external record is a
+// timestamp node of the captured graph).
+int mark(gp_ctx *c, int phase) {
+  if (!c->marks) return GP_OK;
+  GP_CK(cudaEventRecordWithFlags(c->marks[phase], c->stream, cudaEventRecordExternal));
+  return GP_OK;
+}
+
 int enqueue_advance(gp_ctx *c) {
+  cudaEvent_t mid = c->marks ? c->marks[GP_PHASE_GATHER] : nullptr;
   if (c->prm.precision == GP_PREC_MIXED)
     launch_advance_mixed(c->d_inst, c->d_pv, c->d_pv_alt, c->sa.sorted, c->n, c->d_fluid_cols, c->d_status,
-                         c->grid, c->stream);
+                         c->grid, mid, c->stream);
   else
     launch_advance_fp64(c->d_inst, c->d_pv, c->d_pv_alt, c->sa.sorted, c->n, c->d_fluid_cols, c->d_status,
-                        c->grid, c->stream);
+                        c->grid, mid, c->stream);
   GP_CK(cudaGetLastError());
-  return GP_OK;
+  return mark(c, GP_PHASE_INTEGRATE);
 }
 
 int enqueue_collision(gp_ctx *c) {
@@ -299,15 +310,18 @@ int enqueue_collision(gp_ctx *c) {
   launch_bin_count(c->d_inst, c->d_pv, c->n, sa, c->d_status, c->grid, c->stream);
   launch_scan(sa.cell_count, sa.cell_start, c->ncells, c->d_scan_tmp, c->stream);
   launch_bin_scatter(c->d_inst, c->d_pv, c->n, sa, c->d_status, c->grid, c->stream);
+  GP_TRY(mark(c, GP_PHASE_BIN));
   launch_search(c->d_inst, c->n, sa, c->d_pairs, c->d_counters + 0, c->cap_pairs, c->d_status, c->grid, c->stream);
+  GP_TRY(mark(c, GP_PHASE_SEARCH));
   launch_contact(c->d_inst, c->d_pv, c->d_pairs, c->d_counters + 0, c->cap_pairs, c->d_coll, c->d_counters + 1,
                  c->cap_coll, c->d_counters + 3, c->d_status, c->contact_grid, c->stream);
+  GP_TRY(mark(c, GP_PHASE_CONTACT));
   launch_match(c->d_coll, c->d_counters + 1, c->cap_coll, c->d_best1, c->d_best2, c->d_matched, c->d_state,
                c->d_status, c->stream);
   launch_response(c->d_inst, c->d_pv, c->d_coll, c->d_counters + 1, c->cap_coll, c->d_state, c->d_acc,
                   c->d_counters + 2, c->d_status, c->grid, c->stream);
   GP_CK(cudaGetLastError());
-  return GP_OK;
+  return mark(c, GP_PHASE_RESPONSE);
 }
 
 int read_status(gp_ctx *c, Status *h) {
@@ -576,26 +590,22 @@ int gp_step(gp_ctx *c, int32_t nsteps) {
   return GP_OK;
 }
 
-int gp_step_timed(gp_ctx *c, int32_t nsteps, float *total_ms, float *advance_ms_avg, float *collision_ms_avg,
-                  int32_t *kernels_per_step) {
+int gp_step_timed(gp_ctx *c, int32_t nsteps, float *total_ms, float *phase_ms_avg, int32_t *kernels_per_step) {
   if (!c || c->n <= 0 || !c->grid_ready || nsteps <= 0) return GP_EBADARG;
-  std::vector<cudaEvent_t> ev(2 * (size_t)nsteps + 1);
+  // event 0 opens the run; step s closes phase p with event 1 + s * GP_NPHASE + p
+  std::vector<cudaEvent_t> ev(1 + (size_t)nsteps * GP_NPHASE);
   for (auto &e : ev) GP_CK(cudaEventCreate(&e));
   cudaGraph_t g;
   cudaGraphExec_t ge = nullptr;
   GP_CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
   int rc = GP_OK;
+  if (cudaEventRecordWithFlags(ev[0], c->stream, cudaEventRecordExternal) != cudaSuccess) rc = GP_ECUDA;
   for (int s = 0; s < nsteps && !rc; ++s) {
-    // external records: real timestamp nodes in the graph (a plain record inside a
-    // capture only orders work)
-    if (cudaEventRecordWithFlags(ev[2 * s], c->stream, cudaEventRecordExternal) != cudaSuccess) rc = GP_ECUDA;
-    if (!rc) rc = enqueue_advance(c);
-    if (!rc && cudaEventRecordWithFlags(ev[2 * s + 1], c->stream, cudaEventRecordExternal) != cudaSuccess)
-      rc = GP_ECUDA;
+    c->marks = ev.data() + 1 + (size_t)s * GP_NPHASE;
+    rc = enqueue_advance(c);
     if (!rc) rc = enqueue_collision(c);
   }
-  if (!rc && cudaEventRecordWithFlags(ev[2 * nsteps], c->stream, cudaEventRecordExternal) != cudaSuccess)
-    rc = GP_ECUDA;
+  c->marks = nullptr;
   cudaError_t e = cudaStreamEndCapture(c->stream, &g);
   if (!rc && e != cudaSuccess) rc = GP_ECUDA;
   if (!rc && kernels_per_step) {
@@ -615,18 +625,18 @@ int gp_step_timed(gp_ctx *c, int32_t nsteps, float *total_ms, float *advance_ms_
   if (!rc && cudaGraphLaunch(ge, c->stream) != cudaSuccess) rc = GP_ECUDA;
   if (!rc && cudaStreamSynchronize(c->stream) != cudaSuccess) rc = GP_ECUDA;
   if (!rc) {
-    double adv = 0.0, col = 0.0;
+    double acc[GP_NPHASE] = {};
     float t = 0.f;
-    for (int s = 0; s < nsteps && !rc; ++s) {
-      if (cudaEventElapsedTime(&t, ev[2 * s], ev[2 * s + 1]) != cudaSuccess) rc = GP_ECUDA;
-      adv += t;
-      if (cudaEventElapsedTime(&t, ev[2 * s + 1], ev[2 * s + 2]) != cudaSuccess) rc = GP_ECUDA;
-      col += t;
-    }
-    if (cudaEventElapsedTime(&t, ev[0], ev[2 * nsteps]) != cudaSuccess) rc = GP_ECUDA;
-    if (total_ms) *total_ms = t;
-    if (advance_ms_avg) *advance_ms_avg = (float)(adv / nsteps);
-    if (collision_ms_avg) *collision_ms_avg = (float)(col / nsteps);
+    for (int s = 0; s < nsteps && !rc; ++s)
+      for (int p = 0; p < GP_NPHASE && !rc; ++p) {
+        const size_t k = 1 + (size_t)s * GP_NPHASE + p;
+        if (cudaEventElapsedTime(&t, ev[k - 1], ev[k]) != cudaSuccess) rc = GP_ECUDA;
+        acc[p] += t;
+      }
+    if (!rc && cudaEventElapsedTime(&t, ev[0], ev.back()) != cudaSuccess) rc = GP_ECUDA;
+    if (!rc && total_ms) *total_ms = t;
+    if (!rc && phase_ms_avg)
+      for (int p = 0; p < GP_NPHASE; ++p) phase_ms_avg[p] = (float)(acc[p] / nsteps);
   }
   if (ge) cudaGraphExecDestroy(ge);
   for (auto &x : ev) cudaEventDestroy(x);

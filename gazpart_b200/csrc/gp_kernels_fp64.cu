@@ -18,8 +18,9 @@ template __global__ void k_integrate<false>(const InstDev *, const PoolView *, i
 
 void launch_advance_fp64(const InstDev *insts, PoolView *pv, PoolView *pv_alt, const int32_t *perm, int64_t n,
                          double *const *fluid, Status *st,
-                         int grid, cudaStream_t s) {
+                         int grid, cudaEvent_t after_gather, cudaStream_t s) {
   k_gather_move<false><<<148 * GP_GATHER_BLOCKS_PER_SM, 256, 0, s>>>(insts, pv, pv_alt, perm, n, fluid, st);
+  if (after_gather) cudaEventRecordWithFlags(after_gather, s, cudaEventRecordExternal);
   k_swap_pool<<<1, 1, 0, s>>>(pv, pv_alt);
   k_integrate<false><<<grid, 128, 0, s>>>(insts, pv, n, fluid, st);
 }

@@ -11,7 +11,7 @@ namespace gp {
 // ADV_PARTICLE_ELLP: advances particle perm[j] of *pv into slot j of *pv_alt, then swaps
 // the two views (so *pv is current afterwards).
 void launch_advance_fp64(const InstDev *insts, PoolView *pv, PoolView *pv_alt, const int32_t *perm, int64_t n,
-                         double *const *fluid, Status *st, int grid, cudaStream_t s);
+                         double *const *fluid, Status *st, int grid, cudaEvent_t after_gather, cudaStream_t s);
 void launch_interp(const InstDev *inst, int comp, int64_t n, const double *x, const double *y, const double *z,
                    double *out, Status *st, cudaStream_t s);
 void launch_frozen_interp(const double *xain, const double *yain, const double *zain, int nx, int ny, int nz,
@@ -41,7 +41,7 @@ void launch_response_batch(int64_t n, double ecp, double mup, const double *ip /
 
 // --- gp_kernels_mixed.cu ---
 void launch_advance_mixed(const InstDev *insts, PoolView *pv, PoolView *pv_alt, const int32_t *perm, int64_t n,
-                          double *const *fluid, Status *st, int grid, cudaStream_t s);
+                          double *const *fluid, Status *st, int grid, cudaEvent_t after_gather, cudaStream_t s);
 void launch_iota(int32_t *a, int64_t n, cudaStream_t s);
 
 // --- gp_search.cu ---

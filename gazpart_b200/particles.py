@@ -72,7 +72,8 @@ def draw(spec: ParticleSpec, setup: Setup) -> Dict[str, np.ndarray]:
     # (initiation_particle_position.f90:309-316), with the largest semi-axis in place of
     # EMAJ so that no particle starts across the x planes that the wall test watches
     r = np.maximum(emaj, emaj / apr)
-    out["x"] = rx * (setup.lx - 2.0 * r) + r
+    rx_margin = np.maximum(r, spec.x_margin)
+    out["x"] = rx * (setup.lx - 2.0 * rx_margin) + rx_margin
     out["y"] = ry * (setup.ly - 2.0 * r) + r
     out["z"] = rz * (setup.lz - 2.0 * r) + r
     out["emaj"] = emaj

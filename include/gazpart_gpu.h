@@ -144,12 +144,23 @@ int gp_collision(gp_ctx *ctx, int32_t ncycle, double time, int64_t *n_near,
                  int64_t *n_contact, int64_t *n_coll);
 /* nsteps x (ADV_PARTICLE_ELLP + COLLISION) replayed from a captured CUDA graph. */
 int gp_step(gp_ctx *ctx, int32_t nsteps);
-/* nsteps steps with CUDA events recorded on the context's stream around every
- * phase; returns the total and, per step on average, the ADV_PARTICLE_ELLP kernel and
- * the collision phase durations in milliseconds, and the number of kernels one step
- * launches (counted from the captured graph).  Any output pointer may be NULL. */
-int gp_step_timed(gp_ctx *ctx, int32_t nsteps, float *total_ms, float *advance_ms_avg,
-                  float *collision_ms_avg, int32_t *kernels_per_step);
+/* Phases of one step, in launch order, as timed by gp_step_timed. */
+enum {
+    GP_PHASE_GATHER = 0,     /* stencil gather at x_n and the move into cell order */
+    GP_PHASE_INTEGRATE = 1,  /* RK2 predictor/corrector, walls, periodic wrap */
+    GP_PHASE_BIN = 2,        /* search-grid binning: count, scan, scatter */
+    GP_PHASE_SEARCH = 3,     /* candidate pairs */
+    GP_PHASE_CONTACT = 4,    /* contact solves and NVREL test */
+    GP_PHASE_RESPONSE = 5,   /* greedy acceptance and impulse response */
+    GP_NPHASE = 6
+};
+/* nsteps steps captured as one CUDA graph with timestamp nodes between the phases;
+ * returns the total and, per step on average, each phase's duration in milliseconds
+ * (phase_ms_avg: GP_NPHASE floats), and the number of kernels one step launches
+ * (counted from the captured graph).  Any output pointer may be NULL.  No counterpart
+ * in the reference (measurement). */
+int gp_step_timed(gp_ctx *ctx, int32_t nsteps, float *total_ms, float *phase_ms_avg,
+                  int32_t *kernels_per_step);
 /* Last step's accepted collisions as (home, near) original indices, in acceptance
  * (list) order; *count receives the total even if it exceeds cap. */
 int gp_collision_pairs(gp_ctx *ctx, int64_t cap, int32_t *home, int32_t *near, int64_t *count);
