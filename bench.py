@@ -178,7 +178,9 @@ def gather_bytes_per_particle(components: int, field_bytes: int) -> int:
 # DRAM bytes (read + write) per particle of one k_gather_move launch, from ncu
 # (dram__bytes_read.sum + dram__bytes_write.sum) on the steady-state step; the file
 # under profiles/ named in the value gives the command and the capture.
-GATHER_TRAFFIC = {}
+GATHER_TRAFFIC = {
+    ("c3_512cube_n16777216_fp32field", "mixed"): (1092.0, "profiles/k_gather_move_k_integrate_c3_dram.md"),
+}
 
 
 # ---------------------------------------------------------------------------
