@@ -478,19 +478,18 @@ __device__ __forceinline__ void gather_warp_fp32(const InstDev* __restrict__ ins
   }
 }
 
-// ADV_PARTICLE_ELLP, first half: particle perm[j] of the source buffer is moved to slot
-// j of the destination buffer (so that the pool follows the search-grid cell order of
-// the last binning and neighbouring stencils are gathered together) and the six field
-// components are interpolated at its position x_n (adv_particle_new.f90:139-206).  Any
-// permutation is correct: every particle carries its properties, id and instance.
-// kMixed: every instance holds an FP32 field (warp-cooperative gather); otherwise FP64
-// fields, gathered per lane in the reference's summation order.
+// ADV_PARTICLE_ELLP, first half: the six field components at x_n
+// (adv_particle_new.f90:139-206) of the particle that the next integrate pass will
+// place in slot j, perm[j] of the current buffer (the last binning's cell order, so
+// that neighbouring stencils are gathered together).  Reads only positions, instance
+// and id, so it may run while the collision phase updates velocities.  kMixed: every
+// instance holds an FP32 field (warp-cooperative gather); otherwise FP64 fields,
+// gathered per lane in the reference's summation order.
 template <bool kMixed>
-__global__ void __launch_bounds__(256) k_gather_move(const InstDev* __restrict__ insts,
-                                                     const PoolView* __restrict__ src_pv,
-                                                     const PoolView* __restrict__ dst_pv,
-                                                     const int32_t* __restrict__ perm, int64_t n,
-                                                     double* const* __restrict__ fluid, Status* st) {
+__global__ void __launch_bounds__(256) k_gather(const InstDev* __restrict__ insts,
+                                                const PoolView* __restrict__ src_pv,
+                                                const int32_t* __restrict__ perm, int64_t n,
+                                                double* const* __restrict__ fluid, Status* st) {
   const int lane = threadIdx.x & 31;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w * 32 < n; w += nwarps) {
@@ -500,13 +499,6 @@ __global__ void __launch_bounds__(256) k_gather_move(const InstDev* __restrict__
     if (j < n) {
       i = perm[j];
       inst = src_pv->inst[i];
-      dst_pv->inst[j] = inst;
-      dst_pv->id[j] = src_pv->id[i];
-      // one column pointer pair live at a time keeps the register count low
-#pragma unroll 1
-      for (int c = 0; c < kNState; ++c) dst_pv->st[c][j] = src_pv->st[c][i];
-#pragma unroll 1
-      for (int c = 0; c < kNConst; ++c) dst_pv->pc[c][j] = src_pv->pc[c][i];
     }
     int mode = 0;
     Stencil s;
@@ -536,43 +528,57 @@ __global__ void __launch_bounds__(256) k_gather_move(const InstDev* __restrict__
   }
 }
 
-// ADV_PARTICLE_ELLP, second half, in place on the (now cell-ordered) buffer: the RK2
-// predictor/corrector with wall handling (adv_particle_new.f90:268-637) and
-// BOUNDARY_PARTICLE's periodic wrap (boundary_particle.f90:50-59).
+// ADV_PARTICLE_ELLP, second half: particle perm[j] of the source buffer is advanced
+// and written to slot j of the destination buffer with its properties, id and
+// instance (any permutation is correct: every particle carries its own record).  The
+// RK2 predictor/corrector with wall handling (adv_particle_new.f90:268-637) and
+// BOUNDARY_PARTICLE's periodic wrap (boundary_particle.f90:50-59).  A particle whose
+// stencil left the field (NaN fluid values, reported by the gather) is copied unchanged.
 #ifndef GP_INTEGRATE_MIN_BLOCKS
 #define GP_INTEGRATE_MIN_BLOCKS 1
 #endif
 template <bool kMixed>
-__global__ void __launch_bounds__(128, GP_INTEGRATE_MIN_BLOCKS) k_integrate(const InstDev* __restrict__ insts, const PoolView* __restrict__ pv,
-                                                   int64_t n, const double* const* __restrict__ fluid, Status* st) {
-  const PoolView P = *pv;
+__global__ void __launch_bounds__(128, GP_INTEGRATE_MIN_BLOCKS) k_integrate(const InstDev* __restrict__ insts,
+                                                                           const PoolView* __restrict__ src_pv,
+                                                                           const PoolView* __restrict__ dst_pv,
+                                                                           const int32_t* __restrict__ perm, int64_t n,
+                                                                           const double* const* __restrict__ fluid,
+                                                                           Status* st) {
+  const PoolView* __restrict__ S = src_pv;
+  const PoolView* __restrict__ D = dst_pv;
   for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
-    const int inst = P.inst[j];
-    if (inst < 0) continue;
-    const InstDev& I = insts[inst];
+    const int64_t i = perm[j];
+    const int inst = S->inst[i];
+    D->inst[j] = inst;
+    D->id[j] = S->id[i];
+    PartConst pc;
+    load_pc(*S, i, pc);
+#pragma unroll 1
+    for (int c = 0; c < kNConst; ++c) D->pc[c][j] = S->pc[c][i];
+    double X[3] = {S->st[0][i], S->st[1][i], S->st[2][i]};
+    double U[3] = {S->st[3][i], S->st[4][i], S->st[5][i]};
+    Quat Q = {S->st[6][i], S->st[7][i], S->st[8][i], S->st[9][i]};
+    double O[3] = {S->st[10][i], S->st[11][i], S->st[12][i]};
     const double uf[3] = {fluid[0][j], fluid[1][j], fluid[2][j]};
     const double wv[3] = {fluid[3][j], fluid[4][j], fluid[5][j]};
-    if (uf[0] != uf[0] && wv[0] != wv[0]) continue;   // stencil out of range, reported by the gather
-    double X[3] = {P.st[0][j], P.st[1][j], P.st[2][j]};
-    double U[3] = {P.st[3][j], P.st[4][j], P.st[5][j]};
-    Quat Q = {P.st[6][j], P.st[7][j], P.st[8][j], P.st[9][j]};
-    double O[3] = {P.st[10][j], P.st[11][j], P.st[12][j]};
-    PartConst pc;
-    load_pc(P, j, pc);
-    const int err = advance_particle<kMixed>(I, pc, uf, wv, X, U, O, Q);
-    if (err) set_error(st, err, (long long)P.id[j]);
-    if (I.periodicity) {
-      if (X[0] > I.lx) X[0] = X[0] - I.lx;
-      if (X[0] < 0.) X[0] = X[0] + I.lx;
-      if (X[1] > I.ly) X[1] = X[1] - I.ly;
-      if (X[1] < 0.) X[1] = X[1] + I.ly;
-      if (X[2] > I.lz) X[2] = X[2] - I.lz;
-      if (X[2] < 0.) X[2] = X[2] + I.lz;
+    // stencil out of range (reported by the gather): carried over unchanged
+    if (inst >= 0 && !(uf[0] != uf[0] && wv[0] != wv[0])) {
+      const InstDev& I = insts[inst];
+      const int err = advance_particle<kMixed>(I, pc, uf, wv, X, U, O, Q);
+      if (err) set_error(st, err, (long long)S->id[i]);
+      if (I.periodicity) {
+        if (X[0] > I.lx) X[0] = X[0] - I.lx;
+        if (X[0] < 0.) X[0] = X[0] + I.lx;
+        if (X[1] > I.ly) X[1] = X[1] - I.ly;
+        if (X[1] < 0.) X[1] = X[1] + I.ly;
+        if (X[2] > I.lz) X[2] = X[2] - I.lz;
+        if (X[2] < 0.) X[2] = X[2] + I.lz;
+      }
     }
-    P.st[0][j] = X[0]; P.st[1][j] = X[1]; P.st[2][j] = X[2];
-    P.st[3][j] = U[0]; P.st[4][j] = U[1]; P.st[5][j] = U[2];
-    P.st[6][j] = Q.a; P.st[7][j] = Q.b; P.st[8][j] = Q.c; P.st[9][j] = Q.d;
-    P.st[10][j] = O[0]; P.st[11][j] = O[1]; P.st[12][j] = O[2];
+    D->st[0][j] = X[0]; D->st[1][j] = X[1]; D->st[2][j] = X[2];
+    D->st[3][j] = U[0]; D->st[4][j] = U[1]; D->st[5][j] = U[2];
+    D->st[6][j] = Q.a; D->st[7][j] = Q.b; D->st[8][j] = Q.c; D->st[9][j] = Q.d;
+    D->st[10][j] = O[0]; D->st[11][j] = O[1]; D->st[12][j] = O[2];
   }
 }
 

@@ -83,7 +83,12 @@ struct ClassProps {
 struct gp_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
-  // phase boundaries recorded while a timed step is captured (null otherwise)
+  // Second stream of a multi-step graph: the next step's stencil gather runs there
+  // while the collision phase finishes on `stream`.
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // phase begin/end timestamps of the step being captured by gp_step_timed
+  // ([2p] begin, [2p+1] end of phase p; null otherwise)
   cudaEvent_t *marks = nullptr;
   gp_params prm{};
   double ppi = 0.0;
@@ -123,8 +128,8 @@ struct gp_ctx {
   double *d_scratch = nullptr;
   size_t scratch_count = 0;
   std::map<std::pair<int, int>, ClassProps> classes;
-  // graph
-  cudaGraphExec_t graph = nullptr;
+  // captured multi-step graphs, by step count
+  std::map<int, cudaGraphExec_t> graphs;
   int grid = 148 * 4;
   int contact_grid = 148 * 4;   // persistent k_contact grid (resident blocks)
 };
@@ -141,8 +146,8 @@ int ensure_scratch(gp_ctx *c, size_t count) {
 }
 
 void drop_graph(gp_ctx *c) {
-  if (c->graph) cudaGraphExecDestroy(c->graph);
-  c->graph = nullptr;
+  for (auto &g : c->graphs) cudaGraphExecDestroy(g.second);
+  c->graphs.clear();
 }
 
 int upload_inst(gp_ctx *c) {
@@ -282,46 +287,108 @@ int setup_grids(gp_ctx *c, double max_emaj, double rmax, double rsmall) {
   return GP_OK;
 }
 
-// Records the boundary after phase `phase` of a timed step (an external record is a
-// timestamp node of the captured graph).
-int mark(gp_ctx *c, int phase) {
+// Records timestamp `slot` of the step being timed (an external record is a timestamp
+// node of the captured graph); a no-op outside gp_step_timed.
+int mark(gp_ctx *c, int slot, cudaStream_t s) {
   if (!c->marks) return GP_OK;
-  GP_CK(cudaEventRecordWithFlags(c->marks[phase], c->stream, cudaEventRecordExternal));
+  GP_CK(cudaEventRecordWithFlags(c->marks[slot], s, cudaEventRecordExternal));
   return GP_OK;
 }
 
-int enqueue_advance(gp_ctx *c) {
-  cudaEvent_t mid = c->marks ? c->marks[GP_PHASE_GATHER] : nullptr;
+// Stencil gather at x_n for the particles in the last binning's order, on stream s.
+int enqueue_gather(gp_ctx *c, cudaStream_t s) {
+  GP_TRY(mark(c, 2 * GP_PHASE_GATHER, s));
   if (c->prm.precision == GP_PREC_MIXED)
-    launch_advance_mixed(c->d_inst, c->d_pv, c->d_pv_alt, c->sa.sorted, c->n, c->d_fluid_cols, c->d_status,
-                         c->grid, mid, c->stream);
+    launch_gather_mixed(c->d_inst, c->d_pv, c->sa.sorted, c->n, c->d_fluid_cols, c->d_status, s);
   else
-    launch_advance_fp64(c->d_inst, c->d_pv, c->d_pv_alt, c->sa.sorted, c->n, c->d_fluid_cols, c->d_status,
-                        c->grid, mid, c->stream);
+    launch_gather_fp64(c->d_inst, c->d_pv, c->sa.sorted, c->n, c->d_fluid_cols, c->d_status, s);
   GP_CK(cudaGetLastError());
-  return mark(c, GP_PHASE_INTEGRATE);
+  return mark(c, 2 * GP_PHASE_GATHER + 1, s);
 }
 
-int enqueue_collision(gp_ctx *c) {
+int enqueue_integrate(gp_ctx *c) {
+  GP_TRY(mark(c, 2 * GP_PHASE_INTEGRATE, c->stream));
+  if (c->prm.precision == GP_PREC_MIXED)
+    launch_integrate_mixed(c->d_inst, c->d_pv, c->d_pv_alt, c->sa.sorted, c->n, c->d_fluid_cols, c->d_status,
+                           c->grid, c->stream);
+  else
+    launch_integrate_fp64(c->d_inst, c->d_pv, c->d_pv_alt, c->sa.sorted, c->n, c->d_fluid_cols, c->d_status,
+                          c->grid, c->stream);
+  GP_CK(cudaGetLastError());
+  return mark(c, 2 * GP_PHASE_INTEGRATE + 1, c->stream);
+}
+
+int enqueue_advance(gp_ctx *c) {
+  GP_TRY(enqueue_gather(c, c->stream));
+  return enqueue_integrate(c);
+}
+
+// Binning of the search grid and the candidate-pair search.
+int enqueue_bin_search(gp_ctx *c) {
   SearchArrays sa = c->sa;
+  GP_TRY(mark(c, 2 * GP_PHASE_BIN, c->stream));
   GP_CK(cudaMemsetAsync(sa.cell_count, 0, (c->ncells + 1) * sizeof(int32_t), c->stream));
   GP_CK(cudaMemsetAsync(sa.cell_fill, 0, (c->ncells + 1) * sizeof(int32_t), c->stream));
   GP_CK(cudaMemsetAsync(c->d_counters, 0, 4 * sizeof(unsigned long long), c->stream));
   launch_bin_count(c->d_inst, c->d_pv, c->n, sa, c->d_status, c->grid, c->stream);
   launch_scan(sa.cell_count, sa.cell_start, c->ncells, c->d_scan_tmp, c->stream);
   launch_bin_scatter(c->d_inst, c->d_pv, c->n, sa, c->d_status, c->grid, c->stream);
-  GP_TRY(mark(c, GP_PHASE_BIN));
+  GP_TRY(mark(c, 2 * GP_PHASE_BIN + 1, c->stream));
+  GP_TRY(mark(c, 2 * GP_PHASE_SEARCH, c->stream));
   launch_search(c->d_inst, c->n, sa, c->d_pairs, c->d_counters + 0, c->cap_pairs, c->d_status, c->grid, c->stream);
-  GP_TRY(mark(c, GP_PHASE_SEARCH));
+  GP_CK(cudaGetLastError());
+  return mark(c, 2 * GP_PHASE_SEARCH + 1, c->stream);
+}
+
+// Contact solves, greedy acceptance and the impulse response.
+int enqueue_contact_response(gp_ctx *c) {
+  GP_TRY(mark(c, 2 * GP_PHASE_CONTACT, c->stream));
   launch_contact(c->d_inst, c->d_pv, c->d_pairs, c->d_counters + 0, c->cap_pairs, c->d_coll, c->d_counters + 1,
                  c->cap_coll, c->d_counters + 3, c->d_status, c->contact_grid, c->stream);
-  GP_TRY(mark(c, GP_PHASE_CONTACT));
+  GP_TRY(mark(c, 2 * GP_PHASE_CONTACT + 1, c->stream));
+  GP_TRY(mark(c, 2 * GP_PHASE_RESPONSE, c->stream));
   launch_match(c->d_coll, c->d_counters + 1, c->cap_coll, c->d_best1, c->d_best2, c->d_matched, c->d_state,
                c->d_status, c->stream);
   launch_response(c->d_inst, c->d_pv, c->d_coll, c->d_counters + 1, c->cap_coll, c->d_state, c->d_acc,
                   c->d_counters + 2, c->d_status, c->grid, c->stream);
   GP_CK(cudaGetLastError());
-  return mark(c, GP_PHASE_RESPONSE);
+  return mark(c, 2 * GP_PHASE_RESPONSE + 1, c->stream);
+}
+
+int enqueue_collision(gp_ctx *c) {
+  GP_TRY(enqueue_bin_search(c));
+  return enqueue_contact_response(c);
+}
+
+// nsteps x (ADV_PARTICLE_ELLP + COLLISION) for capture into one graph.  The response
+// changes only velocities and angular velocities, so the gather of step s+1, which
+// reads positions and the order of step s's binning, is forked onto the side stream
+// right after step s's search and overlaps its contact solves; step s+1's integrate
+// joins it.  marks: 2*GP_NPHASE timestamps per step, or null.
+int enqueue_steps(gp_ctx *c, int nsteps, cudaEvent_t *marks) {
+  auto marks_of = [&](int s) { return marks ? marks + (size_t)s * 2 * GP_NPHASE : nullptr; };
+  c->marks = marks_of(0);
+  int rc = enqueue_gather(c, c->stream);
+  for (int s = 0; s < nsteps && !rc; ++s) {
+    c->marks = marks_of(s);
+    if (s > 0 && cudaStreamWaitEvent(c->stream, c->ev_join, 0) != cudaSuccess) rc = GP_ECUDA;
+    if (!rc) rc = enqueue_integrate(c);
+    if (!rc) rc = enqueue_bin_search(c);
+    const bool fork = s + 1 < nsteps;
+    if (!rc && fork && cudaEventRecord(c->ev_fork, c->stream) != cudaSuccess) rc = GP_ECUDA;
+    // the contact kernel is captured first so that its persistent grid is resident
+    // before the gather's blocks queue for the SMs it leaves as its queue drains
+    if (!rc) rc = enqueue_contact_response(c);
+    if (!rc && fork) {
+      if (cudaStreamWaitEvent(c->side, c->ev_fork, 0) != cudaSuccess) rc = GP_ECUDA;
+      c->marks = marks_of(s + 1);
+      if (!rc) rc = enqueue_gather(c, c->side);
+      c->marks = marks_of(s);
+      if (!rc && cudaEventRecord(c->ev_join, c->side) != cudaSuccess) rc = GP_ECUDA;
+    }
+  }
+  c->marks = nullptr;
+  return rc;
 }
 
 int read_status(gp_ctx *c, Status *h) {
@@ -346,7 +413,18 @@ int gp_ctx_create(const gp_params *params, gp_ctx **out) {
   gp_ctx *c = new gp_ctx();
   c->prm = p;
   c->ppi = 4.0 * std::atan(1.0);   // init_run.f90:123
-  if (cudaGetDevice(&c->device) != cudaSuccess || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+  // the step's own stream gets the higher priority, so that the collision phase's
+  // blocks are scheduled ahead of the overlapped gather
+  int prio_low = 0, prio_high = 0;
+  if (cudaGetDevice(&c->device) != cudaSuccess ||
+      cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high) != cudaSuccess ||
+      cudaStreamCreateWithPriority(&c->stream, cudaStreamNonBlocking, prio_high) != cudaSuccess ||
+      cudaStreamCreateWithPriority(&c->side, cudaStreamNonBlocking, prio_low) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    if (c->side) cudaStreamDestroy(c->side);
+    if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return GP_ECUDA;
   }
@@ -405,6 +483,9 @@ int gp_ctx_destroy(gp_ctx *c) {
   dfree(c->stage); dfree(c->d_inst); dfree(c->d_pv); dfree(c->d_pv_alt); dfree(c->d_fluid_cols);
   dfree(c->d_counters);
   dfree(c->d_status); dfree(c->d_scratch);
+  if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+  if (c->ev_join) cudaEventDestroy(c->ev_join);
+  if (c->side) cudaStreamDestroy(c->side);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return GP_OK;
@@ -572,42 +653,49 @@ int gp_collision(gp_ctx *c, int32_t /*ncycle*/, double /*time*/, int64_t *n_near
   return GP_OK;
 }
 
+// Captures nsteps steps into one graph (the caller ends the capture).
+int capture_steps(gp_ctx *c, int nsteps, cudaEvent_t *marks, cudaGraph_t *g) {
+  GP_CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = GP_OK;
+  if (marks && cudaEventRecordWithFlags(marks[0], c->stream, cudaEventRecordExternal) != cudaSuccess) rc = GP_ECUDA;
+  if (!rc) rc = enqueue_steps(c, nsteps, marks ? marks + 1 : nullptr);
+  if (!rc && marks &&
+      cudaEventRecordWithFlags(marks[1 + (size_t)nsteps * 2 * GP_NPHASE], c->stream, cudaEventRecordExternal) !=
+          cudaSuccess)
+    rc = GP_ECUDA;
+  const cudaError_t e = cudaStreamEndCapture(c->stream, g);
+  if (!rc && e != cudaSuccess) rc = GP_ECUDA;
+  if (rc && e == cudaSuccess) cudaGraphDestroy(*g);
+  return rc;
+}
+
 int gp_step(gp_ctx *c, int32_t nsteps) {
   if (!c || c->n <= 0 || !c->grid_ready || nsteps < 0) return GP_EBADARG;
-  if (!c->graph) {
+  if (nsteps == 0) return GP_OK;
+  // one graph per step count in use (the cache is bounded; replays reuse it)
+  auto it = c->graphs.find(nsteps);
+  if (it == c->graphs.end()) {
+    if (c->graphs.size() >= 8) drop_graph(c);
     cudaGraph_t g;
-    GP_CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    int rc = enqueue_advance(c);
-    if (!rc) rc = enqueue_collision(c);
-    cudaError_t e = cudaStreamEndCapture(c->stream, &g);
-    if (rc) return rc;
-    if (e != cudaSuccess) return GP_ECUDA;
-    e = cudaGraphInstantiate(&c->graph, g, 0);
+    GP_TRY(capture_steps(c, nsteps, nullptr, &g));
+    cudaGraphExec_t ge = nullptr;
+    const cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
     cudaGraphDestroy(g);
-    if (e != cudaSuccess) { c->graph = nullptr; return GP_ECUDA; }
+    if (e != cudaSuccess) return GP_ECUDA;
+    it = c->graphs.emplace(nsteps, ge).first;
   }
-  for (int s = 0; s < nsteps; ++s) GP_CK(cudaGraphLaunch(c->graph, c->stream));
+  GP_CK(cudaGraphLaunch(it->second, c->stream));
   return GP_OK;
 }
 
 int gp_step_timed(gp_ctx *c, int32_t nsteps, float *total_ms, float *phase_ms_avg, int32_t *kernels_per_step) {
   if (!c || c->n <= 0 || !c->grid_ready || nsteps <= 0) return GP_EBADARG;
-  // event 0 opens the run; step s closes phase p with event 1 + s * GP_NPHASE + p
-  std::vector<cudaEvent_t> ev(1 + (size_t)nsteps * GP_NPHASE);
+  // [0] start, then 2*GP_NPHASE per step (begin/end of each phase), then the end
+  std::vector<cudaEvent_t> ev(2 + (size_t)nsteps * 2 * GP_NPHASE);
   for (auto &e : ev) GP_CK(cudaEventCreate(&e));
   cudaGraph_t g;
   cudaGraphExec_t ge = nullptr;
-  GP_CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-  int rc = GP_OK;
-  if (cudaEventRecordWithFlags(ev[0], c->stream, cudaEventRecordExternal) != cudaSuccess) rc = GP_ECUDA;
-  for (int s = 0; s < nsteps && !rc; ++s) {
-    c->marks = ev.data() + 1 + (size_t)s * GP_NPHASE;
-    rc = enqueue_advance(c);
-    if (!rc) rc = enqueue_collision(c);
-  }
-  c->marks = nullptr;
-  cudaError_t e = cudaStreamEndCapture(c->stream, &g);
-  if (!rc && e != cudaSuccess) rc = GP_ECUDA;
+  int rc = capture_steps(c, nsteps, ev.data(), &g);
   if (!rc && kernels_per_step) {
     size_t nn = 0;
     cudaGraphGetNodes(g, nullptr, &nn);
@@ -620,8 +708,10 @@ int gp_step_timed(gp_ctx *c, int32_t nsteps, float *total_ms, float *phase_ms_av
     }
     *kernels_per_step = nk / nsteps;
   }
-  if (!rc && cudaGraphInstantiate(&ge, g, 0) != cudaSuccess) rc = GP_ECUDA;
-  if (e == cudaSuccess) cudaGraphDestroy(g);
+  if (!rc) {
+    if (cudaGraphInstantiate(&ge, g, 0) != cudaSuccess) rc = GP_ECUDA;
+    cudaGraphDestroy(g);
+  }
   if (!rc && cudaGraphLaunch(ge, c->stream) != cudaSuccess) rc = GP_ECUDA;
   if (!rc && cudaStreamSynchronize(c->stream) != cudaSuccess) rc = GP_ECUDA;
   if (!rc) {
@@ -629,8 +719,8 @@ int gp_step_timed(gp_ctx *c, int32_t nsteps, float *total_ms, float *phase_ms_av
     float t = 0.f;
     for (int s = 0; s < nsteps && !rc; ++s)
       for (int p = 0; p < GP_NPHASE && !rc; ++p) {
-        const size_t k = 1 + (size_t)s * GP_NPHASE + p;
-        if (cudaEventElapsedTime(&t, ev[k - 1], ev[k]) != cudaSuccess) rc = GP_ECUDA;
+        const size_t k = 1 + ((size_t)s * GP_NPHASE + p) * 2;
+        if (cudaEventElapsedTime(&t, ev[k], ev[k + 1]) != cudaSuccess) rc = GP_ECUDA;
         acc[p] += t;
       }
     if (!rc && cudaEventElapsedTime(&t, ev[0], ev.back()) != cudaSuccess) rc = GP_ECUDA;

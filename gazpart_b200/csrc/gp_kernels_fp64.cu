@@ -14,15 +14,20 @@
 
 namespace gp {
 
-template __global__ void k_integrate<false>(const InstDev *, const PoolView *, int64_t, const double *const *, Status *);
+template __global__ void k_integrate<false>(const InstDev *, const PoolView *, const PoolView *, const int32_t *,
+                                            int64_t, const double *const *, Status *);
+template __global__ void k_gather<false>(const InstDev *, const PoolView *, const int32_t *, int64_t,
+                                         double *const *, Status *);
 
-void launch_advance_fp64(const InstDev *insts, PoolView *pv, PoolView *pv_alt, const int32_t *perm, int64_t n,
-                         double *const *fluid, Status *st,
-                         int grid, cudaEvent_t after_gather, cudaStream_t s) {
-  k_gather_move<false><<<148 * GP_GATHER_BLOCKS_PER_SM, 256, 0, s>>>(insts, pv, pv_alt, perm, n, fluid, st);
-  if (after_gather) cudaEventRecordWithFlags(after_gather, s, cudaEventRecordExternal);
+void launch_gather_fp64(const InstDev *insts, const PoolView *pv, const int32_t *perm, int64_t n,
+                      double *const *fluid, Status *st, cudaStream_t s) {
+  k_gather<false><<<148 * GP_GATHER_BLOCKS_PER_SM, 256, 0, s>>>(insts, pv, perm, n, fluid, st);
+}
+
+void launch_integrate_fp64(const InstDev *insts, PoolView *pv, PoolView *pv_alt, const int32_t *perm, int64_t n,
+                         double *const *fluid, Status *st, int grid, cudaStream_t s) {
+  k_integrate<false><<<grid, 128, 0, s>>>(insts, pv, pv_alt, perm, n, fluid, st);
   k_swap_pool<<<1, 1, 0, s>>>(pv, pv_alt);
-  k_integrate<false><<<grid, 128, 0, s>>>(insts, pv, n, fluid, st);
 }
 
 // INTERP_LAG3 (interp_lag3.f90:11-298) for one component at arbitrary points.

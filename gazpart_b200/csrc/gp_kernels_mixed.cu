@@ -10,15 +10,20 @@
 
 namespace gp {
 
-template __global__ void k_integrate<true>(const InstDev *, const PoolView *, int64_t, const double *const *, Status *);
+template __global__ void k_integrate<true>(const InstDev *, const PoolView *, const PoolView *, const int32_t *,
+                                            int64_t, const double *const *, Status *);
+template __global__ void k_gather<true>(const InstDev *, const PoolView *, const int32_t *, int64_t,
+                                         double *const *, Status *);
 
-void launch_advance_mixed(const InstDev *insts, PoolView *pv, PoolView *pv_alt, const int32_t *perm, int64_t n,
-                         double *const *fluid, Status *st,
-                          int grid, cudaEvent_t after_gather, cudaStream_t s) {
-  k_gather_move<true><<<148 * GP_GATHER_BLOCKS_PER_SM, 256, 0, s>>>(insts, pv, pv_alt, perm, n, fluid, st);
-  if (after_gather) cudaEventRecordWithFlags(after_gather, s, cudaEventRecordExternal);
+void launch_gather_mixed(const InstDev *insts, const PoolView *pv, const int32_t *perm, int64_t n,
+                      double *const *fluid, Status *st, cudaStream_t s) {
+  k_gather<true><<<148 * GP_GATHER_BLOCKS_PER_SM, 256, 0, s>>>(insts, pv, perm, n, fluid, st);
+}
+
+void launch_integrate_mixed(const InstDev *insts, PoolView *pv, PoolView *pv_alt, const int32_t *perm, int64_t n,
+                         double *const *fluid, Status *st, int grid, cudaStream_t s) {
+  k_integrate<true><<<grid, 128, 0, s>>>(insts, pv, pv_alt, perm, n, fluid, st);
   k_swap_pool<<<1, 1, 0, s>>>(pv, pv_alt);
-  k_integrate<true><<<grid, 128, 0, s>>>(insts, pv, n, fluid, st);
 }
 
 }  // namespace gp

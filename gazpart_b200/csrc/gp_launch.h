@@ -10,8 +10,10 @@ namespace gp {
 // --- gp_kernels_fp64.cu (FP64 path, -fmad=false) ---
 // ADV_PARTICLE_ELLP: advances particle perm[j] of *pv into slot j of *pv_alt, then swaps
 // the two views (so *pv is current afterwards).
-void launch_advance_fp64(const InstDev *insts, PoolView *pv, PoolView *pv_alt, const int32_t *perm, int64_t n,
-                         double *const *fluid, Status *st, int grid, cudaEvent_t after_gather, cudaStream_t s);
+void launch_gather_fp64(const InstDev *insts, const PoolView *pv, const int32_t *perm, int64_t n,
+                      double *const *fluid, Status *st, cudaStream_t s);
+void launch_integrate_fp64(const InstDev *insts, PoolView *pv, PoolView *pv_alt, const int32_t *perm, int64_t n,
+                         double *const *fluid, Status *st, int grid, cudaStream_t s);
 void launch_interp(const InstDev *inst, int comp, int64_t n, const double *x, const double *y, const double *z,
                    double *out, Status *st, cudaStream_t s);
 void launch_frozen_interp(const double *xain, const double *yain, const double *zain, int nx, int ny, int nz,
@@ -40,8 +42,10 @@ void launch_response_batch(int64_t n, double ecp, double mup, const double *ip /
                            cudaStream_t s);
 
 // --- gp_kernels_mixed.cu ---
-void launch_advance_mixed(const InstDev *insts, PoolView *pv, PoolView *pv_alt, const int32_t *perm, int64_t n,
-                          double *const *fluid, Status *st, int grid, cudaEvent_t after_gather, cudaStream_t s);
+void launch_gather_mixed(const InstDev *insts, const PoolView *pv, const int32_t *perm, int64_t n,
+                      double *const *fluid, Status *st, cudaStream_t s);
+void launch_integrate_mixed(const InstDev *insts, PoolView *pv, PoolView *pv_alt, const int32_t *perm, int64_t n,
+                         double *const *fluid, Status *st, int grid, cudaStream_t s);
 void launch_iota(int32_t *a, int64_t n, cudaStream_t s);
 
 // --- gp_search.cu ---
