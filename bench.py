@@ -42,6 +42,7 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the FP64 comparison run")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default launch grids")
     return ap.parse_args()
 
 
@@ -64,14 +65,16 @@ def x_margin_for(w, steps: int) -> float:
 
 
 def build_inputs(w, device, precision, steps: int = 0):
+    """Field and particles of a workload; a batched workload gives one state per class."""
     import dataclasses
     import torch
-    from gazpart_b200 import field, particles
+    from gazpart_b200 import config, field, particles
     setup = w.setup()
     f = field.generate(w.grid, seed=w.field_seed, device=device)
-    spec = dataclasses.replace(w.spec, x_margin=x_margin_for(w, steps)) if steps else w.spec
-    st = particles.draw(spec, setup)
-    return setup, f, st
+    specs = w.instances if isinstance(w, config.BatchedWorkload) else (w.spec,)
+    m = x_margin_for(w, steps) if steps else 0.0
+    states = [particles.draw(dataclasses.replace(sp, x_margin=m), setup) for sp in specs]
+    return setup, f, states if isinstance(w, config.BatchedWorkload) else states[0]
 
 
 def make_context(setup, f, st, precision, device):
@@ -79,12 +82,17 @@ def make_context(setup, f, st, precision, device):
     from gazpart_b200 import api, particles
     ctx = api.Context(setup, precision)
     ctx.set_fields({k: f[k].contiguous() for k in api.FIELD_KEYS})
-    # initial velocities: u = u_f(x), omega = 1/2 omega_f in the body frame
-    xs = [torch.from_numpy(st[k]).to(device) for k in ("x", "y", "z")]
-    g = [ctx.interp_lag3(c, *xs).cpu().numpy() for c in range(6)]
-    st["u"], st["v"], st["w"] = g[0], g[1], g[2]
-    particles.body_half_vorticity(st, g[3], g[4], g[5])
-    ctx.upload(st)
+    states = st if isinstance(st, list) else [st]
+    for one in states:
+        # initial velocities: u = u_f(x), omega = 1/2 omega_f in the body frame
+        xs = [torch.from_numpy(one[k]).to(device) for k in ("x", "y", "z")]
+        g = [ctx.interp_lag3(c, *xs).cpu().numpy() for c in range(6)]
+        one["u"], one["v"], one["w"] = g[0], g[1], g[2]
+        particles.body_half_vorticity(one, g[3], g[4], g[5])
+    if isinstance(st, list):
+        ctx.upload_classes(states)
+    else:
+        ctx.upload(st)
     return ctx
 
 
@@ -248,6 +256,10 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
+        if isinstance(w, config.BatchedWorkload):
+            print(json.dumps({"impl": "reference", "unavailable": "the CPU port is timed on single-ensemble "
+                              "workloads; a batched workload is many of them"}), flush=True)
+            return
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         threads = os.cpu_count() or 1
         scale = 16 if w.grid >= 256 else 1
@@ -281,11 +293,16 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device(device))
 
-    run_steps = args.warmup + args.steps + args.e2e_steps
+    # the autotuner's trials (60 one-step graphs) and the three one-step gathers also
+    # move the particles before the state is restored
+    run_steps = args.warmup + args.steps + args.e2e_steps + 63
     setup, f, st = build_inputs(w, device, precision, run_steps)
-    max_emaj = float(st["emaj"].max())
+    batched = isinstance(st, list)
+    max_emaj = float(st["emaj"].max()) if not batched else None
     ctx = make_context(setup, f, st, precision, device)
     n = ctx.n
+    tune = None if args.no_autotune else ctx.autotune()
+    ctx.raise_status("autotune")
     ctx.step(args.warmup)
     ctx.sync()
     ctx.raise_status("warm-up")
@@ -344,6 +361,8 @@ def main():
         st2 = build_inputs(w, device, "fp64", run_steps)[2]
         f64 = {k: v for k, v in f.items()}
         pctx = make_context(setup, f64, st2, "fp64", device)
+        if not args.no_autotune:
+            pctx.autotune()
         pctx.step(max(1, args.warmup))
         pctx.sync()
         tms, pph, _ = pctx.step_timed(max(5, args.steps // 5))
@@ -354,7 +373,7 @@ def main():
         ctx.close()
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and not batched:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         threads = os.cpu_count() or 1
         scale = 16 if w.grid >= 256 else 1
@@ -371,7 +390,8 @@ def main():
                 "config": {"workload": w.name, "precision": precision, "particles_per_gpu": n,
                            "field": f"{w.grid}^3 x 6 {'f32' if fbytes == 4 else 'f64'}",
                            "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (state+field > 5 GB)",
-                           "x_margin": x_margin_for(w, run_steps)},
+                           "x_margin": x_margin_for(w, run_steps), "launch_grids": tune,
+                           "classes": len(st) if batched else 1},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": kps * args.steps,
                 "kernels_per_step": kps, "phase_ms": phases,
                 "phase_note": "gather of step s+1 overlaps the contact solves of step s (two streams in the graph)",

@@ -29,6 +29,7 @@ ERRORS = {
 PREC_FP64, PREC_MIXED = 0, 1
 LAYOUT_INTERIOR, LAYOUT_REFERENCE = 0, 1
 PHASES = ("gather", "integrate", "bin", "search", "contact", "response")   # GP_PHASE_*
+TUNABLES = ("gather", "integrate", "bin", "search")   # GP_TUNE_*
 GHOST_PERIODIC, GHOST_ZERO = 0, 1
 
 
@@ -68,6 +69,8 @@ SIGNATURES = {
     "gp_upload_state": [_ctx, C.c_int64, C.POINTER(_vp), C.POINTER(_vp), C.c_int32],
     "gp_download_state": [_ctx, C.c_int64, C.POINTER(_vp), C.POINTER(_vp), C.c_int32],
     "gp_put_state": [_ctx, C.c_int64, C.POINTER(_vp), C.c_int32],
+    "gp_upload_classes": [_ctx, C.c_int32, _i64p, C.POINTER(_vp), C.POINTER(_vp), C.c_int32],
+    "gp_autotune": [_ctx, _ip],
     "gp_step_timed": [_ctx, C.c_int32, C.POINTER(C.c_float), C.POINTER(C.c_float), _ip],
     "gp_adv_particle_ellp": [_ctx, C.c_int32],
     "gp_collision": [_ctx, C.c_int32, C.c_double, _i64p, _i64p, _i64p],

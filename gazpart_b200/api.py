@@ -148,6 +148,27 @@ class Context:
                 raise ValueError("mixed host/device columns")
         check(_lib.lib().gp_upload_state(self._h, n, cols, props, dev), "gp_upload_state")
         self.n = n
+        self.class_counts = np.array([n], dtype=np.int64)
+
+    def upload_classes(self, states) -> None:
+        """Several classes (the reference's IG = 1..NIG) on this context's field, each with
+        its own box and search grids, stepped together.  ``states``: one state dict per
+        class (host numpy arrays).  download() returns the classes concatenated in this
+        order; split_classes() cuts such a dict back into per-class dicts."""
+        counts = np.array([int(st["x"].shape[0]) for st in states], dtype=np.int64)
+        cat = {k: np.ascontiguousarray(np.concatenate([np.asarray(st[k], dtype=np.float64) for st in states]))
+               for k in STATE_KEYS + PROP_KEYS}
+        cols = (C.c_void_p * 13)(*[C.c_void_p(cat[k].ctypes.data) for k in STATE_KEYS])
+        props = (C.c_void_p * 6)(*[C.c_void_p(cat[k].ctypes.data) for k in PROP_KEYS])
+        check(_lib.lib().gp_upload_classes(self._h, len(states), counts.ctypes.data_as(_lib._i64p), cols, props, 0),
+              "gp_upload_classes")
+        self.n = int(counts.sum())
+        self.class_counts = counts
+
+    def split_classes(self, st: Dict[str, np.ndarray]):
+        """Concatenated per-particle arrays -> one dict per class (upload_classes order)."""
+        edges = np.concatenate([[0], np.cumsum(self.class_counts)])
+        return [{k: v[edges[i]:edges[i + 1]] for k, v in st.items()} for i in range(len(self.class_counts))]
 
     def put_state(self, st: Dict[str, object]) -> None:
         """Overwrite the 13 state columns (properties unchanged), caller order."""
@@ -173,6 +194,12 @@ class Context:
         ph = (C.c_float * len(_lib.PHASES))()
         check(_lib.lib().gp_step_timed(self._h, nsteps, C.byref(t), ph, C.byref(k)), "gp_step_timed")
         return t.value, dict(zip(_lib.PHASES, (float(v) for v in ph))), k.value
+
+    def autotune(self) -> Dict[str, int]:
+        """Pick the launch grids on the resident ensemble (state restored afterwards)."""
+        g = (C.c_int32 * len(_lib.TUNABLES))()
+        check(_lib.lib().gp_autotune(self._h, g), "gp_autotune")
+        return dict(zip(_lib.TUNABLES, (int(v) for v in g)))
 
     def download(self, fluid: bool = False) -> Dict[str, np.ndarray]:
         out = {k: np.empty(self.n) for k in STATE_KEYS}

@@ -91,6 +91,9 @@ class ParticleSpec:
     # distance kept between the particles and the x = 0 and x = L planes at t = 0 (at
     # least the particle's own largest semi-axis)
     x_margin: float = 0.0
+    # monodisperse ensembles take exactly the nominal density ratio unless this is set,
+    # in which case the density follows the Stokes number as for polydisperse ones
+    density_from_st: bool = False
 
     def reference_shape(self) -> Tuple[float, float]:
         """(AR, b) of the median particle, used to fix the viscosity."""
@@ -162,4 +165,48 @@ C3 = Workload("c3_512cube_n16777216_fp32field", 512, "f32",
               ParticleSpec(n=16_777_216, ar_range=(0.2, 5.0), b_lognormal=(math.log(1e-3), 0.3),
                            st_uniform=(0.1, 10.0), seed=1), 5.0e-4, 200)
 
-WORKLOADS = {w.name: w for w in (C1, C2, C3)}
+
+
+@dataclasses.dataclass
+class BatchedWorkload:
+    """Independent ensembles (classes) on one shared field, stepped together."""
+    name: str
+    grid: int
+    field_dtype: str
+    instances: Tuple[ParticleSpec, ...]
+    dtime: float
+    steps: int
+    field_seed: int = 0
+
+    @property
+    def spec(self) -> ParticleSpec:
+        """The reference instance that fixes the shared viscosity."""
+        return self.instances[0]
+
+    def setup(self) -> Setup:
+        return Setup(nx=self.grid, ny=self.grid, nz=self.grid,
+                     visc=viscosity_for(_C4_REFERENCE, integral_time()), dtime=self.dtime)
+
+
+def c4_instances(count: int = 64, seed: int = 193) -> Tuple[ParticleSpec, ...]:
+    """64 instances: N log-uniform in [1e3, 2e6], one Stokes number log-uniform in
+    [0.1, 10] and one aspect ratio log-uniform in [0.2, 5] per instance, minor semi-axis
+    0.002 (the 256^3 field's particle size), each with its own seed.  The draw's seed is
+    the one of 0..199 whose total comes closest to the stated sum N ~ 1.7e7
+    (17,031,259 particles)."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    n = np.exp(rng.uniform(math.log(1e3), math.log(2e6), count)).astype(int)
+    st = np.exp(rng.uniform(math.log(0.1), math.log(10.0), count))
+    ar = np.exp(rng.uniform(math.log(0.2), math.log(5.0), count))
+    return tuple(ParticleSpec(n=int(n[i]), ar=float(ar[i]), b=0.002, st=float(st[i]), seed=1000 + i,
+                              density_from_st=True) for i in range(count))
+
+
+# the viscosity of the batched workload: a unit-aspect-ratio particle of b = 0.002 at
+# St = 1 has the density ratio 1000
+_C4_REFERENCE = ParticleSpec(n=1, ar=1.0, b=0.002, st=1.0)
+
+C4 = BatchedWorkload("c4_256cube_64inst_fp32field", 256, "f32", c4_instances(), 5.0e-4, 300)
+
+WORKLOADS = {w.name: w for w in (C1, C2, C3, C4)}

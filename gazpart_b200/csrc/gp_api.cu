@@ -97,8 +97,11 @@ struct gp_ctx {
   size_t field_bytes = 0;
   double *stage = nullptr;
   size_t stage_count = 0;
-  // ensemble table (one instance)
-  InstDev inst{};
+  // Classes (the reference's IG = 1..NIG, PART(:, IG)), each an instance with its own
+  // particle range, box grid and search-grid cells; `tmpl` holds the shared mesh,
+  // physics and field.
+  InstDev tmpl{};
+  std::vector<InstDev> insts;
   InstDev *d_inst = nullptr;
   bool grid_ready = false;
   // pool
@@ -130,7 +133,8 @@ struct gp_ctx {
   std::map<std::pair<int, int>, ClassProps> classes;
   // captured multi-step graphs, by step count
   std::map<int, cudaGraphExec_t> graphs;
-  int grid = 148 * 4;
+  // launch grids (blocks), GP_TUNE_* order; gp_autotune picks them on the live workload
+  int tune[GP_NTUNE] = {148 * 8, 148 * 4, 148 * 4, 148 * 4};
   int contact_grid = 148 * 4;   // persistent k_contact grid (resident blocks)
 };
 
@@ -151,7 +155,9 @@ void drop_graph(gp_ctx *c) {
 }
 
 int upload_inst(gp_ctx *c) {
-  GP_CK(cudaMemcpyAsync(c->d_inst, &c->inst, sizeof(InstDev), cudaMemcpyHostToDevice, c->stream));
+  const std::vector<InstDev> &v = c->insts.empty() ? std::vector<InstDev>{c->tmpl} : c->insts;
+  GP_CK(cudaMemcpyAsync(c->d_inst, v.data(), v.size() * sizeof(InstDev), cudaMemcpyHostToDevice, c->stream));
+  GP_CK(cudaStreamSynchronize(c->stream));
   return GP_OK;
 }
 
@@ -237,8 +243,7 @@ int alloc_pool(gp_ctx *c, int64_t cap) {
 
 // COLLISION_INITIATION (collision_initiation.f90:44-103, INIT_GRID=2, NPROC=1) and the
 // search grid.
-int setup_grids(gp_ctx *c, double max_emaj, double rmax, double rsmall) {
-  InstDev &I = c->inst;
+int setup_grids(gp_ctx *c, InstDev &I, double max_emaj, double rmax, double rsmall, int64_t cell_begin) {
   const gp_params &p = c->prm;
   const double zero_ref = 1.0e-33;
   const double dpmax = 2.0 * max_emaj;
@@ -260,7 +265,8 @@ int setup_grids(gp_ctx *c, double max_emaj, double rmax, double rsmall) {
   // search grid: about two particles per cell, cell edge >= 2 rsmall (1+1e-6) so that
   // all but the largest bounding radii fit the one-cell half stencil
   const double hmin = 2.0 * rsmall * (1.0 + 1.0e-6);
-  const int64_t target = std::max<int64_t>(3, (int64_t)std::ceil(std::cbrt((double)std::max<int64_t>(c->n, 1) / 2.0)));
+  const int64_t target =
+      std::max<int64_t>(3, (int64_t)std::ceil(std::cbrt((double)std::max<int64_t>(I.count, 1) / 2.0)));
   auto nf = [&](double L) {
     int64_t m = (int64_t)std::floor(L / hmin);
     return (int32_t)std::min<int64_t>(m, std::max<int64_t>(target, 3));
@@ -270,8 +276,13 @@ int setup_grids(gp_ctx *c, double max_emaj, double rmax, double rsmall) {
   I.hfx = p.lx / I.nfx; I.hfy = p.ly / I.nfy; I.hfz = p.lz / I.nfz;
   I.rmax = rmax;
   I.rcut = 0.5 * std::min(I.hfx, std::min(I.hfy, I.hfz)) / (1.0 + 1.0e-6);
-  I.cell_begin = 0;
+  I.cell_begin = cell_begin;
   const int64_t ncells = (int64_t)I.nfx * I.nfy * I.nfz;
+  if (ncells >= (int64_t(1) << 31) - 2) return GP_EBADARG;
+  return GP_OK;
+}
+
+int alloc_cells(gp_ctx *c, int64_t ncells) {
   if (ncells >= (int64_t(1) << 31) - 2) return GP_EBADARG;
   if (ncells > c->ncells_cap) {
     free_search(c);
@@ -283,7 +294,6 @@ int setup_grids(gp_ctx *c, double max_emaj, double rmax, double rsmall) {
   }
   c->ncells = ncells;
   c->sa.ncells = ncells;
-  c->grid_ready = true;
   return GP_OK;
 }
 
@@ -299,9 +309,11 @@ int mark(gp_ctx *c, int slot, cudaStream_t s) {
 int enqueue_gather(gp_ctx *c, cudaStream_t s) {
   GP_TRY(mark(c, 2 * GP_PHASE_GATHER, s));
   if (c->prm.precision == GP_PREC_MIXED)
-    launch_gather_mixed(c->d_inst, c->d_pv, c->sa.sorted, c->n, c->d_fluid_cols, c->d_status, s);
+    launch_gather_mixed(c->d_inst, c->d_pv, c->sa.sorted, c->n, c->d_fluid_cols, c->d_status,
+                        c->tune[GP_TUNE_GATHER], s);
   else
-    launch_gather_fp64(c->d_inst, c->d_pv, c->sa.sorted, c->n, c->d_fluid_cols, c->d_status, s);
+    launch_gather_fp64(c->d_inst, c->d_pv, c->sa.sorted, c->n, c->d_fluid_cols, c->d_status,
+                       c->tune[GP_TUNE_GATHER], s);
   GP_CK(cudaGetLastError());
   return mark(c, 2 * GP_PHASE_GATHER + 1, s);
 }
@@ -310,10 +322,10 @@ int enqueue_integrate(gp_ctx *c) {
   GP_TRY(mark(c, 2 * GP_PHASE_INTEGRATE, c->stream));
   if (c->prm.precision == GP_PREC_MIXED)
     launch_integrate_mixed(c->d_inst, c->d_pv, c->d_pv_alt, c->sa.sorted, c->n, c->d_fluid_cols, c->d_status,
-                           c->grid, c->stream);
+                           c->tune[GP_TUNE_INTEGRATE], c->stream);
   else
     launch_integrate_fp64(c->d_inst, c->d_pv, c->d_pv_alt, c->sa.sorted, c->n, c->d_fluid_cols, c->d_status,
-                          c->grid, c->stream);
+                          c->tune[GP_TUNE_INTEGRATE], c->stream);
   GP_CK(cudaGetLastError());
   return mark(c, 2 * GP_PHASE_INTEGRATE + 1, c->stream);
 }
@@ -330,12 +342,13 @@ int enqueue_bin_search(gp_ctx *c) {
   GP_CK(cudaMemsetAsync(sa.cell_count, 0, (c->ncells + 1) * sizeof(int32_t), c->stream));
   GP_CK(cudaMemsetAsync(sa.cell_fill, 0, (c->ncells + 1) * sizeof(int32_t), c->stream));
   GP_CK(cudaMemsetAsync(c->d_counters, 0, 4 * sizeof(unsigned long long), c->stream));
-  launch_bin_count(c->d_inst, c->d_pv, c->n, sa, c->d_status, c->grid, c->stream);
+  launch_bin_count(c->d_inst, c->d_pv, c->n, sa, c->d_status, c->tune[GP_TUNE_BIN], c->stream);
   launch_scan(sa.cell_count, sa.cell_start, c->ncells, c->d_scan_tmp, c->stream);
-  launch_bin_scatter(c->d_inst, c->d_pv, c->n, sa, c->d_status, c->grid, c->stream);
+  launch_bin_scatter(c->d_inst, c->d_pv, c->n, sa, c->d_status, c->tune[GP_TUNE_BIN], c->stream);
   GP_TRY(mark(c, 2 * GP_PHASE_BIN + 1, c->stream));
   GP_TRY(mark(c, 2 * GP_PHASE_SEARCH, c->stream));
-  launch_search(c->d_inst, c->n, sa, c->d_pairs, c->d_counters + 0, c->cap_pairs, c->d_status, c->grid, c->stream);
+  launch_search(c->d_inst, c->n, sa, c->d_pairs, c->d_counters + 0, c->cap_pairs, c->d_status,
+                c->tune[GP_TUNE_SEARCH], c->stream);
   GP_CK(cudaGetLastError());
   return mark(c, 2 * GP_PHASE_SEARCH + 1, c->stream);
 }
@@ -350,7 +363,7 @@ int enqueue_contact_response(gp_ctx *c) {
   launch_match(c->d_coll, c->d_counters + 1, c->cap_coll, c->d_best1, c->d_best2, c->d_matched, c->d_state,
                c->d_status, c->stream);
   launch_response(c->d_inst, c->d_pv, c->d_coll, c->d_counters + 1, c->cap_coll, c->d_state, c->d_acc,
-                  c->d_counters + 2, c->d_status, c->grid, c->stream);
+                  c->d_counters + 2, c->d_status, 148 * 4, c->stream);
   GP_CK(cudaGetLastError());
   return mark(c, 2 * GP_PHASE_RESPONSE + 1, c->stream);
 }
@@ -428,7 +441,7 @@ int gp_ctx_create(const gp_params *params, gp_ctx **out) {
     delete c;
     return GP_ECUDA;
   }
-  InstDev &I = c->inst;
+  InstDev &I = c->tmpl;
   I.begin = 0;
   I.count = 0;
   I.nx = p.nx; I.ny = p.ny; I.nz = p.nz; I.ncomp = 6;
@@ -448,7 +461,7 @@ int gp_ctx_create(const gp_params *params, gp_ctx **out) {
   if (cudaMalloc(&c->field, c->field_bytes) != cudaSuccess || cudaMemset(c->field, 0, c->field_bytes) != cudaSuccess)
     rc = GP_ENOMEM;
   I.field = c->field;
-  if (!rc) rc = dalloc(&c->d_inst, 1);
+  if (!rc) rc = dalloc(&c->d_inst, kMaxClasses);
   if (!rc) rc = dalloc(&c->d_pv, 1);
   if (!rc) rc = dalloc(&c->d_pv_alt, 1);
   if (!rc) rc = dalloc(&c->d_fluid_cols, kNFluid);
@@ -545,8 +558,15 @@ int gp_set_field(gp_ctx *c, int32_t comp, const double *src, int32_t src_layout,
   return GP_OK;
 }
 
-int gp_upload_state(gp_ctx *c, int64_t n, const double *const *cols, const double *const *props, int32_t on_device) {
-  if (!c || !cols || !props || n <= 0 || n >= kMaxInstanceParticles) return GP_EBADARG;
+int gp_upload_classes(gp_ctx *c, int32_t nclass, const int64_t *counts, const double *const *cols,
+                      const double *const *props, int32_t on_device) {
+  if (!c || !cols || !props || !counts || nclass <= 0 || nclass > kMaxClasses) return GP_EBADARG;
+  int64_t n = 0;
+  for (int k = 0; k < nclass; ++k) {
+    if (counts[k] <= 0 || counts[k] >= kMaxInstanceParticles) return GP_EBADARG;
+    n += counts[k];
+  }
+  if (n >= (int64_t(1) << 31)) return GP_EBADARG;
   // per-particle constants on the host (reference expressions, IEEE double)
   std::vector<double> hp[GP_NPROP];
   for (int k = 0; k < GP_NPROP; ++k) {
@@ -559,24 +579,33 @@ int gp_upload_state(gp_ctx *c, int64_t n, const double *const *cols, const doubl
   }
   GP_CK(cudaStreamSynchronize(c->stream));
   std::vector<double> pcs((size_t)kNConst * n);
-  double max_emaj = 0.0, rmax = 0.0;
-  std::vector<double> radii(n);
-  for (int64_t i = 0; i < n; ++i) {
-    double pc[kNConst];
-    const double emaj = hp[0][i], apr = hp[1][i], rhop = hp[2][i];
-    if (!(emaj > 0) || !(apr > 0) || !(rhop > 0)) return GP_EBADARG;
-    part_const(emaj, apr, rhop, c->prm.rhof, c->ppi, hp[3][i], hp[4][i], hp[5][i], pc);
-    for (int k = 0; k < kNConst; ++k) pcs[(size_t)k * n + i] = pc[k];
-    max_emaj = std::max(max_emaj, emaj);
-    rmax = std::max(rmax, std::max(pc[0], pc[1]));
-    radii[i] = std::max(pc[0], pc[1]);
+  std::vector<InstDev> insts(nclass, c->tmpl);
+  struct Sizes { double max_emaj, rmax, rsmall; };
+  std::vector<Sizes> sizes(nclass);
+  int64_t begin = 0;
+  for (int k = 0; k < nclass; ++k) {
+    double max_emaj = 0.0, rmax = 0.0;
+    std::vector<double> radii(counts[k]);
+    for (int64_t i = begin; i < begin + counts[k]; ++i) {
+      double pc[kNConst];
+      const double emaj = hp[0][i], apr = hp[1][i], rhop = hp[2][i];
+      if (!(emaj > 0) || !(apr > 0) || !(rhop > 0)) return GP_EBADARG;
+      part_const(emaj, apr, rhop, c->prm.rhof, c->ppi, hp[3][i], hp[4][i], hp[5][i], pc);
+      for (int q = 0; q < kNConst; ++q) pcs[(size_t)q * n + i] = pc[q];
+      max_emaj = std::max(max_emaj, emaj);
+      rmax = std::max(rmax, std::max(pc[0], pc[1]));
+      radii[i - begin] = std::max(pc[0], pc[1]);
+    }
+    // the search grid is sized for all but the largest 0.1% of bounding radii
+    const int64_t qi = std::min<int64_t>(counts[k] - 1, (int64_t)(0.999 * (double)counts[k]));
+    std::nth_element(radii.begin(), radii.begin() + qi, radii.end());
+    sizes[k] = {max_emaj, rmax, radii[qi]};
+    insts[k].begin = begin;
+    insts[k].count = counts[k];
+    begin += counts[k];
   }
-  // the search grid is sized for all but the largest 0.1% of bounding radii
-  const int64_t qi = std::min<int64_t>(n - 1, (int64_t)(0.999 * (double)n));
-  std::nth_element(radii.begin(), radii.begin() + qi, radii.end());
-  const double rsmall = radii[qi];
-  std::vector<double>().swap(radii);
   drop_graph(c);
+  c->grid_ready = false;
   const int64_t want = std::max<int64_t>(n, c->prm.max_particles);
   if (c->cap < want) GP_TRY(alloc_pool(c, want));
   else
@@ -587,17 +616,27 @@ int gp_upload_state(gp_ctx *c, int64_t n, const double *const *cols, const doubl
   GP_TRY(dalloc(&stage_pc, (size_t)kNConst * n));
   for (int k = 0; k < kNState; ++k) GP_TRY(copy_in(c, stage_cols + (size_t)k * n, cols[k], n, on_device));
   GP_CK(cudaMemcpyAsync(stage_pc, pcs.data(), pcs.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-  launch_init_pool(c->d_pv, 0, n, 0, stage_cols, stage_pc, c->stream);
+  for (int k = 0; k < nclass; ++k)
+    launch_init_pool(c->d_pv, insts[k].begin, insts[k].count, k, stage_cols, stage_pc, n, c->stream);
   launch_iota(c->sa.sorted, n, c->stream);   // the first advance keeps the upload order
   GP_CK(cudaGetLastError());
   GP_CK(cudaStreamSynchronize(c->stream));
   cudaFree(stage_cols);
   cudaFree(stage_pc);
-  c->inst.count = n;
-  GP_TRY(setup_grids(c, max_emaj, rmax, rsmall));
+  int64_t cells = 0;
+  for (int k = 0; k < nclass; ++k) {
+    GP_TRY(setup_grids(c, insts[k], sizes[k].max_emaj, sizes[k].rmax, sizes[k].rsmall, cells));
+    cells += (int64_t)insts[k].nfx * insts[k].nfy * insts[k].nfz;
+  }
+  GP_TRY(alloc_cells(c, cells));
+  c->insts = insts;
+  c->grid_ready = true;
   GP_TRY(upload_inst(c));
-  GP_CK(cudaStreamSynchronize(c->stream));
   return GP_OK;
+}
+
+int gp_upload_state(gp_ctx *c, int64_t n, const double *const *cols, const double *const *props, int32_t on_device) {
+  return gp_upload_classes(c, 1, &n, cols, props, on_device);
 }
 
 int gp_download_state(gp_ctx *c, int64_t n, double *const *cols, double *const *fluid, int32_t on_device) {
@@ -606,7 +645,7 @@ int gp_download_state(gp_ctx *c, int64_t n, double *const *cols, double *const *
   double *tmp = nullptr;
   const size_t per = (size_t)kNState + (fluid ? kNFluid : 0);
   GP_TRY(dalloc(&tmp, per * n));
-  launch_gather_state(c->d_pv, c->n, 0, tmp, c->d_fluid_cols, fluid ? tmp + (size_t)kNState * n : nullptr, n,
+  launch_gather_state(c->d_inst, c->d_pv, c->n, tmp, c->d_fluid_cols, fluid ? tmp + (size_t)kNState * n : nullptr, n,
                       c->stream);
   GP_CK(cudaGetLastError());
   const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
@@ -624,7 +663,7 @@ int gp_put_state(gp_ctx *c, int64_t n, const double *const *cols, int32_t on_dev
   if (!c || !cols || n != c->n) return GP_EBADARG;
   GP_TRY(ensure_scratch(c, (size_t)kNState * n));
   for (int k = 0; k < kNState; ++k) GP_TRY(copy_in(c, c->d_scratch + (size_t)k * n, cols[k], n, on_device));
-  launch_scatter_state(c->d_pv, c->n, 0, c->d_scratch, n, c->stream);
+  launch_scatter_state(c->d_inst, c->d_pv, c->n, c->d_scratch, n, c->stream);
   GP_CK(cudaGetLastError());
   GP_CK(cudaStreamSynchronize(c->stream));
   return GP_OK;
@@ -745,15 +784,17 @@ int gp_collision_pairs(gp_ctx *c, int64_t cap, int32_t *home, int32_t *near, int
     GP_CK(cudaMemcpy(recs.data(), c->d_coll, nc * sizeof(CollRec), cudaMemcpyDeviceToHost));
     GP_CK(cudaMemcpy(st.data(), c->d_state, nc, cudaMemcpyDeviceToHost));
   }
-  std::vector<std::pair<std::pair<unsigned long long, unsigned long long>, int64_t>> acc;
+  // class by class, each in the reference's list order
+  std::vector<std::pair<std::array<unsigned long long, 3>, int64_t>> acc;
   for (int64_t e = 0; e < nc; ++e)
-    if (st[e] == 1) acc.push_back({{recs[e].k1, recs[e].k2}, e});
+    if (st[e] == 1) acc.push_back({{(unsigned long long)recs[e].inst, recs[e].k1, recs[e].k2}, e});
   std::sort(acc.begin(), acc.end());
   if (count) *count = (int64_t)acc.size();
   for (int64_t k = 0; k < (int64_t)acc.size() && k < cap; ++k) {
-    const unsigned long long k2 = acc[k].first.second;
-    if (home) home[k] = (int32_t)(k2 >> 34);
-    if (near) near[k] = (int32_t)(k2 & ((1ull << 30) - 1));
+    const unsigned long long k2 = acc[k].first[2];
+    const int64_t base = c->insts[acc[k].first[0]].begin;
+    if (home) home[k] = (int32_t)(base + (int64_t)(k2 >> 34));
+    if (near) near[k] = (int32_t)(base + (int64_t)(k2 & ((1ull << 30) - 1)));
   }
   return GP_OK;
 }
@@ -761,7 +802,7 @@ int gp_collision_pairs(gp_ctx *c, int64_t cap, int32_t *home, int32_t *near, int
 int gp_collision_box_connectivity(gp_ctx *c, int32_t *nbox, int32_t *ncon, int32_t *con, int32_t *grid_dims,
                                   double *grid_geom) {
   if (!c || !c->grid_ready) return GP_EBADARG;
-  const InstDev &I = c->inst;
+  const InstDev &I = c->insts[0];   // the first class's grid
   const int64_t nb = (int64_t)I.nxbox * I.nybox * I.nzbox;
   if (nbox) *nbox = (int32_t)nb;
   if (grid_dims) { grid_dims[0] = I.nxbox; grid_dims[1] = I.nybox; grid_dims[2] = I.nzbox; }
@@ -1012,6 +1053,48 @@ int gp_collision_response(gp_ctx *c, int32_t ig, int32_t idp, double part1[10], 
   std::memcpy(part1, h + 3, 10 * sizeof(double));
   std::memcpy(part2, h + 13, 10 * sizeof(double));
   return s.code;
+}
+
+// Coordinate descent over the launch grids: each tunable in turn, each candidate timed
+// by one-step graphs on the live ensemble (median of three), the fastest kept.  The
+// state is saved before and restored after, so the ensemble does not move; the pool
+// order and the last binning may change, which no result depends on.
+int gp_autotune(gp_ctx *c, int32_t *grids_out) {
+  if (!c || c->n <= 0 || !c->grid_ready) return GP_EBADARG;
+  const int64_t n = c->n;
+  double *save = nullptr;
+  GP_TRY(dalloc(&save, (size_t)kNState * n));
+  launch_gather_state(c->d_inst, c->d_pv, c->n, save, c->d_fluid_cols, nullptr, n, c->stream);
+  GP_CK(cudaGetLastError());
+  static const int kMult[] = {1, 2, 4, 8, 16};
+  static const int kPhase[GP_NTUNE] = {GP_PHASE_GATHER, GP_PHASE_INTEGRATE, GP_PHASE_BIN, GP_PHASE_SEARCH};
+  int rc = GP_OK;
+  for (int t = 0; t < GP_NTUNE && !rc; ++t) {
+    int best = c->tune[t];
+    float best_ms = 1e30f;
+    for (int m : kMult) {
+      c->tune[t] = 148 * m;
+      drop_graph(c);
+      float ph[GP_NPHASE], trial[3];
+      for (int r = 0; r < 3 && !rc; ++r) {
+        rc = gp_step_timed(c, 1, nullptr, ph, nullptr);
+        trial[r] = ph[kPhase[t]];
+      }
+      if (rc) break;
+      std::sort(trial, trial + 3);
+      if (trial[1] < best_ms) { best_ms = trial[1]; best = c->tune[t]; }
+    }
+    c->tune[t] = best;
+  }
+  drop_graph(c);
+  if (!rc) {
+    launch_scatter_state(c->d_inst, c->d_pv, c->n, save, n, c->stream);
+    if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(c->stream) != cudaSuccess) rc = GP_ECUDA;
+  }
+  cudaFree(save);
+  if (!rc && grids_out)
+    for (int t = 0; t < GP_NTUNE; ++t) grids_out[t] = c->tune[t];
+  return rc;
 }
 
 }  // extern "C"

@@ -8,10 +8,6 @@
 #include "gp_lm.cuh"
 #include "gp_launch.h"
 
-#ifndef GP_GATHER_BLOCKS_PER_SM
-#define GP_GATHER_BLOCKS_PER_SM 8
-#endif
-
 namespace gp {
 
 template __global__ void k_integrate<false>(const InstDev *, const PoolView *, const PoolView *, const int32_t *,
@@ -20,8 +16,8 @@ template __global__ void k_gather<false>(const InstDev *, const PoolView *, cons
                                          double *const *, Status *);
 
 void launch_gather_fp64(const InstDev *insts, const PoolView *pv, const int32_t *perm, int64_t n,
-                      double *const *fluid, Status *st, cudaStream_t s) {
-  k_gather<false><<<148 * GP_GATHER_BLOCKS_PER_SM, 256, 0, s>>>(insts, pv, perm, n, fluid, st);
+                      double *const *fluid, Status *st, int grid, cudaStream_t s) {
+  k_gather<false><<<grid, 256, 0, s>>>(insts, pv, perm, n, fluid, st);
 }
 
 void launch_integrate_fp64(const InstDev *insts, PoolView *pv, PoolView *pv_alt, const int32_t *perm, int64_t n,
@@ -211,6 +207,7 @@ __global__ void __launch_bounds__(128, GP_CONTACT_MIN_BLOCKS) k_contact(const In
     }
     CollRec r;
     r.home = i1; r.near = i2; r.k1 = pr.k1; r.k2 = pr.k2;
+    r.inst = P.inst[i1]; r.pad = 0;
 #pragma unroll
     for (int i = 0; i < 3; ++i) { r.rx1[i] = rx1[i]; r.rx2[i] = rx2[i]; r.cn[i] = cn[i]; }
     coll[slot] = r;

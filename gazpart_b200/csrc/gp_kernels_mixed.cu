@@ -4,10 +4,6 @@
 #include "gp_advance.cuh"
 #include "gp_launch.h"
 
-#ifndef GP_GATHER_BLOCKS_PER_SM
-#define GP_GATHER_BLOCKS_PER_SM 8
-#endif
-
 namespace gp {
 
 template __global__ void k_integrate<true>(const InstDev *, const PoolView *, const PoolView *, const int32_t *,
@@ -16,8 +12,8 @@ template __global__ void k_gather<true>(const InstDev *, const PoolView *, const
                                          double *const *, Status *);
 
 void launch_gather_mixed(const InstDev *insts, const PoolView *pv, const int32_t *perm, int64_t n,
-                      double *const *fluid, Status *st, cudaStream_t s) {
-  k_gather<true><<<148 * GP_GATHER_BLOCKS_PER_SM, 256, 0, s>>>(insts, pv, perm, n, fluid, st);
+                      double *const *fluid, Status *st, int grid, cudaStream_t s) {
+  k_gather<true><<<grid, 256, 0, s>>>(insts, pv, perm, n, fluid, st);
 }
 
 void launch_integrate_mixed(const InstDev *insts, PoolView *pv, PoolView *pv_alt, const int32_t *perm, int64_t n,

@@ -11,7 +11,7 @@ namespace gp {
 // ADV_PARTICLE_ELLP: advances particle perm[j] of *pv into slot j of *pv_alt, then swaps
 // the two views (so *pv is current afterwards).
 void launch_gather_fp64(const InstDev *insts, const PoolView *pv, const int32_t *perm, int64_t n,
-                      double *const *fluid, Status *st, cudaStream_t s);
+                      double *const *fluid, Status *st, int grid, cudaStream_t s);
 void launch_integrate_fp64(const InstDev *insts, PoolView *pv, PoolView *pv_alt, const int32_t *perm, int64_t n,
                          double *const *fluid, Status *st, int grid, cudaStream_t s);
 void launch_interp(const InstDev *inst, int comp, int64_t n, const double *x, const double *y, const double *z,
@@ -43,7 +43,7 @@ void launch_response_batch(int64_t n, double ecp, double mup, const double *ip /
 
 // --- gp_kernels_mixed.cu ---
 void launch_gather_mixed(const InstDev *insts, const PoolView *pv, const int32_t *perm, int64_t n,
-                      double *const *fluid, Status *st, cudaStream_t s);
+                      double *const *fluid, Status *st, int grid, cudaStream_t s);
 void launch_integrate_mixed(const InstDev *insts, PoolView *pv, PoolView *pv_alt, const int32_t *perm, int64_t n,
                          double *const *fluid, Status *st, int grid, cudaStream_t s);
 void launch_iota(int32_t *a, int64_t n, cudaStream_t s);
@@ -61,13 +61,12 @@ void launch_match(const CollRec *coll, const unsigned long long *ncoll, int64_t 
                   unsigned long long *best2, int8_t *matched, int8_t *state, Status *st, cudaStream_t s);
 void launch_field_layout(void *dst, int prec, int nx, int ny, int nz, int ncomp, int comp, const double *src,
                          int src_layout, int ghost_mode, cudaStream_t s);
-void launch_gather_state(const PoolView *pv, int64_t n, int inst, double *out /*13*count*/,
-                         double *const *fluid_cols, double *fluid_out /*6*count or null*/, int64_t count,
-                         cudaStream_t s);
-void launch_scatter_state(const PoolView *pv, int64_t n, int inst, const double *cols /*13*count*/,
+void launch_gather_state(const InstDev *insts, const PoolView *pv, int64_t n, double *out,
+                         double *const *fluid_cols, double *fluid_out, int64_t count, cudaStream_t s);
+void launch_scatter_state(const InstDev *insts, const PoolView *pv, int64_t n, const double *cols,
                           int64_t count, cudaStream_t s);
-void launch_init_pool(const PoolView *pv, int64_t begin, int64_t n, int inst, const double *cols /*13*n*/,
-                      const double *pcs /*10*n*/, cudaStream_t s);
+void launch_init_pool(const PoolView *pv, int64_t begin, int64_t n, int inst, const double *cols,
+                      const double *pcs, int64_t ld, cudaStream_t s);
 void launch_connectivity(int nxb, int nyb, int nzb, int periodicity, int32_t *ncon, int32_t *con, cudaStream_t s);
 
 }  // namespace gp

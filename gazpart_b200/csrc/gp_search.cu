@@ -582,12 +582,16 @@ void launch_field_layout(void *dst, int prec, int nx, int ny, int nz, int ncomp,
 }
 
 // Pool -> caller order for one instance: out[c*count + id] = state column c.
-__global__ void k_gather_state(const PoolView *__restrict__ pv, int64_t n, int inst, double *__restrict__ out,
-                               double *const *fluid, double *__restrict__ fout, int64_t count) {
+// Pool -> caller order: out[c*count + begin(class) + id] = state column c, where the
+// caller's arrays hold the classes one after another.
+__global__ void k_gather_state(const InstDev *__restrict__ insts, const PoolView *__restrict__ pv, int64_t n,
+                               double *__restrict__ out, double *const *fluid, double *__restrict__ fout,
+                               int64_t count) {
   const PoolView P = *pv;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    if (P.inst[i] != inst) continue;
-    const int64_t id = P.id[i];
+    const int inst = P.inst[i];
+    if (inst < 0) continue;
+    const int64_t id = insts[inst].begin + P.id[i];
     if (id < 0 || id >= count) continue;
 #pragma unroll
     for (int c = 0; c < kNState; ++c) out[c * count + id] = P.st[c][i];
@@ -598,48 +602,51 @@ __global__ void k_gather_state(const PoolView *__restrict__ pv, int64_t n, int i
   }
 }
 
-void launch_gather_state(const PoolView *pv, int64_t n, int inst, double *out, double *const *fluid_cols,
+void launch_gather_state(const InstDev *insts, const PoolView *pv, int64_t n, double *out, double *const *fluid_cols,
                          double *fluid_out, int64_t count, cudaStream_t s) {
   const int grid = 148 * 8;
-  k_gather_state<<<grid, 256, 0, s>>>(pv, n, inst, out, fluid_cols, fluid_out, count);
+  k_gather_state<<<grid, 256, 0, s>>>(insts, pv, n, out, fluid_cols, fluid_out, count);
 }
 
-// caller order -> pool for one instance (state columns only)
-__global__ void k_scatter_state(const PoolView *__restrict__ pv, int64_t n, int inst, const double *__restrict__ cols,
-                                int64_t count) {
+// caller order -> pool (state columns only)
+__global__ void k_scatter_state(const InstDev *__restrict__ insts, const PoolView *__restrict__ pv, int64_t n,
+                                const double *__restrict__ cols, int64_t count) {
   const PoolView P = *pv;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    if (P.inst[i] != inst) continue;
-    const int64_t id = P.id[i];
+    const int inst = P.inst[i];
+    if (inst < 0) continue;
+    const int64_t id = insts[inst].begin + P.id[i];
     if (id < 0 || id >= count) continue;
 #pragma unroll
     for (int c = 0; c < kNState; ++c) P.st[c][i] = cols[c * count + id];
   }
 }
 
-void launch_scatter_state(const PoolView *pv, int64_t n, int inst, const double *cols, int64_t count,
+void launch_scatter_state(const InstDev *insts, const PoolView *pv, int64_t n, const double *cols, int64_t count,
                           cudaStream_t s) {
-  k_scatter_state<<<148 * 8, 256, 0, s>>>(pv, n, inst, cols, count);
+  k_scatter_state<<<148 * 8, 256, 0, s>>>(insts, pv, n, cols, count);
 }
 
+// One class into pool slots [begin, begin+n): columns are caller arrays of leading
+// dimension ld holding the class at offset begin; ids are 0-based within the class.
 __global__ void k_init_pool(const PoolView *__restrict__ pv, int64_t begin, int64_t n, int inst,
-                            const double *__restrict__ cols, const double *__restrict__ pcs) {
+                            const double *__restrict__ cols, const double *__restrict__ pcs, int64_t ld) {
   const PoolView P = *pv;
   for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
     const int64_t i = begin + k;
 #pragma unroll
-    for (int c = 0; c < kNState; ++c) P.st[c][i] = cols[c * n + k];
+    for (int c = 0; c < kNState; ++c) P.st[c][i] = cols[c * ld + i];
 #pragma unroll
-    for (int c = 0; c < kNConst; ++c) P.pc[c][i] = pcs[c * n + k];
+    for (int c = 0; c < kNConst; ++c) P.pc[c][i] = pcs[c * ld + i];
     P.id[i] = (int32_t)k;
     P.inst[i] = inst;
   }
 }
 
 void launch_init_pool(const PoolView *pv, int64_t begin, int64_t n, int inst, const double *cols, const double *pcs,
-                      cudaStream_t s) {
+                      int64_t ld, cudaStream_t s) {
   if (n <= 0) return;
-  k_init_pool<<<148 * 8, 256, 0, s>>>(pv, begin, n, inst, cols, pcs);
+  k_init_pool<<<148 * 8, 256, 0, s>>>(pv, begin, n, inst, cols, pcs, ld);
 }
 
 __global__ void k_iota(int32_t *a, int64_t n) {

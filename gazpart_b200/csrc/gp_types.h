@@ -66,10 +66,12 @@ struct PairRec {
   unsigned long long k2;            // (id_home << 34) | (slot << 30) | id_near
 };
 constexpr int64_t kMaxInstanceParticles = (int64_t)1 << 30;
+constexpr int kMaxClasses = 1024;   // classes (instances) per context
 
 // A colliding pair with what COLLISION_RESPONSE needs.
 struct CollRec {
   int32_t home, near;
+  int32_t inst, pad;
   unsigned long long k1, k2;
   double rx1[3], rx2[3], cn[3];
 };

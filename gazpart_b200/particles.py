@@ -65,7 +65,7 @@ def draw(spec: ParticleSpec, setup: Setup) -> Dict[str, np.ndarray]:
     apr = ar.copy()
     deq = (2.0 * emaj) / (apr ** (2.0 / 3.0))
     rhop = st * 18.0 * setup.visc * integral_time() / (deq * deq) * setup.rhof
-    if spec.st is not None and spec.ar is not None and spec.b is not None:
+    if spec.st is not None and spec.ar is not None and spec.b is not None and not spec.density_from_st:
         # monodisperse: exactly the nominal density ratio
         rhop = np.full(n, spec.density_ratio * setup.rhof)
     # positions as the reference draws them, XRAND*(L - 2 EMAJ) + EMAJ

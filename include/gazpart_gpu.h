@@ -127,6 +127,17 @@ int gp_upload_state(gp_ctx *ctx, int64_t n, const double *const *cols,
 int gp_download_state(gp_ctx *ctx, int64_t n, double *const *cols, double *const *fluid,
                       int32_t on_device);
 
+/* Several classes at once: PART(1:N(IG), IG) for IG = 1..nclass (the reference's NIG
+ * classes, mod_particle_parallel.f90:103; each class collides only with itself,
+ * collision.f90:7-200), all on the context's field.  counts: N(IG); cols/props are
+ * arrays of sum(counts) values holding the classes one after another, and
+ * gp_download_state/gp_put_state use the same concatenated order.  Every class gets
+ * its own box grid (COLLISION_INITIATION from its own largest EMAJ) and search grid,
+ * and one step advances and collides all classes in the same launches.
+ * gp_upload_state(n, ...) is the one-class case. */
+int gp_upload_classes(gp_ctx *ctx, int32_t nclass, const int64_t *counts, const double *const *cols,
+                      const double *const *props, int32_t on_device);
+
 /* Replace the state columns of the resident particles (properties unchanged), caller
  * order.  The drop-in form of handing PART back to the device after host-side edits. */
 int gp_put_state(gp_ctx *ctx, int64_t n, const double *const *cols, int32_t on_device);
@@ -161,6 +172,19 @@ enum {
  * in the reference (measurement). */
 int gp_step_timed(gp_ctx *ctx, int32_t nsteps, float *total_ms, float *phase_ms_avg,
                   int32_t *kernels_per_step);
+/* Launch grids (blocks per launch) that gp_autotune chooses, in this order. */
+enum {
+    GP_TUNE_GATHER = 0,      /* stencil gather */
+    GP_TUNE_INTEGRATE = 1,   /* integrate */
+    GP_TUNE_BIN = 2,         /* binning count and scatter */
+    GP_TUNE_SEARCH = 3,      /* candidate-pair search */
+    GP_NTUNE = 4
+};
+/* Autotuner: for each launch above, in turn, times one-step graphs of the resident
+ * ensemble with 148 x {1,2,4,8,16} blocks and keeps the fastest; the particle state
+ * is saved first and restored afterwards.  grids_out: GP_NTUNE ints or NULL.  No
+ * counterpart in the reference. */
+int gp_autotune(gp_ctx *ctx, int32_t *grids_out);
 /* Last step's accepted collisions as (home, near) original indices, in acceptance
  * (list) order; *count receives the total even if it exceeds cap. */
 int gp_collision_pairs(gp_ctx *ctx, int64_t cap, int32_t *home, int32_t *near, int64_t *count);
