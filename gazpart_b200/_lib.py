@@ -62,6 +62,7 @@ SIGNATURES = {
     "gp_ctx_create": [C.POINTER(GPParams), C.POINTER(_ctx)],
     "gp_ctx_destroy": [_ctx],
     "gp_status": [_ctx, _ip, _i64p],
+    "gp_status_class": [_ctx, _ip],
     "gp_clear_status": [_ctx],
     "gp_sync": [_ctx],
     "gp_set_class": [_ctx, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double],
@@ -71,6 +72,13 @@ SIGNATURES = {
     "gp_put_state": [_ctx, C.c_int64, C.POINTER(_vp), C.c_int32],
     "gp_upload_classes": [_ctx, C.c_int32, _i64p, C.POINTER(_vp), C.POINTER(_vp), C.c_int32],
     "gp_autotune": [_ctx, _ip],
+    "gp_add_field": [_ctx, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, _ip],
+    "gp_set_field_slot": [_ctx, C.c_int32, C.c_int32, _vp, C.c_int32, C.c_int32, C.c_int32],
+    "gp_add_class": [_ctx, C.c_int32, C.c_int64, C.POINTER(_vp), C.POINTER(_vp), C.c_int32, _ip],
+    "gp_download_class": [_ctx, C.c_int32, C.POINTER(_vp), C.c_int32],
+    "gp_remove_class": [_ctx, C.c_int32, C.POINTER(_vp), C.c_int32],
+    "gp_class_count": [_ctx, C.c_int32, _i64p],
+    "gp_serve": [_ctx, _vp, C.c_int32, C.c_double, C.c_double, _i64p],
     "gp_step_timed": [_ctx, C.c_int32, C.POINTER(C.c_float), C.POINTER(C.c_float), _ip],
     "gp_adv_particle_ellp": [_ctx, C.c_int32],
     "gp_collision": [_ctx, C.c_int32, C.c_double, _i64p, _i64p, _i64p],

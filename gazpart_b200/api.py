@@ -100,6 +100,12 @@ class Context:
         check(_lib.lib().gp_status(self._h, C.byref(code), C.byref(fid)), "gp_status")
         return code.value, fid.value
 
+    def status_class(self) -> int:
+        """Class (1-based) of the particle behind the first error; 0 if none."""
+        ig = C.c_int32()
+        check(_lib.lib().gp_status_class(self._h, C.byref(ig)), "gp_status_class")
+        return ig.value
+
     def clear_status(self) -> None:
         check(_lib.lib().gp_clear_status(self._h), "gp_clear_status")
 
@@ -121,11 +127,53 @@ class Context:
         gh = {"periodic": _lib.GHOST_PERIODIC, "zero": _lib.GHOST_ZERO}[ghost]
         check(_lib.lib().gp_set_field(self._h, comp, ptr, lay, gh, dev), "gp_set_field")
 
-    def set_fields(self, fields: Dict[str, object], vorticity_ghost: str = "zero") -> None:
+    def set_fields(self, fields: Dict[str, object], vorticity_ghost: str = "zero", slot: int = 0) -> None:
         """Velocity with periodic ghosts; vorticity ghosts as the reference leaves them
-        (never exchanged, hence zero) unless ``vorticity_ghost='periodic'``."""
+        (never exchanged, hence zero) unless ``vorticity_ghost='periodic'``.  ``slot``
+        selects a resident field added by add_field."""
         for c, k in enumerate(FIELD_KEYS):
-            self.set_field(c, fields[k], "interior", "periodic" if c < 3 else vorticity_ghost)
+            ptr, dev, keep = _ptr(fields[k])
+            gh = _lib.GHOST_PERIODIC if (c < 3 or vorticity_ghost == "periodic") else _lib.GHOST_ZERO
+            check(_lib.lib().gp_set_field_slot(self._h, slot, c, ptr, _lib.LAYOUT_INTERIOR, gh, dev),
+                  "gp_set_field_slot")
+
+    def add_field(self, n: int, lbox: float = 2.0 * np.pi) -> int:
+        """One more resident field of n^3 points on a periodic box of side lbox; returns its slot."""
+        f = C.c_int32()
+        check(_lib.lib().gp_add_field(self._h, n, n, n, lbox, lbox, lbox, C.byref(f)), "gp_add_field")
+        return f.value
+
+    def add_class(self, st: Dict[str, object], field: int = 0) -> int:
+        """Admit one more class (host arrays) on field slot ``field``; returns its number."""
+        n = int(np.asarray(st["x"]).shape[0])
+        cat = {k: np.ascontiguousarray(np.asarray(st[k], dtype=np.float64)) for k in STATE_KEYS + PROP_KEYS}
+        cols = (C.c_void_p * 13)(*[C.c_void_p(cat[k].ctypes.data) for k in STATE_KEYS])
+        props = (C.c_void_p * 6)(*[C.c_void_p(cat[k].ctypes.data) for k in PROP_KEYS])
+        ig = C.c_int32()
+        check(_lib.lib().gp_add_class(self._h, field, n, cols, props, 0, C.byref(ig)), "gp_add_class")
+        self.n += n
+        return ig.value
+
+    def class_count(self, ig: int) -> int:
+        n = C.c_int64()
+        check(_lib.lib().gp_class_count(self._h, ig, C.byref(n)), "gp_class_count")
+        return n.value
+
+    def download_class(self, ig: int) -> Dict[str, np.ndarray]:
+        n = self.class_count(ig)
+        out = {k: np.empty(n) for k in STATE_KEYS}
+        cols = (C.c_void_p * 13)(*[C.c_void_p(out[k].ctypes.data) for k in STATE_KEYS])
+        check(_lib.lib().gp_download_class(self._h, ig, cols, 0), "gp_download_class")
+        return out
+
+    def remove_class(self, ig: int) -> Dict[str, np.ndarray]:
+        """Retire class ig and return its final state."""
+        n = self.class_count(ig)
+        out = {k: np.empty(n) for k in STATE_KEYS}
+        cols = (C.c_void_p * 13)(*[C.c_void_p(out[k].ctypes.data) for k in STATE_KEYS])
+        check(_lib.lib().gp_remove_class(self._h, ig, cols, 0), "gp_remove_class")
+        self.n -= n
+        return out
 
     def upload(self, st: Dict[str, object]) -> None:
         n = int(st["x"].shape[0])

@@ -507,7 +507,7 @@ __global__ void __launch_bounds__(256) k_gather(const InstDev* __restrict__ inst
       if (stencil(I, src_pv->st[0][i], src_pv->st[1][i], src_pv->st[2][i], s)) {
         mode = (kMixed && s.contiguous) ? 1 : 2;
       } else {
-        set_error(st, GP_EOUT_OF_GRID, (long long)src_pv->id[i]);
+        set_error(st, GP_EOUT_OF_GRID, (long long)src_pv->id[i], inst);
       }
     }
     if (j < n && mode == 0) {
@@ -565,7 +565,7 @@ __global__ void __launch_bounds__(128, GP_INTEGRATE_MIN_BLOCKS) k_integrate(cons
     if (inst >= 0 && !(uf[0] != uf[0] && wv[0] != wv[0])) {
       const InstDev& I = insts[inst];
       const int err = advance_particle<kMixed>(I, pc, uf, wv, X, U, O, Q);
-      if (err) set_error(st, err, (long long)S->id[i]);
+      if (err) set_error(st, err, (long long)S->id[i], inst);
       if (I.periodicity) {
         if (X[0] > I.lx) X[0] = X[0] - I.lx;
         if (X[0] < 0.) X[0] = X[0] + I.lx;

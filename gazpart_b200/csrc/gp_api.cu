@@ -7,10 +7,12 @@
 // per-particle and per-pair arithmetic runs in the kernels.
 #include <algorithm>
 #include <array>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <thread>
 #include <utility>
 #include <vector>
 
@@ -101,8 +103,18 @@ struct gp_ctx {
   // particle range, box grid and search-grid cells; `tmpl` holds the shared mesh,
   // physics and field.
   InstDev tmpl{};
-  std::vector<InstDev> insts;
+  std::vector<InstDev> insts;      // by class slot; a retired slot has count 0
+  std::vector<char> live;          // slot in use
   InstDev *d_inst = nullptr;
+  // resident fields: slot 0 is the one gp_params describes, more come from gp_add_field
+  struct FieldSlot {
+    void *ptr = nullptr;
+    int nx = 0, ny = 0, nz = 0;
+    double lx = 0, ly = 0, lz = 0;
+  };
+  std::vector<FieldSlot> fields;
+  std::vector<int> class_field;    // field slot of each class slot
+  int64_t n_slots = 0;             // pool slots holding particles, retired ones included
   bool grid_ready = false;
   // pool
   int64_t cap = 0, n = 0;
@@ -243,19 +255,18 @@ int alloc_pool(gp_ctx *c, int64_t cap) {
 
 // COLLISION_INITIATION (collision_initiation.f90:44-103, INIT_GRID=2, NPROC=1) and the
 // search grid.
-int setup_grids(gp_ctx *c, InstDev &I, double max_emaj, double rmax, double rsmall, int64_t cell_begin) {
-  const gp_params &p = c->prm;
+int setup_grids(InstDev &I, double max_emaj, double rmax, double rsmall, int64_t cell_begin) {
   const double zero_ref = 1.0e-33;
   const double dpmax = 2.0 * max_emaj;
   double dxbox = 2.0 * dpmax;
-  I.nxbox = (int32_t)(p.lx / dxbox);
+  I.nxbox = (int32_t)(I.lx / dxbox);
   if (I.nxbox < 3) return GP_EBADARG;
-  I.dxbox = p.lx / (double)I.nxbox;
+  I.dxbox = I.lx / (double)I.nxbox;
   I.xminbox = (double)(1 - 1) * I.dx;
   I.yminbox = I.dy * (double)(1 - 1) - zero_ref;
-  const double ymaxbox = I.dy * (double)(p.ny - 1) + I.dy + zero_ref;
+  const double ymaxbox = I.dy * (double)(I.ny - 1) + I.dy + zero_ref;
   I.zminbox = I.dz * (double)(1 - 1) - zero_ref;
-  const double zmaxbox = I.dz * (double)(p.nz - 1) + I.dz + zero_ref;
+  const double zmaxbox = I.dz * (double)(I.nz - 1) + I.dz + zero_ref;
   I.nybox = (int32_t)((ymaxbox - I.yminbox) / I.dxbox);
   I.nzbox = (int32_t)((zmaxbox - I.zminbox) / I.dxbox);
   if (I.nybox < 3 || I.nzbox < 3) return GP_EBADARG;
@@ -271,9 +282,9 @@ int setup_grids(gp_ctx *c, InstDev &I, double max_emaj, double rmax, double rsma
     int64_t m = (int64_t)std::floor(L / hmin);
     return (int32_t)std::min<int64_t>(m, std::max<int64_t>(target, 3));
   };
-  I.nfx = nf(p.lx); I.nfy = nf(p.ly); I.nfz = nf(p.lz);
+  I.nfx = nf(I.lx); I.nfy = nf(I.ly); I.nfz = nf(I.lz);
   if (I.nfx < 3 || I.nfy < 3 || I.nfz < 3) return GP_EBADARG;
-  I.hfx = p.lx / I.nfx; I.hfy = p.ly / I.nfy; I.hfz = p.lz / I.nfz;
+  I.hfx = I.lx / I.nfx; I.hfy = I.ly / I.nfy; I.hfz = I.lz / I.nfz;
   I.rmax = rmax;
   I.rcut = 0.5 * std::min(I.hfx, std::min(I.hfy, I.hfz)) / (1.0 + 1.0e-6);
   I.cell_begin = cell_begin;
@@ -327,6 +338,7 @@ int enqueue_integrate(gp_ctx *c) {
     launch_integrate_fp64(c->d_inst, c->d_pv, c->d_pv_alt, c->sa.sorted, c->n, c->d_fluid_cols, c->d_status,
                           c->tune[GP_TUNE_INTEGRATE], c->stream);
   GP_CK(cudaGetLastError());
+  c->n_slots = c->n;   // the pass writes the active particles, in cell order, to slots [0, n)
   return mark(c, 2 * GP_PHASE_INTEGRATE + 1, c->stream);
 }
 
@@ -335,16 +347,24 @@ int enqueue_advance(gp_ctx *c) {
   return enqueue_integrate(c);
 }
 
-// Binning of the search grid and the candidate-pair search.
-int enqueue_bin_search(gp_ctx *c) {
+// Binning of the search grid (also the cell order the next advance moves to).
+int enqueue_bin(gp_ctx *c) {
   SearchArrays sa = c->sa;
-  GP_TRY(mark(c, 2 * GP_PHASE_BIN, c->stream));
   GP_CK(cudaMemsetAsync(sa.cell_count, 0, (c->ncells + 1) * sizeof(int32_t), c->stream));
   GP_CK(cudaMemsetAsync(sa.cell_fill, 0, (c->ncells + 1) * sizeof(int32_t), c->stream));
   GP_CK(cudaMemsetAsync(c->d_counters, 0, 4 * sizeof(unsigned long long), c->stream));
-  launch_bin_count(c->d_inst, c->d_pv, c->n, sa, c->d_status, c->tune[GP_TUNE_BIN], c->stream);
+  launch_bin_count(c->d_inst, c->d_pv, c->n_slots, sa, c->d_status, c->tune[GP_TUNE_BIN], c->stream);
   launch_scan(sa.cell_count, sa.cell_start, c->ncells, c->d_scan_tmp, c->stream);
-  launch_bin_scatter(c->d_inst, c->d_pv, c->n, sa, c->d_status, c->tune[GP_TUNE_BIN], c->stream);
+  launch_bin_scatter(c->d_inst, c->d_pv, c->n_slots, sa, c->d_status, c->tune[GP_TUNE_BIN], c->stream);
+  GP_CK(cudaGetLastError());
+  return GP_OK;
+}
+
+// Binning and the candidate-pair search.
+int enqueue_bin_search(gp_ctx *c) {
+  SearchArrays sa = c->sa;
+  GP_TRY(mark(c, 2 * GP_PHASE_BIN, c->stream));
+  GP_TRY(enqueue_bin(c));
   GP_TRY(mark(c, 2 * GP_PHASE_BIN + 1, c->stream));
   GP_TRY(mark(c, 2 * GP_PHASE_SEARCH, c->stream));
   launch_search(c->d_inst, c->n, sa, c->d_pairs, c->d_counters + 0, c->cap_pairs, c->d_status,
@@ -461,6 +481,7 @@ int gp_ctx_create(const gp_params *params, gp_ctx **out) {
   if (cudaMalloc(&c->field, c->field_bytes) != cudaSuccess || cudaMemset(c->field, 0, c->field_bytes) != cudaSuccess)
     rc = GP_ENOMEM;
   I.field = c->field;
+  c->fields.push_back({c->field, p.nx, p.ny, p.nz, p.lx, p.ly, p.lz});
   if (!rc) rc = dalloc(&c->d_inst, kMaxClasses);
   if (!rc) rc = dalloc(&c->d_pv, 1);
   if (!rc) rc = dalloc(&c->d_pv_alt, 1);
@@ -492,6 +513,7 @@ int gp_ctx_destroy(gp_ctx *c) {
   drop_graph(c);
   free_pool(c);
   free_search(c);
+  for (size_t f = 1; f < c->fields.size(); ++f) cudaFree(c->fields[f].ptr);
   if (c->field) cudaFree(c->field);
   dfree(c->stage); dfree(c->d_inst); dfree(c->d_pv); dfree(c->d_pv_alt); dfree(c->d_fluid_cols);
   dfree(c->d_counters);
@@ -510,6 +532,14 @@ int gp_status(gp_ctx *c, int32_t *code, int64_t *first_id) {
   GP_TRY(read_status(c, &h));
   if (code) *code = h.code;
   if (first_id) *first_id = h.first_id;
+  return GP_OK;
+}
+
+int gp_status_class(gp_ctx *c, int32_t *ig) {
+  if (!c || !ig) return GP_EBADARG;
+  Status h;
+  GP_TRY(read_status(c, &h));
+  *ig = h.first_inst;
   return GP_OK;
 }
 
@@ -532,14 +562,14 @@ int gp_set_class(gp_ctx *c, int32_t ig, int32_t idp, double emaj, double apr, do
   return GP_OK;
 }
 
-int gp_set_field(gp_ctx *c, int32_t comp, const double *src, int32_t src_layout, int32_t ghost_mode,
-                 int32_t on_device) {
-  if (!c || !src || comp < 0 || comp > 5) return GP_EBADARG;
+int gp_set_field_slot(gp_ctx *c, int32_t field, int32_t comp, const double *src, int32_t src_layout,
+                      int32_t ghost_mode, int32_t on_device) {
+  if (!c || !src || comp < 0 || comp > 5 || field < 0 || field >= (int)c->fields.size()) return GP_EBADARG;
   if (src_layout != GP_LAYOUT_INTERIOR && src_layout != GP_LAYOUT_REFERENCE) return GP_EBADARG;
   if (ghost_mode != GP_GHOST_PERIODIC && ghost_mode != GP_GHOST_ZERO) return GP_EBADARG;
-  const gp_params &p = c->prm;
-  const size_t count = (src_layout == GP_LAYOUT_REFERENCE) ? (size_t)p.nx * (p.ny + 4) * (p.nz + 4)
-                                                           : (size_t)p.nx * p.ny * p.nz;
+  const gp_ctx::FieldSlot &f = c->fields[field];
+  const size_t count = (src_layout == GP_LAYOUT_REFERENCE) ? (size_t)f.nx * (f.ny + 4) * (f.nz + 4)
+                                                           : (size_t)f.nx * f.ny * f.nz;
   const double *dsrc = src;
   if (!on_device) {
     if (c->stage_count < count) {
@@ -551,12 +581,117 @@ int gp_set_field(gp_ctx *c, int32_t comp, const double *src, int32_t src_layout,
     GP_CK(cudaMemcpyAsync(c->stage, src, count * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     dsrc = c->stage;
   }
-  launch_field_layout(c->field, p.precision, p.nx, p.ny, p.nz, kFieldStride, comp, dsrc, src_layout, ghost_mode,
+  launch_field_layout(f.ptr, c->prm.precision, f.nx, f.ny, f.nz, kFieldStride, comp, dsrc, src_layout, ghost_mode,
                       c->stream);
   GP_CK(cudaGetLastError());
   GP_CK(cudaStreamSynchronize(c->stream));
   return GP_OK;
 }
+
+int gp_set_field(gp_ctx *c, int32_t comp, const double *src, int32_t src_layout, int32_t ghost_mode,
+                 int32_t on_device) {
+  return gp_set_field_slot(c, 0, comp, src, src_layout, ghost_mode, on_device);
+}
+
+int gp_add_field(gp_ctx *c, int32_t nx, int32_t ny, int32_t nz, double lx, double ly, double lz, int32_t *field) {
+  if (!c || !field || nx < 4 || ny < 4 || nz < 4 || !(lx > 0 && ly > 0 && lz > 0)) return GP_EBADARG;
+  const size_t elem = (c->prm.precision == GP_PREC_MIXED) ? sizeof(float) : sizeof(double);
+  const size_t bytes = (size_t)(nx + 3) * (ny + 4) * (nz + 4) * kFieldStride * elem;
+  void *ptr = nullptr;
+  if (cudaMalloc(&ptr, bytes) != cudaSuccess) return GP_ENOMEM;
+  if (cudaMemset(ptr, 0, bytes) != cudaSuccess) { cudaFree(ptr); return GP_ECUDA; }
+  c->fields.push_back({ptr, nx, ny, nz, lx, ly, lz});
+  *field = (int32_t)c->fields.size() - 1;
+  return GP_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// A class on field slot f: the context's physics with that field's mesh
+// (meshing.f90:43-45).
+InstDev class_template(const gp_ctx *c, int f) {
+  InstDev I = c->tmpl;
+  const gp_ctx::FieldSlot &F = c->fields[f];
+  I.field = F.ptr;
+  I.nx = F.nx; I.ny = F.ny; I.nz = F.nz;
+  I.lx = F.lx; I.ly = F.ly; I.lz = F.lz;
+  I.dx = F.lx / (double)(F.nx - 1);
+  I.dy = F.ly / (double)(F.ny - 1);
+  I.dz = F.lz / (double)(F.nz - 1);
+  I.begin = 0;
+  I.count = 0;
+  return I;
+}
+
+// Host copy of the GP_NPROP property columns of n particles.
+int read_props(gp_ctx *c, int64_t n, const double *const *props, int32_t on_device, std::vector<double> *hp) {
+  for (int k = 0; k < GP_NPROP; ++k) {
+    hp[k].resize(n);
+    if (on_device) {
+      GP_CK(cudaMemcpyAsync(hp[k].data(), props[k], n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    } else {
+      std::memcpy(hp[k].data(), props[k], n * sizeof(double));
+    }
+  }
+  GP_CK(cudaStreamSynchronize(c->stream));
+  return GP_OK;
+}
+
+// Per-particle constants of particles [off, off+cnt) (reference expressions, IEEE
+// double) into pcs (kNConst columns of leading dimension ld), and the class's grids.
+int class_setup(gp_ctx *c, const std::vector<double> *hp, int64_t off, int64_t cnt, double *pcs, int64_t ld,
+                InstDev &I) {
+  double max_emaj = 0.0, rmax = 0.0;
+  std::vector<double> radii(cnt);
+  for (int64_t i = off; i < off + cnt; ++i) {
+    double pc[kNConst];
+    const double emaj = hp[0][i], apr = hp[1][i], rhop = hp[2][i];
+    if (!(emaj > 0) || !(apr > 0) || !(rhop > 0)) return GP_EBADARG;
+    part_const(emaj, apr, rhop, c->prm.rhof, c->ppi, hp[3][i], hp[4][i], hp[5][i], pc);
+    for (int q = 0; q < kNConst; ++q) pcs[(size_t)q * ld + i] = pc[q];
+    max_emaj = std::max(max_emaj, emaj);
+    rmax = std::max(rmax, std::max(pc[0], pc[1]));
+    radii[i - off] = std::max(pc[0], pc[1]);
+  }
+  // the search grid is sized for all but the largest 0.1% of bounding radii
+  const int64_t qi = std::min<int64_t>(cnt - 1, (int64_t)(0.999 * (double)cnt));
+  std::nth_element(radii.begin(), radii.begin() + qi, radii.end());
+  I.count = cnt;
+  return setup_grids(I, max_emaj, rmax, radii[qi], 0);
+}
+
+// After a change of the class table: caller-order offsets and search cells of the live
+// classes, the device table, the captured graphs, and (rebin) a binning pass so that
+// the next advance moves exactly the live particles.
+int refresh_classes(gp_ctx *c, bool rebin) {
+  int64_t begin = 0, cells = 0;
+  for (size_t k = 0; k < c->insts.size(); ++k) {
+    InstDev &I = c->insts[k];
+    if (!c->live[k]) I.count = 0;
+    I.begin = begin;
+    I.cell_begin = cells;
+    begin += I.count;
+    if (c->live[k]) cells += (int64_t)I.nfx * I.nfy * I.nfz;
+  }
+  drop_graph(c);
+  c->n = begin;
+  c->grid_ready = false;
+  if (c->n == 0) {
+    c->n_slots = 0;   // every particle left is retired
+    return GP_OK;
+  }
+  GP_TRY(alloc_cells(c, cells));
+  GP_TRY(upload_inst(c));
+  c->grid_ready = true;
+  if (rebin) GP_TRY(enqueue_bin(c));
+  return GP_OK;
+}
+
+}  // namespace
+
+extern "C" {
 
 int gp_upload_classes(gp_ctx *c, int32_t nclass, const int64_t *counts, const double *const *cols,
                       const double *const *props, int32_t on_device) {
@@ -567,41 +702,13 @@ int gp_upload_classes(gp_ctx *c, int32_t nclass, const int64_t *counts, const do
     n += counts[k];
   }
   if (n >= (int64_t(1) << 31)) return GP_EBADARG;
-  // per-particle constants on the host (reference expressions, IEEE double)
   std::vector<double> hp[GP_NPROP];
-  for (int k = 0; k < GP_NPROP; ++k) {
-    hp[k].resize(n);
-    if (on_device) {
-      GP_CK(cudaMemcpyAsync(hp[k].data(), props[k], n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    } else {
-      std::memcpy(hp[k].data(), props[k], n * sizeof(double));
-    }
-  }
-  GP_CK(cudaStreamSynchronize(c->stream));
+  GP_TRY(read_props(c, n, props, on_device, hp));
   std::vector<double> pcs((size_t)kNConst * n);
-  std::vector<InstDev> insts(nclass, c->tmpl);
-  struct Sizes { double max_emaj, rmax, rsmall; };
-  std::vector<Sizes> sizes(nclass);
+  std::vector<InstDev> insts(nclass, class_template(c, 0));
   int64_t begin = 0;
   for (int k = 0; k < nclass; ++k) {
-    double max_emaj = 0.0, rmax = 0.0;
-    std::vector<double> radii(counts[k]);
-    for (int64_t i = begin; i < begin + counts[k]; ++i) {
-      double pc[kNConst];
-      const double emaj = hp[0][i], apr = hp[1][i], rhop = hp[2][i];
-      if (!(emaj > 0) || !(apr > 0) || !(rhop > 0)) return GP_EBADARG;
-      part_const(emaj, apr, rhop, c->prm.rhof, c->ppi, hp[3][i], hp[4][i], hp[5][i], pc);
-      for (int q = 0; q < kNConst; ++q) pcs[(size_t)q * n + i] = pc[q];
-      max_emaj = std::max(max_emaj, emaj);
-      rmax = std::max(rmax, std::max(pc[0], pc[1]));
-      radii[i - begin] = std::max(pc[0], pc[1]);
-    }
-    // the search grid is sized for all but the largest 0.1% of bounding radii
-    const int64_t qi = std::min<int64_t>(counts[k] - 1, (int64_t)(0.999 * (double)counts[k]));
-    std::nth_element(radii.begin(), radii.begin() + qi, radii.end());
-    sizes[k] = {max_emaj, rmax, radii[qi]};
-    insts[k].begin = begin;
-    insts[k].count = counts[k];
+    GP_TRY(class_setup(c, hp, begin, counts[k], pcs.data(), n, insts[k]));
     begin += counts[k];
   }
   drop_graph(c);
@@ -610,28 +717,95 @@ int gp_upload_classes(gp_ctx *c, int32_t nclass, const int64_t *counts, const do
   if (c->cap < want) GP_TRY(alloc_pool(c, want));
   else
     for (int b = 0; b < 2; ++b) GP_CK(cudaMemsetAsync(c->d_instof[b], 0xFF, c->cap * sizeof(int32_t), c->stream));
-  c->n = n;
   double *stage_cols = nullptr, *stage_pc = nullptr;
   GP_TRY(dalloc(&stage_cols, (size_t)kNState * n));
   GP_TRY(dalloc(&stage_pc, (size_t)kNConst * n));
   for (int k = 0; k < kNState; ++k) GP_TRY(copy_in(c, stage_cols + (size_t)k * n, cols[k], n, on_device));
   GP_CK(cudaMemcpyAsync(stage_pc, pcs.data(), pcs.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-  for (int k = 0; k < nclass; ++k)
-    launch_init_pool(c->d_pv, insts[k].begin, insts[k].count, k, stage_cols, stage_pc, n, c->stream);
+  begin = 0;
+  for (int k = 0; k < nclass; ++k) {
+    launch_init_pool(c->d_pv, begin, counts[k], k, stage_cols, stage_pc, n, begin, c->stream);
+    begin += counts[k];
+  }
   launch_iota(c->sa.sorted, n, c->stream);   // the first advance keeps the upload order
   GP_CK(cudaGetLastError());
   GP_CK(cudaStreamSynchronize(c->stream));
   cudaFree(stage_cols);
   cudaFree(stage_pc);
-  int64_t cells = 0;
-  for (int k = 0; k < nclass; ++k) {
-    GP_TRY(setup_grids(c, insts[k], sizes[k].max_emaj, sizes[k].rmax, sizes[k].rsmall, cells));
-    cells += (int64_t)insts[k].nfx * insts[k].nfy * insts[k].nfz;
-  }
-  GP_TRY(alloc_cells(c, cells));
   c->insts = insts;
-  c->grid_ready = true;
-  GP_TRY(upload_inst(c));
+  c->live.assign(nclass, 1);
+  c->class_field.assign(nclass, 0);
+  c->n_slots = n;
+  return refresh_classes(c, false);
+}
+
+int gp_add_class(gp_ctx *c, int32_t field, int64_t n, const double *const *cols, const double *const *props,
+                 int32_t on_device, int32_t *ig) {
+  if (!c || !cols || !props || !ig || n <= 0 || n >= kMaxInstanceParticles) return GP_EBADARG;
+  if (field < 0 || field >= (int)c->fields.size()) return GP_EBADARG;
+  if (c->cap == 0) GP_TRY(alloc_pool(c, std::max<int64_t>(n, c->prm.max_particles)));
+  if (c->n_slots + n > c->cap) return GP_ENOMEM;
+  size_t slot = 0;
+  while (slot < c->live.size() && c->live[slot]) ++slot;
+  if (slot >= (size_t)kMaxClasses) return GP_ENOMEM;
+  std::vector<double> hp[GP_NPROP];
+  GP_TRY(read_props(c, n, props, on_device, hp));
+  std::vector<double> pcs((size_t)kNConst * n);
+  InstDev I = class_template(c, field);
+  GP_TRY(class_setup(c, hp, 0, n, pcs.data(), n, I));
+  double *stage_cols = nullptr, *stage_pc = nullptr;
+  GP_TRY(dalloc(&stage_cols, (size_t)kNState * n));
+  GP_TRY(dalloc(&stage_pc, (size_t)kNConst * n));
+  for (int k = 0; k < kNState; ++k) GP_TRY(copy_in(c, stage_cols + (size_t)k * n, cols[k], n, on_device));
+  GP_CK(cudaMemcpyAsync(stage_pc, pcs.data(), pcs.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  launch_init_pool(c->d_pv, c->n_slots, n, (int)slot, stage_cols, stage_pc, n, 0, c->stream);
+  GP_CK(cudaGetLastError());
+  GP_CK(cudaStreamSynchronize(c->stream));
+  cudaFree(stage_cols);
+  cudaFree(stage_pc);
+  c->n_slots += n;
+  if (slot == c->live.size()) {
+    c->insts.push_back(I);
+    c->live.push_back(1);
+    c->class_field.push_back(field);
+  } else {
+    c->insts[slot] = I;
+    c->live[slot] = 1;
+    c->class_field[slot] = field;
+  }
+  *ig = (int32_t)slot + 1;
+  return refresh_classes(c, true);
+}
+
+int gp_download_class(gp_ctx *c, int32_t ig, double *const *cols, int32_t on_device) {
+  if (!c || !cols || ig < 1 || ig > (int)c->live.size() || !c->live[ig - 1]) return GP_EBADARG;
+  const int64_t n = c->insts[ig - 1].count;
+  double *tmp = nullptr;
+  GP_TRY(dalloc(&tmp, (size_t)kNState * n));
+  launch_gather_state(c->d_inst, c->d_pv, c->n_slots, ig - 1, tmp, c->d_fluid_cols, nullptr, n, c->stream);
+  GP_CK(cudaGetLastError());
+  const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  for (int k = 0; k < kNState; ++k)
+    GP_CK(cudaMemcpyAsync(cols[k], tmp + (size_t)k * n, n * sizeof(double), kind, c->stream));
+  GP_CK(cudaStreamSynchronize(c->stream));
+  cudaFree(tmp);
+  return GP_OK;
+}
+
+int gp_remove_class(gp_ctx *c, int32_t ig, double *const *cols, int32_t on_device) {
+  if (!c || ig < 1 || ig > (int)c->live.size() || !c->live[ig - 1]) return GP_EBADARG;
+  if (cols) GP_TRY(gp_download_class(c, ig, cols, on_device));
+  launch_retire(c->d_pv, c->n_slots, ig - 1, c->stream);
+  GP_CK(cudaGetLastError());
+  c->live[ig - 1] = 0;
+  GP_TRY(refresh_classes(c, true));
+  GP_CK(cudaStreamSynchronize(c->stream));
+  return GP_OK;
+}
+
+int gp_class_count(gp_ctx *c, int32_t ig, int64_t *n) {
+  if (!c || !n || ig < 1 || ig > (int)c->live.size()) return GP_EBADARG;
+  *n = c->live[ig - 1] ? c->insts[ig - 1].count : 0;
   return GP_OK;
 }
 
@@ -645,7 +819,8 @@ int gp_download_state(gp_ctx *c, int64_t n, double *const *cols, double *const *
   double *tmp = nullptr;
   const size_t per = (size_t)kNState + (fluid ? kNFluid : 0);
   GP_TRY(dalloc(&tmp, per * n));
-  launch_gather_state(c->d_inst, c->d_pv, c->n, tmp, c->d_fluid_cols, fluid ? tmp + (size_t)kNState * n : nullptr, n,
+  launch_gather_state(c->d_inst, c->d_pv, c->n_slots, -1, tmp, c->d_fluid_cols,
+                      fluid ? tmp + (size_t)kNState * n : nullptr, n,
                       c->stream);
   GP_CK(cudaGetLastError());
   const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
@@ -663,7 +838,7 @@ int gp_put_state(gp_ctx *c, int64_t n, const double *const *cols, int32_t on_dev
   if (!c || !cols || n != c->n) return GP_EBADARG;
   GP_TRY(ensure_scratch(c, (size_t)kNState * n));
   for (int k = 0; k < kNState; ++k) GP_TRY(copy_in(c, c->d_scratch + (size_t)k * n, cols[k], n, on_device));
-  launch_scatter_state(c->d_inst, c->d_pv, c->n, c->d_scratch, n, c->stream);
+  launch_scatter_state(c->d_inst, c->d_pv, c->n_slots, c->d_scratch, n, c->stream);
   GP_CK(cudaGetLastError());
   GP_CK(cudaStreamSynchronize(c->stream));
   return GP_OK;
@@ -1055,6 +1230,108 @@ int gp_collision_response(gp_ctx *c, int32_t ig, int32_t idp, double part1[10], 
   return s.code;
 }
 
+// Serving loop.  Jobs arrive at their times (seconds after the call starts, wall clock);
+// in arrival order, each is admitted as soon as its footprint fits the HBM budget
+// beside the running jobs and its particles fit the pool; every loop iteration steps
+// all running jobs together (one advance and one collision phase for all of them) and
+// retires the jobs that have run their steps, writing their final state back.  A job
+// whose particle raises an error is retired at once with that status; the others go on.
+int gp_serve(gp_ctx *c, gp_job *jobs, int32_t njobs, double hbm_budget, double bytes_per_particle,
+             int64_t *particle_steps) {
+  if (!c || (!jobs && njobs > 0) || njobs < 0 || !(bytes_per_particle > 0)) return GP_EBADARG;
+  using clock = std::chrono::steady_clock;
+  const auto t0 = clock::now();
+  auto now = [&] { return std::chrono::duration<double>(clock::now() - t0).count(); };
+  std::vector<int> order(njobs);
+  for (int j = 0; j < njobs; ++j) {
+    order[j] = j;
+    jobs[j].admitted_s = jobs[j].done_s = -1.0;
+    jobs[j].status = GP_OK;
+    if (jobs[j].n <= 0 || jobs[j].steps < 0 || !jobs[j].cols || !jobs[j].props) return GP_EBADARG;
+  }
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return jobs[a].arrival_s < jobs[b].arrival_s; });
+  std::vector<int> ig_of(njobs, 0), left(njobs, 0);
+  std::vector<int> running;
+  size_t next = 0;
+  double used = 0.0;
+  int64_t done_work = 0;
+  int rc = GP_OK;
+  auto retire = [&](int j, int status) -> int {
+    int r = gp_remove_class(c, ig_of[j], jobs[j].cols, 0);
+    jobs[j].done_s = now();
+    jobs[j].status = status;
+    used -= (double)jobs[j].n * bytes_per_particle;
+    running.erase(std::find(running.begin(), running.end(), j));
+    return r;
+  };
+  while (!rc && (next < order.size() || !running.empty())) {
+    // admission, first come first served
+    while (next < order.size()) {
+      gp_job &J = jobs[order[next]];
+      if (J.arrival_s > now()) break;
+      const double need = (double)J.n * bytes_per_particle;
+      if ((c->cap > 0 && J.n > c->cap) || (need > hbm_budget)) {   // can never run here
+        J.admitted_s = J.done_s = now();
+        J.status = GP_ENOMEM;
+        ++next;
+        continue;
+      }
+      if (used + need > hbm_budget) break;
+      if (c->cap > 0 && c->n_slots + J.n > c->cap) break;   // room after the next compaction
+      int32_t ig = 0;
+      rc = gp_add_class(c, J.field, J.n, J.cols, J.props, 0, &ig);
+      if (rc) break;
+      ig_of[order[next]] = ig;
+      left[order[next]] = J.steps;
+      J.admitted_s = now();
+      used += need;
+      running.push_back(order[next]);
+      ++next;
+    }
+    if (rc) break;
+    // jobs with no steps to run leave at once
+    for (size_t k = 0; k < running.size() && !rc;) {
+      const int j = running[k];
+      if (left[j] == 0) rc = retire(j, GP_OK); else ++k;
+    }
+    if (rc) break;
+    if (running.empty()) {
+      if (next < order.size()) {
+        const double wait = jobs[order[next]].arrival_s - now();
+        if (wait > 0) std::this_thread::sleep_for(std::chrono::duration<double>(std::min(wait, 0.01)));
+      }
+      continue;
+    }
+    // one step of every running job
+    GP_CK(cudaMemsetAsync(&c->d_status->n_near, 0, 5 * sizeof(unsigned long long), c->stream));
+    rc = enqueue_advance(c);
+    if (!rc) rc = enqueue_collision(c);
+    if (rc) break;
+    Status h;
+    rc = read_status(c, &h);
+    if (rc) break;
+    for (int j : running) {
+      --left[j];
+      done_work += jobs[j].n;
+    }
+    if (h.code) {
+      const int bad_ig = h.first_inst;
+      int bad = -1;
+      for (int j : running)
+        if (ig_of[j] == bad_ig) bad = j;
+      if (bad < 0) { rc = h.code; break; }   // not attributable to one job
+      rc = retire(bad, h.code);
+      if (!rc) rc = gp_clear_status(c);
+    }
+    for (size_t k = 0; k < running.size() && !rc;) {
+      const int j = running[k];
+      if (left[j] <= 0) rc = retire(j, GP_OK); else ++k;
+    }
+  }
+  if (particle_steps) *particle_steps = done_work;
+  return rc;
+}
+
 // Coordinate descent over the launch grids: each tunable in turn, each candidate timed
 // by one-step graphs on the live ensemble (median of three), the fastest kept.  The
 // state is saved before and restored after, so the ensemble does not move; the pool
@@ -1064,7 +1341,7 @@ int gp_autotune(gp_ctx *c, int32_t *grids_out) {
   const int64_t n = c->n;
   double *save = nullptr;
   GP_TRY(dalloc(&save, (size_t)kNState * n));
-  launch_gather_state(c->d_inst, c->d_pv, c->n, save, c->d_fluid_cols, nullptr, n, c->stream);
+  launch_gather_state(c->d_inst, c->d_pv, c->n_slots, -1, save, c->d_fluid_cols, nullptr, n, c->stream);
   GP_CK(cudaGetLastError());
   static const int kMult[] = {1, 2, 4, 8, 16};
   static const int kPhase[GP_NTUNE] = {GP_PHASE_GATHER, GP_PHASE_INTEGRATE, GP_PHASE_BIN, GP_PHASE_SEARCH};
@@ -1088,7 +1365,7 @@ int gp_autotune(gp_ctx *c, int32_t *grids_out) {
   }
   drop_graph(c);
   if (!rc) {
-    launch_scatter_state(c->d_inst, c->d_pv, c->n, save, n, c->stream);
+    launch_scatter_state(c->d_inst, c->d_pv, c->n_slots, save, n, c->stream);
     if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(c->stream) != cudaSuccess) rc = GP_ECUDA;
   }
   cudaFree(save);

@@ -202,7 +202,7 @@ __global__ void __launch_bounds__(128, GP_CONTACT_MIN_BLOCKS) k_contact(const In
     const unsigned long long slot = atomicAdd(ncoll, 1ull);
     if ((int64_t)slot >= cap_coll) {
       atomicAdd(&st->overflow, 1ull);
-      set_error(st, GP_EPAIR_OVERFLOW, (long long)P.id[i1]);
+      set_error(st, GP_EPAIR_OVERFLOW, (long long)P.id[i1], P.inst[i1]);
       continue;
     }
     CollRec r;
@@ -250,7 +250,7 @@ __global__ void k_response(const InstDev *__restrict__ insts, const PoolView *__
     const Quat q2 = {P.st[6][i2], P.st[7][i2], P.st[8][i2], P.st[9][i2]};
     const int rc = collision_response(I.ecp, I.mup, P.pc[7][i1], P.pc[8][i1], P.pc[9][i1], u1, o1, q1, u2, o2, q2,
                                       r.rx1, r.rx2, r.cn);
-    if (rc) set_error(st, rc, (long long)P.id[i1]);
+    if (rc) set_error(st, rc, (long long)P.id[i1], P.inst[i1]);
     P.st[3][i1] = u1[0]; P.st[4][i1] = u1[1]; P.st[5][i1] = u1[2];
     P.st[10][i1] = o1[0]; P.st[11][i1] = o1[1]; P.st[12][i1] = o1[2];
     P.st[3][i2] = u2[0]; P.st[4][i2] = u2[1]; P.st[5][i2] = u2[2];

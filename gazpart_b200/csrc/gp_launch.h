@@ -61,12 +61,13 @@ void launch_match(const CollRec *coll, const unsigned long long *ncoll, int64_t 
                   unsigned long long *best2, int8_t *matched, int8_t *state, Status *st, cudaStream_t s);
 void launch_field_layout(void *dst, int prec, int nx, int ny, int nz, int ncomp, int comp, const double *src,
                          int src_layout, int ghost_mode, cudaStream_t s);
-void launch_gather_state(const InstDev *insts, const PoolView *pv, int64_t n, double *out,
+void launch_gather_state(const InstDev *insts, const PoolView *pv, int64_t n, int only, double *out,
                          double *const *fluid_cols, double *fluid_out, int64_t count, cudaStream_t s);
+void launch_retire(const PoolView *pv, int64_t n, int inst, cudaStream_t s);
 void launch_scatter_state(const InstDev *insts, const PoolView *pv, int64_t n, const double *cols,
                           int64_t count, cudaStream_t s);
 void launch_init_pool(const PoolView *pv, int64_t begin, int64_t n, int inst, const double *cols,
-                      const double *pcs, int64_t ld, cudaStream_t s);
+                      const double *pcs, int64_t ld, int64_t src, cudaStream_t s);
 void launch_connectivity(int nxb, int nyb, int nzb, int periodicity, int32_t *ncon, int32_t *con, cudaStream_t s);
 
 }  // namespace gp

@@ -223,7 +223,7 @@ __global__ void k_bin_scatter(const InstDev *__restrict__ insts, const PoolView 
       if (i0 >= 1 && i0 <= I.nxbox && j0 >= 1 && j0 <= I.nybox && k0 >= 1 && k0 <= I.nzbox)
         box = (long long)(i0 - 1) | ((long long)(j0 - 1) << 21) | ((long long)(k0 - 1) << 42);
     }
-    if (box < 0) set_error(st, GP_EOUT_OF_GRID, (long long)P.id[i]);
+    if (box < 0) set_error(st, GP_EOUT_OF_GRID, (long long)P.id[i], P.inst[i]);
     sa.sbox[pos] = box;
   }
 }
@@ -583,15 +583,16 @@ void launch_field_layout(void *dst, int prec, int nx, int ny, int nz, int ncomp,
 
 // Pool -> caller order for one instance: out[c*count + id] = state column c.
 // Pool -> caller order: out[c*count + begin(class) + id] = state column c, where the
-// caller's arrays hold the classes one after another.
+// caller's arrays hold the classes one after another; with only >= 0, class `only`
+// alone at offset 0.
 __global__ void k_gather_state(const InstDev *__restrict__ insts, const PoolView *__restrict__ pv, int64_t n,
-                               double *__restrict__ out, double *const *fluid, double *__restrict__ fout,
+                               int only, double *__restrict__ out, double *const *fluid, double *__restrict__ fout,
                                int64_t count) {
   const PoolView P = *pv;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const int inst = P.inst[i];
-    if (inst < 0) continue;
-    const int64_t id = insts[inst].begin + P.id[i];
+    if (inst < 0 || (only >= 0 && inst != only)) continue;
+    const int64_t id = (only >= 0 ? 0 : insts[inst].begin) + P.id[i];
     if (id < 0 || id >= count) continue;
 #pragma unroll
     for (int c = 0; c < kNState; ++c) out[c * count + id] = P.st[c][i];
@@ -602,10 +603,21 @@ __global__ void k_gather_state(const InstDev *__restrict__ insts, const PoolView
   }
 }
 
-void launch_gather_state(const InstDev *insts, const PoolView *pv, int64_t n, double *out, double *const *fluid_cols,
-                         double *fluid_out, int64_t count, cudaStream_t s) {
+void launch_gather_state(const InstDev *insts, const PoolView *pv, int64_t n, int only, double *out,
+                         double *const *fluid_cols, double *fluid_out, int64_t count, cudaStream_t s) {
   const int grid = 148 * 8;
-  k_gather_state<<<grid, 256, 0, s>>>(insts, pv, n, out, fluid_cols, fluid_out, count);
+  k_gather_state<<<grid, 256, 0, s>>>(insts, pv, n, only, out, fluid_cols, fluid_out, count);
+}
+
+// Retires class `inst`: its particles leave the binning, and the next advance drops them.
+__global__ void k_retire(const PoolView *__restrict__ pv, int64_t n, int inst) {
+  const PoolView P = *pv;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    if (P.inst[i] == inst) P.inst[i] = -1;
+}
+
+void launch_retire(const PoolView *pv, int64_t n, int inst, cudaStream_t s) {
+  if (n > 0) k_retire<<<148 * 8, 256, 0, s>>>(pv, n, inst);
 }
 
 // caller order -> pool (state columns only)
@@ -627,26 +639,27 @@ void launch_scatter_state(const InstDev *insts, const PoolView *pv, int64_t n, c
   k_scatter_state<<<148 * 8, 256, 0, s>>>(insts, pv, n, cols, count);
 }
 
-// One class into pool slots [begin, begin+n): columns are caller arrays of leading
-// dimension ld holding the class at offset begin; ids are 0-based within the class.
+// One class into pool slots [begin, begin+n): particle k of the class is column entry
+// src + k of the staged arrays (leading dimension ld); ids are 0-based within the class.
 __global__ void k_init_pool(const PoolView *__restrict__ pv, int64_t begin, int64_t n, int inst,
-                            const double *__restrict__ cols, const double *__restrict__ pcs, int64_t ld) {
+                            const double *__restrict__ cols, const double *__restrict__ pcs, int64_t ld,
+                            int64_t src) {
   const PoolView P = *pv;
   for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t i = begin + k;
+    const int64_t i = begin + k, e = src + k;
 #pragma unroll
-    for (int c = 0; c < kNState; ++c) P.st[c][i] = cols[c * ld + i];
+    for (int c = 0; c < kNState; ++c) P.st[c][i] = cols[c * ld + e];
 #pragma unroll
-    for (int c = 0; c < kNConst; ++c) P.pc[c][i] = pcs[c * ld + i];
+    for (int c = 0; c < kNConst; ++c) P.pc[c][i] = pcs[c * ld + e];
     P.id[i] = (int32_t)k;
     P.inst[i] = inst;
   }
 }
 
 void launch_init_pool(const PoolView *pv, int64_t begin, int64_t n, int inst, const double *cols, const double *pcs,
-                      int64_t ld, cudaStream_t s) {
+                      int64_t ld, int64_t src, cudaStream_t s) {
   if (n <= 0) return;
-  k_init_pool<<<148 * 8, 256, 0, s>>>(pv, begin, n, inst, cols, pcs, ld);
+  k_init_pool<<<148 * 8, 256, 0, s>>>(pv, begin, n, inst, cols, pcs, ld, src);
 }
 
 __global__ void k_iota(int32_t *a, int64_t n) {

@@ -45,7 +45,7 @@ struct PoolView {
 // Device status word: first error code, the id that raised it, counters.
 struct Status {
   int32_t code;
-  int32_t pad;
+  int32_t first_inst;   // class of the first error + 1 (0: not a particle's error)
   long long first_id;
   unsigned long long n_near;      // candidate pairs within bounding distance
   unsigned long long n_contact;   // pairs in contact
@@ -54,8 +54,11 @@ struct Status {
   unsigned long long overflow;    // pairs dropped by a full buffer
 };
 
-__device__ inline void set_error(Status *s, int code, long long id) {
-  if (atomicCAS(&s->code, 0, code) == 0) s->first_id = id;
+__device__ inline void set_error(Status *s, int code, long long id, int inst = -1) {
+  if (atomicCAS(&s->code, 0, code) == 0) {
+    s->first_id = id;
+    s->first_inst = inst + 1;
+  }
 }
 
 // A candidate pair in the pool: HOME/NEAR pool slots plus the reference order key

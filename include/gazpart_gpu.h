@@ -107,6 +107,8 @@ int gp_ctx_destroy(gp_ctx *ctx);
 /* First error recorded on the device since the last gp_clear_status: code and the
  * particle (or pair home) index that raised it. */
 int gp_status(gp_ctx *ctx, int32_t *code, int64_t *first_id);
+/* Class (IG, 1-based) of the particle that raised the first error, 0 if none. */
+int gp_status_class(gp_ctx *ctx, int32_t *ig);
 int gp_clear_status(gp_ctx *ctx);
 int gp_sync(gp_ctx *ctx);
 
@@ -137,6 +139,54 @@ int gp_download_state(gp_ctx *ctx, int64_t n, double *const *cols, double *const
  * gp_upload_state(n, ...) is the one-class case. */
 int gp_upload_classes(gp_ctx *ctx, int32_t nclass, const int64_t *counts, const double *const *cols,
                       const double *const *props, int32_t on_device);
+
+/* ------------------------------------------------ resident fields and jobs ---- */
+/* No counterpart in the reference (serving).  More resident fields beside the one of
+ * gp_params: an (nx, ny, nz) mesh of the box (lx, ly, lz), same precision; *field
+ * receives its slot (the context's own field is slot 0). */
+int gp_add_field(gp_ctx *ctx, int32_t nx, int32_t ny, int32_t nz, double lx, double ly, double lz,
+                 int32_t *field);
+/* gp_set_field for field slot `field`. */
+int gp_set_field_slot(gp_ctx *ctx, int32_t field, int32_t comp, const double *src, int32_t src_layout,
+                      int32_t ghost_mode, int32_t on_device);
+/* No counterpart in the reference (serving).  Admits one more class of n particles on
+ * field slot `field` while others are resident: its particles join the pool (capacity
+ * max_particles), it gets its own box and search grids, and from the next step on it is
+ * advanced and collided (within itself) together with the others.  *ig receives its
+ * class number (1-based, reused after gp_remove_class). */
+int gp_add_class(gp_ctx *ctx, int32_t field, int64_t n, const double *const *cols,
+                 const double *const *props, int32_t on_device, int32_t *ig);
+/* One class's state columns in its own particle order (cols: GP_NSTATE pointers). */
+int gp_download_class(gp_ctx *ctx, int32_t ig, double *const *cols, int32_t on_device);
+/* Retires class ig, first downloading its state into cols unless cols is NULL; its
+ * slots are reclaimed by the next advance. */
+int gp_remove_class(gp_ctx *ctx, int32_t ig, double *const *cols, int32_t on_device);
+/* Particles of class ig (0 once retired). */
+int gp_class_count(gp_ctx *ctx, int32_t ig, int64_t *n);
+
+/* No counterpart in the reference (serving).  One tracking job: a class of n particles
+ * on resident field slot `field`, run for `steps` steps.  cols: GP_NSTATE host columns,
+ * the initial state in and the final state out; props: GP_NPROP host columns. */
+typedef struct {
+    int32_t field;
+    int32_t steps;
+    int64_t n;
+    double arrival_s;              /* arrival, seconds after gp_serve starts */
+    double *const *cols;
+    const double *const *props;
+    double admitted_s, done_s;     /* out: admission and completion times (seconds) */
+    int32_t status;                /* out: GP_OK, or the error that stopped this job */
+    int32_t pad;
+} gp_job;
+/* Continuous batching over a job stream: jobs are admitted in arrival order as soon as
+ * n * bytes_per_particle fits the HBM budget beside the running ones (and the pool,
+ * capacity max_particles, has room); every iteration advances and collides all running
+ * jobs in the same launches; finished jobs leave with their final state, and a job
+ * whose particle raises an error leaves at once with that status while the others
+ * continue.  Fields and particle state stay resident throughout.  *particle_steps:
+ * the sum over steps of the particles stepped. */
+int gp_serve(gp_ctx *ctx, gp_job *jobs, int32_t njobs, double hbm_budget, double bytes_per_particle,
+             int64_t *particle_steps);
 
 /* Replace the state columns of the resident particles (properties unchanged), caller
  * order.  The drop-in form of handing PART back to the device after host-side edits. */
