@@ -43,6 +43,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the FP64 comparison run")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch grids")
+    ap.add_argument("--serve-seconds", type=float, default=2.0, help="arrival window of the serving workload")
     return ap.parse_args()
 
 
@@ -244,9 +245,96 @@ def workload_max_emaj(w) -> float:
 
 
 # ---------------------------------------------------------------------------
+# serving: a Poisson job stream through gp_serve
+# ---------------------------------------------------------------------------
+def run_serving(args, rank: int, world: int, local: int):
+    """Jobs arriving at 20/s for --serve-seconds, each on one of eight resident fields,
+    admitted against the HBM budget and stepped together until all are done."""
+    import dataclasses
+    import torch
+    from gazpart_b200 import api, config, field, particles, serving
+    w = config.C5
+    device = f"cuda:{local}"
+    torch.cuda.set_device(local)
+    stream = w.jobs(args.serve_seconds, seed=5 + rank)
+    fields = [field.generate(n, seed=sd, device=device) for n, sd in w.fields]
+    jobs = []
+    for fid, (n, _) in enumerate(w.fields):
+        mine = [(t, spec, steps) for t, f_, spec, steps in stream if f_ == fid]
+        if not mine:
+            continue
+        setup = w.setup(n)
+        with api.Context(setup, "mixed") as tmp:
+            tmp.set_fields({k: fields[fid][k].contiguous() for k in api.FIELD_KEYS})
+            for t, spec, steps in mine:
+                m = min(setup.lx / 4.0, 1.1 * 6.0 * w.dtime * steps)
+                st = particles.draw(dataclasses.replace(spec, x_margin=m), setup)
+                xs = [torch.from_numpy(st[k]).to(device) for k in ("x", "y", "z")]
+                g = [tmp.interp_lag3(c, *xs).cpu().numpy() for c in range(6)]
+                st["u"], st["v"], st["w"] = g[0], g[1], g[2]
+                particles.body_half_vorticity(st, g[3], g[4], g[5])
+                jobs.append(serving.Job(state=st, steps=steps, arrival_s=t, field=fid))
+    jobs.sort(key=lambda j: j.arrival_s)
+    field_bytes = sum((n + 3) * (n + 4) ** 2 * 8 * 4 for n, _ in w.fields)
+    budget = w.hbm_budget - field_bytes
+    total = sum(j.n for j in jobs)
+    cap = int(min(budget / serving.BYTES_PER_PARTICLE, 1.5 * total))   # pool sized for the stream
+    ctx = api.Context(w.setup(w.fields[0][0]), "mixed", max_particles=cap)
+    ctx.set_fields({k: fields[0][k].contiguous() for k in api.FIELD_KEYS})
+    for fid in range(1, len(w.fields)):
+        assert ctx.add_field(w.fields[fid][0]) == fid
+        ctx.set_fields({k: fields[fid][k].contiguous() for k in api.FIELD_KEYS}, slot=fid)
+    del fields
+    torch.cuda.synchronize()
+    with Clocks(local) as clk:
+        summary = serving.serve(ctx, jobs, budget)
+    clocks = clk.summary()
+    ctx.close()
+    value = summary["particle_steps_per_s"]
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([value], dtype=torch.float64, device=device)
+        dist.all_reduce(t)
+        value = float(t.item())
+    if rank == 0:
+        line = {"metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
+                "steps": None, "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32/f64", "data": "synthetic",
+                "config": {"workload": w.name, "precision": "mixed", "arrival_rate_per_s": w.rate_per_s,
+                           "window_s": args.serve_seconds, "jobs": len(jobs), "particles": total,
+                           "hbm_budget_bytes": budget, "dtime": w.dtime},
+                "latency_p50_s": summary["latency_p50_s"], "latency_p99_s": summary["latency_p99_s"],
+                "serving": summary, "clocks": clocks,
+                "e2e": {"value": value, "unit": "particle-steps/s",
+                        "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
+                        "note": "every job enters from and returns to host arrays"}}
+        print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
 def main():
     args = parse()
     from gazpart_b200 import config
+    if args.workload == config.C5.name:
+        if args.impl == "reference":
+            if int(os.environ.get("RANK", "0")) == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "serving is a form of the GPU path; the "
+                                  "CPU port is timed on single-ensemble workloads"}), flush=True)
+            return
+        rank, world = int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1"))
+        local = int(os.environ.get("LOCAL_RANK", "0"))
+        dist = None
+        if world > 1:
+            import torch
+            import torch.distributed as dist
+            from datetime import timedelta
+            dist.init_process_group("nccl", timeout=timedelta(seconds=600),
+                                    device_id=torch.device(f"cuda:{local}"))
+        run_serving(args, rank, world, local)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
     w = config.WORKLOADS[args.workload]
     precision = args.precision or ("mixed" if w.field_dtype == "f32" else "fp64")
     rank = int(os.environ.get("RANK", "0"))

@@ -209,4 +209,51 @@ _C4_REFERENCE = ParticleSpec(n=1, ar=1.0, b=0.002, st=1.0)
 
 C4 = BatchedWorkload("c4_256cube_64inst_fp32field", 256, "f32", c4_instances(), 5.0e-4, 300)
 
+
+
+@dataclasses.dataclass
+class ServingWorkload:
+    """A Poisson stream of tracking jobs on resident fields."""
+    name: str
+    fields: Tuple[Tuple[int, int], ...]     # (grid points per side, seed) of each resident field
+    rate_per_s: float
+    n_range: Tuple[float, float]            # log-uniform particle count
+    steps_range: Tuple[int, int]            # uniform step count
+    ar_range: Tuple[float, float]           # log-uniform aspect ratio, one per job
+    st_range: Tuple[float, float]           # log-uniform Stokes number, one per job
+    b: float
+    dtime: float
+    hbm_budget: float
+
+    def setup(self, grid: int) -> Setup:
+        return Setup(nx=grid, ny=grid, nz=grid, visc=viscosity_for(_C4_REFERENCE, integral_time()),
+                     dtime=self.dtime)
+
+    def jobs(self, window_s: float, seed: int = 5):
+        """(arrival, field slot, spec, steps) of the jobs that arrive within window_s."""
+        import numpy as np
+        rng = np.random.default_rng(seed)
+        t, out, j = 0.0, [], 0
+        while True:
+            t += rng.exponential(1.0 / self.rate_per_s)
+            if t > window_s:
+                return out
+            n = int(np.exp(rng.uniform(math.log(self.n_range[0]), math.log(self.n_range[1]))))
+            steps = int(rng.integers(self.steps_range[0], self.steps_range[1] + 1))
+            ar = float(np.exp(rng.uniform(math.log(self.ar_range[0]), math.log(self.ar_range[1]))))
+            st = float(np.exp(rng.uniform(math.log(self.st_range[0]), math.log(self.st_range[1]))))
+            fid = int(rng.integers(0, len(self.fields)))
+            out.append((t, fid, ParticleSpec(n=n, ar=ar, b=self.b, st=st, seed=1_000_000 + j,
+                                             density_from_st=True), steps))
+            j += 1
+
+
+# Jobs at 20/s on eight resident FP32 fields (four 128^3, four 256^3), N log-uniform in
+# [1e3, 4e6], steps uniform in [100, 2000], one aspect ratio and Stokes number per job,
+# 150 GB of HBM for the jobs.  dt = 1e-4 keeps a 2000-step job clear of the x planes
+# (see bench.x_margin_for).
+C5 = ServingWorkload("c5_serving_8fields_20jobs_per_s", ((128, 0), (128, 1), (128, 2), (128, 3),
+                                                        (256, 4), (256, 5), (256, 6), (256, 7)),
+                     20.0, (1e3, 4e6), (100, 2000), (0.2, 5.0), (0.1, 10.0), 0.002, 1.0e-4, 150e9)
+
 WORKLOADS = {w.name: w for w in (C1, C2, C3, C4)}
