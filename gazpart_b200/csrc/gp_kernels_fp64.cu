@@ -164,7 +164,15 @@ __global__ void __launch_bounds__(128, GP_CONTACT_MIN_BLOCKS) k_contact(const In
             q1 = {P.st[6][i1], P.st[7][i1], P.st[8][i1], P.st[9][i1]};
             q2 = {P.st[6][i2], P.st[7][i2], P.st[8][i2], P.st[9][i2]};
             a1 = P.pc[0][i1]; b1 = P.pc[1][i1]; a2 = P.pc[0][i2]; b2 = P.pc[1][i2];
-            if (contact_setup(a1, b1, a2, b2, c1, q1, c2, q2, CP, S.x)) {
+            // symmetry axes (first columns of R(q)); disjoint bodies need no solve
+            const double e1[3] = {1.0 - 2.0 * (q1.c * q1.c + q1.d * q1.d), 2.0 * (q1.b * q1.c + q1.a * q1.d),
+                                  2.0 * (q1.b * q1.d - q1.a * q1.c)};
+            const double e2[3] = {1.0 - 2.0 * (q2.c * q2.c + q2.d * q2.d), 2.0 * (q2.b * q2.c + q2.a * q2.d),
+                                  2.0 * (q2.b * q2.d - q2.a * q2.c)};
+            const double dd = sqrt(vkx * vkx + vky * vky + vkz * vkz);
+            const bool apart = dd > 0.0 && separated(vkx, vky, vkz, e1, a1 * a1, b1 * b1, e2, a2 * a2, b2 * b2,
+                                                     vkx / dd, vky / dd, vkz / dd);
+            if (!apart && contact_setup(a1, b1, a2, b2, c1, q1, c2, q2, CP, S.x)) {
               lm_begin(CP, S);
               active = true;
             }

@@ -587,6 +587,63 @@ GP_LM_FN int lm_step(const ContactProb& P, LmState& S, double tol) {
 }
 
 // Margin function mod_particle_parallel.f90:145-201: v^T (R diag(1/a^2,1/b^2,1/b^2) R^T) v
+// Separating-direction test for two spheroids whose bounding spheres overlap and whose
+// extents along the centre line do too.  With support functions
+// h_i(n) = sqrt(b_i^2 + (a_i^2 - b_i^2) (e_i.n)^2), the bodies are disjoint if some unit
+// n has g(n) = n.d - h_1(n) - h_2(n) > 0 (d from body 1 to body 2).  g is concave, so
+// a few projected-gradient steps from the centre line (the best of four step lengths
+// each) find such an n for nearly every disjoint pair.  Disjoint bodies cannot hold
+// each other's support points, so ellipsoid_contact_detection.f90:125 cannot flag the
+// pair; g must exceed 1e-9 of its terms, far above rounding, so a pair is dropped only
+// when it is disjoint.
+static __device__ __forceinline__ double support_gap(const double n[3], double dx, double dy, double dz, const double e1[3],
+                                              double a1, double b1, const double e2[3], double a2, double b2,
+                                              double &h1, double &h2, double &c1, double &c2) {
+  c1 = e1[0] * n[0] + e1[1] * n[1] + e1[2] * n[2];
+  c2 = e2[0] * n[0] + e2[1] * n[1] + e2[2] * n[2];
+  h1 = sqrt(fmax(b1 + (a1 - b1) * c1 * c1, 0.0));
+  h2 = sqrt(fmax(b2 + (a2 - b2) * c2 * c2, 0.0));
+  return n[0] * dx + n[1] * dy + n[2] * dz - h1 - h2;
+}
+
+static __device__ __noinline__ bool separated(double dx, double dy, double dz, const double e1[3], double a1, double b1,
+                                       const double e2[3], double a2, double b2, double ux, double uy, double uz) {
+  double n[3] = {ux, uy, uz};
+  const double dist = sqrt(dx * dx + dy * dy + dz * dz);
+  double h1, h2, c1, c2;
+  double g = support_gap(n, dx, dy, dz, e1, a1, b1, e2, a2, b2, h1, h2, c1, c2);
+  for (int it = 0; it < 4; ++it) {
+    // gradient of g: d - E1 n / h1 - E2 n / h2, with E n = b^2 n + (a^2 - b^2)(e.n) e
+    double gr[3];
+    for (int k = 0; k < 3; ++k) {
+      const double d_k = k == 0 ? dx : (k == 1 ? dy : dz);
+      gr[k] = d_k - (b1 * n[k] + (a1 - b1) * c1 * e1[k]) / h1 - (b2 * n[k] + (a2 - b2) * c2 * e2[k]) / h2;
+    }
+    const double gn = gr[0] * n[0] + gr[1] * n[1] + gr[2] * n[2];
+    const double t[3] = {(gr[0] - gn * n[0]) / dist, (gr[1] - gn * n[1]) / dist, (gr[2] - gn * n[2]) / dist};
+    double best = -1e300, bn[3] = {n[0], n[1], n[2]}, bh1 = h1, bh2 = h2, bc1 = c1, bc2 = c2;
+    for (double alpha = 0.25; alpha <= 2.0; alpha *= 2.0) {
+      double m[3] = {n[0] + alpha * t[0], n[1] + alpha * t[1], n[2] + alpha * t[2]};
+      const double inv = 1.0 / sqrt(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
+      m[0] *= inv; m[1] *= inv; m[2] *= inv;
+      double mh1, mh2, mc1, mc2;
+      const double gm = support_gap(m, dx, dy, dz, e1, a1, b1, e2, a2, b2, mh1, mh2, mc1, mc2);
+      if (gm > best) {
+        best = gm;
+        bn[0] = m[0]; bn[1] = m[1]; bn[2] = m[2];
+        bh1 = mh1; bh2 = mh2; bc1 = mc1; bc2 = mc2;
+      }
+    }
+    if (!(best > g)) return false;   // no progress (or NaN): keep the pair
+    n[0] = bn[0]; n[1] = bn[1]; n[2] = bn[2];
+    h1 = bh1; h2 = bh2; c1 = bc1; c2 = bc2;
+    g = best;
+    const double scale = fabs(n[0] * dx + n[1] * dy + n[2] * dz) + h1 + h2;
+    if (g > 1e-9 * scale) return true;
+  }
+  return false;
+}
+
 GP_LM_FN double fmargin(double a, double b, const double pt[3], const double c[3], const Quat& q) {
   double ell[9];
   rot_diag(q, 1.0 / (a * a), 1.0 / (b * b), 1.0 / (b * b), ell);
