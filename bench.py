@@ -285,6 +285,13 @@ def run_serving(args, rank: int, world: int, local: int):
         assert ctx.add_field(w.fields[fid][0]) == fid
         ctx.set_fields({k: fields[fid][k].contiguous() for k in api.FIELD_KEYS}, slot=fid)
     del fields
+    tune = None
+    if not args.no_autotune:
+        # launch grids tuned on the largest job's particles, which then leave again
+        big = max(jobs, key=lambda j: j.n)
+        ig = ctx.add_class({k: np.array(v, copy=True) for k, v in big.state.items()}, big.field)
+        tune = ctx.autotune()
+        ctx.remove_class(ig)
     torch.cuda.synchronize()
     with Clocks(local) as clk:
         summary = serving.serve(ctx, jobs, budget)
@@ -302,7 +309,7 @@ def run_serving(args, rank: int, world: int, local: int):
                 "vs_baseline": None, "dtype": "f32/f64", "data": "synthetic",
                 "config": {"workload": w.name, "precision": "mixed", "arrival_rate_per_s": w.rate_per_s,
                            "window_s": args.serve_seconds, "jobs": len(jobs), "particles": total,
-                           "hbm_budget_bytes": budget, "dtime": w.dtime},
+                           "hbm_budget_bytes": budget, "dtime": w.dtime, "launch_grids": tune},
                 "latency_p50_s": summary["latency_p50_s"], "latency_p99_s": summary["latency_p99_s"],
                 "serving": summary, "clocks": clocks,
                 "e2e": {"value": value, "unit": "particle-steps/s",

@@ -123,3 +123,36 @@ def test_replica_timing_reduction_two_ranks():
         p.join(120)
         assert p.exitcode == 0
     assert out[0] == 20.0 and out[1] == 20.0
+
+
+def test_batched_workload_instances():
+    w = config.C4
+    assert len(w.instances) == 64
+    n = np.array([s.n for s in w.instances])
+    assert n.min() >= 1000 and n.max() <= 2_000_000
+    assert abs(n.sum() - 1.7e7) < 1e5                    # the stated total
+    st = np.array([s.st for s in w.instances])
+    ar = np.array([s.ar for s in w.instances])
+    assert st.min() >= 0.1 and st.max() <= 10 and ar.min() >= 0.2 and ar.max() <= 5
+    assert len({s.seed for s in w.instances}) == 64
+    one = particles.draw(config.ParticleSpec(**{**w.instances[0].__dict__, "n": 500}), w.setup())
+    deq = 2 * one["emaj"] / one["apr"] ** (2 / 3)
+    st_num = one["rhop"] * deq ** 2 / (18 * w.setup().visc) / config.integral_time()
+    assert np.allclose(st_num, w.instances[0].st)      # density follows the instance's Stokes number
+
+
+def test_serving_stream_and_concurrency_count():
+    from gazpart_b200 import serving
+    w = config.C5
+    jobs = w.jobs(50.0, seed=3)
+    t = np.array([j[0] for j in jobs])
+    assert np.all(np.diff(t) > 0) and t[-1] <= 50.0
+    assert abs(len(jobs) / 50.0 - w.rate_per_s) < 3.0    # Poisson at 20/s
+    steps = np.array([j[3] for j in jobs])
+    n = np.array([j[2].n for j in jobs])
+    assert steps.min() >= 100 and steps.max() <= 2000
+    assert n.min() >= 1000 and n.max() <= 4_000_000
+    assert set(j[1] for j in jobs) == set(range(len(w.fields)))
+    fake = [serving.Job(state={"x": np.zeros(1)}, steps=1, admitted_s=a, done_s=d)
+            for a, d in ((0.0, 2.0), (1.0, 3.0), (2.5, 4.0), (5.0, 6.0))]
+    assert serving.max_concurrent(fake) == 2
