@@ -390,7 +390,7 @@ def main():
 
     # the autotuner's trials (60 one-step graphs) and the three one-step gathers also
     # move the particles before the state is restored
-    run_steps = args.warmup + args.steps + args.e2e_steps + 63
+    run_steps = args.warmup + args.steps + args.e2e_steps + 64
     setup, f, st = build_inputs(w, device, precision, run_steps)
     batched = isinstance(st, list)
     max_emaj = float(st["emaj"].max()) if not batched else None
@@ -437,16 +437,28 @@ def main():
     pinned = {k: torch.empty(n, dtype=torch.float64, pin_memory=True).numpy() for k in api.STATE_KEYS}
     ctx.download_into(pinned)
     ctx.sync()
+    ctx.step(1)            # capture the one-step graph outside the timed loop
+    ctx.sync()
+    parts = {"h2d": 0.0, "step": 0.0, "d2h": 0.0}
     t0 = time.perf_counter()
     for _ in range(args.e2e_steps):
+        ta = time.perf_counter()
         ctx.put_state(pinned)
+        tb = time.perf_counter()
         ctx.step(1)
+        ctx.sync()
+        tc = time.perf_counter()
         ctx.download_into(pinned)
+        td = time.perf_counter()
+        parts["h2d"] += tb - ta
+        parts["step"] += tc - tb
+        parts["d2h"] += td - tc
     e2e_s = (time.perf_counter() - t0) / args.e2e_steps
     ctx.raise_status("e2e steps")
     bytes_state = 13 * 8 * n
     e2e = {"value": n / e2e_s, "unit": "particle-steps/s", "h2d_bytes_per_step": bytes_state,
-           "d2h_bytes_per_step": bytes_state, "ms_per_step": 1e3 * e2e_s}
+           "d2h_bytes_per_step": bytes_state, "ms_per_step": 1e3 * e2e_s,
+           "ms_parts": {k: 1e3 * v / args.e2e_steps for k, v in parts.items()}}
 
     plain = None
     if not args.no_plain and precision == "mixed":

@@ -178,7 +178,7 @@ __device__ __forceinline__ void gather6_fp32(const InstDev& I, const Stencil& s,
 // Mixed-precision force and torque: relative velocities and frames in FP64, the
 // Zastawny correlation coefficients in FP32, forces assembled in FP64.
 // ---------------------------------------------------------------------------
-static __device__ __noinline__ bool fluid_force_mixed(const PartConst& pc, double visc, double up, double vp,
+static __device__ __forceinline__ bool fluid_force_mixed(const PartConst& pc, double visc, double up, double vp,
                                                   double wp, double uf, double vf, double wf, const double r[9],
                                                   double f[3]) {
   double p[3] = {uf - up, vf - vp, wf - wp};
@@ -216,7 +216,7 @@ static __device__ __noinline__ bool fluid_force_mixed(const PartConst& pc, doubl
   return !(cdrag != cdrag) && isfinite(f[0]) && isfinite(f[1]) && isfinite(f[2]);
 }
 
-static __device__ __noinline__ void fluid_torque_mixed(const PartConst& pc, double visc, double upn, double vpn,
+static __device__ __forceinline__ void fluid_torque_mixed(const PartConst& pc, double visc, double upn, double vpn,
                                                    double wpn, double uf, double vf, double wf, double wx,
                                                    double wy, double wz, double ox, double oy, double oz,
                                                    const double r[9], double t[3]) {
@@ -262,7 +262,7 @@ static __device__ __noinline__ void fluid_torque_mixed(const PartConst& pc, doub
 template <bool kMixed>
 struct Forces {
   // F (lab frame, per unit mass) and T (body frame) for stage velocities.
-  __device__ __noinline__ static bool eval(const PartConst& pc, double visc, const double u[3],
+  __device__ __forceinline__ static bool eval(const PartConst& pc, double visc, const double u[3],
                                               const double un[3], const double uf[3], const double wv[3],
                                               double ox, double oy, double oz, const Quat& q, double f[3],
                                               double t[3]) {

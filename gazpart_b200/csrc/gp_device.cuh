@@ -101,7 +101,7 @@ __host__ __device__ inline Quat mult_quat(const Quat& x, const Quat& y) {
 }
 
 // adv_quaternion.f90:39-84 (direct multiplication, no renormalisation)
-inline __host__ __device__ __noinline__ void quaternion_integration(Quat& q, double ox, double oy, double oz, double dt) {
+__host__ __device__ __forceinline__ void quaternion_integration(Quat& q, double ox, double oy, double oz, double dt) {
   double omg[3] = {ox, oy, oz};
   rot_vec(q, omg);
   const double nrm = sqrt(omg[0] * omg[0] + omg[1] * omg[1] + omg[2] * omg[2]);
@@ -152,7 +152,7 @@ struct PartConst {
 // fluid_force_ellipsoid.f90:1-161 (guards: zero relative speed -> zero force; zero
 // transverse speed -> zero transverse lift; the reference stops or yields NaN there).
 // Returns false if CDRAG is NaN (the reference's stop at :150-159).
-static __device__ __noinline__ bool fluid_force(const PartConst& pc, double visc, double up, double vp, double wp,
+static __device__ __forceinline__ bool fluid_force(const PartConst& pc, double visc, double up, double vp, double wp,
                                    double uf, double vf, double wf, const Quat& q, double fd[3], double fl[3]) {
   constexpr double a0 = 1.95, a1 = 18.12, a2 = 1.023, a3 = 4.26, a4 = 0.384;
   constexpr double a5 = 21.52, a6 = 0.990, a7 = 2.86, a8 = 0.260;
@@ -196,7 +196,7 @@ static __device__ __noinline__ bool fluid_force(const PartConst& pc, double visc
 
 // fluid_torque_ellipsoid.f90:1-190.  Relative velocity from the particle's stored
 // velocity u_n (:88-105).  Guards as in fluid_force.  Pitching and rotation torques.
-static __device__ __noinline__ void fluid_torque(const PartConst& pc, double visc, double upn, double vpn, double wpn,
+static __device__ __forceinline__ void fluid_torque(const PartConst& pc, double visc, double upn, double vpn, double wpn,
                                     double uf, double vf, double wf, double wx, double wy, double wz,
                                     double ox, double oy, double oz, const Quat& q, double tp[3],
                                     double tr[3]) {
@@ -264,7 +264,7 @@ __host__ __device__ inline void k_matrix(const double inv_ip[9], const double rx
 // A centre farther than 1.5 bounding radii from the chosen plane cannot give margin<1
 // (margin >= dist^2/rmax^2 = 2.25), so that case skips the matrix work with the same
 // outcome.  Returns error code (0 ok, GP_ESINGULAR).
-static __device__ __noinline__ int wall_test(double lx, const PartConst& pc, double rmax, double xp, double yp, double zp,
+static __device__ __forceinline__ int wall_test(double lx, const PartConst& pc, double rmax, double xp, double yp, double zp,
                                 const Quat& q, double wn[3], double arm[3], double& delta_x, bool& isect) {
   arm[0] = arm[1] = arm[2] = 0.0;
   isect = false;
@@ -303,7 +303,7 @@ static __device__ __noinline__ int wall_test(double lx, const PartConst& pc, dou
 }
 
 // wall_ellipsoid_rebound.f90:1-387.  Returns 0, GP_ESINGULAR or GP_EENERGY.
-static __device__ __noinline__ int wall_rebound(double ecw, double muw, const PartConst& pc, double& u, double& v, double& w,
+static __device__ __forceinline__ int wall_rebound(double ecw, double muw, const PartConst& pc, double& u, double& v, double& w,
                                    double& ox, double& oy, double& oz, const Quat& q, const double ri[3],
                                    const double nw[3]) {
   double omg[3] = {ox, oy, oz};
