@@ -25,6 +25,8 @@ namespace gp {
 #else
 #define GP_LM_FN static __device__ __noinline__
 #endif
+// The pieces of one iteration are folded into the iteration itself.
+#define GP_LM_INNER static __device__ __forceinline__
 
 // MINPACK's scaled Euclidean norm (minpack_reduc.f90:180-232): three accumulators
 // for tiny, mid-range and huge components.
@@ -182,7 +184,7 @@ struct ContactProb {
 };
 
 // Support points along +-c(x) (ellipsoid_pair_depth.f90:117-142).
-GP_LM_FN void support_points(const ContactProb& P, const double x[2], double c1[3], double tmp1[3],
+GP_LM_INNER void support_points(const ContactProb& P, const double x[2], double c1[3], double tmp1[3],
                                                double tmp2[3], double& l1, double& l2, double pt1[3],
                                                double pt2[3]) {
   double s0, k0, s1, k1;
@@ -205,7 +207,7 @@ GP_LM_FN void support_points(const ContactProb& P, const double x[2], double c1[
 }
 
 // fcn, iflag=1 (ellipsoid_contact_detection.f90:290-295)
-GP_LM_FN void lm_fcn(const ContactProb& P, const double x[2], double fvec[3]) {
+GP_LM_INNER void lm_fcn(const ContactProb& P, const double x[2], double fvec[3]) {
   double c1[3], t1[3], t2[3], l1, l2, pt1[3], pt2[3];
   support_points(P, x, c1, t1, t2, l1, l2, pt1, pt2);
 #pragma unroll
@@ -215,7 +217,7 @@ GP_LM_FN void lm_fcn(const ContactProb& P, const double x[2], double fvec[3]) {
   }
 }
 
-GP_LM_FN void grad_coeff(const double e[9], const double c[3], double l, double co[9]) {
+GP_LM_INNER void grad_coeff(const double e[9], const double c[3], double l, double co[9]) {
   double row[3];
 #pragma unroll
   for (int j = 0; j < 3; ++j) row[j] = c[0] * e[3 * j] + c[1] * e[1 + 3 * j] + c[2] * e[2 + 3 * j];
@@ -233,7 +235,7 @@ GP_LM_FN void grad_coeff(const double e[9], const double c[3], double l, double 
 
 // fcn, iflag=2: analytic Jacobian (ellipsoid_contact_detection.f90:296-332), 3x2
 // column-major.
-GP_LM_FN void lm_jac(const ContactProb& P, const double x[2], double fj[6]) {
+GP_LM_INNER void lm_jac(const ContactProb& P, const double x[2], double fj[6]) {
   double c1[3], t1[3], t2[3], l1, l2, pt1[3], pt2[3];
   support_points(P, x, c1, t1, t2, l1, l2, pt1, pt2);
   const double depth[3] = {pt1[0] - pt2[0], pt1[1] - pt2[1], pt1[2] - pt2[2]};
@@ -258,7 +260,7 @@ GP_LM_FN void lm_jac(const ContactProb& P, const double x[2], double fj[6]) {
 }
 
 // QR with column pivoting (3x2), Householder vectors left in a.
-GP_LM_FN void lm_qrfac(double a[6], int ipvt[2], double rdiag[2], double acnorm[2]) {
+GP_LM_INNER void lm_qrfac(double a[6], int ipvt[2], double rdiag[2], double acnorm[2]) {
   double wa[2];
 #pragma unroll
   for (int j = 0; j < 2; ++j) {
@@ -307,7 +309,7 @@ GP_LM_FN void lm_qrfac(double a[6], int ipvt[2], double rdiag[2], double acnorm[
   }
 }
 
-GP_LM_FN void lm_qrsolv(double r[6], const int ipvt[2], const double diag[2], const double qtb[2],
+GP_LM_INNER void lm_qrsolv(double r[6], const int ipvt[2], const double diag[2], const double qtb[2],
                                           double x[2], double sdiag[2]) {
   double wa[2];
 #pragma unroll
@@ -368,7 +370,7 @@ GP_LM_FN void lm_qrsolv(double r[6], const int ipvt[2], const double diag[2], co
   x[ipvt[1]] = wa[1];
 }
 
-GP_LM_FN void lm_lmpar(double r[6], const int ipvt[2], const double diag[2], const double qtb[2],
+GP_LM_INNER void lm_lmpar(double r[6], const int ipvt[2], const double diag[2], const double qtb[2],
                                          double delta, double& par, double x[2], double sdiag[2]) {
   const double dwarf = DBL_MIN;
   double wa1[2], wa2[2];
