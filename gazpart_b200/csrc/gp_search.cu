@@ -401,18 +401,37 @@ __global__ void __launch_bounds__(256) k_search(const InstDev *__restrict__ inst
     const int cx = cell_coord(h.xp, I.hfx, nfx), cy = cell_coord(h.yp, I.hfy, nfy), cz = cell_coord(h.zp, I.hfz, nfz);
     const int64_t lc = ((int64_t)cz * nfy + cy) * nfx + cx;
     if (sa.spk[s].w >= 0.f) {
+      // Small candidates have radius <= rcut, so only cells whose box comes within
+      // R = rp + rcut of this particle can hold a partner: rows and end cells farther
+      // away are skipped (distances to the neighbour boxes from the offsets inside the
+      // home cell, shortened by 1e-9 of the cell edge against rounding).
+      const double R = (h.rp + I.rcut) * (1.0 + 1e-9), R2 = R * R;
+      const double fx = h.xp - cx * I.hfx, fy = h.yp - cy * I.hfy, fz = h.zp - cz * I.hfz;
+      const double ex = 1e-9 * I.hfx, ey = 1e-9 * I.hfy, ez = 1e-9 * I.hfz;
+      const double dxl = fmax(fx - ex, 0.0), dxh = fmax(I.hfx - fx - ex, 0.0);
+      const double dyl = fmax(fy - ey, 0.0), dyh = fmax(I.hfy - fy - ey, 0.0);
+      const double dzh = fmax(I.hfz - fz - ez, 0.0);
       for (int r = 0; r < 5; ++r) {
         int ry = cy, rz = cz, lo = cx - 1, hi = cx + 1;
+        double dyz2 = 0.0;
         if (r == 0) {
           lo = hi = cx + 1;                    // the rest of the home cell is swept below
         } else if (r == 1) {
           ry = wrap_cell(cy + 1, nfy);
+          dyz2 = dyh * dyh;
         } else {
           rz = wrap_cell(cz + 1, nfz);
           ry = wrap_cell(cy + (r - 3), nfy);
+          const double dyb = (r == 2) ? dyl : (r == 4 ? dyh : 0.0);
+          dyz2 = dyb * dyb + dzh * dzh;
         }
+        if (r > 0 && dyz2 > R2) continue;
+        if (r > 0 && dxl * dxl + dyz2 > R2) lo = cx;
+        const bool right = dxh * dxh + dyz2 <= R2;
+        if (r > 0 && !right) hi = cx;
         const int64_t base = I.cell_begin + ((int64_t)rz * nfy + ry) * nfx;
-        RowRanges rr = row_ranges(sa, base, nfx, lo, hi, h.perx);
+        RowRanges rr = {0, 0, 0, 0};
+        if (r > 0 || right) rr = row_ranges(sa, base, nfx, lo, hi, h.perx);
         if (r == 0) {
           // home cell from s+1, contiguous with cell cx+1 when that is not wrapped
           if (rr.a1 == 0 && rr.a0 == 0) rr.a1 = sa.cell_start[I.cell_begin + lc + 1];
