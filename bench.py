@@ -409,7 +409,9 @@ def main():
         # In a multi-step graph the gather of step s+1 overlaps step s's contact solves,
         # so its phase time spans both.  The first step of a graph gathers alone: one-step
         # graphs give the kernel's own duration for the roofline.
-        alone = sorted(ctx.step_timed(1)[1]["gather"] for _ in range(3))[1]
+        singles = [ctx.step_timed(1)[1] for _ in range(3)]
+        alone = sorted(ph["gather"] for ph in singles)[1]
+        phases_alone = {k: sorted(ph[k] for ph in singles)[1] for k in singles[0]}
     clocks = clk.summary()
     ctx.raise_status("timed steps")
     torch.cuda.synchronize()
@@ -502,6 +504,7 @@ def main():
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": kps * args.steps,
                 "kernels_per_step": kps, "phase_ms": phases,
                 "phase_note": "gather of step s+1 overlaps the contact solves of step s (two streams in the graph)",
+                "phase_ms_one_step_graphs": phases_alone,
                 "clocks": clocks, "fp64_plain": plain}
         print(json.dumps(line), flush=True)
     if dist:

@@ -191,7 +191,7 @@ int class_props(gp_ctx *c, int ig, int idp, double pc[kNConst]) {
 }
 
 void free_search(gp_ctx *c) {
-  dfree(c->sa.cell_count); dfree(c->sa.cell_start); dfree(c->sa.cell_fill);
+  dfree(c->sa.cell_count); dfree(c->sa.cell_start); dfree(c->sa.cell_fill); dfree(c->sa.cell_rmax);
   dfree(c->d_scan_tmp);
   c->ncells_cap = 0;
 }
@@ -300,6 +300,7 @@ int alloc_cells(gp_ctx *c, int64_t ncells) {
     GP_TRY(dalloc(&c->sa.cell_count, ncells + 1));
     GP_TRY(dalloc(&c->sa.cell_start, ncells + 1));
     GP_TRY(dalloc(&c->sa.cell_fill, ncells + 1));
+    GP_TRY(dalloc(&c->sa.cell_rmax, ncells + 1));
     GP_TRY(dalloc(&c->d_scan_tmp, (size_t)scan_block_sums_size(ncells)));
     c->ncells_cap = ncells;
   }
@@ -352,6 +353,7 @@ int enqueue_bin(gp_ctx *c) {
   SearchArrays sa = c->sa;
   GP_CK(cudaMemsetAsync(sa.cell_count, 0, (c->ncells + 1) * sizeof(int32_t), c->stream));
   GP_CK(cudaMemsetAsync(sa.cell_fill, 0, (c->ncells + 1) * sizeof(int32_t), c->stream));
+  GP_CK(cudaMemsetAsync(sa.cell_rmax, 0, (c->ncells + 1) * sizeof(float), c->stream));
   GP_CK(cudaMemsetAsync(c->d_counters, 0, 4 * sizeof(unsigned long long), c->stream));
   launch_bin_count(c->d_inst, c->d_pv, c->n_slots, sa, c->d_status, c->tune[GP_TUNE_BIN], c->stream);
   launch_scan(sa.cell_count, sa.cell_start, c->ncells, c->d_scan_tmp, c->stream);

@@ -206,6 +206,8 @@ __global__ void k_bin_scatter(const InstDev *__restrict__ insts, const PoolView 
     // w carries the bounding radius, negated for particles above the small-particle cut
     const double rb = fmax(ea, eb);
     sa.spk[pos] = make_float4((float)x, (float)y, (float)z, rb > I.rcut ? -(float)rb : (float)rb);
+    // a float rounded up bounds the radius; non-negative floats order like their bits
+    if (rb <= I.rcut) atomicMax(reinterpret_cast<int *>(sa.cell_rmax) + c, __float_as_int(__double2float_ru(rb)));
     sa.sa2[pos] = ea * ea;
     sa.sb2[pos] = eb * eb;
     {
@@ -426,10 +428,19 @@ __global__ void __launch_bounds__(256) k_search(const InstDev *__restrict__ inst
           dyz2 = dyb * dyb + dzh * dzh;
         }
         if (r > 0 && dyz2 > R2) continue;
-        if (r > 0 && dxl * dxl + dyz2 > R2) lo = cx;
-        const bool right = dxh * dxh + dyz2 <= R2;
-        if (r > 0 && !right) hi = cx;
         const int64_t base = I.cell_begin + ((int64_t)rz * nfy + ry) * nfx;
+        // each end cell within reach of its own largest radius
+        auto reach2 = [&](int cell) {
+          const int w = cell < 0 ? cell + nfx : (cell >= nfx ? cell - nfx : cell);
+          const double rr_ = (h.rp + (double)sa.cell_rmax[base + w]) * (1.0 + 1e-9);
+          return rr_ * rr_;
+        };
+        const bool left_ok = (cx - 1 >= 0 || h.perx);
+        const bool right_ok = (cx + 1 < nfx || h.perx);
+        if (r > 0 && (!left_ok || dxl * dxl + dyz2 > R2 || dxl * dxl + dyz2 > reach2(cx - 1))) lo = cx;
+        const bool right = right_ok && dxh * dxh + dyz2 <= R2 && dxh * dxh + dyz2 <= reach2(cx + 1);
+        if (r > 0 && !right) hi = cx;
+        if (r > 0 && lo == cx && hi == cx && dyz2 > reach2(cx)) continue;
         RowRanges rr = {0, 0, 0, 0};
         if (r > 0 || right) rr = row_ranges(sa, base, nfx, lo, hi, h.perx);
         if (r == 0) {

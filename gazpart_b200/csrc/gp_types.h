@@ -84,6 +84,7 @@ struct SearchArrays {
   int32_t *cell_count;   // per search cell (+1 zero sentinel)
   int32_t *cell_start;   // exclusive scan, ncells+1
   int32_t *cell_fill;
+  float *cell_rmax;       // per search cell: largest bounding radius of its small particles
   int32_t *cell_of;      // per pool slot
   int32_t *sorted;       // pool slot of each sorted position
   double *sx, *sy, *sz, *sr;
