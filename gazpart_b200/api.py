@@ -245,9 +245,11 @@ class Context:
 
     def autotune(self) -> Dict[str, int]:
         """Pick the launch grids on the resident ensemble (state restored afterwards)."""
-        g = (C.c_int32 * len(_lib.TUNABLES))()
+        g = (C.c_int32 * (len(_lib.TUNABLES) + 1))()
         check(_lib.lib().gp_autotune(self._h, g), "gp_autotune")
-        return dict(zip(_lib.TUNABLES, (int(v) for v in g)))
+        out = dict(zip(_lib.TUNABLES, (int(v) for v in g)))
+        out["overlap_gather"] = bool(g[len(_lib.TUNABLES)])
+        return out
 
     def download(self, fluid: bool = False) -> Dict[str, np.ndarray]:
         out = {k: np.empty(self.n) for k in STATE_KEYS}

@@ -147,6 +147,9 @@ struct gp_ctx {
   std::map<int, cudaGraphExec_t> graphs;
   // launch grids (blocks), GP_TUNE_* order; gp_autotune picks them on the live workload
   int tune[GP_NTUNE] = {148 * 8, 148 * 4, 148 * 4, 148 * 4};
+  // gather of step s+1 on the side stream, overlapping step s's contact solves; the
+  // autotuner keeps it only where it shortens the step
+  bool overlap = false;
   int contact_grid = 148 * 4;   // persistent k_contact grid (resident blocks)
 };
 
@@ -406,10 +409,11 @@ int enqueue_steps(gp_ctx *c, int nsteps, cudaEvent_t *marks) {
   int rc = enqueue_gather(c, c->stream);
   for (int s = 0; s < nsteps && !rc; ++s) {
     c->marks = marks_of(s);
-    if (s > 0 && cudaStreamWaitEvent(c->stream, c->ev_join, 0) != cudaSuccess) rc = GP_ECUDA;
+    if (s > 0 && c->overlap && cudaStreamWaitEvent(c->stream, c->ev_join, 0) != cudaSuccess) rc = GP_ECUDA;
+    if (s > 0 && !c->overlap && !rc) rc = enqueue_gather(c, c->stream);
     if (!rc) rc = enqueue_integrate(c);
     if (!rc) rc = enqueue_bin_search(c);
-    const bool fork = s + 1 < nsteps;
+    const bool fork = c->overlap && s + 1 < nsteps;
     if (!rc && fork && cudaEventRecord(c->ev_fork, c->stream) != cudaSuccess) rc = GP_ECUDA;
     // the contact kernel is captured first so that its persistent grid is resident
     // before the gather's blocks queue for the SMs it leaves as its queue drains
@@ -1365,14 +1369,29 @@ int gp_autotune(gp_ctx *c, int32_t *grids_out) {
     }
     c->tune[t] = best;
   }
+  // overlapped gather or not: whichever four-step graph is faster (median of three)
+  if (!rc) {
+    float best_ms[2];
+    for (int o = 0; o < 2 && !rc; ++o) {
+      c->overlap = o == 1;
+      drop_graph(c);
+      float trial[3];
+      for (int r = 0; r < 3 && !rc; ++r) rc = gp_step_timed(c, 4, &trial[r], nullptr, nullptr);
+      std::sort(trial, trial + 3);
+      best_ms[o] = trial[1];
+    }
+    c->overlap = !rc && best_ms[1] < best_ms[0];
+  }
   drop_graph(c);
   if (!rc) {
     launch_scatter_state(c->d_inst, c->d_pv, c->n_slots, save, n, c->stream);
     if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(c->stream) != cudaSuccess) rc = GP_ECUDA;
   }
   cudaFree(save);
-  if (!rc && grids_out)
+  if (!rc && grids_out) {
     for (int t = 0; t < GP_NTUNE; ++t) grids_out[t] = c->tune[t];
+    grids_out[GP_NTUNE] = c->overlap ? 1 : 0;
+  }
   return rc;
 }
 

@@ -231,9 +231,11 @@ enum {
     GP_NTUNE = 4
 };
 /* Autotuner: for each launch above, in turn, times one-step graphs of the resident
- * ensemble with 148 x {1,2,4,8,16} blocks and keeps the fastest; the particle state
- * is saved first and restored afterwards.  grids_out: GP_NTUNE ints or NULL.  No
- * counterpart in the reference. */
+ * ensemble with 148 x {1,2,4,8,16} blocks and keeps the fastest; then times four-step
+ * graphs with the next step's gather run on a second stream beside the contact solves
+ * and without, and keeps the faster.  The particle state is saved first and restored
+ * afterwards.  grids_out: GP_NTUNE + 1 ints (the grids, then 1 if the gather is
+ * overlapped) or NULL.  No counterpart in the reference. */
 int gp_autotune(gp_ctx *ctx, int32_t *grids_out);
 /* Last step's accepted collisions as (home, near) original indices, in acceptance
  * (list) order; *count receives the total even if it exceeds cap. */
