@@ -43,6 +43,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the FP64 comparison run")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch grids")
+    ap.add_argument("--grids", default=None,
+                    help="gather,integrate,bin,search,overlap: fixed launch grids instead of autotuning")
     ap.add_argument("--serve-seconds", type=float, default=2.0, help="arrival window of the serving workload")
     return ap.parse_args()
 
@@ -176,7 +178,7 @@ def reduce_max_ms(ms: float, dist, device) -> float:
 
 
 def gather_bytes_per_particle(components: int, field_bytes: int) -> int:
-    """Algorithmic bytes of one particle in the stencil-gather kernel (k_gather_move):
+    """Algorithmic bytes of one particle in the stencil-gather kernel (k_gather):
     64 stencil points x C components x field word, the position read (24 B) and the C
     interpolated values written (8 B each, as the reference stores them).  No credit is
     taken for stencil reuse between particles; the reordering copy of the particle
@@ -184,11 +186,11 @@ def gather_bytes_per_particle(components: int, field_bytes: int) -> int:
     return 64 * components * field_bytes + 24 + 8 * components
 
 
-# DRAM bytes (read + write) per particle of one k_gather_move launch, from ncu
+# DRAM bytes (read + write) per particle of one k_gather launch, from ncu
 # (dram__bytes_read.sum + dram__bytes_write.sum) on the steady-state step; the file
 # under profiles/ named in the value gives the command and the capture.
 GATHER_TRAFFIC = {
-    ("c3_512cube_n16777216_fp32field", "mixed"): (1092.0, "profiles/k_gather_move_k_integrate_c3_dram.md"),
+    ("c3_512cube_n16777216_fp32field", "mixed"): (375.5, "profiles/k_gather_k_integrate_c3_dram.md"),
 }
 
 
@@ -396,7 +398,13 @@ def main():
     max_emaj = float(st["emaj"].max()) if not batched else None
     ctx = make_context(setup, f, st, precision, device)
     n = ctx.n
-    tune = None if args.no_autotune else ctx.autotune()
+    if args.grids:
+        g = [int(v) for v in args.grids.split(",")]
+        tune = dict(zip(("gather", "integrate", "bin", "search"), g[:4]))
+        tune["overlap_gather"] = bool(g[4]) if len(g) > 4 else False
+        ctx.set_launch(tune)
+    else:
+        tune = None if args.no_autotune else ctx.autotune()
     ctx.raise_status("autotune")
     ctx.step(args.warmup)
     ctx.sync()
@@ -428,7 +436,7 @@ def main():
     peak, peak_kind = hbm_peak()
     achieved = bpp * n / (alone / 1e3) / 1e9
     tr = GATHER_TRAFFIC.get((w.name, precision))
-    roofline = {"bound": "hbm", "kernel": "k_gather_move", "achieved": achieved, "peak": peak, "unit": "GB/s",
+    roofline = {"bound": "hbm", "kernel": "k_gather", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": peak_kind,
                 "bytes_per_launch": bpp * n, "bytes_per_particle": bpp, "kernel_ms": alone,
                 "kernel_ms_source": "median of three one-step graphs run right after the timed region",

@@ -72,6 +72,7 @@ SIGNATURES = {
     "gp_put_state": [_ctx, C.c_int64, C.POINTER(_vp), C.c_int32],
     "gp_upload_classes": [_ctx, C.c_int32, _i64p, C.POINTER(_vp), C.POINTER(_vp), C.c_int32],
     "gp_autotune": [_ctx, _ip],
+    "gp_set_launch": [_ctx, _ip],
     "gp_add_field": [_ctx, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, _ip],
     "gp_set_field_slot": [_ctx, C.c_int32, C.c_int32, _vp, C.c_int32, C.c_int32, C.c_int32],
     "gp_add_class": [_ctx, C.c_int32, C.c_int64, C.POINTER(_vp), C.POINTER(_vp), C.c_int32, _ip],

@@ -251,6 +251,12 @@ class Context:
         out["overlap_gather"] = bool(g[len(_lib.TUNABLES)])
         return out
 
+    def set_launch(self, grids: Dict[str, int]) -> None:
+        """Launch grids and overlap choice as autotune() reports them."""
+        g = (C.c_int32 * (len(_lib.TUNABLES) + 1))(*[int(grids[k]) for k in _lib.TUNABLES],
+                                                     int(bool(grids.get("overlap_gather", False))))
+        check(_lib.lib().gp_set_launch(self._h, g), "gp_set_launch")
+
     def download(self, fluid: bool = False) -> Dict[str, np.ndarray]:
         out = {k: np.empty(self.n) for k in STATE_KEYS}
         cols = (C.c_void_p * 13)(*[C.c_void_p(out[k].ctypes.data) for k in STATE_KEYS])

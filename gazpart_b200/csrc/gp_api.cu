@@ -1338,6 +1338,16 @@ int gp_serve(gp_ctx *c, gp_job *jobs, int32_t njobs, double hbm_budget, double b
   return rc;
 }
 
+int gp_set_launch(gp_ctx *c, const int32_t *grids) {
+  if (!c || !grids) return GP_EBADARG;
+  for (int t = 0; t < GP_NTUNE; ++t)
+    if (grids[t] < 1 || grids[t] > 148 * 64) return GP_EBADARG;
+  for (int t = 0; t < GP_NTUNE; ++t) c->tune[t] = grids[t];
+  c->overlap = grids[GP_NTUNE] != 0;
+  drop_graph(c);
+  return GP_OK;
+}
+
 // Coordinate descent over the launch grids: each tunable in turn, each candidate timed
 // by one-step graphs on the live ensemble (median of three), the fastest kept.  The
 // state is saved before and restored after, so the ensemble does not move; the pool

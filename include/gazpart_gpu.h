@@ -237,6 +237,9 @@ enum {
  * afterwards.  grids_out: GP_NTUNE + 1 ints (the grids, then 1 if the gather is
  * overlapped) or NULL.  No counterpart in the reference. */
 int gp_autotune(gp_ctx *ctx, int32_t *grids_out);
+/* Sets the launch grids and the overlap choice directly (GP_NTUNE + 1 ints, as
+ * gp_autotune reports them), e.g. to replay a tuned configuration. */
+int gp_set_launch(gp_ctx *ctx, const int32_t *grids);
 /* Last step's accepted collisions as (home, near) original indices, in acceptance
  * (list) order; *count receives the total even if it exceeds cap. */
 int gp_collision_pairs(gp_ctx *ctx, int64_t cap, int32_t *home, int32_t *near, int64_t *count);
