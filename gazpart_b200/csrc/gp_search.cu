@@ -383,7 +383,10 @@ __device__ __forceinline__ RowRanges row_ranges(const SearchArrays &sa, int64_t 
 // particles; the home cell is swept from the next sorted particle on.  A large particle
 // (radius above the cut, rare) sweeps every cell within its radius plus the largest
 // radius.  Every pair is visited exactly once.
-__global__ void __launch_bounds__(256) k_search(const InstDev *__restrict__ insts, int64_t n, SearchArrays sa,
+#ifndef GP_SEARCH_MIN_BLOCKS
+#define GP_SEARCH_MIN_BLOCKS 4
+#endif
+__global__ void __launch_bounds__(256, GP_SEARCH_MIN_BLOCKS) k_search(const InstDev *__restrict__ insts, int64_t n, SearchArrays sa,
                                                 PairRec *__restrict__ pairs, unsigned long long *npairs,
                                                 int64_t cap, Status *st) {
   const int64_t nact = sa.cell_start[sa.ncells];
