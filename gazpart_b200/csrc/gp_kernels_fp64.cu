@@ -116,10 +116,12 @@ void launch_frozen_interp(const double *xain, const double *yain, const double *
 // (flag && NVREL < ZERO) are appended.  Persistent warps with lane refill: a lane whose
 // Levenberg-Marquardt solve has returned finishes its pair and takes the next one from
 // a global queue, so warps do not idle on their slowest pair.
+#ifndef GP_CONTACT_MIN_BLOCKS
 #ifdef GP_LM_INLINE
 #define GP_CONTACT_MIN_BLOCKS 2
 #else
-#define GP_CONTACT_MIN_BLOCKS 4
+#define GP_CONTACT_MIN_BLOCKS 8
+#endif
 #endif
 
 __global__ void __launch_bounds__(128, GP_CONTACT_MIN_BLOCKS) k_contact(const InstDev *__restrict__ insts,
