@@ -485,8 +485,11 @@ __device__ __forceinline__ void gather_warp_fp32(const InstDev* __restrict__ ins
 // and id, so it may run while the collision phase updates velocities.  kMixed: every
 // instance holds an FP32 field (warp-cooperative gather); otherwise FP64 fields,
 // gathered per lane in the reference's summation order.
+#ifndef GP_GATHER_MIN_BLOCKS
+#define GP_GATHER_MIN_BLOCKS 3
+#endif
 template <bool kMixed>
-__global__ void __launch_bounds__(256) k_gather(const InstDev* __restrict__ insts,
+__global__ void __launch_bounds__(256, GP_GATHER_MIN_BLOCKS) k_gather(const InstDev* __restrict__ insts,
                                                 const PoolView* __restrict__ src_pv,
                                                 const int32_t* __restrict__ perm, int64_t n,
                                                 double* const* __restrict__ fluid, Status* st) {
@@ -535,7 +538,7 @@ __global__ void __launch_bounds__(256) k_gather(const InstDev* __restrict__ inst
 // BOUNDARY_PARTICLE's periodic wrap (boundary_particle.f90:50-59).  A particle whose
 // stencil left the field (NaN fluid values, reported by the gather) is copied unchanged.
 #ifndef GP_INTEGRATE_MIN_BLOCKS
-#define GP_INTEGRATE_MIN_BLOCKS 1
+#define GP_INTEGRATE_MIN_BLOCKS 4
 #endif
 template <bool kMixed>
 __global__ void __launch_bounds__(128, GP_INTEGRATE_MIN_BLOCKS) k_integrate(const InstDev* __restrict__ insts,
