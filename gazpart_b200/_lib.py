@@ -30,6 +30,7 @@ PREC_FP64, PREC_MIXED = 0, 1
 LAYOUT_INTERIOR, LAYOUT_REFERENCE = 0, 1
 PHASES = ("gather", "integrate", "bin", "search", "contact", "response")   # GP_PHASE_*
 TUNABLES = ("gather", "integrate", "bin", "search")   # GP_TUNE_*
+COUNTERS = ("near", "candidates", "solves", "contacts", "colliding", "accepted", "evaluations", "max_evaluations")
 GHOST_PERIODIC, GHOST_ZERO = 0, 1
 
 
@@ -63,6 +64,7 @@ SIGNATURES = {
     "gp_ctx_destroy": [_ctx],
     "gp_status": [_ctx, _ip, _i64p],
     "gp_status_class": [_ctx, _ip],
+    "gp_collision_counters": [_ctx, _i64p],
     "gp_clear_status": [_ctx],
     "gp_sync": [_ctx],
     "gp_set_class": [_ctx, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double],

@@ -100,6 +100,12 @@ class Context:
         check(_lib.lib().gp_status(self._h, C.byref(code), C.byref(fid)), "gp_status")
         return code.value, fid.value
 
+    def collision_counters(self) -> Dict[str, int]:
+        """Counters of the last collision phase (_lib.COUNTERS)."""
+        v = (C.c_int64 * len(_lib.COUNTERS))()
+        check(_lib.lib().gp_collision_counters(self._h, v), "gp_collision_counters")
+        return dict(zip(_lib.COUNTERS, (int(x) for x in v)))
+
     def status_class(self) -> int:
         """Class (1-based) of the particle behind the first error; 0 if none."""
         ig = C.c_int32()

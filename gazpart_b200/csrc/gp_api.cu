@@ -541,6 +541,18 @@ int gp_status(gp_ctx *c, int32_t *code, int64_t *first_id) {
   return GP_OK;
 }
 
+int gp_collision_counters(gp_ctx *c, int64_t *vals) {
+  if (!c || !vals) return GP_EBADARG;
+  Status h;
+  GP_TRY(read_status(c, &h));
+  unsigned long long cnt[4];
+  GP_CK(cudaMemcpy(cnt, c->d_counters, sizeof(cnt), cudaMemcpyDeviceToHost));
+  const unsigned long long v[GP_NCOUNTER] = {h.n_near, cnt[0], h.n_solve, h.n_contact, cnt[1], cnt[2],
+                                             h.n_eval, h.max_eval};
+  for (int k = 0; k < GP_NCOUNTER; ++k) vals[k] = (int64_t)v[k];
+  return GP_OK;
+}
+
 int gp_status_class(gp_ctx *c, int32_t *ig) {
   if (!c || !ig) return GP_EBADARG;
   Status h;
@@ -858,7 +870,7 @@ int gp_adv_particle_ellp(gp_ctx *c, int32_t /*ncycle*/) {
 int gp_collision(gp_ctx *c, int32_t /*ncycle*/, double /*time*/, int64_t *n_near, int64_t *n_contact,
                  int64_t *n_coll) {
   if (!c || c->n <= 0 || !c->grid_ready) return GP_EBADARG;
-  GP_CK(cudaMemsetAsync(&c->d_status->n_near, 0, 5 * sizeof(unsigned long long), c->stream));
+  GP_CK(cudaMemsetAsync(&c->d_status->n_near, 0, 8 * sizeof(unsigned long long), c->stream));
   GP_TRY(enqueue_collision(c));
   if (n_near || n_contact || n_coll) {
     Status h;
@@ -1309,7 +1321,7 @@ int gp_serve(gp_ctx *c, gp_job *jobs, int32_t njobs, double hbm_budget, double b
       continue;
     }
     // one step of every running job
-    GP_CK(cudaMemsetAsync(&c->d_status->n_near, 0, 5 * sizeof(unsigned long long), c->stream));
+    GP_CK(cudaMemsetAsync(&c->d_status->n_near, 0, 8 * sizeof(unsigned long long), c->stream));
     rc = enqueue_advance(c);
     if (!rc) rc = enqueue_collision(c);
     if (rc) break;

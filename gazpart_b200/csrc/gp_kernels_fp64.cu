@@ -189,6 +189,9 @@ __global__ void __launch_bounds__(128, GP_CONTACT_MIN_BLOCKS) k_contact(const In
     if (!active) continue;
     if (lm_step(CP, S, kContactTol) == 0) continue;
     active = false;
+    atomicAdd(&st->n_solve, 1ull);
+    atomicAdd(&st->n_eval, (unsigned long long)S.nfev);
+    atomicMax(&st->max_eval, (unsigned long long)S.nfev);
     double ept1[3], ept2[3], cn[3];
     if (!contact_finish(a1, b1, a2, b2, q1, q2, CP, S.x, ept1, ept2, cn)) continue;
     atomicAdd(&st->n_contact, 1ull);

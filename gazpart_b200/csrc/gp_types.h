@@ -52,6 +52,9 @@ struct Status {
   unsigned long long n_coll;      // colliding pairs (flag && NVREL < ZERO)
   unsigned long long n_accept;    // accepted (responded) pairs
   unsigned long long overflow;    // pairs dropped by a full buffer
+  unsigned long long n_solve;     // contact solves run (pairs not proven disjoint)
+  unsigned long long n_eval;      // function evaluations of those solves
+  unsigned long long max_eval;    // largest evaluation count of one solve
 };
 
 __device__ inline void set_error(Status *s, int code, long long id, int inst = -1) {

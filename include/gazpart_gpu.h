@@ -107,6 +107,14 @@ int gp_ctx_destroy(gp_ctx *ctx);
 /* First error recorded on the device since the last gp_clear_status: code and the
  * particle (or pair home) index that raised it. */
 int gp_status(gp_ctx *ctx, int32_t *code, int64_t *first_id);
+/* Counters of the last gp_collision call (accumulated over all steps since then when
+ * stepping through graphs), GP_NCOUNTER values in this order: pairs within bounding
+ * and centre-line reach, pairs handed to the contact stage, contact solves run (pairs
+ * not proven disjoint), contacts, colliding pairs (NVREL < ZERO), accepted pairs,
+ * function evaluations of the solves, largest evaluation count of one solve.  No
+ * counterpart in the reference, which reports none of these. */
+#define GP_NCOUNTER 8
+int gp_collision_counters(gp_ctx *ctx, int64_t *vals);
 /* Class (IG, 1-based) of the particle that raised the first error, 0 if none. */
 int gp_status_class(gp_ctx *ctx, int32_t *ig);
 int gp_clear_status(gp_ctx *ctx);
