@@ -43,6 +43,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the FP64 comparison run")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch grids")
+    ap.add_argument("--no-io", action="store_true", help="skip the restart-file measurement")
     ap.add_argument("--grids", default=None,
                     help="gather,integrate,bin,search,overlap: fixed launch grids instead of autotuning")
     ap.add_argument("--serve-seconds", type=float, default=2.0, help="arrival window of the serving workload")
@@ -249,6 +250,35 @@ def workload_max_emaj(w) -> float:
 # ---------------------------------------------------------------------------
 # serving: a Poisson job stream through gp_serve
 # ---------------------------------------------------------------------------
+def time_restart_io(ctx, n: int, state) -> dict:
+    """The ensemble as a class restart file (save_particle.f90:116-180 layout): written
+    straight from the device by gp_save_part_class and read back by gp_read_part_class,
+    with a check that the file holds the state the context holds (state: the host copy
+    of the current state, in particle order).  The file carries one table entry per
+    class; the per-particle shapes of the synthetic workloads are not part of it."""
+    import shutil
+    from gazpart_b200 import restart
+    tables = restart.default_tables(n, 1.0, 1.0, 1.0)
+    d = tempfile.mkdtemp(prefix="gp_restart_")
+    path = os.path.join(d, restart.part_file_name(1, 0))
+    try:
+        t0 = time.perf_counter()
+        restart.save_class(ctx, 1, path, tables)
+        t1 = time.perf_counter()
+        cols, _ = restart.read_part_class(path)
+        t2 = time.perf_counter()
+        size = os.path.getsize(path)
+        same = all(np.array_equal(cols[k], state[k]) for k in state)
+        return {"file": restart.part_file_name(1, 0), "bytes": size, "particles": n,
+                "save_s": t1 - t0, "save_gbs": size / (t1 - t0) / 1e9,
+                "read_s": t2 - t1, "read_gbs": size / (t2 - t1) / 1e9, "matches_state": bool(same),
+                "note": "save = D2H into pageable memory + write; read right after the write (page cache)"}
+    except Exception as e:      # a full or read-only scratch disk leaves the step numbers valid
+        return {"error": str(e)}
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+
+
 def run_serving(args, rank: int, world: int, local: int):
     """Jobs arriving at 20/s for --serve-seconds, each on one of eight resident fields,
     admitted against the HBM budget and stepped together until all are done."""
@@ -470,6 +500,10 @@ def main():
            "d2h_bytes_per_step": bytes_state, "ms_per_step": 1e3 * e2e_s,
            "ms_parts": {k: 1e3 * v / args.e2e_steps for k, v in parts.items()}}
 
+    restart_io = None
+    if rank == 0 and not batched and not args.no_io:
+        restart_io = time_restart_io(ctx, n, pinned)
+
     plain = None
     if not args.no_plain and precision == "mixed":
         ctx.close()
@@ -513,7 +547,7 @@ def main():
                 "kernels_per_step": kps, "phase_ms": phases,
                 "phase_note": "gather of step s+1 overlaps the contact solves of step s (two streams in the graph)",
                 "phase_ms_one_step_graphs": phases_alone,
-                "clocks": clocks, "fp64_plain": plain}
+                "clocks": clocks, "fp64_plain": plain, "restart_io": restart_io}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

@@ -1,4 +1,5 @@
-"""ctypes binding of ``libgazpart_b200.so`` (the C ABI in ``include/gazpart_gpu.h``).
+"""ctypes binding of ``libgazpart_b200.so`` (the C ABI in ``include/gazpart_gpu.h`` and
+``include/gazpart_files.h``).
 
 The shared library is built in-tree (``gazpart_b200/csrc/Makefile``).  Loading fails
 loudly if it is missing: there is no CPU fallback for any entry point.
@@ -11,7 +12,8 @@ import subprocess
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libgazpart_b200.so")
-HEADER = os.path.join(os.path.dirname(HERE), "include", "gazpart_gpu.h")
+INCLUDE = os.path.join(os.path.dirname(HERE), "include")
+HEADERS = tuple(os.path.join(INCLUDE, h) for h in ("gazpart_gpu.h", "gazpart_files.h"))
 
 GP_OK = 0
 ERRORS = {
@@ -25,7 +27,11 @@ ERRORS = {
     8: "GP_ECUDA: CUDA runtime error",
     9: "GP_EBADARG: invalid argument or unsupported configuration",
     10: "GP_ENOMEM: device allocation refused",
+    11: "GP_EIO: file could not be opened, read or written, or is truncated",
+    12: "GP_ERECORD: read past the end of a record, or inconsistent record markers",
+    13: "GP_EEOF: end of file where a record was expected",
 }
+GP_EIO, GP_ERECORD, GP_EEOF = 11, 12, 13
 PREC_FP64, PREC_MIXED = 0, 1
 LAYOUT_INTERIOR, LAYOUT_REFERENCE = 0, 1
 PHASES = ("gather", "integrate", "bin", "search", "contact", "response")   # GP_PHASE_*
@@ -109,6 +115,20 @@ SIGNATURES = {
     "gp_ellipsoid_contact_detection_batch_noalloc": [C.c_int64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, C.c_int32,
                                                      _vp],
     "gp_collision_response": [_ctx, C.c_int32, C.c_int32, _dp, _dp, _dp, _dp, _dp],
+    # gazpart_files.h
+    "gp_funf_open": [C.c_char_p, C.c_int32, C.POINTER(_vp)],
+    "gp_funf_close": [_vp],
+    "gp_funf_set_max_subrecord": [_vp, C.c_int64],
+    "gp_funf_write": [_vp, _vp, C.c_int64],
+    "gp_funf_record_size": [_vp, _i64p],
+    "gp_funf_read": [_vp, _vp, C.c_int64],
+    "gp_write_part_class": [C.c_char_p, C.c_int64, C.c_int32, _ip, _dp, _dp, C.c_double, C.POINTER(_vp)],
+    "gp_read_part_class_header": [C.c_char_p, _i64p, _ip],
+    "gp_read_part_class": [C.c_char_p, C.c_int64, C.c_int32, _ip, _dp, _dp, _dp, C.POINTER(_vp)],
+    "gp_write_part_snapshot": [C.c_char_p, C.c_int64, C.POINTER(_vp)],
+    "gp_read_part_snapshot": [C.c_char_p, C.c_int64, C.POINTER(_vp)],
+    "gp_save_part_class": [_ctx, C.c_int32, C.c_char_p, C.c_int32, _ip, _dp, _dp, C.c_double, _ip],
+    "gp_load_part_class": [_ctx, C.c_char_p, C.c_int32, _ip, _i64p],
 }
 
 _lib = None
@@ -144,7 +164,9 @@ def check(rc: int, where: str) -> None:
 
 
 def exported_symbols():
-    """Names declared in include/gazpart_gpu.h (parsed from the header)."""
+    """Names declared in the C ABI headers (parsed from them)."""
     import re
-    text = open(HEADER).read()
-    return sorted(set(re.findall(r"^int\s+(gp_\w+)\s*\(", text, flags=re.M)))
+    names = set()
+    for h in HEADERS:
+        names.update(re.findall(r"^int\s+(gp_\w+)\s*\(", open(h).read(), flags=re.M))
+    return sorted(names)

@@ -51,7 +51,11 @@ enum {
     GP_ETIMEOUT = 7,        /* a bounded device loop or host wait gave up */
     GP_ECUDA = 8,           /* CUDA runtime error */
     GP_EBADARG = 9,         /* invalid argument / unsupported configuration */
-    GP_ENOMEM = 10          /* device allocation or HBM budget refused */
+    GP_ENOMEM = 10,         /* device allocation or HBM budget refused */
+    GP_EIO = 11,            /* a file could not be opened, read or written, or is truncated */
+    GP_ERECORD = 12,        /* a read asked for more than the record holds (gfortran's
+                               'I/O past end of record'), or a record marker is inconsistent */
+    GP_EEOF = 13            /* end of file where a record was expected */
 };
 
 /* precision modes */
