@@ -44,6 +44,7 @@ def parse():
     ap.add_argument("--no-plain", action="store_true", help="skip the FP64 comparison run")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch grids")
     ap.add_argument("--no-io", action="store_true", help="skip the restart-file measurement")
+    ap.add_argument("--no-stats", action="store_true", help="skip the statistics measurement")
     ap.add_argument("--grids", default=None,
                     help="gather,integrate,bin,search,overlap: fixed launch grids instead of autotuning")
     ap.add_argument("--serve-seconds", type=float, default=2.0, help="arrival window of the serving workload")
@@ -279,6 +280,31 @@ def time_restart_io(ctx, n: int, state) -> dict:
         shutil.rmtree(d, ignore_errors=True)
 
 
+def time_stats(ctx) -> dict:
+    """Statistics beside the step on the whole ensemble: STAT_PARTFLUID of class 1
+    (one kernel over the pool, its 36 sums copied out; median of three calls, each
+    synchronised) and the cost of the collision statistics in a step (four-step graphs
+    with and without them, median of three each)."""
+    import statistics as stt
+    t = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        m = ctx.stat_partfluid(1)
+        t.append(time.perf_counter() - t0)
+    out = {"partfluid_ms": 1e3 * stt.median(t), "partfluid_count": int(m[0, -1]),
+           "partfluid_mean_rep": float(m[0, 0])}
+    steps = {}
+    for on in (False, True):
+        ctx.enable_collision_stats(on)
+        steps[on] = stt.median(ctx.step_timed(4)[0] for _ in range(3)) / 4
+    cs, nsteps = ctx.collision_stats(1)
+    ctx.enable_collision_stats(False)
+    out.update({"step_ms": steps[False], "step_ms_with_collision_stats": steps[True],
+                "collision_stats_steps": nsteps, "contacts_examined_per_step": float(cs[0, 0, 0]) / max(nsteps, 1),
+                "collisions_per_step": float(cs[0, 0, 1]) / max(nsteps, 1)})
+    return out
+
+
 def run_serving(args, rank: int, world: int, local: int):
     """Jobs arriving at 20/s for --serve-seconds, each on one of eight resident fields,
     admitted against the HBM budget and stepped together until all are done."""
@@ -421,8 +447,8 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device(device))
 
     # the autotuner's trials (60 one-step and 24 graph steps) and the three one-step graphs also
-    # move the particles before the state is restored
-    run_steps = args.warmup + args.steps + args.e2e_steps + 90
+    # move the particles before the state is restored, and the statistics timing adds 24 steps
+    run_steps = args.warmup + args.steps + args.e2e_steps + 90 + 28
     setup, f, st = build_inputs(w, device, precision, run_steps)
     batched = isinstance(st, list)
     max_emaj = float(st["emaj"].max()) if not batched else None
@@ -503,6 +529,10 @@ def main():
     restart_io = None
     if rank == 0 and not batched and not args.no_io:
         restart_io = time_restart_io(ctx, n, pinned)
+    stats = None
+    if not batched and not args.no_stats:
+        stats = time_stats(ctx)
+        ctx.raise_status("statistics")
 
     plain = None
     if not args.no_plain and precision == "mixed":
@@ -547,7 +577,7 @@ def main():
                 "kernels_per_step": kps, "phase_ms": phases,
                 "phase_note": "gather of step s+1 overlaps the contact solves of step s (two streams in the graph)",
                 "phase_ms_one_step_graphs": phases_alone,
-                "clocks": clocks, "fp64_plain": plain, "restart_io": restart_io}
+                "clocks": clocks, "fp64_plain": plain, "restart_io": restart_io, "stats": stats}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

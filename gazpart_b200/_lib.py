@@ -37,6 +37,14 @@ LAYOUT_INTERIOR, LAYOUT_REFERENCE = 0, 1
 PHASES = ("gather", "integrate", "bin", "search", "contact", "response")   # GP_PHASE_*
 TUNABLES = ("gather", "integrate", "bin", "search")   # GP_TUNE_*
 COUNTERS = ("near", "candidates", "solves", "contacts", "colliding", "accepted", "evaluations", "max_evaluations")
+NSTAT_PARTFLUID, NSTAT_COLLISION, STAT_MAX_GROUPS = 36, 8, 8   # GP_NSTAT_*, GP_STAT_MAX_GROUPS
+# MEAN_PARTFLUID(1:36) in stat_partfluid.f90's order
+STAT_PARTFLUID = ("rep", "cdrag", "clift", "fdrag_x", "fdrag_y", "fdrag_z", "flift_x", "flift_y", "flift_z",
+                  "fdrag", "flift", "re_r", "ctpitch", "ctrotation", "tpitch_x", "tpitch_y", "tpitch_z",
+                  "trot_x", "trot_y", "trot_z", "tpitch", "trot", "taupf", "gravity", "phi",
+                  "axis_x", "axis_y", "axis_z", "invtaup", "up", "vp", "wp", "omegax", "omegay", "omegaz", "count")
+# MEAN_PART_COL(1:8) in collision_interaction.f90's order
+STAT_COLLISION = ("contacts", "collisions", "frequency", "depth", "depth_per_contact", "nvrel", "vrel", "angle")
 GHOST_PERIODIC, GHOST_ZERO = 0, 1
 
 
@@ -71,6 +79,10 @@ SIGNATURES = {
     "gp_status": [_ctx, _ip, _i64p],
     "gp_status_class": [_ctx, _ip],
     "gp_collision_counters": [_ctx, _i64p],
+    "gp_set_class_groups": [_ctx, C.c_int32, C.c_int32, _ip],
+    "gp_stat_partfluid": [_ctx, C.c_int32, _dp],
+    "gp_collision_stats_enable": [_ctx, C.c_int32],
+    "gp_collision_stats": [_ctx, C.c_int32, _dp, _i64p, C.c_int32],
     "gp_clear_status": [_ctx],
     "gp_sync": [_ctx],
     "gp_set_class": [_ctx, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double],

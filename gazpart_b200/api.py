@@ -75,6 +75,7 @@ class Context:
         self._h = C.c_void_p()
         check(_lib.lib().gp_ctx_create(C.byref(p), C.byref(self._h)), "gp_ctx_create")
         self.n = 0
+        self._groups: Dict[int, int] = {}   # class -> polydisperse indices (gp_set_class_groups)
 
     # -- lifetime ------------------------------------------------------------
     def close(self) -> None:
@@ -105,6 +106,46 @@ class Context:
         v = (C.c_int64 * len(_lib.COUNTERS))()
         check(_lib.lib().gp_collision_counters(self._h, v), "gp_collision_counters")
         return dict(zip(_lib.COUNTERS, (int(x) for x in v)))
+
+    # ---- statistics beside the step (gp_stats.cu) ----
+    def set_class_groups(self, ig: int, idp: Optional[np.ndarray] = None, ngroups: Optional[int] = None) -> None:
+        """Polydisperse index PART(I,IG)%IDP of each particle of class ig, in its own order
+        (None: all 1)."""
+        if idp is None:
+            check(_lib.lib().gp_set_class_groups(self._h, int(ig), 1, None), "gp_set_class_groups")
+            self._groups.pop(int(ig), None)
+            return
+        idp = np.ascontiguousarray(idp, dtype=np.int32)
+        ng = int(idp.max()) if ngroups is None else int(ngroups)
+        check(_lib.lib().gp_set_class_groups(self._h, int(ig), ng, idp.ctypes.data_as(_lib._ip)),
+              "gp_set_class_groups")
+        self._groups[int(ig)] = ng
+
+    def stat_partfluid(self, ig: int = 1, sums: bool = False) -> np.ndarray:
+        """STAT_PARTFLUID for class ig: MEAN_PARTFLUID(:, IG, IDP) per index, shape
+        [ngroups, 36] (the last column the particle count), or the raw sums."""
+        ng = self._groups.get(int(ig), 1)
+        out = np.empty(ng * _lib.NSTAT_PARTFLUID)
+        check(_lib.lib().gp_stat_partfluid(self._h, int(ig), out.ctypes.data_as(_lib._dp)), "gp_stat_partfluid")
+        out = out.reshape(ng, _lib.NSTAT_PARTFLUID)
+        if sums:
+            return out
+        mean = out / out[:, -1:]
+        mean[:, -1] = out[:, -1]
+        return mean
+
+    def enable_collision_stats(self, on: bool = True) -> None:
+        check(_lib.lib().gp_collision_stats_enable(self._h, 1 if on else 0), "gp_collision_stats_enable")
+
+    def collision_stats(self, ig: int = 1, reset: bool = True):
+        """MEAN_PART_COL(1:8, IDP1, IDP2) of class ig summed over the collision steps since
+        the last reset: (array [ngroups, ngroups, 8], steps)."""
+        ng = self._groups.get(int(ig), 1)
+        out = np.empty(ng * ng * _lib.NSTAT_COLLISION)
+        steps = C.c_int64()
+        check(_lib.lib().gp_collision_stats(self._h, int(ig), out.ctypes.data_as(_lib._dp), C.byref(steps),
+                                            1 if reset else 0), "gp_collision_stats")
+        return out.reshape(ng, ng, _lib.NSTAT_COLLISION), steps.value
 
     def status_class(self) -> int:
         """Class (1-based) of the particle behind the first error; 0 if none."""
@@ -157,6 +198,7 @@ class Context:
         props = (C.c_void_p * 6)(*[C.c_void_p(cat[k].ctypes.data) for k in PROP_KEYS])
         ig = C.c_int32()
         check(_lib.lib().gp_add_class(self._h, field, n, cols, props, 0, C.byref(ig)), "gp_add_class")
+        self._groups.pop(ig.value, None)
         self.n += n
         return ig.value
 
@@ -178,6 +220,7 @@ class Context:
         out = {k: np.empty(n) for k in STATE_KEYS}
         cols = (C.c_void_p * 13)(*[C.c_void_p(out[k].ctypes.data) for k in STATE_KEYS])
         check(_lib.lib().gp_remove_class(self._h, ig, cols, 0), "gp_remove_class")
+        self._groups.pop(int(ig), None)
         self.n -= n
         return out
 
@@ -201,6 +244,7 @@ class Context:
             if d != dev:
                 raise ValueError("mixed host/device columns")
         check(_lib.lib().gp_upload_state(self._h, n, cols, props, dev), "gp_upload_state")
+        self._groups.clear()
         self.n = n
         self.class_counts = np.array([n], dtype=np.int64)
 
@@ -216,6 +260,7 @@ class Context:
         props = (C.c_void_p * 6)(*[C.c_void_p(cat[k].ctypes.data) for k in PROP_KEYS])
         check(_lib.lib().gp_upload_classes(self._h, len(states), counts.ctypes.data_as(_lib._i64p), cols, props, 0),
               "gp_upload_classes")
+        self._groups.clear()
         self.n = int(counts.sum())
         self.class_counts = counts
 

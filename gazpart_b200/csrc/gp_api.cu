@@ -134,7 +134,8 @@ struct gp_ctx {
   int64_t cap_pairs = 0;
   CollRec *d_coll = nullptr;
   int64_t cap_coll = 0;
-  unsigned long long *d_counters = nullptr;   // [0] npairs [1] ncoll [2] nacc [3] contact queue
+  unsigned long long *d_counters = nullptr;   // [0] npairs [1] ncoll [2] nacc [3] contact queue [4] contacts kept
+                                              // for the statistics [5] collision steps in the statistics
   unsigned long long *d_best1 = nullptr, *d_best2 = nullptr;
   int8_t *d_matched = nullptr, *d_state = nullptr;
   int32_t *d_acc = nullptr;
@@ -151,6 +152,19 @@ struct gp_ctx {
   // autotuner keeps it only where it shortens the step
   bool overlap = false;
   int contact_grid = 148 * 4;   // persistent k_contact grid (resident blocks)
+  // statistics beside the step: polydisperse index of each particle per class slot
+  // (device arrays by particle id, null = all 1), the fluid sample the last step left
+  // at each particle, the collision statistics' contact records and sums
+  std::vector<int32_t *> group_dev;
+  std::vector<int32_t> group_n;
+  int32_t **d_group_tab = nullptr;      // [kMaxClasses]
+  int32_t *d_group_n = nullptr;         // [kMaxClasses]
+  bool fluid_ok = false;
+  bool colstats = false;
+  ContactStatRec *d_cst = nullptr;
+  int64_t cap_cst = 0;
+  double *d_colacc = nullptr;           // [kMaxClasses][G][G][GP_NSTAT_COLLISION]
+  double *d_stat_partial = nullptr, *d_stat_out = nullptr;
 };
 
 namespace {
@@ -343,6 +357,7 @@ int enqueue_integrate(gp_ctx *c) {
                           c->tune[GP_TUNE_INTEGRATE], c->stream);
   GP_CK(cudaGetLastError());
   c->n_slots = c->n;   // the pass writes the active particles, in cell order, to slots [0, n)
+  c->fluid_ok = true;  // and the fluid it used, at the same slots
   return mark(c, 2 * GP_PHASE_INTEGRATE + 1, c->stream);
 }
 
@@ -357,7 +372,7 @@ int enqueue_bin(gp_ctx *c) {
   GP_CK(cudaMemsetAsync(sa.cell_count, 0, (c->ncells + 1) * sizeof(int32_t), c->stream));
   GP_CK(cudaMemsetAsync(sa.cell_fill, 0, (c->ncells + 1) * sizeof(int32_t), c->stream));
   GP_CK(cudaMemsetAsync(sa.cell_rmax, 0, (c->ncells + 1) * sizeof(float), c->stream));
-  GP_CK(cudaMemsetAsync(c->d_counters, 0, 4 * sizeof(unsigned long long), c->stream));
+  GP_CK(cudaMemsetAsync(c->d_counters, 0, 5 * sizeof(unsigned long long), c->stream));
   launch_bin_count(c->d_inst, c->d_pv, c->n_slots, sa, c->d_status, c->tune[GP_TUNE_BIN], c->stream);
   launch_scan(sa.cell_count, sa.cell_start, c->ncells, c->d_scan_tmp, c->stream);
   launch_bin_scatter(c->d_inst, c->d_pv, c->n_slots, sa, c->d_status, c->tune[GP_TUNE_BIN], c->stream);
@@ -382,13 +397,18 @@ int enqueue_bin_search(gp_ctx *c) {
 int enqueue_contact_response(gp_ctx *c) {
   GP_TRY(mark(c, 2 * GP_PHASE_CONTACT, c->stream));
   launch_contact(c->d_inst, c->d_pv, c->d_pairs, c->d_counters + 0, c->cap_pairs, c->d_coll, c->d_counters + 1,
-                 c->cap_coll, c->d_counters + 3, c->d_status, c->contact_grid, c->stream);
+                 c->cap_coll, c->d_counters + 3, c->colstats ? c->d_cst : nullptr, c->d_counters + 4, c->cap_cst,
+                 c->d_status, c->contact_grid, c->stream);
   GP_TRY(mark(c, 2 * GP_PHASE_CONTACT + 1, c->stream));
   GP_TRY(mark(c, 2 * GP_PHASE_RESPONSE, c->stream));
   launch_match(c->d_coll, c->d_counters + 1, c->cap_coll, c->d_best1, c->d_best2, c->d_matched, c->d_state,
                c->d_status, c->stream);
   launch_response(c->d_inst, c->d_pv, c->d_coll, c->d_counters + 1, c->cap_coll, c->d_state, c->d_acc,
                   c->d_counters + 2, c->d_status, 148 * 4, c->stream);
+  if (c->colstats)
+    launch_collision_stats(c->d_coll, c->d_counters + 1, c->cap_coll, c->d_state, c->d_best1, c->d_best2, c->d_cst,
+                           c->d_counters + 4, c->cap_cst, c->d_pv, c->d_group_tab, c->d_group_n, c->d_colacc,
+                           c->d_counters + 5, c->d_status, c->stream);
   GP_CK(cudaGetLastError());
   return mark(c, 2 * GP_PHASE_RESPONSE + 1, c->stream);
 }
@@ -492,7 +512,18 @@ int gp_ctx_create(const gp_params *params, gp_ctx **out) {
   if (!rc) rc = dalloc(&c->d_pv, 1);
   if (!rc) rc = dalloc(&c->d_pv_alt, 1);
   if (!rc) rc = dalloc(&c->d_fluid_cols, kNFluid);
-  if (!rc) rc = dalloc(&c->d_counters, 4);
+  if (!rc) rc = dalloc(&c->d_counters, 6);
+  if (!rc && cudaMemset(c->d_counters, 0, 6 * sizeof(unsigned long long)) != cudaSuccess) rc = GP_ECUDA;
+  if (!rc) rc = dalloc(&c->d_group_tab, kMaxClasses);
+  if (!rc) rc = dalloc(&c->d_group_n, kMaxClasses);
+  if (!rc) {
+    std::vector<int32_t *> tab(kMaxClasses, nullptr);
+    std::vector<int32_t> ng(kMaxClasses, 1);
+    if (cudaMemcpy(c->d_group_tab, tab.data(), kMaxClasses * sizeof(int32_t *), cudaMemcpyHostToDevice) !=
+            cudaSuccess ||
+        cudaMemcpy(c->d_group_n, ng.data(), kMaxClasses * sizeof(int32_t), cudaMemcpyHostToDevice) != cudaSuccess)
+      rc = GP_ECUDA;
+  }
   if (!rc) rc = dalloc(&c->d_status, 1);
   if (!rc && cudaMemset(c->d_status, 0, sizeof(Status)) != cudaSuccess) rc = GP_ECUDA;
   if (!rc) rc = upload_inst(c);
@@ -523,6 +554,9 @@ int gp_ctx_destroy(gp_ctx *c) {
   if (c->field) cudaFree(c->field);
   dfree(c->stage); dfree(c->d_inst); dfree(c->d_pv); dfree(c->d_pv_alt); dfree(c->d_fluid_cols);
   dfree(c->d_counters);
+  for (auto &g : c->group_dev) dfree(g);
+  dfree(c->d_group_tab); dfree(c->d_group_n); dfree(c->d_cst); dfree(c->d_colacc);
+  dfree(c->d_stat_partial); dfree(c->d_stat_out);
   dfree(c->d_status); dfree(c->d_scratch);
   if (c->ev_fork) cudaEventDestroy(c->ev_fork);
   if (c->ev_join) cudaEventDestroy(c->ev_join);
@@ -683,6 +717,28 @@ int class_setup(gp_ctx *c, const std::vector<double> *hp, int64_t off, int64_t c
 // After a change of the class table: caller-order offsets and search cells of the live
 // classes, the device table, the captured graphs, and (rebin) a binning pass so that
 // the next advance moves exactly the live particles.
+void size_groups(gp_ctx *c, int slot) {
+  if ((int)c->group_dev.size() <= slot) {
+    c->group_dev.resize(slot + 1, nullptr);
+    c->group_n.resize(slot + 1, 1);
+  }
+}
+
+// Class slot `slot` goes back to one polydisperse index (all particles IDP = 1).
+int clear_groups(gp_ctx *c, int slot) {
+  size_groups(c, slot);
+  if (!c->group_dev[slot] && c->group_n[slot] == 1) return GP_OK;
+  GP_CK(cudaStreamSynchronize(c->stream));
+  dfree(c->group_dev[slot]);
+  c->group_dev[slot] = nullptr;
+  c->group_n[slot] = 1;
+  int32_t *null_ptr = nullptr;
+  const int32_t one = 1;
+  GP_CK(cudaMemcpy(c->d_group_tab + slot, &null_ptr, sizeof(int32_t *), cudaMemcpyHostToDevice));
+  GP_CK(cudaMemcpy(c->d_group_n + slot, &one, sizeof(int32_t), cudaMemcpyHostToDevice));
+  return GP_OK;
+}
+
 int refresh_classes(gp_ctx *c, bool rebin) {
   int64_t begin = 0, cells = 0;
   for (size_t k = 0; k < c->insts.size(); ++k) {
@@ -754,6 +810,8 @@ int gp_upload_classes(gp_ctx *c, int32_t nclass, const int64_t *counts, const do
   c->live.assign(nclass, 1);
   c->class_field.assign(nclass, 0);
   c->n_slots = n;
+  c->fluid_ok = false;
+  for (int k = 0; k < nclass; ++k) GP_TRY(clear_groups(c, k));
   return refresh_classes(c, false);
 }
 
@@ -792,6 +850,8 @@ int gp_add_class(gp_ctx *c, int32_t field, int64_t n, const double *const *cols,
     c->class_field[slot] = field;
   }
   *ig = (int32_t)slot + 1;
+  c->fluid_ok = false;
+  GP_TRY(clear_groups(c, (int)slot));
   return refresh_classes(c, true);
 }
 
@@ -816,6 +876,7 @@ int gp_remove_class(gp_ctx *c, int32_t ig, double *const *cols, int32_t on_devic
   launch_retire(c->d_pv, c->n_slots, ig - 1, c->stream);
   GP_CK(cudaGetLastError());
   c->live[ig - 1] = 0;
+  GP_TRY(clear_groups(c, ig - 1));
   GP_TRY(refresh_classes(c, true));
   GP_CK(cudaStreamSynchronize(c->stream));
   return GP_OK;
@@ -824,6 +885,101 @@ int gp_remove_class(gp_ctx *c, int32_t ig, double *const *cols, int32_t on_devic
 int gp_class_count(gp_ctx *c, int32_t ig, int64_t *n) {
   if (!c || !n || ig < 1 || ig > (int)c->live.size()) return GP_EBADARG;
   *n = c->live[ig - 1] ? c->insts[ig - 1].count : 0;
+  return GP_OK;
+}
+
+int gp_set_class_groups(gp_ctx *c, int32_t ig, int32_t ngroups, const int32_t *idp) {
+  if (!c || ig < 1 || ig > (int)c->live.size() || !c->live[ig - 1]) return GP_EBADARG;
+  if (ngroups < 1 || ngroups > kStatMaxGroups || (!idp && ngroups != 1)) return GP_EBADARG;
+  const int slot = ig - 1;
+  GP_TRY(clear_groups(c, slot));
+  if (!idp) return GP_OK;
+  const int64_t n = c->insts[slot].count;
+  for (int64_t i = 0; i < n; ++i)
+    if (idp[i] < 1 || idp[i] > ngroups) return GP_EBADARG;
+  int32_t *d = nullptr;
+  GP_TRY(dalloc(&d, n));
+  if (cudaMemcpy(d, idp, n * sizeof(int32_t), cudaMemcpyHostToDevice) != cudaSuccess) {
+    dfree(d);
+    return GP_ECUDA;
+  }
+  c->group_dev[slot] = d;
+  c->group_n[slot] = ngroups;
+  GP_CK(cudaMemcpy(c->d_group_tab + slot, &d, sizeof(int32_t *), cudaMemcpyHostToDevice));
+  GP_CK(cudaMemcpy(c->d_group_n + slot, &ngroups, sizeof(int32_t), cudaMemcpyHostToDevice));
+  return GP_OK;
+}
+
+int gp_stat_partfluid(gp_ctx *c, int32_t ig, double *out) {
+  if (!c || !out || ig < 1 || ig > (int)c->live.size() || !c->live[ig - 1]) return GP_EBADARG;
+  if (!c->fluid_ok) return GP_EBADARG;   // no step has sampled the fluid at these particles
+  const int slot = ig - 1;
+  size_groups(c, slot);
+  const int ng = c->group_n[slot];
+  constexpr int kBlocks = 148 * 3;
+  if (!c->d_stat_partial) {
+    GP_TRY(dalloc(&c->d_stat_partial, (size_t)kBlocks * kStatMaxGroups * kNStatPartfluid));
+    GP_TRY(dalloc(&c->d_stat_out, (size_t)kStatMaxGroups * kNStatPartfluid));
+  }
+  launch_stat_partfluid(c->d_inst, c->d_pv, c->n_slots, slot, c->d_fluid_cols, c->group_dev[slot], ng,
+                        c->prm.rhof, c->ppi, c->d_stat_partial, kBlocks, c->d_stat_out, c->d_status, c->stream);
+  GP_CK(cudaGetLastError());
+  GP_CK(cudaMemcpyAsync(out, c->d_stat_out, (size_t)ng * kNStatPartfluid * sizeof(double), cudaMemcpyDeviceToHost,
+                        c->stream));
+  GP_CK(cudaStreamSynchronize(c->stream));
+  return GP_OK;
+}
+
+int gp_collision_stats_enable(gp_ctx *c, int32_t on) {
+  if (!c) return GP_EBADARG;
+  if ((on != 0) == c->colstats) return GP_OK;
+  GP_CK(cudaStreamSynchronize(c->stream));
+  if (on && (!c->d_colacc || c->cap_cst < c->cap_pairs)) {
+    dfree(c->d_cst);
+    c->cap_cst = 0;
+    if (!c->d_colacc) {
+      GP_TRY(dalloc(&c->d_colacc, (size_t)kMaxClasses * kStatMaxGroups * kStatMaxGroups * kNStatCollision));
+      GP_CK(cudaMemset(c->d_colacc, 0,
+                       (size_t)kMaxClasses * kStatMaxGroups * kStatMaxGroups * kNStatCollision * sizeof(double)));
+    }
+    // every candidate pair may be in contact
+    GP_TRY(dalloc(&c->d_cst, (size_t)std::max<int64_t>(c->cap_pairs, 1)));
+    c->cap_cst = std::max<int64_t>(c->cap_pairs, 1);
+  }
+  c->colstats = on != 0;
+  drop_graph(c);
+  return GP_OK;
+}
+
+int gp_collision_stats(gp_ctx *c, int32_t ig, double *out, int64_t *steps, int32_t reset) {
+  if (!c || !out || ig < 1 || ig > (int)c->live.size()) return GP_EBADARG;
+  const int slot = ig - 1;
+  size_groups(c, slot);
+  const int ng = c->group_n[slot];
+  const size_t per_class = (size_t)kStatMaxGroups * kStatMaxGroups * kNStatCollision;
+  std::vector<double> acc(per_class, 0.0);
+  unsigned long long cnt[6] = {};
+  GP_CK(cudaStreamSynchronize(c->stream));
+  if (c->d_colacc)
+    GP_CK(cudaMemcpy(acc.data(), c->d_colacc + (size_t)slot * per_class, per_class * sizeof(double),
+                     cudaMemcpyDeviceToHost));
+  GP_CK(cudaMemcpy(cnt, c->d_counters, sizeof(cnt), cudaMemcpyDeviceToHost));
+  const double dtime = c->insts.empty() ? c->tmpl.dtime : c->insts[slot].dtime;
+  for (int g1 = 0; g1 < ng; ++g1)
+    for (int g2 = 0; g2 < ng; ++g2) {
+      const double *a = acc.data() + ((size_t)g1 * kStatMaxGroups + g2) * kNStatCollision;
+      double *o = out + ((size_t)g1 * ng + g2) * kNStatCollision;
+      for (int k = 0; k < kNStatCollision; ++k) o[k] = a[k];
+      o[2] = 2.0 * o[1] / dtime;   // collision_interaction.f90:429
+      o[4] = o[3] / o[0];          // collision_interaction.f90:430
+    }
+  if (steps) *steps = (int64_t)cnt[5];
+  if (reset) {
+    if (c->d_colacc)
+      GP_CK(cudaMemsetAsync(c->d_colacc, 0, (size_t)kMaxClasses * per_class * sizeof(double), c->stream));
+    GP_CK(cudaMemsetAsync(c->d_counters + 5, 0, sizeof(unsigned long long), c->stream));
+    GP_CK(cudaStreamSynchronize(c->stream));
+  }
   return GP_OK;
 }
 
@@ -859,6 +1015,7 @@ int gp_put_state(gp_ctx *c, int64_t n, const double *const *cols, int32_t on_dev
   launch_scatter_state(c->d_inst, c->d_pv, c->n_slots, c->d_scratch, n, c->stream);
   GP_CK(cudaGetLastError());
   GP_CK(cudaStreamSynchronize(c->stream));
+  c->fluid_ok = false;
   return GP_OK;
 }
 
@@ -917,6 +1074,7 @@ int gp_step(gp_ctx *c, int32_t nsteps) {
     it = c->graphs.emplace(nsteps, ge).first;
   }
   GP_CK(cudaGraphLaunch(it->second, c->stream));
+  c->fluid_ok = true;   // a replay samples the fluid as the capture did
   return GP_OK;
 }
 
@@ -1369,6 +1527,8 @@ int gp_autotune(gp_ctx *c, int32_t *grids_out) {
   const int64_t n = c->n;
   double *save = nullptr;
   GP_TRY(dalloc(&save, (size_t)kNState * n));
+  const bool colstats = c->colstats;   // the trials add nothing to the statistics
+  c->colstats = false;
   launch_gather_state(c->d_inst, c->d_pv, c->n_slots, -1, save, c->d_fluid_cols, nullptr, n, c->stream);
   GP_CK(cudaGetLastError());
   static const int kMult[] = {1, 2, 4, 8, 16};
@@ -1410,6 +1570,8 @@ int gp_autotune(gp_ctx *c, int32_t *grids_out) {
     if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(c->stream) != cudaSuccess) rc = GP_ECUDA;
   }
   cudaFree(save);
+  c->colstats = colstats;
+  c->fluid_ok = false;
   if (!rc && grids_out) {
     for (int t = 0; t < GP_NTUNE; ++t) grids_out[t] = c->tune[t];
     grids_out[GP_NTUNE] = c->overlap ? 1 : 0;

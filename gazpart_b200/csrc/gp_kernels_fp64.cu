@@ -129,7 +129,9 @@ __global__ void __launch_bounds__(128, GP_CONTACT_MIN_BLOCKS) k_contact(const In
                                                     const PairRec *__restrict__ pairs,
                                                     const unsigned long long *__restrict__ npairs, int64_t cap_pairs,
                                                     CollRec *__restrict__ coll, unsigned long long *ncoll,
-                                                    int64_t cap_coll, unsigned long long *queue, Status *st) {
+                                                    int64_t cap_coll, unsigned long long *queue,
+                                                    ContactStatRec *__restrict__ cst, unsigned long long *ncst,
+                                                    int64_t cap_cst, Status *st) {
   const PoolView P = *pv;
   const int64_t np = (int64_t)min(*npairs, (unsigned long long)cap_pairs);
   const unsigned lane = threadIdx.x & 31u;
@@ -211,6 +213,22 @@ __global__ void __launch_bounds__(128, GP_CONTACT_MIN_BLOCKS) k_contact(const In
     const double vp2 = P.st[4][i2] + (om2[2] * rx2[0] - om2[0] * rx2[2]);
     const double wp2 = P.st[5][i2] + (om2[0] * rx2[1] - om2[1] * rx2[0]);
     const double nvrel = (up2 - up1) * cn[0] + (vp2 - vp1) * cn[1] + (wp2 - wp1) * cn[2];
+    if (cst != nullptr) {
+      // every contact, for the collision statistics (collision_interaction.f90:253-328)
+      const unsigned long long k = atomicAdd(ncst, 1ull);
+      if ((int64_t)k < cap_cst) {
+        ContactStatRec c;
+        c.home = i1; c.near = i2; c.inst = P.inst[i1]; c.pad = 0; c.k1 = pr.k1; c.k2 = pr.k2;
+        const double v0 = ept1[0] - ept2[0], v1 = ept1[1] - ept2[1], v2 = ept1[2] - ept2[2];
+        c.depth = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
+        c.nvrel = nvrel;
+        const double vx = up2 - up1, vy = vp2 - vp1, vz = wp2 - wp1;
+        c.nrm = sqrt(vx * vx + vy * vy + vz * vz);
+        cst[k] = c;
+      } else {
+        set_error(st, GP_EPAIR_OVERFLOW, (long long)P.id[i1], P.inst[i1]);
+      }
+    }
     if (!(nvrel < kZeroRef)) continue;
     const unsigned long long slot = atomicAdd(ncoll, 1ull);
     if ((int64_t)slot >= cap_coll) {
@@ -240,8 +258,10 @@ int contact_grid_blocks() {
 
 void launch_contact(const InstDev *insts, const PoolView *pv, const PairRec *pairs, const unsigned long long *npairs,
                     int64_t cap_pairs, CollRec *coll, unsigned long long *ncoll, int64_t cap_coll,
-                    unsigned long long *queue, Status *st, int grid, cudaStream_t s) {
-  k_contact<<<grid, 128, 0, s>>>(insts, pv, pairs, npairs, cap_pairs, coll, ncoll, cap_coll, queue, st);
+                    unsigned long long *queue, ContactStatRec *cst, unsigned long long *ncst, int64_t cap_cst,
+                    Status *st, int grid, cudaStream_t s) {
+  k_contact<<<grid, 128, 0, s>>>(insts, pv, pairs, npairs, cap_pairs, coll, ncoll, cap_coll, queue, cst, ncst,
+                                 cap_cst, st);
 }
 
 // COLLISION_RESPONSE (collision_response.f90) for the accepted pairs; each particle is

@@ -22,7 +22,8 @@ void launch_frozen_interp(const double *xain, const double *yain, const double *
 int contact_grid_blocks();
 void launch_contact(const InstDev *insts, const PoolView *pv, const PairRec *pairs, const unsigned long long *npairs,
                     int64_t cap_pairs, CollRec *coll, unsigned long long *ncoll, int64_t cap_coll,
-                    unsigned long long *queue, Status *st, int grid, cudaStream_t s);
+                    unsigned long long *queue, ContactStatRec *cst, unsigned long long *ncst, int64_t cap_cst,
+                    Status *st, int grid, cudaStream_t s);
 void launch_response(const InstDev *insts, const PoolView *pv, const CollRec *coll, const unsigned long long *ncoll,
                      int64_t cap_coll, const int8_t *state, int32_t *acc_list, unsigned long long *nacc, Status *st,
                      int grid, cudaStream_t s);
@@ -40,6 +41,16 @@ void launch_contact_batch(int64_t n, const double *shapes /*n*4: a1 b1 a2 b2*/, 
 void launch_response_batch(int64_t n, double ecp, double mup, const double *ip /*n*3*/, double *p1 /*n*10*/,
                            double *p2, const double *r1, const double *r2, const double *nrm, Status *st,
                            cudaStream_t s);
+
+// --- gp_stats.cu (-fmad=false) ---
+void launch_stat_partfluid(const InstDev *insts, const PoolView *pv, int64_t n, int inst, double *const *fluid,
+                           const int32_t *groups, int ngroups, double rhof, double ppi, double *partial,
+                           int nblocks, double *out, Status *st, cudaStream_t s);
+void launch_collision_stats(const CollRec *coll, const unsigned long long *ncoll, int64_t cap_coll,
+                            const int8_t *state, unsigned long long *best1, unsigned long long *best2,
+                            const ContactStatRec *rec, const unsigned long long *nrec, int64_t cap_rec,
+                            const PoolView *pv, const int32_t *const *group_tab, const int32_t *ngroups, double *acc,
+                            unsigned long long *steps, Status *st, cudaStream_t s);
 
 // --- gp_kernels_mixed.cu ---
 void launch_gather_mixed(const InstDev *insts, const PoolView *pv, const int32_t *perm, int64_t n,

@@ -82,6 +82,20 @@ struct CollRec {
   double rx1[3], rx2[3], cn[3];
 };
 
+// Statistics beside the step (gp_stats.cu).
+constexpr int kNStatPartfluid = GP_NSTAT_PARTFLUID;   // MEAN_PARTFLUID(1:36, J, IDP)
+constexpr int kNStatCollision = GP_NSTAT_COLLISION;   // MEAN_PART_COL(1:8, IDP1, IDP2)
+constexpr int kStatMaxGroups = GP_STAT_MAX_GROUPS;    // polydisperse indices per class
+
+// A pair found in contact, kept for the collision statistics when they are on:
+// overlap depth |EPT1 - EPT2|, NVREL and |v_rel| (collision_interaction.f90:253-328).
+struct ContactStatRec {
+  int32_t home, near;
+  int32_t inst, pad;
+  unsigned long long k1, k2;
+  double depth, nvrel, nrm;
+};
+
 // Binned particles of the collision search grid (see gp_search.cu).
 struct SearchArrays {
   int32_t *cell_count;   // per search cell (+1 zero sentinel)

@@ -121,6 +121,41 @@ int gp_status(gp_ctx *ctx, int32_t *code, int64_t *first_id);
 int gp_collision_counters(gp_ctx *ctx, int64_t *vals);
 /* Class (IG, 1-based) of the particle that raised the first error, 0 if none. */
 int gp_status_class(gp_ctx *ctx, int32_t *ig);
+/* ------------------------------------------------------------- statistics ---- */
+/* Polydisperse index of each particle of class ig (PART(I,IG)%IDP): n values in
+ * 1..ngroups, in the class's own particle order (host array), or NULL for all 1
+ * (ngroups = 1).  The statistics below are kept per index, as the reference keeps
+ * them per (IG, IDP). */
+#define GP_STAT_MAX_GROUPS 8
+int gp_set_class_groups(gp_ctx *ctx, int32_t ig, int32_t ngroups, const int32_t *idp);
+
+/* STAT_PARTFLUID (stat_partfluid.f90:1-472) for class ig on the device: for each
+ * index g, the sums over the class's particles of the 35 quantities the reference
+ * averages (in its order: Re_p, C_D, C_L, F_drag xyz, F_lift xyz, |F_drag|, |F_lift|,
+ * Re_R, C_T pitch, C_T rot, T_pitch xyz, T_rot xyz, |T_pitch|, |T_rot|, tau_p, gravity,
+ * phi, symmetry axis xyz, 1/tau_p, u xyz, omega xyz) and the particle count:
+ * out[g * GP_NSTAT_PARTFLUID + k], k < 35 the sums and k = 35 the count.  Dividing by
+ * the count gives MEAN_PARTFLUID(:, IG, g+1).  The quantities use the fluid velocity
+ * and vorticity the last step interpolated at each particle (PART%UFAP.., as the
+ * reference's do), so the context must have stepped since its particles were last
+ * uploaded or admitted (GP_EBADARG otherwise).  Synchronises the context's stream. */
+#define GP_NSTAT_PARTFLUID 36
+int gp_stat_partfluid(gp_ctx *ctx, int32_t ig, double *out);
+
+/* Collision statistics of COLLISION_INTERACTION (collision_interaction.f90:171,
+ * 330-345,397-398,423-450).  While on, every collision step adds, per class and pair of
+ * indices (IDP of HOME, IDP of NEAR), over the pairs found in contact while both
+ * particles were uncoloured: [0] their number, [1] the collisions among them
+ * (NVREL < ZERO), [3] the overlap depth |EPT1-EPT2|, [5] NVREL, [6] |v_rel|,
+ * [7] the collision angle acos(NVREL/|v_rel|).  gp_collision_stats returns class ig's
+ * sums since the last reset, ngroups x ngroups x GP_NSTAT_COLLISION values, with the
+ * reference's derived entries filled in from them: [2] = 2 [1] / DTIME per step
+ * accumulated and [4] = [3] / [0]; *steps receives the number of collision steps
+ * summed.  reset != 0 clears the sums afterwards.  Turning the statistics on or off
+ * drops the captured step graphs. */
+#define GP_NSTAT_COLLISION 8
+int gp_collision_stats_enable(gp_ctx *ctx, int32_t on);
+int gp_collision_stats(gp_ctx *ctx, int32_t ig, double *out, int64_t *steps, int32_t reset);
 int gp_clear_status(gp_ctx *ctx);
 int gp_sync(gp_ctx *ctx);
 

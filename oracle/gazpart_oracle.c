@@ -213,6 +213,114 @@ int orc_fluid_force(const orc_setup *s, double emaj, double apr, double rhop,
     return ORC_OK;
 }
 
+/* stat_partfluid.f90:122-293 for one particle: the 35 quantities the reference sums,
+ * in its order, then 1.0 (the count).  No guards: the reference divides as written. */
+void orc_stat_partfluid_particle(const orc_setup *s, double emaj, double apr, double rhop, const double u[3],
+                                 const double om[3], const double q[4], const double uf[3], const double wv[3],
+                                 double v[36]) {
+    const double a0 = 1.95, a1 = 18.12, a2 = 1.023, a3 = 4.26, a4 = 0.384;
+    const double a5 = 21.52, a6 = 0.990, a7 = 2.86, a8 = 0.260;
+    const double b1 = 0.083, b2 = -0.21, b3 = 1.582, b4 = 0.851, b5 = 1.842;
+    const double b6 = -0.802, b7 = -0.006, b8 = 0.874, b9 = 0.009, b10 = 0.570;
+    const double c1 = 0.935, c2 = 0.146, c3 = -0.469, c4 = 0.145, c5 = 0.116;
+    const double c6 = 0.748, c7 = 0.041, c8 = 0.221, c9 = 0.657, c10 = 0.044;
+    const double r1 = 0.573, r2 = -0.154, r3 = 116.61, r4 = 1.0;
+    const double r1_ = 1.244, r2_ = 0.239, r3_ = 378.12, r4_ = 0.789;
+    const double ppi = s->ppi, rhof = s->rhof, visc = s->visc;
+    double pa[3] = {1.0, 0.0, 0.0};                                          /* :127-129 */
+    double pmass = pmass_of(s, emaj, apr, rhop);                            /* :131 */
+    double urel[3] = {uf[0] - u[0], uf[1] - u[1], uf[2] - u[2]};            /* :134-136 */
+    double urel_mag = sqrt(urel[0] * urel[0] + urel[1] * urel[1] + urel[2] * urel[2]);
+    double dequiv = 2.0 * emaj / pow(apr, 2.0 / 3.0);                       /* :140 */
+    double rep = (urel_mag * dequiv) / visc;
+    double pf[3] = {uf[0] - u[0], uf[1] - u[1], uf[2] - u[2]};
+    double cq[4];
+    conjq(q, cq);
+    orc_transform_vec(pf, cq);                                               /* :150 */
+    double phi = fabs(atan((sqrt(pf[1] * pf[1] + pf[2] * pf[2])) / (pf[0])));
+    double umag = sqrt(pf[0] * pf[0] + pf[1] * pf[1] + pf[2] * pf[2]);
+    double cd0 = a1 / pow(rep, a2) + a3 / pow(rep, a4);                     /* :160-166 */
+    double cd90 = a5 / pow(rep, a6) + a7 / pow(rep, a8);
+    double cdrag = cd0 + (cd90 - cd0) * pow(sin(phi), a0);
+    double clift = (b1 / pow(rep, b2) + b3 / pow(rep, b4)) * pow(sin(phi), b5 + b6 * pow(rep, b7)) *
+                   pow(cos(phi), b8 + b9 * pow(rep, b10));
+    double fd[3], fl[3];
+    double syz = sqrt(pf[1] * pf[1] + pf[2] * pf[2]);
+    for (int k = 0; k < 3; ++k)                                              /* :170-178 */
+        fd[k] = (1.0 / 2.0) * (rhof / pmass) * (1.0 / 4.0) * (ppi * (dequiv * dequiv)) * cdrag * umag * pf[k];
+    fl[0] = (1.0 / 2.0) * (rhof / pmass) * (1.0 / 4.0) * (ppi * (dequiv * dequiv)) * clift * (umag * umag) *
+            sin(phi) * copysign(1.0, -pf[0]);
+    fl[1] = (1.0 / 2.0) * (rhof / pmass) * (1.0 / 4.0) * (ppi * (dequiv * dequiv)) * clift * (umag * umag) *
+            cos(phi) * (pf[1] / syz);
+    fl[2] = (1.0 / 2.0) * (rhof / pmass) * (1.0 / 4.0) * (ppi * (dequiv * dequiv)) * clift * (umag * umag) *
+            cos(phi) * (pf[2] / syz);
+    orc_transform_vec(fd, q);
+    orc_transform_vec(fl, q);
+    v[0] = rep; v[1] = cdrag; v[2] = clift;                                  /* :183-195 */
+    v[3] = fd[0]; v[4] = fd[1]; v[5] = fd[2];
+    v[6] = fl[0]; v[7] = fl[1]; v[8] = fl[2];
+    v[9] = sqrt(fd[0] * fd[0] + fd[1] * fd[1] + fd[2] * fd[2]);
+    v[10] = sqrt(fl[0] * fl[0] + fl[1] * fl[1] + fl[2] * fl[2]);
+    double curl[3] = {wv[0], wv[1], wv[2]};                                  /* :199-203 */
+    orc_transform_vec(curl, cq);
+    double o0 = 0.5 * curl[0] - om[0], o1 = 0.5 * curl[1] - om[1], o2 = 0.5 * curl[2] - om[2];
+    double omag = sqrt(o0 * o0 + o1 * o1 + o2 * o2);
+    double oyz = sqrt(o2 * o2 + o1 * o1);
+    double re_r = (omag * (dequiv * dequiv)) / visc;                         /* :214 */
+    double ctp = (c1 / pow(rep, c2) + c3 / pow(rep, c4)) * pow(sin(phi), c5 + c6 * pow(rep, c7)) *
+                 pow(cos(phi), c8 + c9 * pow(rep, c10));
+    double ctr = r1 * pow(re_r, r2) + r3 / pow(re_r, r4);
+    double ctr2 = r1_ * pow(re_r, r2_) + r3_ / pow(re_r, r4_);
+    double tp[3], tr[3];                                                     /* :224-243 */
+    tp[0] = 0.0;
+    tp[1] = (1.0 / 4.0) * (rhof / pmass) * (1.0 / 4.0) * ppi * ((dequiv * dequiv) * dequiv) * ctp * (umag * umag) *
+            (fabs(pf[2]) / sqrt(pf[1] * pf[1] + pf[2] * pf[2])) * copysign(1.0, pf[0] * pf[2]);
+    tp[2] = (1.0 / 4.0) * (rhof / pmass) * (1.0 / 4.0) * ppi * ((dequiv * dequiv) * dequiv) * ctp * (umag * umag) *
+            (fabs(pf[1]) / sqrt(pf[1] * pf[1] + pf[2] * pf[2])) * copysign(1.0, pf[0] * pf[1]);
+    double h = dequiv / 2.0, h2 = h * h, h5 = h2 * h2 * h;
+    tr[0] = ctr * (rhof / pmass) / 2.0 * h5 * fabs(o0) * o0;
+    tr[1] = ctr2 * (rhof / pmass) / 2.0 * h5 * oyz * o1;
+    tr[2] = ctr2 * (rhof / pmass) / 2.0 * h5 * oyz * o2;
+    orc_transform_vec(pa, q);                                                /* :245 */
+    v[11] = re_r; v[12] = ctp; v[13] = ctr;                                  /* :247-263 */
+    v[14] = tp[0]; v[15] = tp[1]; v[16] = tp[2];
+    v[17] = tr[0]; v[18] = tr[1]; v[19] = tr[2];
+    v[20] = sqrt(tp[0] * tp[0] + tp[1] * tp[1] + tp[2] * tp[2]);
+    v[21] = sqrt(tr[0] * tr[0] + tr[1] * tr[1] + tr[2] * tr[2]);
+    double minax = emaj / apr;                                               /* :265-276 */
+    double fbeta;
+    if (apr == 1.0) fbeta = 1.0;
+    else fbeta = (apr * log(apr + sqrt(apr * apr - 1.0))) / (sqrt(apr * apr - 1.0));
+    double taupf = (2.0 / 9.0) * (rhop * (minax * minax)) / (rhof * visc);
+    taupf = taupf * fbeta;
+    v[22] = taupf;
+    v[23] = s->gravity;
+    v[24] = phi;
+    v[25] = pa[0]; v[26] = pa[1]; v[27] = pa[2];
+    v[28] = (0.5 * rhof * cdrag * (ppi / 4.0) * (dequiv * dequiv) * umag) / pmass;   /* :285 */
+    v[29] = u[0]; v[30] = u[1]; v[31] = u[2];
+    v[32] = om[0]; v[33] = om[1]; v[34] = om[2];
+    v[35] = 1.0;
+}
+
+/* stat_partfluid.f90:115-299: the sums over the particles, in their order, per index
+ * (group[i] in 1..ngroups, or all 1 when group is NULL); out: ngroups*36. */
+void orc_stat_partfluid(const orc_setup *s, const orc_props *p, const orc_state *st, const int32_t *group,
+                        int32_t ngroups, double *out) {
+    for (int64_t k = 0; k < (int64_t)ngroups * 36; ++k) out[k] = 0.0;
+    for (int64_t i = 0; i < st->n; ++i) {
+        double v[36];
+        const double u[3] = {st->u[i], st->v[i], st->w[i]};
+        const double om[3] = {st->ox[i], st->oy[i], st->oz[i]};
+        const double q[4] = {st->qa[i], st->qb[i], st->qc[i], st->qd[i]};
+        const double uf[3] = {st->ufap[i], st->vfap[i], st->wfap[i]};
+        const double wv[3] = {st->vortx[i], st->vorty[i], st->vortz[i]};
+        orc_stat_partfluid_particle(s, p->emaj[i], p->apr[i], p->rhop[i], u, om, q, uf, wv, v);
+        double *o = out + (int64_t)(group ? group[i] - 1 : 0) * 36;
+        for (int k = 0; k < 36; ++k) o[k] = o[k] + v[k];
+    }
+}
+
 /* fluid_torque_ellipsoid.f90:1-190.  Pitching and rotation torque per unit mass in the
  * body frame.  The relative velocity uses the particle's stored velocity u_n
  * (fluid_torque_ellipsoid.f90:88-105), not the stage velocity.
@@ -1565,9 +1673,12 @@ static inline double bound_radius(double emaj, double apr) {
 }
 
 /* collision_interaction.f90:216-348 for one pair (HOME i1, NEAR i2). */
-int32_t orc_pair_eval(const orc_setup *s, const orc_props *p, const orc_state *st,
-                      int64_t i1, int64_t i2, double ept1[3], double ept2[3],
-                      double cn[3], double rx1[3], double rx2[3], int32_t *flag_out) {
+/* collision_interaction.f90:216-328; also returns NVREL and |v_rel| (NRM_VREL) of a
+ * pair in contact, for the collision statistics (:330-345). */
+static int32_t pair_eval_full(const orc_setup *s, const orc_props *p, const orc_state *st,
+                              int64_t i1, int64_t i2, double ept1[3], double ept2[3],
+                              double cn[3], double rx1[3], double rx2[3], int32_t *flag_out,
+                              double *nvrel_out, double *nrm_out) {
     double xn = st->x[i1], yn = st->y[i1], zn = st->z[i1];
     double vkx = st->x[i2] - xn, vky = st->y[i2] - yn, vkz = st->z[i2] - zn;
     if ((fabs(vkx) > s->lx / 2) && s->periodicity) vkx = vkx - copysign(s->lx, vkx);
@@ -1597,7 +1708,15 @@ int32_t orc_pair_eval(const orc_setup *s, const orc_props *p, const orc_state *s
     double wp2 = st->w[i2] + (om2[0] * rx2[1] - om2[1] * rx2[0]);
     double vrelx = up2 - up1, vrely = vp2 - vp1, vrelz = wp2 - wp1;
     double nvrel = vrelx * cn[0] + vrely * cn[1] + vrelz * cn[2];
+    if (nvrel_out) *nvrel_out = nvrel;
+    if (nrm_out) *nrm_out = sqrt(vrelx * vrelx + vrely * vrely + vrelz * vrelz);
     return (nvrel < ZERO_REF) ? 1 : 0;
+}
+
+int32_t orc_pair_eval(const orc_setup *s, const orc_props *p, const orc_state *st,
+                      int64_t i1, int64_t i2, double ept1[3], double ept2[3],
+                      double cn[3], double rx1[3], double rx2[3], int32_t *flag_out) {
+    return pair_eval_full(s, p, st, i1, i2, ept1, ept2, cn, rx1, rx2, flag_out, NULL, NULL);
 }
 
 static int prefilter_pass(const orc_setup *s, const orc_props *p, const orc_state *st,
@@ -1643,13 +1762,14 @@ static int apply_response(const orc_setup *s, const orc_props *p, orc_state *st,
     return rc;
 }
 
-int orc_collision(const orc_setup *s, const orc_props *p, const orc_boxgrid *g,
-                  const int32_t *ncon, const int32_t *con, orc_state *st,
-                  int32_t prefilter, int32_t nthreads,
-                  int64_t coll_cap, int32_t *coll_home, int32_t *coll_near,
-                  int64_t *n_coll, int64_t *n_candidates, int64_t *n_contacts,
-                  int64_t *err_id) {
+static int collision_impl(const orc_setup *s, const orc_props *p, const orc_boxgrid *g,
+                          const int32_t *ncon, const int32_t *con, orc_state *st,
+                          int32_t prefilter, int32_t nthreads,
+                          int64_t coll_cap, int32_t *coll_home, int32_t *coll_near,
+                          int64_t *n_coll, int64_t *n_candidates, int64_t *n_contacts,
+                          int64_t *err_id, const int32_t *group, int32_t ngroups, double *colstat) {
     const int64_t n = st->n;
+    if (colstat) nthreads = 1;   /* the statistics follow the serial walk */
     int rc_out = ORC_OK;
     if (err_id) *err_id = -1;
     int32_t *ijk = (int32_t *)malloc((size_t)(n > 0 ? n : 1) * sizeof(int32_t));
@@ -1684,8 +1804,22 @@ int orc_collision(const orc_setup *s, const orc_props *p, const orc_boxgrid *g,
                         if (prefilter && !prefilter_pass(s, p, st, i1, i2)) continue;
                         coll_rec r;
                         int32_t flag;
-                        int hit = orc_pair_eval(s, p, st, i1, i2, r.ept1, r.ept2, r.cn, r.rx1, r.rx2, &flag);
+                        double nvrel = 0.0, nrm = 0.0;
+                        int hit = pair_eval_full(s, p, st, i1, i2, r.ept1, r.ept2, r.cn, r.rx1, r.rx2, &flag,
+                                                 &nvrel, &nrm);
                         ncontact += flag;
+                        if (colstat && flag) {
+                            /* collision_interaction.f90:330-345 and :397-398 */
+                            int g1 = group ? group[i1] - 1 : 0, g2 = group ? group[i2] - 1 : 0;
+                            double *a = colstat + ((int64_t)g1 * ngroups + g2) * 8;
+                            double v0 = r.ept1[0] - r.ept2[0], v1 = r.ept1[1] - r.ept2[1], v2 = r.ept1[2] - r.ept2[2];
+                            a[0] = a[0] + 1.0;
+                            a[3] = a[3] + sqrt(v0 * v0 + v1 * v1 + v2 * v2);
+                            a[5] = a[5] + nvrel;
+                            a[6] = a[6] + nrm;
+                            a[7] = a[7] + acos(nvrel / nrm);
+                            if (hit) a[1] = a[1] + 1.0;
+                        }
                         if (!hit) continue;
                         r.home = (int32_t)i1; r.near = (int32_t)i2;
                         int rc = apply_response(s, p, st, &r);
@@ -1777,6 +1911,32 @@ int orc_collision(const orc_setup *s, const orc_props *p, const orc_boxgrid *g,
     if (n_candidates) *n_candidates = ncand;
     if (n_contacts) *n_contacts = ncontact;
     return rc_out;
+}
+
+int orc_collision(const orc_setup *s, const orc_props *p, const orc_boxgrid *g,
+                  const int32_t *ncon, const int32_t *con, orc_state *st,
+                  int32_t prefilter, int32_t nthreads,
+                  int64_t coll_cap, int32_t *coll_home, int32_t *coll_near,
+                  int64_t *n_coll, int64_t *n_candidates, int64_t *n_contacts,
+                  int64_t *err_id) {
+    return collision_impl(s, p, g, ncon, con, st, prefilter, nthreads, coll_cap, coll_home, coll_near,
+                          n_coll, n_candidates, n_contacts, err_id, NULL, 0, NULL);
+}
+
+int orc_collision_stats(const orc_setup *s, const orc_props *p, const orc_boxgrid *g,
+                        const int32_t *ncon, const int32_t *con, orc_state *st, int32_t prefilter,
+                        const int32_t *group, int32_t ngroups, double *colstat, int64_t *n_coll,
+                        int64_t *err_id) {
+    for (int64_t k = 0; k < (int64_t)ngroups * ngroups * 8; ++k) colstat[k] = 0.0;
+    int rc = collision_impl(s, p, g, ncon, con, st, prefilter, 1, 0, NULL, NULL, n_coll, NULL, NULL,
+                            err_id, group, ngroups, colstat);
+    /* collision_interaction.f90:429-430 */
+    for (int64_t k = 0; k < (int64_t)ngroups * ngroups; ++k) {
+        double *a = colstat + k * 8;
+        a[2] = 2.0 * a[1] / s->dtime;
+        a[4] = a[3] / a[0];
+    }
+    return rc;
 }
 
 /* ---- exported pieces of the contact solve, for the scipy MINPACK cross-check ---- */

@@ -176,6 +176,26 @@ int orc_collision(const orc_setup *s, const orc_props *p, const orc_boxgrid *g,
                   int64_t *n_coll, int64_t *n_candidates, int64_t *n_contacts,
                   int64_t *err_id);
 
+/* COLLISION with the statistics of COLLISION_INTERACTION (collision_interaction.f90:
+ * 171,330-345,397-398,429-430), serial walk: colstat (ngroups*ngroups*8, by (IDP of
+ * HOME, IDP of NEAR)) receives for the pairs found in contact while both particles are
+ * uncoloured [0] their number, [1] the collisions, [2] 2[1]/DTIME, [3] sum of the overlap
+ * depth |EPT1-EPT2|, [4] [3]/[0], [5] sum of NVREL, [6] sum of |v_rel|, [7] sum of the
+ * collision angle.  group: IDP per particle (1..ngroups) or NULL. */
+int orc_collision_stats(const orc_setup *s, const orc_props *p, const orc_boxgrid *g,
+                        const int32_t *ncon, const int32_t *con, orc_state *st, int32_t prefilter,
+                        const int32_t *group, int32_t ngroups, double *colstat, int64_t *n_coll,
+                        int64_t *err_id);
+
+/* STAT_PARTFLUID (stat_partfluid.f90:122-299): the 35 per-particle quantities and the
+ * count, and their sums per polydisperse index (st->ufap.. are the fluid values the
+ * last step interpolated at each particle). */
+void orc_stat_partfluid_particle(const orc_setup *s, double emaj, double apr, double rhop, const double u[3],
+                                 const double om[3], const double q[4], const double uf[3], const double wv[3],
+                                 double v[36]);
+void orc_stat_partfluid(const orc_setup *s, const orc_props *p, const orc_state *st, const int32_t *group,
+                        int32_t ngroups, double *out);
+
 /* Evaluate one candidate pair exactly as collision_interaction.f90:216-348 does
  * (minimum image, contact, contact-point velocities, NVREL).  Returns 1 if the
  * pair would collide (flag && NVREL<ZERO), 0 otherwise. */

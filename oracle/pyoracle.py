@@ -150,6 +150,38 @@ class Ensemble:
                 "n_coll": ncoll.value, "n_candidates": ncand.value, "n_contacts": ncont.value,
                 "err_id": eid.value}
 
+    def collide_stats(self, group: Optional[np.ndarray] = None, ngroups: int = 1, prefilter: bool = True,
+                      grid=None):
+        """COLLISION with the collision statistics of COLLISION_INTERACTION (serial walk):
+        returns (rc, stats[ngroups, ngroups, 8], n_coll)."""
+        g = self.boxgrid() if grid is None else grid
+        ncon, con = self.connectivity(g)
+        s = make_setup(self.setup)
+        st = self.state()
+        out = np.zeros(ngroups * ngroups * 8)
+        gp = None
+        if group is not None:
+            group = np.ascontiguousarray(group, dtype=np.int32)
+            gp = iptr(group)
+        ncoll, eid = C.c_int64(), C.c_int64()
+        rc = lib().orc_collision_stats(C.byref(s), C.byref(self.props()), C.byref(g), iptr(ncon), iptr(con),
+                                       C.byref(st), C.c_int32(int(prefilter)), gp, C.c_int32(ngroups),
+                                       dptr(out), C.byref(ncoll), C.byref(eid))
+        return rc, out.reshape(ngroups, ngroups, 8), ncoll.value
+
+    def stat_partfluid(self, group: Optional[np.ndarray] = None, ngroups: int = 1) -> np.ndarray:
+        """STAT_PARTFLUID sums per index over the particles in order: [ngroups, 36], the
+        last entry the count (needs the fluid values of a step, self.a["ufap"]..)."""
+        s = make_setup(self.setup)
+        st = self.state()
+        out = np.zeros(ngroups * 36)
+        gp = None
+        if group is not None:
+            group = np.ascontiguousarray(group, dtype=np.int32)
+            gp = iptr(group)
+        lib().orc_stat_partfluid(C.byref(s), C.byref(self.props()), C.byref(st), gp, C.c_int32(ngroups), dptr(out))
+        return out.reshape(ngroups, 36)
+
 
 def interp_lag3(setup, field_ref: np.ndarray, x, y, z) -> np.ndarray:
     s = make_setup(setup)

@@ -330,3 +330,82 @@ def test_serial_and_parallel_collision_agree():
     assert np.array_equal(ra["home"], rb["home"]) and np.array_equal(ra["near"], rb["near"])
     for k in po.STATE_KEYS:
         assert np.array_equal(a.a[k], b.a[k])
+
+
+# -- statistics beside the step ------------------------------------------------
+# a generic line of centres: the contact solve's initial guess degenerates when the
+# centre line lies along x (it converges to the opposite normal) or has no y part
+# (acos of an undefined ratio), as the reference's does (Q14)
+_E = np.array([0.6, 0.48, 0.64])
+
+
+def _spheres(ss, us, a=0.05):
+    """Spheres centred at 3 + s e with velocity u e, for s in ss and u in us."""
+    n = len(ss)
+    s = config.Setup(nx=32, ny=32, nz=32, visc=0.05, dtime=1e-3)
+    st = {k: np.zeros(n) for k in po.STATE_KEYS}
+    for j, k in enumerate(("x", "y", "z")):
+        st[k] = 3.0 + np.array(ss, dtype=float) * _E[j]
+    for j, k in enumerate(("u", "v", "w")):
+        st[k] = np.array(us, dtype=float) * _E[j]
+    st["qa"][:] = 1.0
+    st["emaj"] = np.full(n, a)
+    st["apr"] = np.ones(n)
+    st["rhop"] = np.full(n, 1000.0)
+    for k in ("ipxx", "ipyy", "ipzz"):
+        st[k] = np.full(n, 2.0 * a * a / 5.0)
+    return s, st
+
+
+def test_collision_stats_head_on_spheres():
+    """Two overlapping spheres closing head on: one contact, one collision, depth
+    2a - d, NVREL = -|v_rel|, angle pi (collision_interaction.f90:330-345), to the
+    accuracy of the contact solve (its residual is the squared depth, so the normal
+    settles within about 1e-2 rad of the centre line)."""
+    a, d, v = 0.05, 0.09, 0.3
+    s, st = _spheres([3.0, 3.0 + d], [v, -v], a)
+    rc, cs, ncoll = po.Ensemble(s, st).collide_stats()
+    assert rc == 0 and ncoll == 1
+    c = cs[0, 0]
+    assert c[0] == 1.0 and c[1] == 1.0 and c[2] == 2.0 / s.dtime
+    assert abs(c[3] - (2 * a - d)) < 1e-2 * (2 * a - d) and c[4] == c[3]
+    assert abs(c[5] + 2 * v) < 1e-3 * v and abs(c[6] - 2 * v) < 1e-12
+    assert abs(c[7] - np.pi) < 2e-2
+
+
+def test_collision_stats_count_only_examined_pairs():
+    """Three spheres in a row, both contacts closing: the COLOR walk accepts the first
+    pair and never examines the second, so one contact is counted although the two
+    pairs are in contact; the indices split the sums by (IDP of HOME, IDP of NEAR)."""
+    a, d, v = 0.05, 0.09, 0.3
+    s, st = _spheres([3.0, 3.0 + d, 3.0 + 2 * d], [v, 0.0, -v], a)
+    ens = po.Ensemble(s, st)
+    full = po.Ensemble(s, st).collide(prefilter=True, nthreads=1)
+    assert full["n_contacts"] == 1 and full["n_coll"] == 1        # the walk evaluates one pair
+    every = po.Ensemble(s, st).collide(prefilter=True, nthreads=4)
+    assert every["n_contacts"] == 2                                # both pairs are in contact
+    rc, cs, ncoll = ens.collide_stats(group=np.array([1, 2, 2]), ngroups=2)
+    assert rc == 0 and ncoll == 1
+    assert cs[:, :, 0].sum() == 1.0 and cs[:, :, 1].sum() == 1.0
+    h, nr = full["home"][0], full["near"][0]
+    g = np.array([1, 2, 2]) - 1
+    assert cs[g[h], g[nr], 0] == 1.0
+
+
+def test_stat_partfluid_known_values():
+    """A sphere at rest in a uniform stream U along x: Re_p = U d / visc, no lift, drag
+    along x, phi = 0, symmetry axis x; tau_p of a sphere (FBETA = 1)."""
+    s = config.Setup(nx=32, ny=32, nz=32, visc=0.05)
+    a, rhop, U = 0.01, 1000.0, 0.7
+    v = np.zeros(36)
+    po.lib().orc_stat_partfluid_particle(C.byref(po.make_setup(s)), C.c_double(a), C.c_double(1.0),
+                                         C.c_double(rhop), po.dptr(np.zeros(3)), po.dptr(np.zeros(3)),
+                                         po.dptr(np.array([1.0, 0, 0, 0])), po.dptr(np.array([U, 0, 0])),
+                                         po.dptr(np.zeros(3)), po.dptr(v))
+    d = 2 * a
+    assert abs(v[0] - U * d / s.visc) < 1e-12 * v[0]
+    assert v[24] == 0.0 and v[25] == 1.0 and v[26] == 0.0 and v[27] == 0.0
+    assert v[3] > 0 and v[4] == 0.0 and v[5] == 0.0                  # drag along the stream
+    assert v[6] == 0.0 or np.isnan(v[7])                           # no transverse lift (0/0 there)
+    assert abs(v[22] - (2.0 / 9.0) * rhop * a * a / (s.rhof * s.visc)) < 1e-12 * v[22]
+    assert v[35] == 1.0 and v[29] == 0.0
