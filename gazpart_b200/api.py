@@ -65,7 +65,7 @@ class Context:
         p.periodicity = int(bool(setup.periodicity))
         p.wall_boundary = int(bool(setup.wall_boundary))
         p.interp_scheme = 3
-        p.frozen_flow = 2
+        p.frozen_flow = int(getattr(setup, "frozen_flow", 2))
         p.precision = {"fp64": _lib.PREC_FP64, "mixed": _lib.PREC_MIXED}[precision]
         p.store_fluid = int(bool(store_fluid))
         p.max_particles = int(max_particles)

@@ -54,6 +54,7 @@ class Setup:
     muw: float = 0.0
     periodicity: bool = True
     wall_boundary: bool = False
+    frozen_flow: int = 2          # FROZEN_FLOW: 3 = channel (walls at x = 0, L; y and z wrap)
 
     @property
     def dx(self) -> float:

@@ -569,7 +569,14 @@ __global__ void __launch_bounds__(128, GP_INTEGRATE_MIN_BLOCKS) k_integrate(cons
       const InstDev& I = insts[inst];
       const int err = advance_particle<kMixed>(I, pc, uf, wv, X, U, O, Q);
       if (err) set_error(st, err, (long long)S->id[i], inst);
-      if (I.periodicity) {
+      // adv_particle_new.f90:685-686: the channel wraps y and z only
+      // (boundary_particle_yz.f90:44-70), the others every direction when periodic
+      if (I.frozen_flow == 3) {
+        if (X[1] > I.ly) X[1] = X[1] - I.ly;
+        else if (X[1] < 0.) X[1] = X[1] + I.ly;
+        if (X[2] > I.lz) X[2] = X[2] - I.lz;
+        else if (X[2] < 0.) X[2] = X[2] + I.lz;
+      } else if (I.periodicity) {
         if (X[0] > I.lx) X[0] = X[0] - I.lx;
         if (X[0] < 0.) X[0] = X[0] + I.lx;
         if (X[1] > I.ly) X[1] = X[1] - I.ly;

@@ -466,7 +466,7 @@ int gp_ctx_create(const gp_params *params, gp_ctx **out) {
   const gp_params &p = *params;
   if (p.nx < 4 || p.ny < 4 || p.nz < 4) return GP_EBADARG;
   if (p.interp_scheme != 3) return GP_EBADARG;
-  if (p.frozen_flow != 2) return GP_EBADARG;
+  if (p.frozen_flow < 1 || p.frozen_flow > 3) return GP_EBADARG;   // a frozen field; 3 = channel
   if (p.precision != GP_PREC_FP64 && p.precision != GP_PREC_MIXED) return GP_EBADARG;
   if (!(p.lx > 0 && p.ly > 0 && p.lz > 0 && p.dtime > 0 && p.visc > 0)) return GP_EBADARG;
   gp_ctx *c = new gp_ctx();
@@ -494,6 +494,7 @@ int gp_ctx_create(const gp_params *params, gp_ctx **out) {
   I.fprec = p.precision;
   I.periodicity = p.periodicity ? 1 : 0;
   I.wall_boundary = p.wall_boundary ? 1 : 0;
+  I.frozen_flow = p.frozen_flow;
   I.store_fluid = p.store_fluid ? 1 : 0;
   I.lx = p.lx; I.ly = p.ly; I.lz = p.lz;
   I.dx = p.lx / (double)(p.nx - 1);   // meshing.f90:43-45

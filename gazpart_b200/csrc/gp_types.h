@@ -19,7 +19,8 @@ struct InstDev {
   double dx, dy, dz, lx, ly, lz;
   double visc, dtime, gravity, ecp, mup, ecw, muw;
   // collision box grid (collision_initiation.f90:44-103)
-  int32_t nxbox, nybox, nzbox, pad0;
+  int32_t nxbox, nybox, nzbox;
+  int32_t frozen_flow;         // FROZEN_FLOW: 3 = channel (y and z wrap only)
   double dxbox, dybox, dzbox, xminbox, yminbox, zminbox;
   // search grid (cell edge >= 2 * largest bounding radius)
   int32_t nfx, nfy, nfz, pad1;

@@ -131,3 +131,60 @@ def reference_layout(interior: torch.Tensor, ghost: str) -> torch.Tensor:
     elif ghost != "zero":
         raise ValueError(f"ghost must be 'periodic' or 'zero', not {ghost!r}")
     return out
+
+
+# ---------------------------------------------------------------------------------
+# Channel profile (FROZEN_FLOW = 3)
+# ---------------------------------------------------------------------------------
+CHANNEL_POINTS = 21   # N of initiation_frozen_flow.f90:80
+
+
+def read_channel_profiles(ug_path: str, vorty_path: str):
+    """The two profile files INITIATION_FROZEN_FLOW reads (initiation_frozen_flow.f90:
+    82-93): 'Ug_mean.in', 21 records of (x, mean streamwise velocity), and
+    'vorticity_y.txt', 21 records of the y vorticity, each read list-directed."""
+    from .params import _ListReader
+    ru = _ListReader(open(ug_path).read())
+    rv = _ListReader(open(vorty_path).read())
+    x_in, ug_in, vorty_in = [], [], []
+    for _ in range(CHANNEL_POINTS):
+        x, u = ru.read("rr")
+        x_in.append(x)
+        ug_in.append(u)
+        vorty_in.append(rv.read("r")[0])
+    return x_in, ug_in, vorty_in
+
+
+def channel(setup, x_in, ug_in, vorty_in, frozen_interp) -> Dict[str, torch.Tensor]:
+    """The frozen channel field of initiation_frozen_flow.f90:77-155 on the mesh
+    XMESH(i) = (i-1) L/(N-1), interior arrays (NZ, NY, NX) = [z][y][x].
+
+    The 21 profile values fill 21^3 tables constant in y and z; FROZEN_INTERP_LAG3
+    samples them at the mesh diagonal (XMESH(i), YMESH(i), ZMESH(i)), i = 1..NX for the
+    velocity and 1..NY for the vorticity.  Then U = V = 0, W(i,:,:) = WINT(i),
+    VORTICITY_Y(:,j,:) = VORTY_INT(j) -- the vorticity profile lies along y, as the
+    reference assigns it -- and the other vorticity components are 0.  The diagonal
+    reads YMESH and ZMESH up to index NX and XMESH up to NY, so the reference needs
+    NY, NZ >= NX and NX >= NY; other meshes are refused.
+
+    frozen_interp(xain, yain, zain, uain, x, y, z) is FROZEN_INTERP_LAG3 with uain of
+    shape (NZA, NYA, NXA): the device's (Context.frozen_interp_lag3) or the checker's."""
+    import numpy as np
+    n = CHANNEL_POINTS
+    nx, ny, nz = setup.nx, setup.ny, setup.nz
+    if not (ny >= nx and nz >= nx and nx >= ny):
+        raise ValueError("the channel profile needs NY = NX <= NZ (the reference's mesh-diagonal sampling)")
+    x_in = np.asarray(x_in, dtype=np.float64)
+    y_in = setup.ly / float(n - 1) * np.arange(n, dtype=np.float64)    # dy_frozen*(I-1)
+    z_in = setup.lz / float(n - 1) * np.arange(n, dtype=np.float64)
+    wtmp = np.broadcast_to(np.asarray(ug_in, dtype=np.float64)[None, None, :], (n, n, n)).copy()
+    vtmp = np.broadcast_to(np.asarray(vorty_in, dtype=np.float64)[None, None, :], (n, n, n)).copy()
+    xmesh = setup.dx * np.arange(nx, dtype=np.float64)
+    ymesh = setup.dy * np.arange(ny, dtype=np.float64)
+    zmesh = setup.dz * np.arange(nz, dtype=np.float64)
+    wint = frozen_interp(x_in, y_in, z_in, wtmp, xmesh[:nx], ymesh[:nx], zmesh[:nx])
+    vorty_int = frozen_interp(x_in, y_in, z_in, vtmp, xmesh[:ny], ymesh[:ny], zmesh[:ny])
+    zero = torch.zeros((nz, ny, nx), dtype=torch.float64)
+    w = torch.from_numpy(np.ascontiguousarray(np.broadcast_to(wint[None, None, :], (nz, ny, nx))))
+    vy = torch.from_numpy(np.ascontiguousarray(np.broadcast_to(vorty_int[None, :, None], (nz, ny, nx))))
+    return {"u": zero.clone(), "v": zero.clone(), "w": w, "vortx": zero.clone(), "vorty": vy, "vortz": zero.clone()}

@@ -186,16 +186,20 @@ class Params:
         """The mesh and physics of class ig as this package's Setup.
 
         Only the paths this package implements are accepted: Lagrange cubic
-        interpolation (INTERP_SCHEME = 3) and inertial particles (PARTDEF = 2)."""
+        interpolation (INTERP_SCHEME = 3), inertial particles (PARTDEF = 2) and a frozen
+        field (FROZEN_FLOW = 1, 2 or 3, the last the channel)."""
         if self.interp_scheme != 3:
             raise ValueError(f"INTERP_SCHEME = {self.interp_scheme}: only 3 (interp_lag3.f90) is implemented")
         c = self.classes[ig - 1]
         if c.partdef != 2:
             raise ValueError(f"class {ig}: PARTDEF = {c.partdef}: only inertial particles (2) are advanced")
+        if self.frozen_flow not in (1, 2, 3):
+            raise ValueError(f"FROZEN_FLOW = {self.frozen_flow}: only a frozen field (1, 2, 3) is advanced")
         return config.Setup(nx=self.nx, ny=self.ny, nz=self.nz, lx=self.lxmax, ly=self.lymax, lz=self.lzmax,
                             visc=self.visc, rhof=self.rhof, dtime=self.dtime_user, gravity=c.gravity,
                             ecp=c.ecp, mup=c.mup, ecw=self.ecw, muw=self.muw,
-                            periodicity=self.periodicity, wall_boundary=self.wall_boundary)
+                            periodicity=self.periodicity, wall_boundary=self.wall_boundary,
+                            frozen_flow=self.frozen_flow)
 
     def tables(self, ig: int = 1):
         """Class ig's polydisperse tables as a fresh run builds them before any particle

@@ -93,7 +93,8 @@ typedef struct {
     int32_t periodicity;         /* PERIODICITY */
     int32_t wall_boundary;       /* WALL_BOUNDARY (stencil x mirror) */
     int32_t interp_scheme;       /* INTERP_SCHEME, must be 3 */
-    int32_t frozen_flow;         /* FROZEN_FLOW: 2 = interpolate a frozen field */
+    int32_t frozen_flow;         /* FROZEN_FLOW: 1-3 = a frozen field; 3 = channel: after the
+                                    advance only y and z wrap (adv_particle_new.f90:685-686) */
     int32_t precision;           /* GP_PREC_FP64 or GP_PREC_MIXED */
     int32_t store_fluid;         /* 1: write the interpolated field at each particle
                                     (PART%UFAP..VORTZAP) every step */

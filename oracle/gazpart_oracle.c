@@ -825,8 +825,18 @@ int orc_adv_particle_ellp(const orc_setup *s, const orc_props *p,
         st->ox[i] = P.ox; st->oy[i] = P.oy; st->oz[i] = P.oz;
         st->qa[i] = P.q[0]; st->qb[i] = P.q[1]; st->qc[i] = P.q[2]; st->qd[i] = P.q[3];
     }
-    /* 3. BOUNDARY_PARTICLE (boundary_particle.f90:45-62), periodic wrap */
-    if (s->periodicity) {
+    /* 3. particle boundary conditions (adv_particle_new.f90:685-686): the channel
+     * (FROZEN_FLOW = 3) wraps y and z only, BOUNDARY_PARTICLE_Y_Z
+     * (boundary_particle_yz.f90:44-70); below it, a periodic box wraps every direction,
+     * BOUNDARY_PARTICLE (boundary_particle.f90:45-62) */
+    if (s->frozen_flow == 3) {
+        for (int64_t i = 0; i < n; ++i) {
+            if (st->y[i] > s->ly) st->y[i] = st->y[i] - s->ly;
+            else if (st->y[i] < 0.) st->y[i] = st->y[i] + s->ly;
+            if (st->z[i] > s->lz) st->z[i] = st->z[i] - s->lz;
+            else if (st->z[i] < 0.) st->z[i] = st->z[i] + s->lz;
+        }
+    } else if (s->periodicity) {
         for (int64_t i = 0; i < n; ++i) {
             if (st->x[i] > s->lx) st->x[i] = st->x[i] - s->lx;
             if (st->x[i] < 0.) st->x[i] = st->x[i] + s->lx;

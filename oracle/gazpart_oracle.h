@@ -43,6 +43,7 @@ typedef struct {
     double ecw, muw;             /* ECW, MUW: particle-wall */
     int32_t periodicity;         /* PERIODICITY (x wrap of positions/boxes) */
     int32_t wall_boundary;       /* WALL_BOUNDARY (x wrap of the stencil) */
+    int32_t frozen_flow;         /* FROZEN_FLOW (3: channel, y and z wrap only) */
 } orc_setup;
 
 /* Per-particle shape/density (reference: per class; see header comment). */

@@ -31,7 +31,7 @@ class OrcSetup(C.Structure):
                 ("visc", C.c_double), ("rhof", C.c_double), ("ppi", C.c_double),
                 ("dtime", C.c_double), ("gravity", C.c_double),
                 ("ecp", C.c_double), ("mup", C.c_double), ("ecw", C.c_double), ("muw", C.c_double),
-                ("periodicity", C.c_int32), ("wall_boundary", C.c_int32)]
+                ("periodicity", C.c_int32), ("wall_boundary", C.c_int32), ("frozen_flow", C.c_int32)]
 
 
 class OrcProps(C.Structure):
@@ -86,7 +86,7 @@ def make_setup(s) -> OrcSetup:
     """OrcSetup from a gazpart_b200.config.Setup (or any object with the same fields)."""
     return OrcSetup(s.nx, s.ny, s.nz, s.lx, s.ly, s.lz, s.dx, s.dy, s.dz, s.visc, s.rhof,
                     4.0 * np.arctan(1.0), s.dtime, s.gravity, s.ecp, s.mup, s.ecw, s.muw,
-                    int(bool(s.periodicity)), int(bool(s.wall_boundary)))
+                    int(bool(s.periodicity)), int(bool(s.wall_boundary)), int(getattr(s, "frozen_flow", 2)))
 
 
 class Ensemble:
