@@ -45,6 +45,7 @@ def parse():
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch grids")
     ap.add_argument("--no-io", action="store_true", help="skip the restart-file measurement")
     ap.add_argument("--no-stats", action="store_true", help="skip the statistics measurement")
+    ap.add_argument("--no-dns", action="store_true", help="skip the live-fluid measurement")
     ap.add_argument("--grids", default=None,
                     help="gather,integrate,bin,search,overlap: fixed launch grids instead of autotuning")
     ap.add_argument("--serve-seconds", type=float, default=2.0, help="arrival window of the serving workload")
@@ -305,6 +306,32 @@ def time_stats(ctx) -> dict:
     return out
 
 
+def time_live_fluid(ctx, setup, f) -> dict:
+    """The live-fluid step (ADV_FLUID, gp_adv_fluid) on the workload's own mesh, started
+    from its field, and the refresh of the context's field from it (gp_dns_couple):
+    median of three synchronised calls each, after one untimed step."""
+    import statistics as stt
+    from gazpart_b200 import dns
+    out = {"mesh": f"{setup.nx}x{setup.ny}x{setup.nz}", "ffts_per_step": 21}
+    with dns.Fluid(setup) as fl:
+        fl.set_velocity(f["u"], f["v"], f["w"])
+        fl.adv_fluid(0)
+        t = []
+        for k in range(3):
+            t0 = time.perf_counter()
+            fl.adv_fluid(k + 1)
+            t.append(time.perf_counter() - t0)
+        c = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            fl.couple(ctx)
+            c.append(time.perf_counter() - t0)
+    points = setup.nx * setup.ny * setup.nz
+    out.update({"adv_fluid_ms": 1e3 * stt.median(t), "couple_ms": 1e3 * stt.median(c),
+                "mesh_points_per_s": points / stt.median(t)})
+    return out
+
+
 def run_serving(args, rank: int, world: int, local: int):
     """Jobs arriving at 20/s for --serve-seconds, each on one of eight resident fields,
     admitted against the HBM budget and stepped together until all are done."""
@@ -533,6 +560,9 @@ def main():
     if not batched and not args.no_stats:
         stats = time_stats(ctx)
         ctx.raise_status("statistics")
+    live_fluid = None
+    if rank == 0 and not batched and not args.no_dns:
+        live_fluid = time_live_fluid(ctx, setup, f)
 
     plain = None
     if not args.no_plain and precision == "mixed":
@@ -577,7 +607,8 @@ def main():
                 "kernels_per_step": kps, "phase_ms": phases,
                 "phase_note": "gather of step s+1 overlaps the contact solves of step s (two streams in the graph)",
                 "phase_ms_one_step_graphs": phases_alone,
-                "clocks": clocks, "fp64_plain": plain, "restart_io": restart_io, "stats": stats}
+                "clocks": clocks, "fp64_plain": plain, "restart_io": restart_io, "stats": stats,
+                "live_fluid": live_fluid}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

@@ -379,6 +379,31 @@ int gp_collision_response(gp_ctx *ctx, int32_t ig, int32_t idp, double part1[10]
                           double part2[10], const double r_impact1[3],
                           const double r_impact2[3], const double normal[3]);
 
+/* ------------------------------------------------------------ live fluid ---- */
+/* The periodic pseudo-spectral solver of the reference's DNS mode (SOLVE_FLUID = 1),
+ * on the device with cuFFT.  A solver holds the velocity on the NX x NY x NZ mesh of
+ * *params (interior arrays [z][y][x], x fastest; NX, NY, NZ even), the wavenumbers of
+ * meshing.f90:96-140 (KFIRST = 2 pi / LX for every direction) and the aliasing filter of
+ * meshing.f90:144-180: aliascontrol 0 none, 1 sharp, 2 smooth with RTRUNC = rtrunc (the
+ * reference uses 2 and 8/9).  No stochastic forcing (STEADY = .false.). */
+typedef struct gp_dns gp_dns;
+int gp_dns_create(const gp_params *params, int32_t aliascontrol, double rtrunc, gp_dns **out);
+int gp_dns_destroy(gp_dns *dns);
+int gp_dns_set_velocity(gp_dns *dns, const double *u, const double *v, const double *w, int32_t on_device);
+int gp_dns_get_velocity(gp_dns *dns, double *u, double *v, double *w, int32_t on_device);
+/* ADV_FLUID(NCYCLE) (adv_fluid.f90:1-271): one step of the two-stage scheme with the
+ * viscous integrating factor, the rotational nonlinear term projected onto the
+ * divergence-free plane (nonlinear_terms.f90), PROJ_DIVFREE and the filter. */
+int gp_adv_fluid(gp_dns *dns, int32_t ncycle);
+/* Vorticity of the current velocity, spectrally (i k x u, as nonlinear_terms.f90:81-99
+ * forms it). */
+int gp_dns_vorticity(gp_dns *dns, double *ox, double *oy, double *oz, int32_t on_device);
+/* The velocity into field slot `field` of a context, with periodic y and z ghosts as
+ * FLUIDCOMM leaves them (main.f90:499-505), so that the next particle step interpolates
+ * the live field.  with_vorticity != 0 also writes the spectral vorticity (zero ghosts);
+ * the reference leaves its vorticity arrays as initialised in DNS mode. */
+int gp_dns_couple(gp_dns *dns, gp_ctx *ctx, int32_t field, int32_t with_vorticity);
+
 #ifdef __cplusplus
 }
 #endif
