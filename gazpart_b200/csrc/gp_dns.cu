@@ -9,8 +9,9 @@
 //   5. û = û_{n+1}^* + dt/2 RHS2; PROJ_DIVFREE; û *= FILTER        (:145-170, proj_divfree.f90)
 //   6. u = IFFT(û)                                                (:178-187)
 // The transforms are cuFFT's (D2Z forward, Z2D backward, both unnormalised as P3DFFT's
-// are); every step between them is one element-wise kernel per stage, in FP64 and
-// without FMA contraction, in the reference's evaluation order.  Wavenumbers follow
+// are), the three components of a vector field in one batched call; every step between
+// them is one element-wise kernel per stage, in FP64 and without FMA contraction, in the
+// reference's evaluation order.  A step makes 7 batched calls (21 transforms).  Wavenumbers follow
 // meshing.f90:96-140 (KX = (I-1) KFIRST on the half-spectrum, KY and KZ signed), and the
 // aliasing filter meshing.f90:144-180 (sharp or smooth, RTRUNC), computed per mode.
 // The stochastic forcing of STEADY runs (ADV_FORCING, ADD_FORCING3) is not part of it.
@@ -27,11 +28,14 @@ struct gp_dns {
   double kfirst = 0, klast = 0, visc = 0, dtime = 0, factor = 0, rtrunc = 0;
   int aliascontrol = 0;
   cudaStream_t stream = nullptr;
-  cufftHandle fwd = 0, bwd = 0;
+  cufftHandle fwd = 0, bwd = 0;   // three transforms per call
   bool plans = false;
-  double *u[3] = {};           // physical velocity, [z][y][x]
-  double *t[3] = {};           // physical vorticity, then u x ω
-  cufftDoubleComplex *uh[3] = {}, *unp1[3] = {}, *w[3] = {}, *tmp = nullptr;
+  // each a block of three components back to back: physical [3][z][y][x], spectral
+  // [3][z][y][x/2+1]
+  double *u = nullptr;            // velocity
+  double *t = nullptr;            // vorticity, then u x ω
+  cufftDoubleComplex *uh = nullptr, *unp1 = nullptr, *w = nullptr, *tmp = nullptr;
+  size_t np = 0, nh = 0;          // points of one component
 };
 
 namespace gp {
@@ -65,10 +69,10 @@ __device__ __forceinline__ cufftDoubleComplex cmul_i_real(cufftDoubleComplex a, 
 
 // VORTX..Z = i k x û (nonlinear_terms.f90:81-92); the outputs are copies the backward
 // transform may overwrite.
-__global__ void k_vorticity_hat(Spec s, const cufftDoubleComplex *__restrict__ uh,
-                                const cufftDoubleComplex *__restrict__ vh, const cufftDoubleComplex *__restrict__ wh,
-                                cufftDoubleComplex *ox, cufftDoubleComplex *oy, cufftDoubleComplex *oz) {
+__global__ void k_vorticity_hat(Spec s, const cufftDoubleComplex *__restrict__ in, cufftDoubleComplex *out) {
   const int64_t n = (int64_t)s.nxh * s.ny * s.nz;
+  const cufftDoubleComplex *uh = in, *vh = in + n, *wh = in + 2 * n;
+  cufftDoubleComplex *ox = out, *oy = out + n, *oz = out + 2 * n;
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
     double kx, ky, kz;
     wavenumbers(s, e, kx, ky, kz);
@@ -83,8 +87,9 @@ __global__ void k_vorticity_hat(Spec s, const cufftDoubleComplex *__restrict__ u
 }
 
 // TX..TZ = u x ζ in physical space (nonlinear_terms.f90:105-113), in place over ζ.
-__global__ void k_cross(int64_t n, const double *__restrict__ u, const double *__restrict__ v,
-                        const double *__restrict__ w, double *zx, double *zy, double *zz) {
+__global__ void k_cross(int64_t n, const double *__restrict__ vel, double *z) {
+  const double *u = vel, *v = vel + n, *w = vel + 2 * n;
+  double *zx = z, *zy = z + n, *zz = z + 2 * n;
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
     const double a = zx[e], b = zy[e], c = zz[e];
     zx[e] = v[e] * c - w[e] * b;
@@ -120,11 +125,12 @@ __device__ __forceinline__ void rhs_of(double kx, double ky, double kz, double f
 }
 
 // adv_fluid.f90:95-110: the first stage with the integrating factor.
-__global__ void k_stage1(Spec s, double factor, double visc, double dtime, cufftDoubleComplex *uh,
-                         cufftDoubleComplex *vh, cufftDoubleComplex *wh, cufftDoubleComplex *unp1,
-                         cufftDoubleComplex *vnp1, cufftDoubleComplex *wnp1, const cufftDoubleComplex *__restrict__ tx,
-                         const cufftDoubleComplex *__restrict__ ty, const cufftDoubleComplex *__restrict__ tz) {
+__global__ void k_stage1(Spec s, double factor, double visc, double dtime, cufftDoubleComplex *hat,
+                         cufftDoubleComplex *np1, const cufftDoubleComplex *__restrict__ t3) {
   const int64_t n = (int64_t)s.nxh * s.ny * s.nz;
+  cufftDoubleComplex *uh = hat, *vh = hat + n, *wh = hat + 2 * n;
+  cufftDoubleComplex *unp1 = np1, *vnp1 = np1 + n, *wnp1 = np1 + 2 * n;
+  const cufftDoubleComplex *tx = t3, *ty = t3 + n, *tz = t3 + 2 * n;
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
     double kx, ky, kz;
     wavenumbers(s, e, kx, ky, kz);
@@ -146,11 +152,12 @@ __global__ void k_stage1(Spec s, double factor, double visc, double dtime, cufft
 // adv_fluid.f90:145-170 with PROJ_DIVFREE (proj_divfree.f90:28-44) and the aliasing
 // filter (meshing.f90:144-180) applied per mode.
 __global__ void k_stage2(Spec s, double factor, double dtime, double klast, int aliascontrol, double rtrunc,
-                         double ppi, cufftDoubleComplex *uh, cufftDoubleComplex *vh, cufftDoubleComplex *wh,
-                         const cufftDoubleComplex *__restrict__ unp1, const cufftDoubleComplex *__restrict__ vnp1,
-                         const cufftDoubleComplex *__restrict__ wnp1, const cufftDoubleComplex *__restrict__ tx,
-                         const cufftDoubleComplex *__restrict__ ty, const cufftDoubleComplex *__restrict__ tz) {
+                         double ppi, cufftDoubleComplex *hat, const cufftDoubleComplex *__restrict__ np1,
+                         const cufftDoubleComplex *__restrict__ t3) {
   const int64_t n = (int64_t)s.nxh * s.ny * s.nz;
+  cufftDoubleComplex *uh = hat, *vh = hat + n, *wh = hat + 2 * n;
+  const cufftDoubleComplex *unp1 = np1, *vnp1 = np1 + n, *wnp1 = np1 + 2 * n;
+  const cufftDoubleComplex *tx = t3, *ty = t3 + n, *tz = t3 + 2 * n;
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
     double kx, ky, kz;
     wavenumbers(s, e, kx, ky, kz);
@@ -192,24 +199,13 @@ __global__ void k_scale_spec(int64_t n, double factor, cufftDoubleComplex *a) {
 
 int grid_of(int64_t n) { return (int)std::min<int64_t>((n + 255) / 256, 148 * 16); }
 
-// Backward transform of a spectrum that must survive: copy, then Z2D (which overwrites
-// its input), as adv_fluid.f90 copies into TMPFOU first.
-int backward(gp_dns *d, const cufftDoubleComplex *src, double *dst) {
-  const size_t bytes = (size_t)d->nxh * d->ny * d->nz * sizeof(cufftDoubleComplex);
-  if (cudaMemcpyAsync(d->tmp, src, bytes, cudaMemcpyDeviceToDevice, d->stream) != cudaSuccess) return GP_ECUDA;
-  if (cufftExecZ2D(d->bwd, d->tmp, dst) != CUFFT_SUCCESS) return GP_ECUDA;
-  return GP_OK;
-}
-
 // NONLINEAR_TERMS: leaves FFT(u x ζ) (unscaled) in d->w.
 int nonlinear(gp_dns *d, const Spec &s) {
-  const int64_t nh = (int64_t)s.nxh * s.ny * s.nz, np = (int64_t)d->nx * d->ny * d->nz;
-  k_vorticity_hat<<<grid_of(nh), 256, 0, d->stream>>>(s, d->uh[0], d->uh[1], d->uh[2], d->w[0], d->w[1], d->w[2]);
-  for (int c = 0; c < 3; ++c)
-    if (cufftExecZ2D(d->bwd, d->w[c], d->t[c]) != CUFFT_SUCCESS) return GP_ECUDA;
-  k_cross<<<grid_of(np), 256, 0, d->stream>>>(np, d->u[0], d->u[1], d->u[2], d->t[0], d->t[1], d->t[2]);
-  for (int c = 0; c < 3; ++c)
-    if (cufftExecD2Z(d->fwd, d->t[c], d->w[c]) != CUFFT_SUCCESS) return GP_ECUDA;
+  const int64_t nh = (int64_t)d->nh, np = (int64_t)d->np;
+  k_vorticity_hat<<<grid_of(nh), 256, 0, d->stream>>>(s, d->uh, d->w);
+  if (cufftExecZ2D(d->bwd, d->w, d->t) != CUFFT_SUCCESS) return GP_ECUDA;
+  k_cross<<<grid_of(np), 256, 0, d->stream>>>(np, d->u, d->t);
+  if (cufftExecD2Z(d->fwd, d->t, d->w) != CUFFT_SUCCESS) return GP_ECUDA;
   return cudaGetLastError() == cudaSuccess ? GP_OK : GP_ECUDA;
 }
 
@@ -240,29 +236,33 @@ int gp_dns_create(const gp_params *p, int32_t aliascontrol, double rtrunc, gp_dn
   d->factor = 1.0 / (double)((int64_t)p->nx * p->ny * p->nz);   // FACTOR = 1/NGLOB (main.f90:213)
   d->aliascontrol = aliascontrol;
   d->rtrunc = rtrunc;
-  const size_t nh = (size_t)d->nxh * d->ny * d->nz, np = (size_t)d->nx * d->ny * d->nz;
+  d->nh = (size_t)d->nxh * d->ny * d->nz;
+  d->np = (size_t)d->nx * d->ny * d->nz;
   int rc = cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking) == cudaSuccess ? GP_OK : GP_ECUDA;
-  for (int c = 0; c < 3 && !rc; ++c) {
-    rc = alloc(&d->u[c], np);
-    if (!rc) rc = alloc(&d->t[c], np);
-    if (!rc) rc = alloc(&d->uh[c], nh);
-    if (!rc) rc = alloc(&d->unp1[c], nh);
-    if (!rc) rc = alloc(&d->w[c], nh);
-  }
-  if (!rc) rc = alloc(&d->tmp, nh);
+  if (!rc) rc = alloc(&d->u, 3 * d->np);
+  if (!rc) rc = alloc(&d->t, 3 * d->np);
+  if (!rc) rc = alloc(&d->uh, 3 * d->nh);
+  if (!rc) rc = alloc(&d->unp1, 3 * d->nh);
+  if (!rc) rc = alloc(&d->w, 3 * d->nh);
+  if (!rc) rc = alloc(&d->tmp, 3 * d->nh);
   if (!rc) {
-    if (cufftPlan3d(&d->fwd, d->nz, d->ny, d->nx, CUFFT_D2Z) != CUFFT_SUCCESS ||
-        cufftPlan3d(&d->bwd, d->nz, d->ny, d->nx, CUFFT_Z2D) != CUFFT_SUCCESS ||
-        cufftSetStream(d->fwd, d->stream) != CUFFT_SUCCESS || cufftSetStream(d->bwd, d->stream) != CUFFT_SUCCESS)
+    long long dims[3] = {d->nz, d->ny, d->nx};
+    size_t ws = 0;
+    // three components back to back: the basic layout with batch 3 (64-bit sizes)
+    if (cufftCreate(&d->fwd) != CUFFT_SUCCESS || cufftCreate(&d->bwd) != CUFFT_SUCCESS) {
       rc = GP_ECUDA;
-    else
+    } else {
       d->plans = true;
+      if (cufftMakePlanMany64(d->fwd, 3, dims, nullptr, 1, (long long)d->np, nullptr, 1, (long long)d->nh, CUFFT_D2Z,
+                              3, &ws) != CUFFT_SUCCESS ||
+          cufftMakePlanMany64(d->bwd, 3, dims, nullptr, 1, (long long)d->nh, nullptr, 1, (long long)d->np, CUFFT_Z2D,
+                              3, &ws) != CUFFT_SUCCESS ||
+          cufftSetStream(d->fwd, d->stream) != CUFFT_SUCCESS || cufftSetStream(d->bwd, d->stream) != CUFFT_SUCCESS)
+        rc = GP_ECUDA;
+    }
   }
-  if (!rc) {
-    for (int c = 0; c < 3; ++c)
-      if (cudaMemsetAsync(d->u[c], 0, np * sizeof(double), d->stream) != cudaSuccess) rc = GP_ECUDA;
-    if (!rc && cudaStreamSynchronize(d->stream) != cudaSuccess) rc = GP_ECUDA;
-  }
+  if (!rc && cudaMemsetAsync(d->u, 0, 3 * d->np * sizeof(double), d->stream) != cudaSuccess) rc = GP_ECUDA;
+  if (!rc && cudaStreamSynchronize(d->stream) != cudaSuccess) rc = GP_ECUDA;
   if (rc) {
     gp_dns_destroy(d);
     return rc;
@@ -278,10 +278,7 @@ int gp_dns_destroy(gp_dns *d) {
     cufftDestroy(d->fwd);
     cufftDestroy(d->bwd);
   }
-  for (int c = 0; c < 3; ++c) {
-    cudaFree(d->u[c]); cudaFree(d->t[c]); cudaFree(d->uh[c]); cudaFree(d->unp1[c]); cudaFree(d->w[c]);
-  }
-  cudaFree(d->tmp);
+  cudaFree(d->u); cudaFree(d->t); cudaFree(d->uh); cudaFree(d->unp1); cudaFree(d->w); cudaFree(d->tmp);
   if (d->stream) cudaStreamDestroy(d->stream);
   delete d;
   return GP_OK;
@@ -289,21 +286,21 @@ int gp_dns_destroy(gp_dns *d) {
 
 int gp_dns_set_velocity(gp_dns *d, const double *u, const double *v, const double *w, int32_t on_device) {
   if (!d || !u || !v || !w) return GP_EBADARG;
-  const size_t bytes = (size_t)d->nx * d->ny * d->nz * sizeof(double);
   const double *src[3] = {u, v, w};
   const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
   for (int c = 0; c < 3; ++c)
-    if (cudaMemcpyAsync(d->u[c], src[c], bytes, kind, d->stream) != cudaSuccess) return GP_ECUDA;
+    if (cudaMemcpyAsync(d->u + c * d->np, src[c], d->np * sizeof(double), kind, d->stream) != cudaSuccess)
+      return GP_ECUDA;
   return cudaStreamSynchronize(d->stream) == cudaSuccess ? GP_OK : GP_ECUDA;
 }
 
 int gp_dns_get_velocity(gp_dns *d, double *u, double *v, double *w, int32_t on_device) {
   if (!d || !u || !v || !w) return GP_EBADARG;
-  const size_t bytes = (size_t)d->nx * d->ny * d->nz * sizeof(double);
   double *dst[3] = {u, v, w};
   const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
   for (int c = 0; c < 3; ++c)
-    if (cudaMemcpyAsync(dst[c], d->u[c], bytes, kind, d->stream) != cudaSuccess) return GP_ECUDA;
+    if (cudaMemcpyAsync(dst[c], d->u + c * d->np, d->np * sizeof(double), kind, d->stream) != cudaSuccess)
+      return GP_ECUDA;
   return cudaStreamSynchronize(d->stream) == cudaSuccess ? GP_OK : GP_ECUDA;
 }
 
@@ -311,56 +308,53 @@ int gp_adv_fluid(gp_dns *d, int32_t /*ncycle*/) {
   using namespace gp;
   if (!d) return GP_EBADARG;
   const Spec s = {d->nxh, d->ny, d->nz, d->kfirst};
-  const int64_t nh = (int64_t)d->nxh * d->ny * d->nz;
-  const int g = grid_of(nh);
-  // 1. û = FFT(u) * FACTOR
-  for (int c = 0; c < 3; ++c) {
-    if (cudaMemcpyAsync(d->t[c], d->u[c], (size_t)d->nx * d->ny * d->nz * sizeof(double), cudaMemcpyDeviceToDevice,
-                        d->stream) != cudaSuccess)
-      return GP_ECUDA;
-    if (cufftExecD2Z(d->fwd, d->t[c], d->uh[c]) != CUFFT_SUCCESS) return GP_ECUDA;
-    k_scale_spec<<<g, 256, 0, d->stream>>>(nh, d->factor, d->uh[c]);
-  }
+  const int64_t n3 = 3 * (int64_t)d->nh;
+  const int g = grid_of((int64_t)d->nh);
+  // 1. û = FFT(u) * FACTOR (the forward transform leaves u as it is)
+  if (cufftExecD2Z(d->fwd, d->u, d->uh) != CUFFT_SUCCESS) return GP_ECUDA;
+  k_scale_spec<<<grid_of(n3), 256, 0, d->stream>>>(n3, d->factor, d->uh);
   // 2-3. first stage
   int rc = nonlinear(d, s);
   if (rc) return rc;
-  k_stage1<<<g, 256, 0, d->stream>>>(s, d->factor, d->visc, d->dtime, d->uh[0], d->uh[1], d->uh[2], d->unp1[0],
-                                     d->unp1[1], d->unp1[2], d->w[0], d->w[1], d->w[2]);
-  // 4. the predictor in physical space, then the second nonlinear term
-  for (int c = 0; c < 3; ++c) GP_DTRY(backward(d, d->uh[c], d->u[c]));
+  k_stage1<<<g, 256, 0, d->stream>>>(s, d->factor, d->visc, d->dtime, d->uh, d->unp1, d->w);
+  // 4. the predictor in physical space (from a copy: the backward transform overwrites
+  //    its input, and û is still needed), then the second nonlinear term
+  if (cudaMemcpyAsync(d->tmp, d->uh, n3 * sizeof(cufftDoubleComplex), cudaMemcpyDeviceToDevice, d->stream) !=
+      cudaSuccess)
+    return GP_ECUDA;
+  if (cufftExecZ2D(d->bwd, d->tmp, d->u) != CUFFT_SUCCESS) return GP_ECUDA;
   rc = nonlinear(d, s);
   if (rc) return rc;
   // 5. corrector, projection, filter
   k_stage2<<<g, 256, 0, d->stream>>>(s, d->factor, d->dtime, d->klast, d->aliascontrol, d->rtrunc,
-                                     4.0 * std::atan(1.0), d->uh[0], d->uh[1], d->uh[2], d->unp1[0], d->unp1[1],
-                                     d->unp1[2], d->w[0], d->w[1], d->w[2]);
-  // 6. back to physical space
-  for (int c = 0; c < 3; ++c) GP_DTRY(backward(d, d->uh[c], d->u[c]));
+                                     4.0 * std::atan(1.0), d->uh, d->unp1, d->w);
+  // 6. back to physical space (û is not needed after this)
+  if (cufftExecZ2D(d->bwd, d->uh, d->u) != CUFFT_SUCCESS) return GP_ECUDA;
   if (cudaGetLastError() != cudaSuccess) return GP_ECUDA;
   return cudaStreamSynchronize(d->stream) == cudaSuccess ? GP_OK : GP_ECUDA;
 }
 
-int gp_dns_vorticity(gp_dns *d, double *ox, double *oy, double *oz, int32_t on_device) {
+// Spectral vorticity of the current velocity into d->t (three components).
+static int vorticity_to_t(gp_dns *d) {
   using namespace gp;
-  if (!d || !ox || !oy || !oz) return GP_EBADARG;
   const Spec s = {d->nxh, d->ny, d->nz, d->kfirst};
-  const int64_t nh = (int64_t)d->nxh * d->ny * d->nz;
-  const size_t bytes = (size_t)d->nx * d->ny * d->nz * sizeof(double);
-  for (int c = 0; c < 3; ++c) {
-    if (cudaMemcpyAsync(d->t[c], d->u[c], bytes, cudaMemcpyDeviceToDevice, d->stream) != cudaSuccess) return GP_ECUDA;
-    if (cufftExecD2Z(d->fwd, d->t[c], d->w[c]) != CUFFT_SUCCESS) return GP_ECUDA;
-    k_scale_spec<<<grid_of(nh), 256, 0, d->stream>>>(nh, d->factor, d->w[c]);
-  }
-  k_vorticity_hat<<<grid_of(nh), 256, 0, d->stream>>>(s, d->w[0], d->w[1], d->w[2], d->unp1[0], d->unp1[1],
-                                                      d->unp1[2]);
+  const int64_t n3 = 3 * (int64_t)d->nh;
+  if (cufftExecD2Z(d->fwd, d->u, d->w) != CUFFT_SUCCESS) return GP_ECUDA;
+  k_scale_spec<<<grid_of(n3), 256, 0, d->stream>>>(n3, d->factor, d->w);
+  k_vorticity_hat<<<grid_of((int64_t)d->nh), 256, 0, d->stream>>>(s, d->w, d->unp1);
+  if (cufftExecZ2D(d->bwd, d->unp1, d->t) != CUFFT_SUCCESS) return GP_ECUDA;
+  return cudaGetLastError() == cudaSuccess ? GP_OK : GP_ECUDA;
+}
+
+int gp_dns_vorticity(gp_dns *d, double *ox, double *oy, double *oz, int32_t on_device) {
+  if (!d || !ox || !oy || !oz) return GP_EBADARG;
+  const int rc = vorticity_to_t(d);
+  if (rc) return rc;
   double *dst[3] = {ox, oy, oz};
-  for (int c = 0; c < 3; ++c) {
-    double *o = on_device ? dst[c] : d->t[c];
-    if (cufftExecZ2D(d->bwd, d->unp1[c], o) != CUFFT_SUCCESS) return GP_ECUDA;
-    if (!on_device && cudaMemcpyAsync(dst[c], o, bytes, cudaMemcpyDeviceToHost, d->stream) != cudaSuccess)
+  const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  for (int c = 0; c < 3; ++c)
+    if (cudaMemcpyAsync(dst[c], d->t + c * d->np, d->np * sizeof(double), kind, d->stream) != cudaSuccess)
       return GP_ECUDA;
-  }
-  if (cudaGetLastError() != cudaSuccess) return GP_ECUDA;
   return cudaStreamSynchronize(d->stream) == cudaSuccess ? GP_OK : GP_ECUDA;
 }
 
@@ -369,14 +363,15 @@ int gp_dns_couple(gp_dns *d, gp_ctx *ctx, int32_t field, int32_t with_vorticity)
   if (cudaStreamSynchronize(d->stream) != cudaSuccess) return GP_ECUDA;
   // FLUIDCOMM (main.f90:499-505): the velocity's y and z ghosts are periodic copies
   for (int c = 0; c < 3; ++c) {
-    const int rc = gp_set_field_slot(ctx, field, c, d->u[c], GP_LAYOUT_INTERIOR, GP_GHOST_PERIODIC, 1);
+    const int rc = gp_set_field_slot(ctx, field, c, d->u + c * d->np, GP_LAYOUT_INTERIOR, GP_GHOST_PERIODIC, 1);
     if (rc) return rc;
   }
   if (with_vorticity) {
     // vorticity of the current field, with zero ghosts as the reference's arrays have
-    double *o[3] = {d->t[0], d->t[1], d->t[2]};
-    int rc = gp_dns_vorticity(d, o[0], o[1], o[2], 1);
-    for (int c = 0; c < 3 && !rc; ++c) rc = gp_set_field_slot(ctx, field, 3 + c, o[c], GP_LAYOUT_INTERIOR, GP_GHOST_ZERO, 1);
+    int rc = vorticity_to_t(d);
+    if (!rc && cudaStreamSynchronize(d->stream) != cudaSuccess) rc = GP_ECUDA;
+    for (int c = 0; c < 3 && !rc; ++c)
+      rc = gp_set_field_slot(ctx, field, 3 + c, d->t + c * d->np, GP_LAYOUT_INTERIOR, GP_GHOST_ZERO, 1);
     if (rc) return rc;
   }
   return GP_OK;

@@ -197,6 +197,12 @@ __global__ void __launch_bounds__(128, GP_CONTACT_MIN_BLOCKS) k_contact(const In
     double ept1[3], ept2[3], cn[3];
     if (!contact_finish(a1, b1, a2, b2, q1, q2, CP, S.x, ept1, ept2, cn)) continue;
     atomicAdd(&st->n_contact, 1ull);
+    // overlap depth |EPT1 - EPT2| for the collision statistics, while the points are at hand
+    double depth = 0.0;
+    if (cst != nullptr) {
+      const double v0 = ept1[0] - ept2[0], v1 = ept1[1] - ept2[1], v2 = ept1[2] - ept2[2];
+      depth = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
+    }
     const PairRec pr = pairs[e];
     const int i1 = pr.home, i2 = pr.near;
     const double x1 = CP.b1[0], y1 = CP.b1[1], z1 = CP.b1[2];
@@ -219,8 +225,7 @@ __global__ void __launch_bounds__(128, GP_CONTACT_MIN_BLOCKS) k_contact(const In
       if ((int64_t)k < cap_cst) {
         ContactStatRec c;
         c.home = i1; c.near = i2; c.inst = P.inst[i1]; c.pad = 0; c.k1 = pr.k1; c.k2 = pr.k2;
-        const double v0 = ept1[0] - ept2[0], v1 = ept1[1] - ept2[1], v2 = ept1[2] - ept2[2];
-        c.depth = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
+        c.depth = depth;
         c.nvrel = nvrel;
         const double vx = up2 - up1, vy = vp2 - vp1, vz = wp2 - wp1;
         c.nrm = sqrt(vx * vx + vy * vy + vz * vz);
