@@ -70,14 +70,18 @@ def x_margin_for(w, steps: int) -> float:
     return min(w.setup().lx / 4.0, 1.1 * 6.0 * w.dtime * steps)
 
 
-def build_inputs(w, device, precision, steps: int = 0):
-    """Field and particles of a workload; a batched workload gives one state per class."""
+def build_inputs(w, device, precision, steps: int = 0, rank: int = 0, world: int = 1):
+    """Field and particles of a workload; a batched workload gives one state per class,
+    and on several GPUs only this rank's share of the classes (config.shard_instances)."""
     import dataclasses
     import torch
     from gazpart_b200 import config, field, particles
     setup = w.setup()
     f = field.generate(w.grid, seed=w.field_seed, device=device)
     specs = w.instances if isinstance(w, config.BatchedWorkload) else (w.spec,)
+    if isinstance(w, config.BatchedWorkload) and world > 1:
+        share = config.shard_instances([sp.n for sp in specs], world)[rank]
+        specs = tuple(specs[i] for i in share)
     m = x_margin_for(w, steps) if steps else 0.0
     states = [particles.draw(dataclasses.replace(sp, x_margin=m), setup) for sp in specs]
     return setup, f, states if isinstance(w, config.BatchedWorkload) else states[0]
@@ -476,7 +480,7 @@ def main():
     # the autotuner's trials (60 one-step and 24 graph steps) and the three one-step graphs also
     # move the particles before the state is restored, and the statistics timing adds 24 steps
     run_steps = args.warmup + args.steps + args.e2e_steps + 90 + 28
-    setup, f, st = build_inputs(w, device, precision, run_steps)
+    setup, f, st = build_inputs(w, device, precision, run_steps, rank, world)
     batched = isinstance(st, list)
     max_emaj = float(st["emaj"].max()) if not batched else None
     ctx = make_context(setup, f, st, precision, device)
@@ -510,7 +514,14 @@ def main():
         dist.barrier()
     total_ms = reduce_max_ms(total_ms, dist, device)
     ms_per_step = total_ms / args.steps
-    value = n * world * args.steps / (total_ms / 1e3)
+    # a batched workload is split over the ranks (strong scaling): its particles are the
+    # sum of the shares; a single ensemble is replicated (weak scaling)
+    n_job = n * world
+    if batched and dist:
+        tot = torch.tensor([n], dtype=torch.int64, device=device)
+        dist.all_reduce(tot)
+        n_job = int(tot.item())
+    value = n_job * args.steps / (total_ms / 1e3)
 
     # roofline of the HBM-bound kernel of the step: the stencil gather (the phase
     # timestamps around it bracket that one kernel on the library's stream)
@@ -596,11 +607,14 @@ def main():
     if rank == 0:
         line = {"metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if precision == "fp64" else "f32/f64",
+                "scaling": "strong" if batched else "weak", "vs_baseline": None,
+                "dtype": "f64" if precision == "fp64" else "f32/f64",
                 "data": "synthetic",
-                "config": {"workload": w.name, "precision": precision, "particles_per_gpu": n,
+                "config": {"workload": w.name, "precision": precision, "particles_per_gpu": n, "particles": n_job,
                            "field": f"{w.grid}^3 x 6 {'f32' if fbytes == 4 else 'f64'}",
-                           "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (state+field > 5 GB)",
+                           "parallelism": (f"classes sharded over {world} GPUs" if batched and world > 1
+                                           else f"replicas x{world}"),
+                           "l2": "inputs larger than L2 (state+field > 5 GB)",
                            "x_margin": x_margin_for(w, run_steps), "launch_grids": tune,
                            "classes": len(st) if batched else 1},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": kps * args.steps,

@@ -25,7 +25,7 @@ from __future__ import annotations
 
 import dataclasses
 import math
-from typing import Optional, Tuple
+from typing import List, Optional, Sequence, Tuple
 
 TWO_PI = 2.0 * math.pi
 
@@ -209,6 +209,20 @@ def c4_instances(count: int = 64, seed: int = 193) -> Tuple[ParticleSpec, ...]:
 _C4_REFERENCE = ParticleSpec(n=1, ar=1.0, b=0.002, st=1.0)
 
 C4 = BatchedWorkload("c4_256cube_64inst_fp32field", 256, "f32", c4_instances(), 5.0e-4, 300)
+
+
+def shard_instances(counts: Sequence[int], world: int) -> List[List[int]]:
+    """Instances of a batched workload split over `world` GPUs, each GPU one batched step
+    over its share: largest first, each to the GPU with the fewest particles so far
+    (ties to the lower rank).  Every instance lands on exactly one GPU; the shares are
+    deterministic and differ by at most the largest instance."""
+    loads = [0] * world
+    shares: List[List[int]] = [[] for _ in range(world)]
+    for i in sorted(range(len(counts)), key=lambda k: (-counts[k], k)):
+        r = min(range(world), key=lambda q: (loads[q], q))
+        shares[r].append(i)
+        loads[r] += counts[i]
+    return [sorted(sh) for sh in shares]
 
 
 

@@ -141,6 +141,42 @@ def test_batched_workload_instances():
     assert np.allclose(st_num, w.instances[0].st)      # density follows the instance's Stokes number
 
 
+def _shard_rank_main(rank, world, port, out):
+    import torch
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    counts = [s.n for s in config.C4.instances]
+    mine = config.shard_instances(counts, world)[rank]
+    n = torch.tensor([sum(counts[i] for i in mine)], dtype=torch.int64)
+    dist.all_reduce(n)                                  # as bench.py sums the shares
+    out[rank] = (mine, int(n.item()))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_batched_classes_shard_over_ranks(world):
+    """bench.py --gpus N splits C4's 64 classes over the ranks: every class on one rank,
+    the particle total summed across ranks equals the workload's, the shares balanced."""
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    out = ctx.Manager().dict()
+    port = _free_port()
+    procs = [ctx.Process(target=_shard_rank_main, args=(r, world, port, out)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+        assert p.exitcode == 0
+    counts = [s.n for s in config.C4.instances]
+    shares = [out[r][0] for r in range(world)]
+    assert sorted(i for sh in shares for i in sh) == list(range(64))
+    assert all(out[r][1] == sum(counts) for r in range(world))
+    loads = [sum(counts[i] for i in sh) for sh in shares]
+    assert max(loads) - min(loads) <= max(counts)
+
+
 def test_serving_stream_and_concurrency_count():
     from gazpart_b200 import serving
     w = config.C5
