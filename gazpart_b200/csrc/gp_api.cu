@@ -267,6 +267,12 @@ int alloc_pool(gp_ctx *c, int64_t cap) {
   GP_CK(cudaMemcpyAsync(c->d_pv_alt, &pv[1], sizeof(PoolView), cudaMemcpyHostToDevice, c->stream));
   GP_CK(cudaStreamSynchronize(c->stream));
   GP_CK(cudaMemcpyAsync(c->d_fluid_cols, c->d_fluid, sizeof(c->d_fluid), cudaMemcpyHostToDevice, c->stream));
+  if (c->colstats && c->cap_cst < c->cap_pairs) {   // every candidate pair may be in contact
+    dfree(c->d_cst);
+    c->cap_cst = 0;
+    GP_TRY(dalloc(&c->d_cst, (size_t)c->cap_pairs));
+    c->cap_cst = c->cap_pairs;
+  }
   return GP_OK;
 }
 
@@ -655,6 +661,14 @@ int gp_add_field(gp_ctx *c, int32_t nx, int32_t ny, int32_t nz, double lx, doubl
   if (cudaMemset(ptr, 0, bytes) != cudaSuccess) { cudaFree(ptr); return GP_ECUDA; }
   c->fields.push_back({ptr, nx, ny, nz, lx, ly, lz});
   *field = (int32_t)c->fields.size() - 1;
+  return GP_OK;
+}
+
+int gp_field_shape(gp_ctx *c, int32_t field, int32_t dims[3]) {
+  if (!c || !dims || field < 0 || field >= (int)c->fields.size()) return GP_EBADARG;
+  dims[0] = c->fields[field].nx;
+  dims[1] = c->fields[field].ny;
+  dims[2] = c->fields[field].nz;
   return GP_OK;
 }
 

@@ -360,6 +360,10 @@ int gp_dns_vorticity(gp_dns *d, double *ox, double *oy, double *oz, int32_t on_d
 
 int gp_dns_couple(gp_dns *d, gp_ctx *ctx, int32_t field, int32_t with_vorticity) {
   if (!d || !ctx) return GP_EBADARG;
+  int32_t dims[3];
+  const int rs = gp_field_shape(ctx, field, dims);
+  if (rs) return rs;
+  if (dims[0] != d->nx || dims[1] != d->ny || dims[2] != d->nz) return GP_EBADARG;   // other meshes
   if (cudaStreamSynchronize(d->stream) != cudaSuccess) return GP_ECUDA;
   // FLUIDCOMM (main.f90:499-505): the velocity's y and z ghosts are periodic copies
   for (int c = 0; c < 3; ++c) {

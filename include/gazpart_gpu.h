@@ -189,6 +189,8 @@ int gp_upload_classes(gp_ctx *ctx, int32_t nclass, const int64_t *counts, const 
                       const double *const *props, int32_t on_device);
 
 /* ------------------------------------------------ resident fields and jobs ---- */
+/* Mesh (nx, ny, nz) of field slot `field`. */
+int gp_field_shape(gp_ctx *ctx, int32_t field, int32_t dims[3]);
 /* No counterpart in the reference (serving).  More resident fields beside the one of
  * gp_params: an (nx, ny, nz) mesh of the box (lx, ly, lz), same precision; *field
  * receives its slot (the context's own field is slot 0). */

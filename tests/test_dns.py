@@ -128,3 +128,14 @@ def test_particles_follow_the_live_field():
         ctx.raise_status()
         got = ctx.download()
     assert rel_err(got, ens.a, api.STATE_KEYS) < 1e-10
+
+
+@pytest.mark.gpu
+def test_coupling_refuses_another_mesh():
+    from gazpart_b200 import dns
+    s32 = config.Setup(nx=32, ny=32, nz=32, visc=0.02, dtime=0.005)
+    s16 = config.Setup(nx=16, ny=16, nz=16, visc=0.02, dtime=0.005)
+    with api.Context(s16, "fp64") as ctx, dns.Fluid(s32) as fl:
+        with pytest.raises(api.GPError) as e:
+            fl.couple(ctx)
+        assert e.value.code == 9                        # GP_EBADARG: the meshes differ
