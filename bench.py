@@ -46,8 +46,10 @@ def parse():
     ap.add_argument("--no-io", action="store_true", help="skip the restart-file measurement")
     ap.add_argument("--no-stats", action="store_true", help="skip the statistics measurement")
     ap.add_argument("--no-dns", action="store_true", help="skip the live-fluid measurement")
+    ap.add_argument("--contact-tail", type=int, default=None,
+                    help="evaluations after which a contact solve moves to the inlined-solver kernel (0: never)")
     ap.add_argument("--grids", default=None,
-                    help="gather,integrate,bin,search,overlap: fixed launch grids instead of autotuning")
+                    help="gather,integrate,bin,search,overlap[,contact_tail]: fixed launch choices instead of autotuning")
     ap.add_argument("--serve-seconds", type=float, default=2.0, help="arrival window of the serving workload")
     return ap.parse_args()
 
@@ -477,18 +479,22 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device(device))
 
-    # the autotuner's trials (60 one-step and 24 graph steps) and the three one-step graphs also
+    # the autotuner's trials (60 one-step and 48 graph steps) and the three one-step graphs also
     # move the particles before the state is restored, and the statistics timing adds 24 steps
-    run_steps = args.warmup + args.steps + args.e2e_steps + 90 + 28
+    run_steps = args.warmup + args.steps + args.e2e_steps + 114 + 28
     setup, f, st = build_inputs(w, device, precision, run_steps, rank, world)
     batched = isinstance(st, list)
     max_emaj = float(st["emaj"].max()) if not batched else None
     ctx = make_context(setup, f, st, precision, device)
     n = ctx.n
+    if args.contact_tail is not None:
+        ctx.set_contact_tail(args.contact_tail)
     if args.grids:
         g = [int(v) for v in args.grids.split(",")]
         tune = dict(zip(("gather", "integrate", "bin", "search"), g[:4]))
         tune["overlap_gather"] = bool(g[4]) if len(g) > 4 else False
+        if len(g) > 5:
+            tune["contact_tail"] = g[5]
         ctx.set_launch(tune)
     else:
         tune = None if args.no_autotune else ctx.autotune()

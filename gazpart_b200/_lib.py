@@ -128,6 +128,8 @@ SIGNATURES = {
                                                      _vp],
     "gp_collision_response": [_ctx, C.c_int32, C.c_int32, _dp, _dp, _dp, _dp, _dp],
     "gp_field_shape": [_ctx, C.c_int32, _ip],
+    "gp_set_contact_tail": [_ctx, C.c_int32],
+    "gp_get_contact_tail": [_ctx, _ip],
     "gp_dns_create": [C.POINTER(GPParams), C.c_int32, C.c_double, C.POINTER(_vp)],
     "gp_dns_destroy": [_vp],
     "gp_dns_set_velocity": [_vp, _vp, _vp, _vp, C.c_int32],

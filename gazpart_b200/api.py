@@ -134,6 +134,16 @@ class Context:
         mean[:, -1] = out[:, -1]
         return mean
 
+    def set_contact_tail(self, budget: int) -> None:
+        """Solves running past `budget` evaluations finish in the inlined-solver kernel
+        (0: none do); results are unchanged."""
+        check(_lib.lib().gp_set_contact_tail(self._h, int(budget)), "gp_set_contact_tail")
+
+    def contact_tail(self) -> int:
+        b = C.c_int32()
+        check(_lib.lib().gp_get_contact_tail(self._h, C.byref(b)), "gp_get_contact_tail")
+        return b.value
+
     def enable_collision_stats(self, on: bool = True) -> None:
         check(_lib.lib().gp_collision_stats_enable(self._h, 1 if on else 0), "gp_collision_stats_enable")
 
@@ -300,6 +310,7 @@ class Context:
         check(_lib.lib().gp_autotune(self._h, g), "gp_autotune")
         out = dict(zip(_lib.TUNABLES, (int(v) for v in g)))
         out["overlap_gather"] = bool(g[len(_lib.TUNABLES)])
+        out["contact_tail"] = self.contact_tail()
         return out
 
     def set_launch(self, grids: Dict[str, int]) -> None:
@@ -307,6 +318,8 @@ class Context:
         g = (C.c_int32 * (len(_lib.TUNABLES) + 1))(*[int(grids[k]) for k in _lib.TUNABLES],
                                                      int(bool(grids.get("overlap_gather", False))))
         check(_lib.lib().gp_set_launch(self._h, g), "gp_set_launch")
+        if "contact_tail" in grids:
+            self.set_contact_tail(int(grids["contact_tail"]))
 
     def download(self, fluid: bool = False) -> Dict[str, np.ndarray]:
         out = {k: np.empty(self.n) for k in STATE_KEYS}

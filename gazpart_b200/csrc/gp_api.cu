@@ -135,7 +135,8 @@ struct gp_ctx {
   CollRec *d_coll = nullptr;
   int64_t cap_coll = 0;
   unsigned long long *d_counters = nullptr;   // [0] npairs [1] ncoll [2] nacc [3] contact queue [4] contacts kept
-                                              // for the statistics [5] collision steps in the statistics
+                                              // for the statistics [5] solves handed to the tail kernel
+                                              // [7] collision steps in the statistics
   unsigned long long *d_best1 = nullptr, *d_best2 = nullptr;
   int8_t *d_matched = nullptr, *d_state = nullptr;
   int32_t *d_acc = nullptr;
@@ -165,6 +166,11 @@ struct gp_ctx {
   int64_t cap_cst = 0;
   double *d_colacc = nullptr;           // [kMaxClasses][G][G][GP_NSTAT_COLLISION]
   double *d_stat_partial = nullptr, *d_stat_out = nullptr;
+  // contact solves still running after tail_budget evaluations finish in k_contact_tail
+  // (0: no hand-over)
+  TailRec *d_tail = nullptr;
+  int64_t cap_tail = 0;
+  int tail_budget = 64;
 };
 
 namespace {
@@ -378,7 +384,7 @@ int enqueue_bin(gp_ctx *c) {
   GP_CK(cudaMemsetAsync(sa.cell_count, 0, (c->ncells + 1) * sizeof(int32_t), c->stream));
   GP_CK(cudaMemsetAsync(sa.cell_fill, 0, (c->ncells + 1) * sizeof(int32_t), c->stream));
   GP_CK(cudaMemsetAsync(sa.cell_rmax, 0, (c->ncells + 1) * sizeof(float), c->stream));
-  GP_CK(cudaMemsetAsync(c->d_counters, 0, 5 * sizeof(unsigned long long), c->stream));
+  GP_CK(cudaMemsetAsync(c->d_counters, 0, 6 * sizeof(unsigned long long), c->stream));
   launch_bin_count(c->d_inst, c->d_pv, c->n_slots, sa, c->d_status, c->tune[GP_TUNE_BIN], c->stream);
   launch_scan(sa.cell_count, sa.cell_start, c->ncells, c->d_scan_tmp, c->stream);
   launch_bin_scatter(c->d_inst, c->d_pv, c->n_slots, sa, c->d_status, c->tune[GP_TUNE_BIN], c->stream);
@@ -402,9 +408,14 @@ int enqueue_bin_search(gp_ctx *c) {
 // Contact solves, greedy acceptance and the impulse response.
 int enqueue_contact_response(gp_ctx *c) {
   GP_TRY(mark(c, 2 * GP_PHASE_CONTACT, c->stream));
+  ContactStatRec *cst = c->colstats ? c->d_cst : nullptr;
+  TailRec *tail = c->tail_budget > 0 ? c->d_tail : nullptr;
   launch_contact(c->d_inst, c->d_pv, c->d_pairs, c->d_counters + 0, c->cap_pairs, c->d_coll, c->d_counters + 1,
-                 c->cap_coll, c->d_counters + 3, c->colstats ? c->d_cst : nullptr, c->d_counters + 4, c->cap_cst,
-                 c->d_status, c->contact_grid, c->stream);
+                 c->cap_coll, c->d_counters + 3, cst, c->d_counters + 4, c->cap_cst, tail, c->d_counters + 5,
+                 c->cap_tail, c->tail_budget, c->d_status, c->contact_grid, c->stream);
+  if (tail)
+    launch_contact_tail(c->d_pv, c->d_pairs, tail, c->d_counters + 5, c->cap_tail, c->d_coll, c->d_counters + 1,
+                        c->cap_coll, cst, c->d_counters + 4, c->cap_cst, c->d_status, c->stream);
   GP_TRY(mark(c, 2 * GP_PHASE_CONTACT + 1, c->stream));
   GP_TRY(mark(c, 2 * GP_PHASE_RESPONSE, c->stream));
   launch_match(c->d_coll, c->d_counters + 1, c->cap_coll, c->d_best1, c->d_best2, c->d_matched, c->d_state,
@@ -414,7 +425,7 @@ int enqueue_contact_response(gp_ctx *c) {
   if (c->colstats)
     launch_collision_stats(c->d_coll, c->d_counters + 1, c->cap_coll, c->d_state, c->d_best1, c->d_best2, c->d_cst,
                            c->d_counters + 4, c->cap_cst, c->d_pv, c->d_group_tab, c->d_group_n, c->d_colacc,
-                           c->d_counters + 5, c->d_status, c->stream);
+                           c->d_counters + 7, c->d_status, c->stream);
   GP_CK(cudaGetLastError());
   return mark(c, 2 * GP_PHASE_RESPONSE + 1, c->stream);
 }
@@ -519,8 +530,13 @@ int gp_ctx_create(const gp_params *params, gp_ctx **out) {
   if (!rc) rc = dalloc(&c->d_pv, 1);
   if (!rc) rc = dalloc(&c->d_pv_alt, 1);
   if (!rc) rc = dalloc(&c->d_fluid_cols, kNFluid);
-  if (!rc) rc = dalloc(&c->d_counters, 6);
-  if (!rc && cudaMemset(c->d_counters, 0, 6 * sizeof(unsigned long long)) != cudaSuccess) rc = GP_ECUDA;
+  if (!rc) rc = dalloc(&c->d_counters, 8);
+  if (!rc && cudaMemset(c->d_counters, 0, 8 * sizeof(unsigned long long)) != cudaSuccess) rc = GP_ECUDA;
+  if (!rc) {
+    c->cap_tail = 16384;
+    if (cudaMalloc(reinterpret_cast<void **>(&c->d_tail), (size_t)c->cap_tail * tail_record_bytes()) != cudaSuccess)
+      rc = GP_ENOMEM;
+  }
   if (!rc) rc = dalloc(&c->d_group_tab, kMaxClasses);
   if (!rc) rc = dalloc(&c->d_group_n, kMaxClasses);
   if (!rc) {
@@ -564,6 +580,7 @@ int gp_ctx_destroy(gp_ctx *c) {
   for (auto &g : c->group_dev) dfree(g);
   dfree(c->d_group_tab); dfree(c->d_group_n); dfree(c->d_cst); dfree(c->d_colacc);
   dfree(c->d_stat_partial); dfree(c->d_stat_out);
+  if (c->d_tail) cudaFree(c->d_tail);
   dfree(c->d_status); dfree(c->d_scratch);
   if (c->ev_fork) cudaEventDestroy(c->ev_fork);
   if (c->ev_join) cudaEventDestroy(c->ev_join);
@@ -945,6 +962,19 @@ int gp_stat_partfluid(gp_ctx *c, int32_t ig, double *out) {
   return GP_OK;
 }
 
+int gp_set_contact_tail(gp_ctx *c, int32_t budget) {
+  if (!c || budget < 0 || budget > 300) return GP_EBADARG;
+  c->tail_budget = budget;
+  drop_graph(c);
+  return GP_OK;
+}
+
+int gp_get_contact_tail(gp_ctx *c, int32_t *budget) {
+  if (!c || !budget) return GP_EBADARG;
+  *budget = c->tail_budget;
+  return GP_OK;
+}
+
 int gp_collision_stats_enable(gp_ctx *c, int32_t on) {
   if (!c) return GP_EBADARG;
   if ((on != 0) == c->colstats) return GP_OK;
@@ -973,7 +1003,7 @@ int gp_collision_stats(gp_ctx *c, int32_t ig, double *out, int64_t *steps, int32
   const int ng = c->group_n[slot];
   const size_t per_class = (size_t)kStatMaxGroups * kStatMaxGroups * kNStatCollision;
   std::vector<double> acc(per_class, 0.0);
-  unsigned long long cnt[6] = {};
+  unsigned long long cnt[8] = {};
   GP_CK(cudaStreamSynchronize(c->stream));
   if (c->d_colacc)
     GP_CK(cudaMemcpy(acc.data(), c->d_colacc + (size_t)slot * per_class, per_class * sizeof(double),
@@ -988,11 +1018,11 @@ int gp_collision_stats(gp_ctx *c, int32_t ig, double *out, int64_t *steps, int32
       o[2] = 2.0 * o[1] / dtime;   // collision_interaction.f90:429
       o[4] = o[3] / o[0];          // collision_interaction.f90:430
     }
-  if (steps) *steps = (int64_t)cnt[5];
+  if (steps) *steps = (int64_t)cnt[7];
   if (reset) {
     if (c->d_colacc)
       GP_CK(cudaMemsetAsync(c->d_colacc, 0, (size_t)kMaxClasses * per_class * sizeof(double), c->stream));
-    GP_CK(cudaMemsetAsync(c->d_counters + 5, 0, sizeof(unsigned long long), c->stream));
+    GP_CK(cudaMemsetAsync(c->d_counters + 7, 0, sizeof(unsigned long long), c->stream));
     GP_CK(cudaStreamSynchronize(c->stream));
   }
   return GP_OK;
@@ -1566,18 +1596,25 @@ int gp_autotune(gp_ctx *c, int32_t *grids_out) {
     }
     c->tune[t] = best;
   }
-  // overlapped gather or not: whichever four-step graph is faster (median of three)
+  // overlapped gather or not, long contact solves handed over or not: whichever
+  // four-step graph is faster (median of three)
   if (!rc) {
-    float best_ms[2];
-    for (int o = 0; o < 2 && !rc; ++o) {
-      c->overlap = o == 1;
-      drop_graph(c);
-      float trial[3];
-      for (int r = 0; r < 3 && !rc; ++r) rc = gp_step_timed(c, 4, &trial[r], nullptr, nullptr);
-      std::sort(trial, trial + 3);
-      best_ms[o] = trial[1];
-    }
-    c->overlap = !rc && best_ms[1] < best_ms[0];
+    static const int kTail[2] = {0, 64};
+    float best = 1e30f;
+    bool best_overlap = false;
+    int best_tail = 0;
+    for (int o = 0; o < 2 && !rc; ++o)
+      for (int t = 0; t < 2 && !rc; ++t) {
+        c->overlap = o == 1;
+        c->tail_budget = kTail[t];
+        drop_graph(c);
+        float trial[3];
+        for (int r = 0; r < 3 && !rc; ++r) rc = gp_step_timed(c, 4, &trial[r], nullptr, nullptr);
+        std::sort(trial, trial + 3);
+        if (trial[1] < best) { best = trial[1]; best_overlap = c->overlap; best_tail = c->tail_budget; }
+      }
+    c->overlap = best_overlap;
+    c->tail_budget = best_tail;
   }
   drop_graph(c);
   if (!rc) {

@@ -5,7 +5,7 @@
 #include <math_constants.h>
 
 #include "gp_advance.cuh"
-#include "gp_lm.cuh"
+#include "gp_contact.cuh"
 #include "gp_launch.h"
 
 namespace gp {
@@ -131,7 +131,9 @@ __global__ void __launch_bounds__(128, GP_CONTACT_MIN_BLOCKS) k_contact(const In
                                                     CollRec *__restrict__ coll, unsigned long long *ncoll,
                                                     int64_t cap_coll, unsigned long long *queue,
                                                     ContactStatRec *__restrict__ cst, unsigned long long *ncst,
-                                                    int64_t cap_cst, Status *st) {
+                                                    int64_t cap_cst, TailRec *__restrict__ tail,
+                                                    unsigned long long *ntail, int64_t cap_tail, int tail_budget,
+                                                    Status *st) {
   const PoolView P = *pv;
   const int64_t np = (int64_t)min(*npairs, (unsigned long long)cap_pairs);
   const unsigned lane = threadIdx.x & 31u;
@@ -189,64 +191,24 @@ __global__ void __launch_bounds__(128, GP_CONTACT_MIN_BLOCKS) k_contact(const In
       continue;
     }
     if (!active) continue;
-    if (lm_step(CP, S, kContactTol) == 0) continue;
-    active = false;
-    atomicAdd(&st->n_solve, 1ull);
-    atomicAdd(&st->n_eval, (unsigned long long)S.nfev);
-    atomicMax(&st->max_eval, (unsigned long long)S.nfev);
-    double ept1[3], ept2[3], cn[3];
-    if (!contact_finish(a1, b1, a2, b2, q1, q2, CP, S.x, ept1, ept2, cn)) continue;
-    atomicAdd(&st->n_contact, 1ull);
-    // overlap depth |EPT1 - EPT2| for the collision statistics, while the points are at hand
-    double depth = 0.0;
-    if (cst != nullptr) {
-      const double v0 = ept1[0] - ept2[0], v1 = ept1[1] - ept2[1], v2 = ept1[2] - ept2[2];
-      depth = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
-    }
-    const PairRec pr = pairs[e];
-    const int i1 = pr.home, i2 = pr.near;
-    const double x1 = CP.b1[0], y1 = CP.b1[1], z1 = CP.b1[2];
-    double rx1[3] = {(ept1[0] - x1), (ept1[1] - y1), (ept1[2] - z1)};
-    double om1[3] = {P.st[10][i1], P.st[11][i1], P.st[12][i1]};
-    rot_vec(q1, om1);
-    const double up1 = P.st[3][i1] + (om1[1] * rx1[2] - om1[2] * rx1[1]);
-    const double vp1 = P.st[4][i1] + (om1[2] * rx1[0] - om1[0] * rx1[2]);
-    const double wp1 = P.st[5][i1] + (om1[0] * rx1[1] - om1[1] * rx1[0]);
-    double rx2[3] = {(ept2[0] - CP.b2[0]), (ept2[1] - CP.b2[1]), (ept2[2] - CP.b2[2])};
-    double om2[3] = {P.st[10][i2], P.st[11][i2], P.st[12][i2]};
-    rot_vec(q2, om2);
-    const double up2 = P.st[3][i2] + (om2[1] * rx2[2] - om2[2] * rx2[1]);
-    const double vp2 = P.st[4][i2] + (om2[2] * rx2[0] - om2[0] * rx2[2]);
-    const double wp2 = P.st[5][i2] + (om2[0] * rx2[1] - om2[1] * rx2[0]);
-    const double nvrel = (up2 - up1) * cn[0] + (vp2 - vp1) * cn[1] + (wp2 - wp1) * cn[2];
-    if (cst != nullptr) {
-      // every contact, for the collision statistics (collision_interaction.f90:253-328)
-      const unsigned long long k = atomicAdd(ncst, 1ull);
-      if ((int64_t)k < cap_cst) {
-        ContactStatRec c;
-        c.home = i1; c.near = i2; c.inst = P.inst[i1]; c.pad = 0; c.k1 = pr.k1; c.k2 = pr.k2;
-        c.depth = depth;
-        c.nvrel = nvrel;
-        const double vx = up2 - up1, vy = vp2 - vp1, vz = wp2 - wp1;
-        c.nrm = sqrt(vx * vx + vy * vy + vz * vz);
-        cst[k] = c;
-      } else {
-        set_error(st, GP_EPAIR_OVERFLOW, (long long)P.id[i1], P.inst[i1]);
+    if (lm_step(CP, S, kContactTol) == 0) {
+      // a long solve goes to k_contact_tail, which finishes it with the solver folded
+      // into one kernel; the lane takes a new pair (if the hand-over buffer is full the
+      // lane keeps the solve)
+      if (tail != nullptr && S.nfev >= tail_budget) {
+        const unsigned long long k = atomicAdd(ntail, 1ull);
+        if ((int64_t)k < cap_tail) {
+          TailRec t;
+          t.e = e; t.CP = CP; t.S = S; t.q1 = q1; t.q2 = q2;
+          t.a1 = a1; t.b1 = b1; t.a2 = a2; t.b2 = b2;
+          tail[k] = t;
+          active = false;
+        }
       }
-    }
-    if (!(nvrel < kZeroRef)) continue;
-    const unsigned long long slot = atomicAdd(ncoll, 1ull);
-    if ((int64_t)slot >= cap_coll) {
-      atomicAdd(&st->overflow, 1ull);
-      set_error(st, GP_EPAIR_OVERFLOW, (long long)P.id[i1], P.inst[i1]);
       continue;
     }
-    CollRec r;
-    r.home = i1; r.near = i2; r.k1 = pr.k1; r.k2 = pr.k2;
-    r.inst = P.inst[i1]; r.pad = 0;
-#pragma unroll
-    for (int i = 0; i < 3; ++i) { r.rx1[i] = rx1[i]; r.rx2[i] = rx2[i]; r.cn[i] = cn[i]; }
-    coll[slot] = r;
+    active = false;
+    finish_pair(P, pairs, e, CP, S, q1, q2, a1, b1, a2, b2, coll, ncoll, cap_coll, cst, ncst, cap_cst, st);
   }
 }
 
@@ -264,9 +226,10 @@ int contact_grid_blocks() {
 void launch_contact(const InstDev *insts, const PoolView *pv, const PairRec *pairs, const unsigned long long *npairs,
                     int64_t cap_pairs, CollRec *coll, unsigned long long *ncoll, int64_t cap_coll,
                     unsigned long long *queue, ContactStatRec *cst, unsigned long long *ncst, int64_t cap_cst,
-                    Status *st, int grid, cudaStream_t s) {
+                    TailRec *tail, unsigned long long *ntail, int64_t cap_tail, int tail_budget, Status *st,
+                    int grid, cudaStream_t s) {
   k_contact<<<grid, 128, 0, s>>>(insts, pv, pairs, npairs, cap_pairs, coll, ncoll, cap_coll, queue, cst, ncst,
-                                 cap_cst, st);
+                                 cap_cst, tail, ntail, cap_tail, tail_budget, st);
 }
 
 // COLLISION_RESPONSE (collision_response.f90) for the accepted pairs; each particle is

@@ -7,6 +7,8 @@
 
 namespace gp {
 
+struct TailRec;   // gp_contact.cuh
+
 // --- gp_kernels_fp64.cu (FP64 path, -fmad=false) ---
 // ADV_PARTICLE_ELLP: advances particle perm[j] of *pv into slot j of *pv_alt, then swaps
 // the two views (so *pv is current afterwards).
@@ -23,7 +25,14 @@ int contact_grid_blocks();
 void launch_contact(const InstDev *insts, const PoolView *pv, const PairRec *pairs, const unsigned long long *npairs,
                     int64_t cap_pairs, CollRec *coll, unsigned long long *ncoll, int64_t cap_coll,
                     unsigned long long *queue, ContactStatRec *cst, unsigned long long *ncst, int64_t cap_cst,
-                    Status *st, int grid, cudaStream_t s);
+                    TailRec *tail, unsigned long long *ntail, int64_t cap_tail, int tail_budget, Status *st,
+                    int grid, cudaStream_t s);
+// --- gp_contact_tail.cu (-fmad=false, solver inlined) ---
+void launch_contact_tail(const PoolView *pv, const PairRec *pairs, const TailRec *tail,
+                         const unsigned long long *ntail, int64_t cap_tail, CollRec *coll, unsigned long long *ncoll,
+                         int64_t cap_coll, ContactStatRec *cst, unsigned long long *ncst, int64_t cap_cst,
+                         Status *st, cudaStream_t s);
+size_t tail_record_bytes();
 void launch_response(const InstDev *insts, const PoolView *pv, const CollRec *coll, const unsigned long long *ncoll,
                      int64_t cap_coll, const int8_t *state, int32_t *acc_list, unsigned long long *nacc, Status *st,
                      int grid, cudaStream_t s);

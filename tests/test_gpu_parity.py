@@ -137,3 +137,26 @@ def test_mixed_precision_error_budget():
     err = du / (nu + 1e-30)
     assert np.median(err) < 1e-6
     assert np.quantile(err, 0.99) < 1e-5
+
+
+@pytest.mark.parametrize("name", ["dense", "bimodal"])
+def test_contact_tail_hand_over_changes_nothing(name):
+    """Solves handed from the persistent contact kernel to the inlined-solver kernel
+    (gp_set_contact_tail) run the same iterates: with every solve handed over after its
+    first iteration, with none handed over and with the default, the colliding pairs and
+    the states after a step are identical."""
+    setup, fn, refs, st = case(name)
+    res = po.Ensemble(setup, copy_state(st)).collide(prefilter=True, nthreads=8)
+    out = {}
+    for budget in (0, 1, 64):
+        with _ctx(setup, fn, st) as ctx:
+            ctx.set_contact_tail(budget)
+            ctx.collision(1, 0.0)
+            ctx.raise_status()
+            out[budget] = (ctx.collision_pairs(), ctx.download(), ctx.collision_counters())
+    for budget in (0, 1, 64):
+        (home, near), got, cnt = out[budget]
+        assert np.array_equal(home, res["home"]) and np.array_equal(near, res["near"]), budget
+        for k in api.STATE_KEYS:
+            assert np.array_equal(got[k], out[0][1][k]), (budget, k)
+        assert cnt == out[0][2], budget
