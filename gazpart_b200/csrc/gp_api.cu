@@ -167,10 +167,10 @@ struct gp_ctx {
   double *d_colacc = nullptr;           // [kMaxClasses][G][G][GP_NSTAT_COLLISION]
   double *d_stat_partial = nullptr, *d_stat_out = nullptr;
   // contact solves still running after tail_budget evaluations finish in k_contact_tail
-  // (0: no hand-over)
+  // (0: no hand-over, the default: with the gather overlapped it did not shorten the step)
   TailRec *d_tail = nullptr;
   int64_t cap_tail = 0;
-  int tail_budget = 64;
+  int tail_budget = 0;
 };
 
 namespace {
@@ -1596,25 +1596,18 @@ int gp_autotune(gp_ctx *c, int32_t *grids_out) {
     }
     c->tune[t] = best;
   }
-  // overlapped gather or not, long contact solves handed over or not: whichever
-  // four-step graph is faster (median of three)
+  // overlapped gather or not: whichever four-step graph is faster (median of three)
   if (!rc) {
-    static const int kTail[2] = {0, 64};
-    float best = 1e30f;
-    bool best_overlap = false;
-    int best_tail = 0;
-    for (int o = 0; o < 2 && !rc; ++o)
-      for (int t = 0; t < 2 && !rc; ++t) {
-        c->overlap = o == 1;
-        c->tail_budget = kTail[t];
-        drop_graph(c);
-        float trial[3];
-        for (int r = 0; r < 3 && !rc; ++r) rc = gp_step_timed(c, 4, &trial[r], nullptr, nullptr);
-        std::sort(trial, trial + 3);
-        if (trial[1] < best) { best = trial[1]; best_overlap = c->overlap; best_tail = c->tail_budget; }
-      }
-    c->overlap = best_overlap;
-    c->tail_budget = best_tail;
+    float best_ms[2];
+    for (int o = 0; o < 2 && !rc; ++o) {
+      c->overlap = o == 1;
+      drop_graph(c);
+      float trial[3];
+      for (int r = 0; r < 3 && !rc; ++r) rc = gp_step_timed(c, 4, &trial[r], nullptr, nullptr);
+      std::sort(trial, trial + 3);
+      best_ms[o] = trial[1];
+    }
+    c->overlap = !rc && best_ms[1] < best_ms[0];
   }
   drop_graph(c);
   if (!rc) {

@@ -191,10 +191,9 @@ int gp_upload_classes(gp_ctx *ctx, int32_t nclass, const int64_t *counts, const 
 /* ------------------------------------------------ resident fields and jobs ---- */
 /* No counterpart in the reference.  Contact solves still running after `budget`
  * function evaluations are finished by a second kernel with the solver inlined, whose
- * iterations are shorter; the results do not change.  0 keeps every solve in the
- * persistent contact kernel.  Default 64; at most 300 (MINPACK's maxfev). */
+ * iterations are shorter; the results do not change.  0 (the default) keeps every
+ * solve in the persistent contact kernel; at most 300 (MINPACK's maxfev). */
 int gp_set_contact_tail(gp_ctx *ctx, int32_t budget);
-/* The budget in force (gp_autotune picks 0 or 64 with the gather overlap). */
 int gp_get_contact_tail(gp_ctx *ctx, int32_t *budget);
 /* Mesh (nx, ny, nz) of field slot `field`. */
 int gp_field_shape(gp_ctx *ctx, int32_t field, int32_t dims[3]);
@@ -289,9 +288,8 @@ enum {
 };
 /* Autotuner: for each launch above, in turn, times one-step graphs of the resident
  * ensemble with 148 x {1,2,4,8,16} blocks and keeps the fastest; then times four-step
- * graphs with and without the next step's gather run on a second stream beside the
- * contact solves, each with the long solves handed over (gp_set_contact_tail 64) and
- * not, and keeps the fastest of the four.  The particle state is saved first and restored
+ * graphs with the next step's gather run on a second stream beside the contact solves
+ * and without, and keeps the faster.  The particle state is saved first and restored
  * afterwards.  grids_out: GP_NTUNE + 1 ints (the grids, then 1 if the gather is
  * overlapped) or NULL.  No counterpart in the reference. */
 int gp_autotune(gp_ctx *ctx, int32_t *grids_out);
