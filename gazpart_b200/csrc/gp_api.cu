@@ -890,15 +890,14 @@ int gp_add_class(gp_ctx *c, int32_t field, int64_t n, const double *const *cols,
 int gp_download_class(gp_ctx *c, int32_t ig, double *const *cols, int32_t on_device) {
   if (!c || !cols || ig < 1 || ig > (int)c->live.size() || !c->live[ig - 1]) return GP_EBADARG;
   const int64_t n = c->insts[ig - 1].count;
-  double *tmp = nullptr;
-  GP_TRY(dalloc(&tmp, (size_t)kNState * n));
+  GP_TRY(ensure_scratch(c, (size_t)kNState * n));
+  double *tmp = c->d_scratch;
   launch_gather_state(c->d_inst, c->d_pv, c->n_slots, ig - 1, tmp, c->d_fluid_cols, nullptr, n, c->stream);
   GP_CK(cudaGetLastError());
   const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
   for (int k = 0; k < kNState; ++k)
     GP_CK(cudaMemcpyAsync(cols[k], tmp + (size_t)k * n, n * sizeof(double), kind, c->stream));
   GP_CK(cudaStreamSynchronize(c->stream));
-  cudaFree(tmp);
   return GP_OK;
 }
 
@@ -1035,9 +1034,11 @@ int gp_upload_state(gp_ctx *c, int64_t n, const double *const *cols, const doubl
 int gp_download_state(gp_ctx *c, int64_t n, double *const *cols, double *const *fluid, int32_t on_device) {
   if (!c || !cols || n != c->n) return GP_EBADARG;
   if (fluid && !c->prm.store_fluid) return GP_EBADARG;
-  double *tmp = nullptr;
+  // the context's scratch buffer, kept between calls: a fresh allocation and its
+  // release (which waits for the device) would cost more than the gather itself
   const size_t per = (size_t)kNState + (fluid ? kNFluid : 0);
-  GP_TRY(dalloc(&tmp, per * n));
+  GP_TRY(ensure_scratch(c, per * n));
+  double *tmp = c->d_scratch;
   launch_gather_state(c->d_inst, c->d_pv, c->n_slots, -1, tmp, c->d_fluid_cols,
                       fluid ? tmp + (size_t)kNState * n : nullptr, n,
                       c->stream);
@@ -1049,7 +1050,6 @@ int gp_download_state(gp_ctx *c, int64_t n, double *const *cols, double *const *
     for (int k = 0; k < kNFluid; ++k)
       GP_CK(cudaMemcpyAsync(fluid[k], tmp + (size_t)(kNState + k) * n, n * sizeof(double), kind, c->stream));
   GP_CK(cudaStreamSynchronize(c->stream));
-  cudaFree(tmp);
   return GP_OK;
 }
 
