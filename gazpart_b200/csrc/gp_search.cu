@@ -386,75 +386,164 @@ __device__ __forceinline__ RowRanges row_ranges(const SearchArrays &sa, int64_t 
 #ifndef GP_SEARCH_MIN_BLOCKS
 #define GP_SEARCH_MIN_BLOCKS 4
 #endif
-__global__ void __launch_bounds__(256, GP_SEARCH_MIN_BLOCKS) k_search(const InstDev *__restrict__ insts, int64_t n, SearchArrays sa,
-                                                PairRec *__restrict__ pairs, unsigned long long *npairs,
-                                                int64_t cap, Status *st) {
+
+// A home particle's data, kept in shared memory for the lanes that test its candidates.
+struct HomeRec {
+  double xp, yp, zp, rp;
+  long long bp;
+  int32_t s, pslot, idp, inst;
+};
+constexpr int kSearchThreads = 256;
+constexpr int kMaxRanges = 10;   // 5 rows, each at most two contiguous ranges
+
+// Each lane takes one home particle (32 consecutive sorted particles per warp) and works
+// out the ranges of sorted particles its half stencil must test: the five forward rows
+// of cells, trimmed to the cells within reach.  The warp then tests all its homes'
+// candidates together, 32 at a time: candidate idx of the warp's concatenated lists goes
+// to lane idx mod 32, which looks up the owning home and range in shared memory.  Lanes
+// stay busy however unevenly the candidates fall among the homes.  Homes above the cut
+// radius sweep their wide stencil afterwards, each on its own lane.
+__global__ void __launch_bounds__(kSearchThreads, GP_SEARCH_MIN_BLOCKS) k_search(
+    const InstDev *__restrict__ insts, int64_t n, SearchArrays sa, PairRec *__restrict__ pairs,
+    unsigned long long *npairs, int64_t cap, Status *st) {
+  __shared__ HomeRec homes[kSearchThreads];
+  __shared__ int32_t rstart[kSearchThreads][kMaxRanges];   // first sorted particle of a range
+  __shared__ int32_t rcum[kSearchThreads][kMaxRanges];     // candidates of the home before it
+  __shared__ int8_t rnum[kSearchThreads];
+  constexpr unsigned kFull = 0xffffffffu;
+  const int t = threadIdx.x, lane = t & 31, wbase = t & ~31;
   const int64_t nact = sa.cell_start[sa.ncells];
-  for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < nact; s += (int64_t)gridDim.x * blockDim.x) {
-    const InstDev &I = insts[sa.sinst[s]];
-    SearchHome h;
-    h.s = (int32_t)s;
-    h.xp = sa.sx[s]; h.yp = sa.sy[s]; h.zp = sa.sz[s]; h.rp = sa.sr[s];
-    h.bp = sa.sbox[s];
-    h.pslot = sa.sorted[s];
-    h.idp = sa.sid[s];
-    h.perx = I.periodicity != 0;
-    h.xpf = (float)h.xp; h.ypf = (float)h.yp; h.zpf = (float)h.zp; h.rpf = (float)h.rp;
-    h.lxf = (float)I.lx; h.lyf = (float)I.ly; h.lzf = (float)I.lz;
-    const int nfx = I.nfx, nfy = I.nfy, nfz = I.nfz;
-    // the binning pass's own cell of this particle (same inputs, same function)
-    const int cx = cell_coord(h.xp, I.hfx, nfx), cy = cell_coord(h.yp, I.hfy, nfy), cz = cell_coord(h.zp, I.hfz, nfz);
-    const int64_t lc = ((int64_t)cz * nfy + cy) * nfx + cx;
-    if (sa.spk[s].w >= 0.f) {
-      // Small candidates have radius <= rcut, so only cells whose box comes within
-      // R = rp + rcut of this particle can hold a partner: rows and end cells farther
-      // away are skipped (distances to the neighbour boxes from the offsets inside the
-      // home cell, shortened by 1e-9 of the cell edge against rounding).
-      const double R = (h.rp + I.rcut) * (1.0 + 1e-9), R2 = R * R;
-      const double fx = h.xp - cx * I.hfx, fy = h.yp - cy * I.hfy, fz = h.zp - cz * I.hfz;
-      const double ex = 1e-9 * I.hfx, ey = 1e-9 * I.hfy, ez = 1e-9 * I.hfz;
-      const double dxl = fmax(fx - ex, 0.0), dxh = fmax(I.hfx - fx - ex, 0.0);
-      const double dyl = fmax(fy - ey, 0.0), dyh = fmax(I.hfy - fy - ey, 0.0);
-      const double dzh = fmax(I.hfz - fz - ez, 0.0);
-      for (int r = 0; r < 5; ++r) {
-        int ry = cy, rz = cz, lo = cx - 1, hi = cx + 1;
-        double dyz2 = 0.0;
-        if (r == 0) {
-          lo = hi = cx + 1;                    // the rest of the home cell is swept below
-        } else if (r == 1) {
-          ry = wrap_cell(cy + 1, nfy);
-          dyz2 = dyh * dyh;
-        } else {
-          rz = wrap_cell(cz + 1, nfz);
-          ry = wrap_cell(cy + (r - 3), nfy);
-          const double dyb = (r == 2) ? dyl : (r == 4 ? dyh : 0.0);
-          dyz2 = dyb * dyb + dzh * dzh;
-        }
-        if (r > 0 && dyz2 > R2) continue;
-        const int64_t base = I.cell_begin + ((int64_t)rz * nfy + ry) * nfx;
-        // each end cell within reach of its own largest radius
-        auto reach2 = [&](int cell) {
-          const int w = cell < 0 ? cell + nfx : (cell >= nfx ? cell - nfx : cell);
-          const double rr_ = (h.rp + (double)sa.cell_rmax[base + w]) * (1.0 + 1e-9);
-          return rr_ * rr_;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t s0 = (int64_t)blockIdx.x * blockDim.x + wbase; s0 < nact; s0 += stride) {
+    const int64_t s = s0 + lane;
+    int nr = 0;
+    int32_t c = 0;
+    bool large = false;
+    int cx = 0, cy = 0, cz = 0;
+    HomeRec hr;
+    if (s < nact) {
+      hr.inst = sa.sinst[s];
+      const InstDev &I = insts[hr.inst];
+      hr.s = (int32_t)s;
+      hr.xp = sa.sx[s]; hr.yp = sa.sy[s]; hr.zp = sa.sz[s]; hr.rp = sa.sr[s];
+      hr.bp = sa.sbox[s];
+      hr.pslot = sa.sorted[s];
+      hr.idp = sa.sid[s];
+      homes[t] = hr;
+      const int nfx = I.nfx, nfy = I.nfy, nfz = I.nfz;
+      const bool perx = I.periodicity != 0;
+      // the binning pass's own cell of this particle (same inputs, same function)
+      cx = cell_coord(hr.xp, I.hfx, nfx); cy = cell_coord(hr.yp, I.hfy, nfy); cz = cell_coord(hr.zp, I.hfz, nfz);
+      const int64_t lc = ((int64_t)cz * nfy + cy) * nfx + cx;
+      large = sa.spk[s].w < 0.f;
+      if (!large) {
+        // Small candidates have radius <= rcut, so only cells whose box comes within
+        // R = rp + rcut of this particle can hold a partner: rows and end cells farther
+        // away are skipped (distances to the neighbour boxes from the offsets inside the
+        // home cell, shortened by 1e-9 of the cell edge against rounding).
+        const double R = (hr.rp + I.rcut) * (1.0 + 1e-9), R2 = R * R;
+        const double fx = hr.xp - cx * I.hfx, fy = hr.yp - cy * I.hfy, fz = hr.zp - cz * I.hfz;
+        const double ex = 1e-9 * I.hfx, ey = 1e-9 * I.hfy, ez = 1e-9 * I.hfz;
+        const double dxl = fmax(fx - ex, 0.0), dxh = fmax(I.hfx - fx - ex, 0.0);
+        const double dyl = fmax(fy - ey, 0.0), dyh = fmax(I.hfy - fy - ey, 0.0);
+        const double dzh = fmax(I.hfz - fz - ez, 0.0);
+        auto add = [&](int32_t a0, int32_t a1) {
+          if (a1 > a0) {
+            rstart[t][nr] = a0;
+            rcum[t][nr] = c;
+            c += a1 - a0;
+            ++nr;
+          }
         };
-        const bool left_ok = (cx - 1 >= 0 || h.perx);
-        const bool right_ok = (cx + 1 < nfx || h.perx);
-        if (r > 0 && (!left_ok || dxl * dxl + dyz2 > R2 || dxl * dxl + dyz2 > reach2(cx - 1))) lo = cx;
-        const bool right = right_ok && dxh * dxh + dyz2 <= R2 && dxh * dxh + dyz2 <= reach2(cx + 1);
-        if (r > 0 && !right) hi = cx;
-        if (r > 0 && lo == cx && hi == cx && dyz2 > reach2(cx)) continue;
-        RowRanges rr = {0, 0, 0, 0};
-        if (r > 0 || right) rr = row_ranges(sa, base, nfx, lo, hi, h.perx);
-        if (r == 0) {
-          // home cell from s+1, contiguous with cell cx+1 when that is not wrapped
-          if (rr.a1 == 0 && rr.a0 == 0) rr.a1 = sa.cell_start[I.cell_begin + lc + 1];
-          rr.a0 = (int32_t)s + 1;
+        for (int r = 0; r < 5; ++r) {
+          int ry = cy, rz = cz, lo = cx - 1, hi = cx + 1;
+          double dyz2 = 0.0;
+          if (r == 0) {
+            lo = hi = cx + 1;                    // the rest of the home cell is taken below
+          } else if (r == 1) {
+            ry = wrap_cell(cy + 1, nfy);
+            dyz2 = dyh * dyh;
+          } else {
+            rz = wrap_cell(cz + 1, nfz);
+            ry = wrap_cell(cy + (r - 3), nfy);
+            const double dyb = (r == 2) ? dyl : (r == 4 ? dyh : 0.0);
+            dyz2 = dyb * dyb + dzh * dzh;
+          }
+          if (r > 0 && dyz2 > R2) continue;
+          const int64_t base = I.cell_begin + ((int64_t)rz * nfy + ry) * nfx;
+          // each end cell within reach of its own largest radius
+          auto reach2 = [&](int cell) {
+            const int w = cell < 0 ? cell + nfx : (cell >= nfx ? cell - nfx : cell);
+            const double rr_ = (hr.rp + (double)sa.cell_rmax[base + w]) * (1.0 + 1e-9);
+            return rr_ * rr_;
+          };
+          const bool left_ok = (cx - 1 >= 0 || perx);
+          const bool right_ok = (cx + 1 < nfx || perx);
+          if (r > 0 && (!left_ok || dxl * dxl + dyz2 > R2 || dxl * dxl + dyz2 > reach2(cx - 1))) lo = cx;
+          const bool right = right_ok && dxh * dxh + dyz2 <= R2 && dxh * dxh + dyz2 <= reach2(cx + 1);
+          if (r > 0 && !right) hi = cx;
+          if (r > 0 && lo == cx && hi == cx && dyz2 > reach2(cx)) continue;
+          RowRanges rr = {0, 0, 0, 0};
+          if (r > 0 || right) rr = row_ranges(sa, base, nfx, lo, hi, perx);
+          if (r == 0) {
+            // home cell from s+1, contiguous with cell cx+1 when that is not wrapped
+            if (rr.a1 == 0 && rr.a0 == 0) rr.a1 = sa.cell_start[I.cell_begin + lc + 1];
+            rr.a0 = (int32_t)s + 1;
+          }
+          add(rr.a0, rr.a1);
+          add(rr.b0, rr.b1);
         }
-        for (int32_t qs = rr.a0; qs < rr.a1; ++qs) search_candidate<false>(I, sa, h, qs, pairs, npairs, cap, st);
-        for (int32_t qs = rr.b0; qs < rr.b1; ++qs) search_candidate<false>(I, sa, h, qs, pairs, npairs, cap, st);
       }
-    } else {
+    }
+    rnum[t] = (int8_t)nr;
+    __syncwarp();
+    // the warp's candidate lists, concatenated in lane order
+    int32_t incl = c;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const int32_t v = __shfl_up_sync(kFull, incl, d);
+      if (lane >= d) incl += v;
+    }
+    const int32_t total = __shfl_sync(kFull, incl, 31);
+    const int32_t excl = incl - c;
+    for (int32_t base = 0; base < total; base += 32) {
+      const int32_t idx = base + lane;
+      // the last lane o whose list starts at or before idx owns it
+      int o = 0;
+#pragma unroll
+      for (int step = 16; step > 0; step >>= 1) {
+        const int32_t e = __shfl_sync(kFull, excl, (o + step) & 31);
+        if (o + step < 32 && e <= idx) o += step;
+      }
+      const int32_t eo = __shfl_sync(kFull, excl, o);
+      if (idx < total) {
+        const int to = wbase + o;
+        const int32_t k = idx - eo;
+        int j = 0;
+        const int no = rnum[to];
+        while (j + 1 < no && rcum[to][j + 1] <= k) ++j;
+        const int32_t q = rstart[to][j] + (k - rcum[to][j]);
+        const HomeRec ho = homes[to];
+        const InstDev &I = insts[ho.inst];
+        SearchHome h;
+        h.s = ho.s; h.xp = ho.xp; h.yp = ho.yp; h.zp = ho.zp; h.rp = ho.rp;
+        h.bp = ho.bp; h.pslot = ho.pslot; h.idp = ho.idp;
+        h.perx = I.periodicity != 0;
+        h.xpf = (float)h.xp; h.ypf = (float)h.yp; h.zpf = (float)h.zp; h.rpf = (float)h.rp;
+        h.lxf = (float)I.lx; h.lyf = (float)I.ly; h.lzf = (float)I.lz;
+        search_candidate<false>(I, sa, h, q, pairs, npairs, cap, st);
+      }
+    }
+    if (large) {
+      // a particle above the cut: every cell within its radius plus the largest radius
+      const InstDev &I = insts[hr.inst];
+      const int nfx = I.nfx, nfy = I.nfy, nfz = I.nfz;
+      SearchHome h;
+      h.s = hr.s; h.xp = hr.xp; h.yp = hr.yp; h.zp = hr.zp; h.rp = hr.rp;
+      h.bp = hr.bp; h.pslot = hr.pslot; h.idp = hr.idp;
+      h.perx = I.periodicity != 0;
+      h.xpf = (float)h.xp; h.ypf = (float)h.yp; h.zpf = (float)h.zp; h.rpf = (float)h.rp;
+      h.lxf = (float)I.lx; h.lyf = (float)I.ly; h.lzf = (float)I.lz;
       const double reach = (h.rp + I.rmax) * (1.0 + 1.0e-6);
       const int rx = (int)ceil(reach / I.hfx), ry = (int)ceil(reach / I.hfy), rz = (int)ceil(reach / I.hfz);
       const bool ally = 2 * ry + 1 >= nfy, allz = 2 * rz + 1 >= nfz;
@@ -474,6 +563,7 @@ __global__ void __launch_bounds__(256, GP_SEARCH_MIN_BLOCKS) k_search(const Inst
         }
       }
     }
+    __syncwarp();   // the records are rewritten by the warp's next 32 homes
   }
 }
 
