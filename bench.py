@@ -479,9 +479,9 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device(device))
 
-    # the autotuner's trials (60 one-step and 24 graph steps) and the three one-step graphs also
+    # the autotuner's trials (60 one-step and 72 graph steps) and the three one-step graphs also
     # move the particles before the state is restored, and the statistics timing adds 24 steps
-    run_steps = args.warmup + args.steps + args.e2e_steps + 90 + 28
+    run_steps = args.warmup + args.steps + args.e2e_steps + 138 + 28
     setup, f, st = build_inputs(w, device, precision, run_steps, rank, world)
     batched = isinstance(st, list)
     max_emaj = float(st["emaj"].max()) if not batched else None

@@ -485,8 +485,9 @@ __device__ __forceinline__ void gather_warp_fp32(const InstDev* __restrict__ ins
 // and id, so it may run while the collision phase updates velocities.  kMixed: every
 // instance holds an FP32 field (warp-cooperative gather); otherwise FP64 fields,
 // gathered per lane in the reference's summation order.
+// two blocks of 256 per SM: 128 registers, no spills (at three, 80 registers spill)
 #ifndef GP_GATHER_MIN_BLOCKS
-#define GP_GATHER_MIN_BLOCKS 3
+#define GP_GATHER_MIN_BLOCKS 2
 #endif
 template <bool kMixed>
 __global__ void __launch_bounds__(256, GP_GATHER_MIN_BLOCKS) k_gather(const InstDev* __restrict__ insts,

@@ -1596,18 +1596,28 @@ int gp_autotune(gp_ctx *c, int32_t *grids_out) {
     }
     c->tune[t] = best;
   }
-  // overlapped gather or not: whichever four-step graph is faster (median of three)
+  // Overlapped gather or not, timed as eight-step graphs (median of three), closer to
+  // the steady state than shorter graphs.  An overlapped gather only gets the SMs the
+  // contact solves leave, so it is also tried at the widest grid, whatever the one-step
+  // trials chose.
   if (!rc) {
-    float best_ms[2];
-    for (int o = 0; o < 2 && !rc; ++o) {
-      c->overlap = o == 1;
+    const int tuned = c->tune[GP_TUNE_GATHER];
+    const int gath[3] = {tuned, tuned, 148 * 16};
+    const bool over[3] = {false, true, true};
+    float best = 1e30f;
+    int pick = 0;
+    for (int k = 0; k < 3 && !rc; ++k) {
+      if (k == 2 && tuned == 148 * 16) break;
+      c->overlap = over[k];
+      c->tune[GP_TUNE_GATHER] = gath[k];
       drop_graph(c);
       float trial[3];
-      for (int r = 0; r < 3 && !rc; ++r) rc = gp_step_timed(c, 4, &trial[r], nullptr, nullptr);
+      for (int r = 0; r < 3 && !rc; ++r) rc = gp_step_timed(c, 8, &trial[r], nullptr, nullptr);
       std::sort(trial, trial + 3);
-      best_ms[o] = trial[1];
+      if (trial[1] < best) { best = trial[1]; pick = k; }
     }
-    c->overlap = !rc && best_ms[1] < best_ms[0];
+    c->overlap = over[pick];
+    c->tune[GP_TUNE_GATHER] = gath[pick];
   }
   drop_graph(c);
   if (!rc) {

@@ -12,9 +12,13 @@
 
 namespace gp {
 
-// One warp per block, at most 128 registers a thread: a block fits in the registers the
-// overlapped stencil gather leaves free on an SM (3 blocks of 256 threads at 80).
-__global__ void __launch_bounds__(32, 16) k_contact_tail(const PoolView *__restrict__ pv, const PairRec *__restrict__ pairs,
+// One warp per block, at most 128 registers a thread by default: a block then fits in the
+// registers the overlapped stencil gather leaves free on an SM (3 blocks of 256 threads
+// at 80).
+#ifndef GP_TAIL_MIN_BLOCKS
+#define GP_TAIL_MIN_BLOCKS 16
+#endif
+__global__ void __launch_bounds__(32, GP_TAIL_MIN_BLOCKS) k_contact_tail(const PoolView *__restrict__ pv, const PairRec *__restrict__ pairs,
                                const TailRec *__restrict__ tail, const unsigned long long *__restrict__ ntail,
                                int64_t cap_tail, CollRec *__restrict__ coll, unsigned long long *ncoll,
                                int64_t cap_coll, ContactStatRec *__restrict__ cst, unsigned long long *ncst,

@@ -287,9 +287,10 @@ enum {
     GP_NTUNE = 4
 };
 /* Autotuner: for each launch above, in turn, times one-step graphs of the resident
- * ensemble with 148 x {1,2,4,8,16} blocks and keeps the fastest; then times four-step
- * graphs with the next step's gather run on a second stream beside the contact solves
- * and without, and keeps the faster.  The particle state is saved first and restored
+ * ensemble with 148 x {1,2,4,8,16} blocks and keeps the fastest; then times eight-step
+ * graphs without and with the next step's gather run on a second stream beside the
+ * contact solves (the latter also with the gather at 148 x 16 blocks), and keeps the
+ * fastest.  The particle state is saved first and restored
  * afterwards.  grids_out: GP_NTUNE + 1 ints (the grids, then 1 if the gather is
  * overlapped) or NULL.  No counterpart in the reference. */
 int gp_autotune(gp_ctx *ctx, int32_t *grids_out);
