@@ -176,39 +176,69 @@ __device__ __forceinline__ void gather6_fp32(const InstDev& I, const Stencil& s,
 
 // ---------------------------------------------------------------------------
 // Mixed-precision force and torque: relative velocities and frames in FP64, the
-// Zastawny correlation coefficients in FP32, forces assembled in FP64.
+// Zastawny correlation coefficients in FP32, forces assembled in FP64.  The FP32
+// coefficients bound the relative error of every force and torque near 1e-7, so the
+// FP64 quotients here use the cheapest forms that stay far inside that: one
+// reciprocal per denominator, per-particle reciprocals of the constants (MixedConst),
+// and the body-frame flow shared by the force and the torque when both see the same
+// particle velocity (the first RK2 stage).
 // ---------------------------------------------------------------------------
-static __device__ __forceinline__ bool fluid_force_mixed(const PartConst& pc, double visc, double up, double vp,
-                                                  double wp, double uf, double vf, double wf, const double r[9],
-                                                  double f[3]) {
-  double p[3] = {uf - up, vf - vp, wf - wp};
-  const double umag = sqrt(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]);
+struct MixedConst {
+  double dv;              // deq / visc: particle Reynolds number per unit slip speed
+  double d2v;             // deq^2 / visc: rotational Reynolds number per unit spin
+  double rix, riy, riz;   // 1 / principal moments of inertia
+};
+
+__device__ __forceinline__ void mixed_const(const PartConst& pc, double visc, MixedConst& mc) {
+  mc.dv = pc.deq / visc;
+  mc.d2v = (pc.deq * pc.deq) / visc;
+  mc.rix = 1.0 / pc.ipxx;
+  mc.riy = 1.0 / pc.ipyy;
+  mc.riz = 1.0 / pc.ipzz;
+}
+
+// Slip velocity u_f - u_p in the body frame (R^T p), its magnitude, the magnitude of its
+// transverse part and the incidence angle phi = |atan(syz / b0)| in [0, pi/2].
+struct RelFlow {
+  double umag, b0, b1, b2, syz, inv_syz;
+  float lr, sphi, cphi;   // log2 of the particle Reynolds number, sin and cos of phi
+};
+
+static __device__ __forceinline__ void rel_flow(const MixedConst& mc, const double u[3], const double uf[3],
+                                                const double r[9], RelFlow& q) {
+  const double p0 = uf[0] - u[0], p1 = uf[1] - u[1], p2 = uf[2] - u[2];
+  q.umag = sqrt(p0 * p0 + p1 * p1 + p2 * p2);
+  q.b0 = r[0] * p0 + r[1] * p1 + r[2] * p2;
+  q.b1 = r[3] * p0 + r[4] * p1 + r[5] * p2;
+  q.b2 = r[6] * p0 + r[7] * p1 + r[8] * p2;
+  q.syz = sqrt(q.b1 * q.b1 + q.b2 * q.b2);
+  q.inv_syz = 1.0 / q.syz;   // used only where syz != 0
+  // atan2 of the magnitudes is |atan(syz / b0)|, pi/2 where b0 = 0
+  const float phi = atan2f((float)q.syz, fabsf((float)q.b0));
+  sincosf(phi, &q.sphi, &q.cphi);
+  q.cphi = fmaxf(q.cphi, 0.f);   // float(pi/2) lies above pi/2: keep cos(phi) >= 0 as in FP64
+  q.lr = __log2f((float)(q.umag * mc.dv));
+}
+
+static __device__ __forceinline__ bool fluid_force_mixed(const PartConst& pc, const RelFlow& q, const double r[9],
+                                                         double f[3]) {
   f[0] = f[1] = f[2] = 0.0;
-  if (umag == 0.0) return true;
-  // body frame: R^T p
-  const double b0 = r[0] * p[0] + r[1] * p[1] + r[2] * p[2];
-  const double b1 = r[3] * p[0] + r[4] * p[1] + r[5] * p[2];
-  const double b2 = r[6] * p[0] + r[7] * p[1] + r[8] * p[2];
-  const double syz = sqrt(b1 * b1 + b2 * b2);
-  const float rep = (float)((umag * pc.deq) / visc);
-  const float phi = fabsf(atanf((float)(syz / b0)));
-  float sphi, cphi;
-  sincosf(phi, &sphi, &cphi);
-  cphi = fmaxf(cphi, 0.f);   // float(pi/2) lies above pi/2: keep cos(phi) >= 0 as in FP64
-  const float lr = __log2f(rep);
+  if (q.umag == 0.0) return true;
+  const float lr = q.lr, sphi = q.sphi, cphi = q.cphi;
   const float cd0 = 18.12f * exp2f(-1.023f * lr) + 4.26f * exp2f(-0.384f * lr);
   const float cd90 = 21.52f * exp2f(-0.990f * lr) + 2.86f * exp2f(-0.260f * lr);
   const float cdrag = cd0 + (cd90 - cd0) * powf(sphi, 1.95f);
   const float clift = (0.083f * exp2f(0.21f * lr) + 1.582f * exp2f(-0.851f * lr)) *
                       powf(sphi, 1.842f - 0.802f * exp2f(-0.006f * lr)) *
                       powf(cphi, 0.874f + 0.009f * exp2f(0.570f * lr));
-  const double kd = pc.cdrag * (double)cdrag * umag;
-  const double kl = pc.cdrag * (double)clift * (umag * umag);
-  double fb0 = kd * b0 + kl * (double)sphi * copysign(1.0, -b0);
-  double fb1 = kd * b1, fb2 = kd * b2;
-  if (syz != 0.0) {
-    fb1 += kl * (double)cphi * (b1 / syz);
-    fb2 += kl * (double)cphi * (b2 / syz);
+  const double kd = pc.cdrag * (double)cdrag * q.umag;
+  const double kl = pc.cdrag * (double)clift * (q.umag * q.umag);
+  double fb0 = kd * q.b0 + kl * (double)sphi * copysign(1.0, -q.b0);
+  double fb1 = kd * q.b1, fb2 = kd * q.b2;
+  if (q.syz != 0.0) {
+    const double kc = kl * (double)cphi * q.inv_syz;
+    fb1 += kc * q.b1;
+    fb2 += kc * q.b2;
   }
   f[0] = r[0] * fb0 + r[3] * fb1 + r[6] * fb2;
   f[1] = r[1] * fb0 + r[4] * fb1 + r[7] * fb2;
@@ -216,38 +246,26 @@ static __device__ __forceinline__ bool fluid_force_mixed(const PartConst& pc, do
   return !(cdrag != cdrag) && isfinite(f[0]) && isfinite(f[1]) && isfinite(f[2]);
 }
 
-static __device__ __forceinline__ void fluid_torque_mixed(const PartConst& pc, double visc, double upn, double vpn,
-                                                   double wpn, double uf, double vf, double wf, double wx,
-                                                   double wy, double wz, double ox, double oy, double oz,
-                                                   const double r[9], double t[3]) {
-  const double p0 = uf - upn, p1 = vf - vpn, p2 = wf - wpn;
-  const double umag = sqrt(p0 * p0 + p1 * p1 + p2 * p2);
-  const double b0 = r[0] * p0 + r[1] * p1 + r[2] * p2;
-  const double b1 = r[3] * p0 + r[4] * p1 + r[5] * p2;
-  const double b2 = r[6] * p0 + r[7] * p1 + r[8] * p2;
-  const double syz = sqrt(b1 * b1 + b2 * b2);
-  const double c0 = r[0] * wx + r[1] * wy + r[2] * wz;
-  const double c1 = r[3] * wx + r[4] * wy + r[5] * wz;
-  const double c2 = r[6] * wx + r[7] * wy + r[8] * wz;
+static __device__ __forceinline__ void fluid_torque_mixed(const PartConst& pc, const MixedConst& mc, const RelFlow& q,
+                                                          const double wv[3], double ox, double oy, double oz,
+                                                          const double r[9], double t[3]) {
+  const double c0 = r[0] * wv[0] + r[1] * wv[1] + r[2] * wv[2];
+  const double c1 = r[3] * wv[0] + r[4] * wv[1] + r[5] * wv[2];
+  const double c2 = r[6] * wv[0] + r[7] * wv[1] + r[8] * wv[2];
   const double o0 = 0.5 * c0 - ox, o1 = 0.5 * c1 - oy, o2 = 0.5 * c2 - oz;
   const double omag = sqrt(o0 * o0 + o1 * o1 + o2 * o2);
   const double oyz = sqrt(o2 * o2 + o1 * o1);
   t[0] = t[1] = t[2] = 0.0;
-  if (umag != 0.0 && syz != 0.0) {
-    const float rep = (float)((umag * pc.deq) / visc);
-    const float lr = __log2f(rep);
-    const float phi = fabsf(atanf((float)(syz / b0)));
-    float sphi, cphi;
-    sincosf(phi, &sphi, &cphi);
-    cphi = fmaxf(cphi, 0.f);
+  if (q.umag != 0.0 && q.syz != 0.0) {
+    const float lr = q.lr, sphi = q.sphi, cphi = q.cphi;
     const float ctp = (0.935f * exp2f(-0.146f * lr) - 0.469f * exp2f(-0.145f * lr)) *
                       powf(sphi, 0.116f + 0.748f * exp2f(0.041f * lr)) *
                       powf(cphi, 0.221f + 0.657f * exp2f(0.044f * lr));
-    const double cp = pc.cpitch * (double)ctp * (umag * umag);
-    t[1] = cp * (fabs(b2) / syz) * copysign(1.0, b0 * b2);
-    t[2] = cp * (fabs(b1) / syz) * copysign(1.0, b0 * b1);
+    const double cp = pc.cpitch * (double)ctp * (q.umag * q.umag) * q.inv_syz;
+    t[1] = cp * fabs(q.b2) * copysign(1.0, q.b0 * q.b2);
+    t[2] = cp * fabs(q.b1) * copysign(1.0, q.b0 * q.b1);
   }
-  const double re_r = (omag * (pc.deq * pc.deq)) / visc;
+  const double re_r = omag * mc.d2v;
   if (re_r != 0.0) {
     const float lr = __log2f((float)re_r);
     const float ctr = 0.573f * exp2f(-0.154f * lr) + 116.61f / (float)re_r;
@@ -261,17 +279,25 @@ static __device__ __forceinline__ void fluid_torque_mixed(const PartConst& pc, d
 
 template <bool kMixed>
 struct Forces {
-  // F (lab frame, per unit mass) and T (body frame) for stage velocities.
-  __device__ __forceinline__ static bool eval(const PartConst& pc, double visc, const double u[3],
-                                              const double un[3], const double uf[3], const double wv[3],
-                                              double ox, double oy, double oz, const Quat& q, double f[3],
+  // F (lab frame, per unit mass) and T (body frame) for stage velocities: the force
+  // sees the stage velocity u, the torque the velocity un at the start of the step
+  // (same_u: u and un are the same values).  r = R(q) (mixed form only).
+  __device__ __forceinline__ static bool eval(const PartConst& pc, double visc, const MixedConst& mc,
+                                              const double u[3], const double un[3], bool same_u,
+                                              const double uf[3], const double wv[3], double ox, double oy,
+                                              double oz, const Quat& q, const double r[9], double f[3],
                                               double t[3]) {
     if (kMixed) {
-      double r[9];
-      rotmat(q, r);
-      const bool ok = fluid_force_mixed(pc, visc, u[0], u[1], u[2], uf[0], uf[1], uf[2], r, f);
-      fluid_torque_mixed(pc, visc, un[0], un[1], un[2], uf[0], uf[1], uf[2], wv[0], wv[1], wv[2], ox, oy, oz, r,
-                         t);
+      RelFlow qf;
+      rel_flow(mc, u, uf, r, qf);
+      const bool ok = fluid_force_mixed(pc, qf, r, f);
+      if (same_u) {
+        fluid_torque_mixed(pc, mc, qf, wv, ox, oy, oz, r, t);
+      } else {
+        RelFlow qt;
+        rel_flow(mc, un, uf, r, qt);
+        fluid_torque_mixed(pc, mc, qt, wv, ox, oy, oz, r, t);
+      }
       return ok;
     } else {
       double fd[3], fl[3], tp[3], tr[3];
@@ -284,18 +310,48 @@ struct Forces {
   }
 };
 
+// adv_particle_new.f90:305-307; the mixed form multiplies by the reciprocal moments.
+template <bool kMixed>
 __device__ __forceinline__ void k_omega(const double t[3], double ox, double oy, double oz, const PartConst& pc,
-                                        double k[3]) {
-  // adv_particle_new.f90:305-307
-  k[0] = (t[0] + oy * oz * (pc.ipyy - pc.ipzz)) / pc.ipxx;
-  k[1] = (t[1] + oz * ox * (pc.ipzz - pc.ipxx)) / pc.ipyy;
-  k[2] = (t[2] + ox * oy * (pc.ipxx - pc.ipyy)) / pc.ipzz;
+                                        const MixedConst& mc, double k[3]) {
+  if (kMixed) {
+    k[0] = (t[0] + oy * oz * (pc.ipyy - pc.ipzz)) * mc.rix;
+    k[1] = (t[1] + oz * ox * (pc.ipzz - pc.ipxx)) * mc.riy;
+    k[2] = (t[2] + ox * oy * (pc.ipxx - pc.ipyy)) * mc.riz;
+  } else {
+    k[0] = (t[0] + oy * oz * (pc.ipyy - pc.ipzz)) / pc.ipxx;
+    k[1] = (t[1] + oz * ox * (pc.ipzz - pc.ipxx)) / pc.ipyy;
+    k[2] = (t[2] + ox * oy * (pc.ipxx - pc.ipyy)) / pc.ipzz;
+  }
 }
 
-__device__ __forceinline__ void renorm(Quat& q) {
-  const double n = sqrt(q.a * q.a + q.b * q.b + q.c * q.c + q.d * q.d);
-  const double inv = 1.0 / n;
+// Quaternion step of adv_quaternion.f90:39-84 followed by renormalisation (mixed form).
+// r = R(q): the body-to-lab rotation that the stage's force evaluation already built.
+__device__ __forceinline__ void quaternion_step_mixed(Quat& q, const double r[9], double ox, double oy, double oz,
+                                                      double dt) {
+  const double om[3] = {ox, oy, oz};
+  double omg[3];
+  matvec(r, om, omg);
+  const double n2 = omg[0] * omg[0] + omg[1] * omg[1] + omg[2] * omg[2];
+  Quat map = {1.0, 0.0, 0.0, 0.0};
+  if (n2 != 0.0) {
+    const double inv = rsqrt(n2);
+    const double h = (n2 * inv) * dt * 0.5;
+    double s, c;
+    sincos(h, &s, &c);
+    const double si = s * inv;
+    map = {c, si * omg[0], si * omg[1], si * omg[2]};
+  }
+  q = mult_quat(map, q);
+  const double inv = rsqrt(q.a * q.a + q.b * q.b + q.c * q.c + q.d * q.d);
   q.a *= inv; q.b *= inv; q.c *= inv; q.d *= inv;
+}
+
+// One quaternion update; r = R(q) is used by the mixed form only.
+template <bool kMixed>
+__device__ __forceinline__ void quat_advance(Quat& q, const double r[9], double ox, double oy, double oz, double dt) {
+  if (kMixed) quaternion_step_mixed(q, r, ox, oy, oz, dt);
+  else quaternion_integration(q, ox, oy, oz, dt);
 }
 
 // One particle of adv_particle_new.f90:268-637.  State in/out in registers.
@@ -308,19 +364,24 @@ __device__ __forceinline__ int advance_particle(const InstDev& I, const PartCons
   const double rmax = fmax(pc.a, pc.b);
   const double un[3] = {U[0], U[1], U[2]};
   double f[3], t[3];
+  MixedConst mc;
+  double r0[9], r1[9];   // R(Q) and R(q1), mixed form only
+  if (kMixed) {
+    mixed_const(pc, I.visc, mc);
+    rotmat(Q, r0);
+  }
   int err = 0;
-  if (!Forces<kMixed>::eval(pc, I.visc, un, un, uf, wv, O[0], O[1], O[2], Q, f, t)) err = GP_ENAN_FORCE;
+  if (!Forces<kMixed>::eval(pc, I.visc, mc, un, un, true, uf, wv, O[0], O[1], O[2], Q, r0, f, t)) err = GP_ENAN_FORCE;
   if (O[0] != O[0] && !err) err = GP_ENAN_TORQUE;
   const double k1x[3] = {U[0], U[1], U[2]};
   const double k1u[3] = {f[0], f[1], f[2] + I.gravity};
   double k1o[3];
-  k_omega(t, O[0], O[1], O[2], pc, k1o);
+  k_omega<kMixed>(t, O[0], O[1], O[2], pc, mc, k1o);
   double xp1 = X[0] + dt * k1x[0], yp1 = X[1] + dt * k1x[1], zp1 = X[2] + dt * k1x[2];
   double u1[3] = {U[0] + dt * k1u[0], U[1] + dt * k1u[1], U[2] + dt * k1u[2]};
   double o1[3] = {O[0] + dt * k1o[0], O[1] + dt * k1o[1], O[2] + dt * k1o[2]};
   Quat q1 = Q;
-  quaternion_integration(q1, o1[0], o1[1], o1[2], dt);
-  if (kMixed) renorm(q1);
+  quat_advance<kMixed>(q1, r0, o1[0], o1[1], o1[2], dt);
   double wn[3], arm[3], delta_x = 0.0;
   bool isect;
   int rc = wall_test(I.lx, pc, rmax, xp1, yp1, zp1, q1, wn, arm, delta_x, isect);
@@ -343,15 +404,17 @@ __device__ __forceinline__ int advance_particle(const InstDev& I, const PartCons
       o1[i] = O[i] + (dt - delt) * k1o[i];
     }
     q1 = Q;
-    quaternion_integration(q1, o1[0], o1[1], o1[2], dt - delt);
-    if (kMixed) renorm(q1);
+    if (kMixed) rotmat(Q, r0);   // rebuilt here, so that R(Q) need not stay live on the common path
+    quat_advance<kMixed>(q1, r0, o1[0], o1[1], o1[2], dt - delt);
     rc = wall_rebound(I.ecw, I.muw, pc, u1[0], u1[1], u1[2], o1[0], o1[1], o1[2], q1, arm, wn);
     if (rc && !err) err = rc;
-    if (!Forces<kMixed>::eval(pc, I.visc, u1, un, uf, wv, o1[0], o1[1], o1[2], q1, f, t) && !err) err = GP_ENAN_FORCE;
+    if (kMixed) rotmat(q1, r1);
+    if (!Forces<kMixed>::eval(pc, I.visc, mc, u1, un, false, uf, wv, o1[0], o1[1], o1[2], q1, r1, f, t) && !err)
+      err = GP_ENAN_FORCE;
     if (o1[0] != o1[0] && !err) err = GP_ENAN_TORQUE;
     const double k2u[3] = {f[0], f[1], f[2] + I.gravity};
     double k2o[3];
-    k_omega(t, o1[0], o1[1], o1[2], pc, k2o);
+    k_omega<kMixed>(t, o1[0], o1[1], o1[2], pc, mc, k2o);
     X[0] = xp1 + (delt) * u1[0];
     X[1] = yp1 + (delt) * u1[1];
     X[2] = zp1 + (delt) * u1[2];
@@ -361,17 +424,18 @@ __device__ __forceinline__ int advance_particle(const InstDev& I, const PartCons
       O[i] = o1[i] + (delt) * k2o[i];
     }
     Q = q1;
-    quaternion_integration(Q, O[0], O[1], O[2], delt);
-    if (kMixed) renorm(Q);
+    quat_advance<kMixed>(Q, r1, O[0], O[1], O[2], delt);
     return err;
   }
   // unbounced second stage, adv_particle_new.f90:513-637
-  if (!Forces<kMixed>::eval(pc, I.visc, u1, un, uf, wv, o1[0], o1[1], o1[2], q1, f, t) && !err) err = GP_ENAN_FORCE;
+  if (kMixed) rotmat(q1, r1);
+  if (!Forces<kMixed>::eval(pc, I.visc, mc, u1, un, false, uf, wv, o1[0], o1[1], o1[2], q1, r1, f, t) && !err)
+    err = GP_ENAN_FORCE;
   if (o1[0] != o1[0] && !err) err = GP_ENAN_TORQUE;
   const double k2x[3] = {u1[0], u1[1], u1[2]};
   const double k2u[3] = {f[0], f[1], f[2] + I.gravity};
   double k2o[3];
-  k_omega(t, o1[0], o1[1], o1[2], pc, k2o);
+  k_omega<kMixed>(t, o1[0], o1[1], o1[2], pc, mc, k2o);
   const double xp2 = X[0] + 0.5 * dt * (k1x[0] + k2x[0]);
   const double yp2 = X[1] + 0.5 * dt * (k1x[1] + k2x[1]);
   const double zp2 = X[2] + 0.5 * dt * (k1x[2] + k2x[2]);
@@ -393,8 +457,7 @@ __device__ __forceinline__ int advance_particle(const InstDev& I, const PartCons
     }
   }
   Q = q1;
-  quaternion_integration(Q, O[0], O[1], O[2], dt);
-  if (kMixed) renorm(Q);
+  quat_advance<kMixed>(Q, r1, O[0], O[1], O[2], dt);
   return err;
 }
 
