@@ -49,7 +49,8 @@ def parse():
     ap.add_argument("--contact-tail", type=int, default=None,
                     help="evaluations after which a contact solve moves to the inlined-solver kernel (0: never)")
     ap.add_argument("--grids", default=None,
-                    help="gather,integrate,bin,search,overlap[,contact_tail]: fixed launch choices instead of autotuning")
+                    help="gather,integrate,bin,search,overlap[,contact_tail]: fixed launch choices instead of "
+                         "autotuning (overlap 0: none, 1: gather, 2: gather and speculative integrate)")
     ap.add_argument("--serve-seconds", type=float, default=2.0, help="arrival window of the serving workload")
     return ap.parse_args()
 
@@ -233,6 +234,16 @@ def cpu_sample(w, scale: int, max_emaj: float):
     g = po.OrcBoxGrid()
     po.lib().orc_collision_initiation(po.C.byref(po.make_setup(setup)), po.C.c_double(max_emaj), po.C.byref(g))
     return ens, refs, g
+
+
+def phase_note(tune) -> str:
+    """What the multi-step graph's phase times cover under the launch choices in use."""
+    if not tune or not tune.get("overlap_gather"):
+        return "one stream: each phase alone"
+    if tune.get("speculative_integrate"):
+        return ("gather and integrate of step s+1 (particles in none of step s's candidate pairs) overlap the "
+                "contact solves of step s on a second stream; 'integrate' times the pair members after the response")
+    return "gather of step s+1 overlaps the contact solves of step s (two streams in the graph)"
 
 
 def time_cpu(w, steps: int, threads: int, scale: int, max_emaj: float):
@@ -497,6 +508,7 @@ def main():
         g = [int(v) for v in args.grids.split(",")]
         tune = dict(zip(("gather", "integrate", "bin", "search"), g[:4]))
         tune["overlap_gather"] = bool(g[4]) if len(g) > 4 else False
+        tune["speculative_integrate"] = len(g) > 4 and g[4] == 2
         if len(g) > 5:
             tune["contact_tail"] = g[5]
         ctx.set_launch(tune)
@@ -629,7 +641,7 @@ def main():
                            "classes": len(st) if batched else 1},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": kps * args.steps,
                 "kernels_per_step": kps, "phase_ms": phases,
-                "phase_note": "gather of step s+1 overlaps the contact solves of step s (two streams in the graph)",
+                "phase_note": phase_note(tune),
                 "phase_ms_one_step_graphs": phases_alone,
                 "clocks": clocks, "fp64_plain": plain, "restart_io": restart_io, "stats": stats,
                 "live_fluid": live_fluid}

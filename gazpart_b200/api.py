@@ -310,13 +310,15 @@ class Context:
         check(_lib.lib().gp_autotune(self._h, g), "gp_autotune")
         out = dict(zip(_lib.TUNABLES, (int(v) for v in g)))
         out["overlap_gather"] = bool(g[len(_lib.TUNABLES)])
+        out["speculative_integrate"] = g[len(_lib.TUNABLES)] == 2
         out["contact_tail"] = self.contact_tail()
         return out
 
     def set_launch(self, grids: Dict[str, int]) -> None:
-        """Launch grids and overlap choice as autotune() reports them."""
-        g = (C.c_int32 * (len(_lib.TUNABLES) + 1))(*[int(grids[k]) for k in _lib.TUNABLES],
-                                                     int(bool(grids.get("overlap_gather", False))))
+        """Launch grids and overlap choices as autotune() reports them
+        (speculative_integrate implies overlap_gather)."""
+        over = 2 if grids.get("speculative_integrate", False) else int(bool(grids.get("overlap_gather", False)))
+        g = (C.c_int32 * (len(_lib.TUNABLES) + 1))(*[int(grids[k]) for k in _lib.TUNABLES], over)
         check(_lib.lib().gp_set_launch(self._h, g), "gp_set_launch")
         if "contact_tail" in grids:
             self.set_contact_tail(int(grids["contact_tail"]))

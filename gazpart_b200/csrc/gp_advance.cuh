@@ -595,12 +595,63 @@ __global__ void __launch_bounds__(256, GP_GATHER_MIN_BLOCKS) k_gather(const Inst
   }
 }
 
-// ADV_PARTICLE_ELLP, second half: particle perm[j] of the source buffer is advanced
-// and written to slot j of the destination buffer with its properties, id and
+// ADV_PARTICLE_ELLP, second half, for one particle: particle i of the source buffer is
+// advanced and written to slot j of the destination buffer with its properties, id and
 // instance (any permutation is correct: every particle carries its own record).  The
 // RK2 predictor/corrector with wall handling (adv_particle_new.f90:268-637) and
 // BOUNDARY_PARTICLE's periodic wrap (boundary_particle.f90:50-59).  A particle whose
 // stencil left the field (NaN fluid values, reported by the gather) is copied unchanged.
+template <bool kMixed>
+__device__ __forceinline__ void integrate_slot(const InstDev* __restrict__ insts, const PoolView* __restrict__ S,
+                                               const PoolView* __restrict__ D, int64_t i, int64_t j,
+                                               const double* const* __restrict__ fluid, Status* st) {
+  const int inst = S->inst[i];
+  D->inst[j] = inst;
+  D->id[j] = S->id[i];
+  PartConst pc;
+  load_pc(*S, i, pc);
+#pragma unroll 1
+  for (int c = 0; c < kNConst; ++c) D->pc[c][j] = S->pc[c][i];
+  double X[3] = {S->st[0][i], S->st[1][i], S->st[2][i]};
+  double U[3] = {S->st[3][i], S->st[4][i], S->st[5][i]};
+  Quat Q = {S->st[6][i], S->st[7][i], S->st[8][i], S->st[9][i]};
+  double O[3] = {S->st[10][i], S->st[11][i], S->st[12][i]};
+  const double uf[3] = {fluid[0][j], fluid[1][j], fluid[2][j]};
+  const double wv[3] = {fluid[3][j], fluid[4][j], fluid[5][j]};
+  // stencil out of range (reported by the gather): carried over unchanged
+  if (inst >= 0 && !(uf[0] != uf[0] && wv[0] != wv[0])) {
+    const InstDev& I = insts[inst];
+    const int err = advance_particle<kMixed>(I, pc, uf, wv, X, U, O, Q);
+    if (err) set_error(st, err, (long long)S->id[i], inst);
+    // adv_particle_new.f90:685-686: the channel wraps y and z only
+    // (boundary_particle_yz.f90:44-70), the others every direction when periodic
+    if (I.frozen_flow == 3) {
+      if (X[1] > I.ly) X[1] = X[1] - I.ly;
+      else if (X[1] < 0.) X[1] = X[1] + I.ly;
+      if (X[2] > I.lz) X[2] = X[2] - I.lz;
+      else if (X[2] < 0.) X[2] = X[2] + I.lz;
+    } else if (I.periodicity) {
+      if (X[0] > I.lx) X[0] = X[0] - I.lx;
+      if (X[0] < 0.) X[0] = X[0] + I.lx;
+      if (X[1] > I.ly) X[1] = X[1] - I.ly;
+      if (X[1] < 0.) X[1] = X[1] + I.ly;
+      if (X[2] > I.lz) X[2] = X[2] - I.lz;
+      if (X[2] < 0.) X[2] = X[2] + I.lz;
+    }
+  }
+  D->st[0][j] = X[0]; D->st[1][j] = X[1]; D->st[2][j] = X[2];
+  D->st[3][j] = U[0]; D->st[4][j] = U[1]; D->st[5][j] = U[2];
+  D->st[6][j] = Q.a; D->st[7][j] = Q.b; D->st[8][j] = Q.c; D->st[9][j] = Q.d;
+  D->st[10][j] = O[0]; D->st[11][j] = O[1]; D->st[12][j] = O[2];
+}
+
+// The pass over the pool: particle perm[j] of the source buffer goes to slot j of the
+// destination.  With mark non-null (the speculative pass, run while the previous step's
+// contact solves and response are still going) a particle that the last search marked
+// (it is in a candidate pair, so the response may still change its velocity) is left
+// alone: mark[i] receives j + 1 and k_integrate_fix advances it once the response is
+// done.  Unmarked particles are ones the response never touches, so both passes read
+// exactly the state a single pass after the response would read.
 #ifndef GP_INTEGRATE_MIN_BLOCKS
 #define GP_INTEGRATE_MIN_BLOCKS 4
 #endif
@@ -610,49 +661,36 @@ __global__ void __launch_bounds__(128, GP_INTEGRATE_MIN_BLOCKS) k_integrate(cons
                                                                            const PoolView* __restrict__ dst_pv,
                                                                            const int32_t* __restrict__ perm, int64_t n,
                                                                            const double* const* __restrict__ fluid,
-                                                                           Status* st) {
-  const PoolView* __restrict__ S = src_pv;
-  const PoolView* __restrict__ D = dst_pv;
+                                                                           uint32_t* __restrict__ mark, Status* st) {
   for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
     const int64_t i = perm[j];
-    const int inst = S->inst[i];
-    D->inst[j] = inst;
-    D->id[j] = S->id[i];
-    PartConst pc;
-    load_pc(*S, i, pc);
-#pragma unroll 1
-    for (int c = 0; c < kNConst; ++c) D->pc[c][j] = S->pc[c][i];
-    double X[3] = {S->st[0][i], S->st[1][i], S->st[2][i]};
-    double U[3] = {S->st[3][i], S->st[4][i], S->st[5][i]};
-    Quat Q = {S->st[6][i], S->st[7][i], S->st[8][i], S->st[9][i]};
-    double O[3] = {S->st[10][i], S->st[11][i], S->st[12][i]};
-    const double uf[3] = {fluid[0][j], fluid[1][j], fluid[2][j]};
-    const double wv[3] = {fluid[3][j], fluid[4][j], fluid[5][j]};
-    // stencil out of range (reported by the gather): carried over unchanged
-    if (inst >= 0 && !(uf[0] != uf[0] && wv[0] != wv[0])) {
-      const InstDev& I = insts[inst];
-      const int err = advance_particle<kMixed>(I, pc, uf, wv, X, U, O, Q);
-      if (err) set_error(st, err, (long long)S->id[i], inst);
-      // adv_particle_new.f90:685-686: the channel wraps y and z only
-      // (boundary_particle_yz.f90:44-70), the others every direction when periodic
-      if (I.frozen_flow == 3) {
-        if (X[1] > I.ly) X[1] = X[1] - I.ly;
-        else if (X[1] < 0.) X[1] = X[1] + I.ly;
-        if (X[2] > I.lz) X[2] = X[2] - I.lz;
-        else if (X[2] < 0.) X[2] = X[2] + I.lz;
-      } else if (I.periodicity) {
-        if (X[0] > I.lx) X[0] = X[0] - I.lx;
-        if (X[0] < 0.) X[0] = X[0] + I.lx;
-        if (X[1] > I.ly) X[1] = X[1] - I.ly;
-        if (X[1] < 0.) X[1] = X[1] + I.ly;
-        if (X[2] > I.lz) X[2] = X[2] - I.lz;
-        if (X[2] < 0.) X[2] = X[2] + I.lz;
-      }
+    if (mark != nullptr && mark[i] != 0u) {
+      mark[i] = (uint32_t)(j + 1);
+      continue;
     }
-    D->st[0][j] = X[0]; D->st[1][j] = X[1]; D->st[2][j] = X[2];
-    D->st[3][j] = U[0]; D->st[4][j] = U[1]; D->st[5][j] = U[2];
-    D->st[6][j] = Q.a; D->st[7][j] = Q.b; D->st[8][j] = Q.c; D->st[9][j] = Q.d;
-    D->st[10][j] = O[0]; D->st[11][j] = O[1]; D->st[12][j] = O[2];
+    integrate_slot<kMixed>(insts, src_pv, dst_pv, i, j, fluid, st);
+  }
+}
+
+// The rest of a speculative pass, after the response: every particle of the stored
+// candidate pairs (pairs[0, min(*npairs, cap))) that the search marked, once each (the
+// first lane to clear its mark takes it), into the slot the speculative pass recorded.
+// The marks are all zero again afterwards.
+template <bool kMixed>
+__global__ void __launch_bounds__(128, GP_INTEGRATE_MIN_BLOCKS) k_integrate_fix(const InstDev* __restrict__ insts,
+                                                                               const PoolView* __restrict__ src_pv,
+                                                                               const PoolView* __restrict__ dst_pv,
+                                                                               const PairRec* __restrict__ pairs,
+                                                                               const unsigned long long* npairs,
+                                                                               int64_t cap,
+                                                                               const double* const* __restrict__ fluid,
+                                                                               uint32_t* __restrict__ mark, Status* st) {
+  const int64_t np = (int64_t)min(*npairs, (unsigned long long)cap);
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < 2 * np; e += (int64_t)gridDim.x * blockDim.x) {
+    const PairRec& r = pairs[e >> 1];
+    const int64_t i = (e & 1) ? r.near : r.home;
+    const uint32_t v = atomicExch(&mark[i], 0u);
+    if (v != 0u) integrate_slot<kMixed>(insts, src_pv, dst_pv, i, (int64_t)v - 1, fluid, st);
   }
 }
 

@@ -152,6 +152,12 @@ struct gp_ctx {
   // gather of step s+1 on the side stream, overlapping step s's contact solves; the
   // autotuner keeps it only where it shortens the step
   bool overlap = false;
+  // with the overlap, step s+1's integrate also runs on the side stream, speculatively,
+  // for the particles in no candidate pair of step s; the rest follow after the response
+  // (d_mark: per pool slot, zero between steps; allocated while spec is on)
+  bool spec = false;
+  uint32_t *d_mark = nullptr;
+  int64_t cap_mark = 0;
   int contact_grid = 148 * 4;   // persistent k_contact grid (resident blocks)
   // statistics beside the step: polydisperse index of each particle per class slot
   // (device arrays by particle id, null = all 1), the fluid sample the last step left
@@ -232,7 +238,20 @@ void free_pool(gp_ctx *c) {
   dfree(c->sa.spk); dfree(c->sa.sex); dfree(c->sa.sey); dfree(c->sa.sez); dfree(c->sa.sa2); dfree(c->sa.sb2);
   dfree(c->d_best1); dfree(c->d_best2); dfree(c->d_matched);
   dfree(c->d_pairs); dfree(c->d_coll); dfree(c->d_state); dfree(c->d_acc);
+  dfree(c->d_mark);
+  c->cap_mark = 0;
   c->cap = 0;
+}
+
+// The speculative integrate's marks, one per pool slot, all zero.
+int ensure_mark(gp_ctx *c) {
+  if (c->cap_mark >= c->cap) return GP_OK;
+  dfree(c->d_mark);
+  c->cap_mark = 0;
+  GP_TRY(dalloc(&c->d_mark, (size_t)c->cap));
+  GP_CK(cudaMemsetAsync(c->d_mark, 0, (size_t)c->cap * sizeof(uint32_t), c->stream));
+  c->cap_mark = c->cap;
+  return GP_OK;
 }
 
 int alloc_pool(gp_ctx *c, int64_t cap) {
@@ -279,6 +298,7 @@ int alloc_pool(gp_ctx *c, int64_t cap) {
     GP_TRY(dalloc(&c->d_cst, (size_t)c->cap_pairs));
     c->cap_cst = c->cap_pairs;
   }
+  if (c->spec) GP_TRY(ensure_mark(c));
   return GP_OK;
 }
 
@@ -373,6 +393,35 @@ int enqueue_integrate(gp_ctx *c) {
   return mark(c, 2 * GP_PHASE_INTEGRATE + 1, c->stream);
 }
 
+// Speculative integrate of the next step on stream s (the side stream): the particles
+// the last search did not mark; no swap.
+int enqueue_integrate_spec(gp_ctx *c, cudaStream_t s) {
+  if (c->prm.precision == GP_PREC_MIXED)
+    launch_integrate_mixed(c->d_inst, c->d_pv, c->d_pv_alt, c->sa.sorted, c->n, c->d_fluid_cols, c->d_status,
+                           c->tune[GP_TUNE_INTEGRATE], s, c->d_mark);
+  else
+    launch_integrate_fp64(c->d_inst, c->d_pv, c->d_pv_alt, c->sa.sorted, c->n, c->d_fluid_cols, c->d_status,
+                          c->tune[GP_TUNE_INTEGRATE], s, c->d_mark);
+  GP_CK(cudaGetLastError());
+  return GP_OK;
+}
+
+// Its completion after the response: the marked particles, then the swap.  Timed as the
+// step's integrate phase.
+int enqueue_integrate_fix(gp_ctx *c) {
+  GP_TRY(mark(c, 2 * GP_PHASE_INTEGRATE, c->stream));
+  if (c->prm.precision == GP_PREC_MIXED)
+    launch_integrate_fix_mixed(c->d_inst, c->d_pv, c->d_pv_alt, c->d_pairs, c->d_counters + 0, c->cap_pairs,
+                               c->d_fluid_cols, c->d_mark, c->d_status, 148 * 4, c->stream);
+  else
+    launch_integrate_fix_fp64(c->d_inst, c->d_pv, c->d_pv_alt, c->d_pairs, c->d_counters + 0, c->cap_pairs,
+                              c->d_fluid_cols, c->d_mark, c->d_status, 148 * 4, c->stream);
+  GP_CK(cudaGetLastError());
+  c->n_slots = c->n;
+  c->fluid_ok = true;
+  return mark(c, 2 * GP_PHASE_INTEGRATE + 1, c->stream);
+}
+
 int enqueue_advance(gp_ctx *c) {
   GP_TRY(enqueue_gather(c, c->stream));
   return enqueue_integrate(c);
@@ -392,9 +441,10 @@ int enqueue_bin(gp_ctx *c) {
   return GP_OK;
 }
 
-// Binning and the candidate-pair search.
-int enqueue_bin_search(gp_ctx *c) {
+// Binning and the candidate-pair search; flag: mark the members of the stored pairs.
+int enqueue_bin_search(gp_ctx *c, bool flag = false) {
   SearchArrays sa = c->sa;
+  sa.mark = flag ? c->d_mark : nullptr;
   GP_TRY(mark(c, 2 * GP_PHASE_BIN, c->stream));
   GP_TRY(enqueue_bin(c));
   GP_TRY(mark(c, 2 * GP_PHASE_BIN + 1, c->stream));
@@ -439,18 +489,25 @@ int enqueue_collision(gp_ctx *c) {
 // changes only velocities and angular velocities, so the gather of step s+1, which
 // reads positions and the order of step s's binning, is forked onto the side stream
 // right after step s's search and overlaps its contact solves; step s+1's integrate
-// joins it.  marks: 2*GP_NPHASE timestamps per step, or null.
+// joins it.  With spec, step s+1's integrate of every particle outside step s's
+// candidate pairs (which the response cannot touch) follows the gather on the side
+// stream, and only the pair members are integrated after the join.  marks:
+// 2*GP_NPHASE timestamps per step, or null.
 int enqueue_steps(gp_ctx *c, int nsteps, cudaEvent_t *marks) {
   auto marks_of = [&](int s) { return marks ? marks + (size_t)s * 2 * GP_NPHASE : nullptr; };
+  const bool spec = c->overlap && c->spec && c->d_mark != nullptr && c->cap_mark >= c->cap && nsteps > 1;
   c->marks = marks_of(0);
-  int rc = enqueue_gather(c, c->stream);
+  int rc = GP_OK;
+  if (spec && cudaMemsetAsync(c->d_mark, 0, (size_t)c->cap * sizeof(uint32_t), c->stream) != cudaSuccess)
+    rc = GP_ECUDA;
+  if (!rc) rc = enqueue_gather(c, c->stream);
   for (int s = 0; s < nsteps && !rc; ++s) {
     c->marks = marks_of(s);
     if (s > 0 && c->overlap && cudaStreamWaitEvent(c->stream, c->ev_join, 0) != cudaSuccess) rc = GP_ECUDA;
     if (s > 0 && !c->overlap && !rc) rc = enqueue_gather(c, c->stream);
-    if (!rc) rc = enqueue_integrate(c);
-    if (!rc) rc = enqueue_bin_search(c);
+    if (!rc) rc = (s > 0 && spec) ? enqueue_integrate_fix(c) : enqueue_integrate(c);
     const bool fork = c->overlap && s + 1 < nsteps;
+    if (!rc) rc = enqueue_bin_search(c, spec && fork);
     if (!rc && fork && cudaEventRecord(c->ev_fork, c->stream) != cudaSuccess) rc = GP_ECUDA;
     // the contact kernel is captured first so that its persistent grid is resident
     // before the gather's blocks queue for the SMs it leaves as its queue drains
@@ -459,6 +516,7 @@ int enqueue_steps(gp_ctx *c, int nsteps, cudaEvent_t *marks) {
       if (cudaStreamWaitEvent(c->side, c->ev_fork, 0) != cudaSuccess) rc = GP_ECUDA;
       c->marks = marks_of(s + 1);
       if (!rc) rc = enqueue_gather(c, c->side);
+      if (!rc && spec) rc = enqueue_integrate_spec(c, c->side);
       c->marks = marks_of(s);
       if (!rc && cudaEventRecord(c->ev_join, c->side) != cudaSuccess) rc = GP_ECUDA;
     }
@@ -1557,8 +1615,11 @@ int gp_set_launch(gp_ctx *c, const int32_t *grids) {
   if (!c || !grids) return GP_EBADARG;
   for (int t = 0; t < GP_NTUNE; ++t)
     if (grids[t] < 1 || grids[t] > 148 * 64) return GP_EBADARG;
+  if (grids[GP_NTUNE] < 0 || grids[GP_NTUNE] > 2) return GP_EBADARG;
+  if (grids[GP_NTUNE] == 2) GP_TRY(ensure_mark(c));
   for (int t = 0; t < GP_NTUNE; ++t) c->tune[t] = grids[t];
   c->overlap = grids[GP_NTUNE] != 0;
+  c->spec = grids[GP_NTUNE] == 2;
   drop_graph(c);
   return GP_OK;
 }
@@ -1596,19 +1657,22 @@ int gp_autotune(gp_ctx *c, int32_t *grids_out) {
     }
     c->tune[t] = best;
   }
-  // Overlapped gather or not, timed as eight-step graphs (median of three), closer to
-  // the steady state than shorter graphs.  An overlapped gather only gets the SMs the
-  // contact solves leave, so it is also tried at the widest grid, whatever the one-step
-  // trials chose.
+  // Overlapped gather (and speculative integrate) or not, timed as eight-step graphs
+  // (median of three), closer to the steady state than shorter graphs.  Overlapped work
+  // only gets the SMs the contact solves leave, so it is also tried with the gather at
+  // the widest grid, whatever the one-step trials chose.
+  if (!rc) rc = ensure_mark(c);
   if (!rc) {
     const int tuned = c->tune[GP_TUNE_GATHER];
-    const int gath[3] = {tuned, tuned, 148 * 16};
-    const bool over[3] = {false, true, true};
+    const int gath[5] = {tuned, tuned, 148 * 16, tuned, 148 * 16};
+    const bool over[5] = {false, true, true, true, true};
+    const bool spec[5] = {false, false, false, true, true};
     float best = 1e30f;
     int pick = 0;
-    for (int k = 0; k < 3 && !rc; ++k) {
-      if (k == 2 && tuned == 148 * 16) break;
+    for (int k = 0; k < 5 && !rc; ++k) {
+      if ((k == 2 || k == 4) && tuned == 148 * 16) continue;
       c->overlap = over[k];
+      c->spec = spec[k];
       c->tune[GP_TUNE_GATHER] = gath[k];
       drop_graph(c);
       float trial[3];
@@ -1617,6 +1681,7 @@ int gp_autotune(gp_ctx *c, int32_t *grids_out) {
       if (trial[1] < best) { best = trial[1]; pick = k; }
     }
     c->overlap = over[pick];
+    c->spec = spec[pick];
     c->tune[GP_TUNE_GATHER] = gath[pick];
   }
   drop_graph(c);
@@ -1629,7 +1694,7 @@ int gp_autotune(gp_ctx *c, int32_t *grids_out) {
   c->fluid_ok = false;
   if (!rc && grids_out) {
     for (int t = 0; t < GP_NTUNE; ++t) grids_out[t] = c->tune[t];
-    grids_out[GP_NTUNE] = c->overlap ? 1 : 0;
+    grids_out[GP_NTUNE] = c->overlap ? (c->spec ? 2 : 1) : 0;
   }
   return rc;
 }

@@ -11,11 +11,15 @@ struct TailRec;   // gp_contact.cuh
 
 // --- gp_kernels_fp64.cu (FP64 path, -fmad=false) ---
 // ADV_PARTICLE_ELLP: advances particle perm[j] of *pv into slot j of *pv_alt, then swaps
-// the two views (so *pv is current afterwards).
+// the two views (so *pv is current afterwards).  With mark non-null, the speculative
+// pass: marked particles are left to launch_integrate_fix_*, which also swaps.
 void launch_gather_fp64(const InstDev *insts, const PoolView *pv, const int32_t *perm, int64_t n,
                       double *const *fluid, Status *st, int grid, cudaStream_t s);
 void launch_integrate_fp64(const InstDev *insts, PoolView *pv, PoolView *pv_alt, const int32_t *perm, int64_t n,
-                         double *const *fluid, Status *st, int grid, cudaStream_t s);
+                         double *const *fluid, Status *st, int grid, cudaStream_t s, uint32_t *mark = nullptr);
+void launch_integrate_fix_fp64(const InstDev *insts, PoolView *pv, PoolView *pv_alt, const PairRec *pairs,
+                             const unsigned long long *npairs, int64_t cap_pairs, double *const *fluid,
+                             uint32_t *mark, Status *st, int grid, cudaStream_t s);
 void launch_interp(const InstDev *inst, int comp, int64_t n, const double *x, const double *y, const double *z,
                    double *out, Status *st, cudaStream_t s);
 void launch_frozen_interp(const double *xain, const double *yain, const double *zain, int nx, int ny, int nz,
@@ -65,7 +69,10 @@ void launch_collision_stats(const CollRec *coll, const unsigned long long *ncoll
 void launch_gather_mixed(const InstDev *insts, const PoolView *pv, const int32_t *perm, int64_t n,
                       double *const *fluid, Status *st, int grid, cudaStream_t s);
 void launch_integrate_mixed(const InstDev *insts, PoolView *pv, PoolView *pv_alt, const int32_t *perm, int64_t n,
-                         double *const *fluid, Status *st, int grid, cudaStream_t s);
+                         double *const *fluid, Status *st, int grid, cudaStream_t s, uint32_t *mark = nullptr);
+void launch_integrate_fix_mixed(const InstDev *insts, PoolView *pv, PoolView *pv_alt, const PairRec *pairs,
+                             const unsigned long long *npairs, int64_t cap_pairs, double *const *fluid,
+                             uint32_t *mark, Status *st, int grid, cudaStream_t s);
 void launch_iota(int32_t *a, int64_t n, cudaStream_t s);
 
 // --- gp_search.cu ---

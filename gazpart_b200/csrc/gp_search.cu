@@ -238,8 +238,10 @@ void launch_bin_scatter(const InstDev *insts, const PoolView *pv, int64_t n, Sea
 // ---------------------------------------------------------------------------
 // 4. half-stencil sweep of the search grid, reference adjacency and order key
 // ---------------------------------------------------------------------------
+// mark (non-null when the next step's integrate runs speculatively): both particles of
+// a stored pair are flagged, since the response may change their velocities.
 __device__ __forceinline__ void emit_pair(PairRec *pairs, unsigned long long *npairs, int64_t cap, const PairRec &r,
-                                          Status *st) {
+                                          uint32_t *mark, Status *st) {
   cg::coalesced_group g = cg::coalesced_threads();
   unsigned long long base = 0;
   if (g.thread_rank() == 0) base = atomicAdd(npairs, (unsigned long long)g.size());
@@ -247,6 +249,10 @@ __device__ __forceinline__ void emit_pair(PairRec *pairs, unsigned long long *np
   const unsigned long long slot = base + g.thread_rank();
   if ((int64_t)slot < cap) {
     pairs[slot] = r;
+    if (mark != nullptr) {
+      mark[r.home] = 1u;
+      mark[r.near] = 1u;
+    }
   } else {
     atomicAdd(&st->overflow, 1ull);
     set_error(st, GP_EPAIR_OVERFLOW, (long long)r.home);
@@ -341,7 +347,7 @@ __device__ __forceinline__ void search_candidate(const InstDev &I, const SearchA
   r.near = home_is_p ? sa.sorted[qs] : h.pslot;
   r.k1 = ijk;
   r.k2 = ((unsigned long long)idh << 34) | ((unsigned long long)slot << 30) | (unsigned long long)idn;
-  emit_pair(pairs, npairs, cap, r, st);
+  emit_pair(pairs, npairs, cap, r, sa.mark, st);
 }
 
 __device__ __forceinline__ int wrap_cell(int c, int n) { return c < 0 ? c + n : (c >= n ? c - n : c); }

@@ -112,6 +112,7 @@ struct SearchArrays {
   long long *sbox;       // packed box coords (I0-1) | (J0-1)<<21 | (K0-1)<<42, -1 if outside
   int32_t *sinst;
   int32_t *sid;          // index of the particle within its instance
+  uint32_t *mark;        // per pool slot, non-null when the search flags pair members (speculative integrate)
   int64_t ncells;
 };
 

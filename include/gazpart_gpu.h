@@ -289,13 +289,15 @@ enum {
 /* Autotuner: for each launch above, in turn, times one-step graphs of the resident
  * ensemble with 148 x {1,2,4,8,16} blocks and keeps the fastest; then times eight-step
  * graphs without and with the next step's gather run on a second stream beside the
- * contact solves (the latter also with the gather at 148 x 16 blocks), and keeps the
- * fastest.  The particle state is saved first and restored
- * afterwards.  grids_out: GP_NTUNE + 1 ints (the grids, then 1 if the gather is
- * overlapped) or NULL.  No counterpart in the reference. */
+ * contact solves, the latter also with the next step's integrate of the particles in
+ * no candidate pair following the gather there (each also with the gather at 148 x 16
+ * blocks), and keeps the fastest.  The particle state is saved first and restored
+ * afterwards.  grids_out: GP_NTUNE + 1 ints (the grids, then 0: no overlap, 1: the
+ * gather overlapped, 2: the gather and the speculative integrate overlapped) or NULL.
+ * Every choice gives the same results bit for bit.  No counterpart in the reference. */
 int gp_autotune(gp_ctx *ctx, int32_t *grids_out);
-/* Sets the launch grids and the overlap choice directly (GP_NTUNE + 1 ints, as
- * gp_autotune reports them), e.g. to replay a tuned configuration. */
+/* Sets the launch grids and the overlap choice (0, 1 or 2) directly (GP_NTUNE + 1 ints,
+ * as gp_autotune reports them), e.g. to replay a tuned configuration. */
 int gp_set_launch(gp_ctx *ctx, const int32_t *grids);
 /* Last step's accepted collisions as (home, near) original indices, in acceptance
  * (list) order; *count receives the total even if it exceeds cap. */

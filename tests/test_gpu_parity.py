@@ -139,6 +139,30 @@ def test_mixed_precision_error_budget():
     assert np.quantile(err, 0.99) < 1e-5
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("name", ["dense", "bimodal"])
+def test_speculative_integrate_changes_nothing(name, precision):
+    """Step s+1's integrate run on the side stream beside step s's contact solves for
+    the particles in none of step s's candidate pairs, and after the response for the
+    pair members, gives the state of the plain order bit for bit: one six-step graph,
+    five of its steps speculative, against the same graph without any overlap and with
+    the gather alone overlapped."""
+    setup, fn, refs, st = case(name)
+    grids = {"gather": 296, "integrate": 592, "bin": 592, "search": 592}
+    out = {}
+    for mode in ("plain", "gather", "spec"):
+        with _ctx(setup, fn, st, precision) as ctx:
+            ctx.set_launch({**grids, "overlap_gather": mode != "plain", "speculative_integrate": mode == "spec"})
+            ctx.step(6)
+            ctx.raise_status()
+            out[mode] = (ctx.download(), ctx.collision_counters())
+    assert out["plain"][1]["accepted"] > 0
+    for mode in ("gather", "spec"):
+        assert out[mode][1] == out["plain"][1], mode
+        for k in api.STATE_KEYS:
+            assert np.array_equal(out[mode][0][k], out["plain"][0][k]), (mode, k)
+
+
 @pytest.mark.parametrize("name", ["dense", "bimodal"])
 def test_contact_tail_hand_over_changes_nothing(name):
     """Solves handed from the persistent contact kernel to the inlined-solver kernel
