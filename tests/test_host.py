@@ -1,6 +1,7 @@
-"""Host-side logic that needs no GPU: the C ABI library's exports, the workload
-conventions, the field generator, the particle initialiser and the replica timing
-reduction across ranks (gloo, two processes)."""
+"""Host-side logic that needs no GPU: the C ABI library's exports, the launch-choice
+mapping of the Python mirror, the workload conventions, the field generator, the
+particle initialiser and the replica timing reduction across ranks (gloo, two
+processes)."""
 from __future__ import annotations
 
 import ctypes as C
@@ -192,3 +193,45 @@ def test_serving_stream_and_concurrency_count():
     fake = [serving.Job(state={"x": np.zeros(1)}, steps=1, admitted_s=a, done_s=d)
             for a, d in ((0.0, 2.0), (1.0, 3.0), (2.5, 4.0), (5.0, 6.0))]
     assert serving.max_concurrent(fake) == 2
+
+
+class _FakeLaunchLib:
+    """Stands in for the library's launch entry points: records what gp_set_launch
+    receives and answers gp_autotune with a fixed choice."""
+
+    def __init__(self, choice):
+        self.choice, self.seen = choice, None
+
+    def gp_set_launch(self, h, g):
+        self.seen = [g[k] for k in range(len(_lib.TUNABLES) + 1)]
+        return 0
+
+    def gp_autotune(self, h, g):
+        for k, v in enumerate([148, 296, 592, 1184, self.choice]):
+            g[k] = v
+        return 0
+
+    def gp_set_contact_tail(self, h, b):
+        return 0
+
+    def gp_get_contact_tail(self, h, b):
+        return 0
+
+
+@pytest.mark.parametrize("choice", [0, 1, 2])
+def test_launch_choices_map_to_the_abi(monkeypatch, choice):
+    """gp_autotune's last value (0 no overlap, 1 gather overlapped, 2 gather and
+    speculative integrate) round-trips through autotune() and set_launch()."""
+    from gazpart_b200 import api
+    fake = _FakeLaunchLib(choice)
+    monkeypatch.setattr(_lib, "lib", lambda: fake)
+    ctx = object.__new__(api.Context)
+    ctx._h = None
+    got = ctx.autotune()
+    assert got["overlap_gather"] == (choice != 0)
+    assert got["speculative_integrate"] == (choice == 2)
+    ctx.set_launch(got)
+    assert fake.seen == [148, 296, 592, 1184, choice]
+    # the speculative integrate implies the overlap
+    ctx.set_launch({"gather": 148, "integrate": 148, "bin": 148, "search": 148, "speculative_integrate": True})
+    assert fake.seen[-1] == 2
