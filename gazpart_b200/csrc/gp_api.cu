@@ -254,6 +254,15 @@ int ensure_mark(gp_ctx *c) {
   return GP_OK;
 }
 
+// The marks are optional: where there is no room for them the speculative integrate
+// stays off.  A failed allocation also leaves its error as the runtime's last error,
+// which later launch checks would read, so it is cleared here.
+bool try_mark(gp_ctx *c) {
+  if (ensure_mark(c) == GP_OK) return true;
+  cudaGetLastError();
+  return false;
+}
+
 int alloc_pool(gp_ctx *c, int64_t cap) {
   free_pool(c);
   for (int b = 0; b < 2; ++b) {
@@ -298,7 +307,7 @@ int alloc_pool(gp_ctx *c, int64_t cap) {
     GP_TRY(dalloc(&c->d_cst, (size_t)c->cap_pairs));
     c->cap_cst = c->cap_pairs;
   }
-  if (c->spec) GP_TRY(ensure_mark(c));
+  if (c->spec && !try_mark(c)) c->spec = false;
   return GP_OK;
 }
 
@@ -1616,7 +1625,7 @@ int gp_set_launch(gp_ctx *c, const int32_t *grids) {
   for (int t = 0; t < GP_NTUNE; ++t)
     if (grids[t] < 1 || grids[t] > 148 * 64) return GP_EBADARG;
   if (grids[GP_NTUNE] < 0 || grids[GP_NTUNE] > 2) return GP_EBADARG;
-  if (grids[GP_NTUNE] == 2) GP_TRY(ensure_mark(c));
+  if (grids[GP_NTUNE] == 2 && !try_mark(c)) return GP_ENOMEM;
   for (int t = 0; t < GP_NTUNE; ++t) c->tune[t] = grids[t];
   c->overlap = grids[GP_NTUNE] != 0;
   c->spec = grids[GP_NTUNE] == 2;
@@ -1661,7 +1670,7 @@ int gp_autotune(gp_ctx *c, int32_t *grids_out) {
   // (median of three), closer to the steady state than shorter graphs.  Overlapped work
   // only gets the SMs the contact solves leave, so it is also tried with the gather at
   // the widest grid, whatever the one-step trials chose.
-  if (!rc) rc = ensure_mark(c);
+  const bool can_spec = !rc && try_mark(c);
   if (!rc) {
     const int tuned = c->tune[GP_TUNE_GATHER];
     const int gath[5] = {tuned, tuned, 148 * 16, tuned, 148 * 16};
@@ -1671,6 +1680,7 @@ int gp_autotune(gp_ctx *c, int32_t *grids_out) {
     int pick = 0;
     for (int k = 0; k < 5 && !rc; ++k) {
       if ((k == 2 || k == 4) && tuned == 148 * 16) continue;
+      if (spec[k] && !can_spec) continue;
       c->overlap = over[k];
       c->spec = spec[k];
       c->tune[GP_TUNE_GATHER] = gath[k];

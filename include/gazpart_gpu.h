@@ -297,7 +297,9 @@ enum {
  * Every choice gives the same results bit for bit.  No counterpart in the reference. */
 int gp_autotune(gp_ctx *ctx, int32_t *grids_out);
 /* Sets the launch grids and the overlap choice (0, 1 or 2) directly (GP_NTUNE + 1 ints,
- * as gp_autotune reports them), e.g. to replay a tuned configuration. */
+ * as gp_autotune reports them), e.g. to replay a tuned configuration.  Choice 2 needs
+ * 4 bytes of device memory per pool slot; without them it returns GP_ENOMEM (and the
+ * autotuner does not try it). */
 int gp_set_launch(gp_ctx *ctx, const int32_t *grids);
 /* Last step's accepted collisions as (home, near) original indices, in acceptance
  * (list) order; *count receives the total even if it exceeds cap. */
