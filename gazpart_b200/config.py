@@ -75,7 +75,7 @@ class Setup:
 
 @dataclasses.dataclass
 class ParticleSpec:
-    """How an ensemble's particles are drawn (BASELINE workload definitions)."""
+    """How an ensemble's particles are drawn (the benchmark workload definitions)."""
     n: int
     # aspect ratio: fixed value, or log-uniform range (lo, hi)
     ar: Optional[float] = None
