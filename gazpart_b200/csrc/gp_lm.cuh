@@ -64,7 +64,7 @@ __device__ __forceinline__ double lm_enorm(const double* x) {
 }
 
 // Trigonometric functions of the contact solve.  The reference calls libm's
-// sin/cos/asin/acos there; the kernels and the CPU checker use these functions
+// sin/cos/asin/acos there; the kernels and the oracle use these functions
 // (same constants, same operation order, compiled without contraction) so that their
 // Levenberg-Marquardt iterates agree bit for bit.  Method: Cody-Waite reduction by
 // pi/2 split into three parts and Taylor polynomials on [-pi/4, pi/4]; asin by its

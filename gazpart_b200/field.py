@@ -168,7 +168,7 @@ def channel(setup, x_in, ug_in, vorty_in, frozen_interp) -> Dict[str, torch.Tens
     NY, NZ >= NX and NX >= NY; other meshes are refused.
 
     frozen_interp(xain, yain, zain, uain, x, y, z) is FROZEN_INTERP_LAG3 with uain of
-    shape (NZA, NYA, NXA): the device's (Context.frozen_interp_lag3) or the checker's."""
+    shape (NZA, NYA, NXA): the device's (Context.frozen_interp_lag3) or the oracle's."""
     import numpy as np
     n = CHANNEL_POINTS
     nx, ny, nz = setup.nx, setup.ny, setup.nz

@@ -4,7 +4,7 @@
  *
  * Every entry point replaces one Fortran routine of the reference; the routine and
  * its file:line (relative to the reference's source/ directory) are given beside it.
- * A Fortran driver binds these through ISO_C_BINDING interfaces with the reference's
+ * A Fortran host program binds these through ISO_C_BINDING interfaces with the reference's
  * argument lists (scalars by VALUE, arrays by reference); the module-level inputs the
  * reference reads implicitly (VISC, RHOF, DTIME, EMAJ_PART, ...) live in the context.
  *

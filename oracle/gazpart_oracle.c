@@ -1,6 +1,6 @@
 /*
  * gazpart_oracle.c -- CPU restatement of GAZPART's frozen-flow ellipsoidal-particle
- * step.  TEST INFRASTRUCTURE ONLY (checker and timed CPU baseline); see the header.
+ * step.  TEST INFRASTRUCTURE ONLY (oracle and timed CPU baseline); see the header.
  *
  * PARITY UNPINNED against the reference binary (no Fortran compiler, no reference
  * tests or fixtures); pinned by analytic known-answer tests and a scipy MINPACK
@@ -1040,7 +1040,7 @@ double orc_enorm(int32_t n, const double *x) {
 
 /* ------------------------------------------------------------------------- */
 /* Trigonometric functions of the contact solve.  The reference calls libm's     */
-/* sin/cos/asin/acos there; this checker and the CUDA kernels both use the       */
+/* sin/cos/asin/acos there; this oracle and the CUDA kernels both use the       */
 /* functions below (same constants, same operation order, no contraction), so    */
 /* the Levenberg-Marquardt iterates of the two agree bit for bit.  The contact   */
 /* solve only resolves its angles to xtol = sqrt(eps), far above the one-ulp     */
@@ -1418,7 +1418,7 @@ static void lm_lmpar(double r[6], const int ipvt[2], const double diag[2], const
     *par = p;
 }
 
-/* lmder driver (minpack_reduc.f90:243-640 control flow). Returns info (1..8, with
+/* lmder control loop (minpack_reduc.f90:243-640 control flow). Returns info (1..8, with
  * lmder1's mapping of 8 to 4). */
 static int lm_lmder(const contact_prob *P, double x[2], double tol, int *nfev_out) {
     const double epsmch = DBL_EPSILON;

@@ -2,7 +2,7 @@
  * gazpart_oracle.h -- CPU restatement of GAZPART's frozen-flow ellipsoidal-particle
  * step (ADV_PARTICLE_ELLP followed by COLLISION), FP64, serial per particle.
  *
- * TEST INFRASTRUCTURE ONLY.  This library is the checker for the CUDA path and the
+ * TEST INFRASTRUCTURE ONLY.  This library is the oracle for the CUDA path and the
  * timed CPU baseline; it is never linked into, called by, or shipped with the product.
  *
  * PARITY UNPINNED against the reference itself: the reference is Fortran (no Fortran

@@ -1,6 +1,6 @@
 """CPU restatement of the reference's pseudo-spectral DNS step (numpy FFTs).
 
-TEST INFRASTRUCTURE ONLY: the checker of the device solver in
+TEST INFRASTRUCTURE ONLY: the oracle of the device solver in
 ``gazpart_b200/csrc/gp_dns.cu``; nothing in the product imports it.
 
 PARITY UNPINNED against the reference itself (its Fortran cannot be built here).  It is

@@ -1,4 +1,4 @@
-"""Seeded parity cases shared by the tests (small enough for the CPU checker)."""
+"""Seeded parity cases shared by the tests (small enough for the oracle)."""
 from __future__ import annotations
 
 import functools

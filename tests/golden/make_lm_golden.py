@@ -4,7 +4,7 @@ The reference solves the ellipsoid contact problem with a vendored copy of MINPA
 lmder (minpack_reduc.f90, called through lmder1 from ellipsoid_contact_detection.f90:92
 with ftol = xtol = sqrt(eps), gtol = 0, maxfev = 300).  scipy.optimize.leastsq wraps
 the same MINPACK routine.  This script restates the residual and Jacobian of
-ellipsoid_contact_detection.f90:193-334 in numpy (independently of the checker), runs
+ellipsoid_contact_detection.f90:193-334 in numpy (independently of the oracle), runs
 leastsq from the reference's initial guess, and records inputs and outputs.
 
 Run from the repository root:  python tests/golden/make_lm_golden.py

@@ -84,7 +84,7 @@ def _channel_state(s, f):
 
 
 @pytest.mark.gpu
-def test_channel_steps_match_checker():
+def test_channel_steps_match_oracle():
     s = _setup()
     x_in, ug, vorty = _profile()
     with api.Context(s, "fp64") as probe:

@@ -1,4 +1,4 @@
-"""Parity of the CUDA path (through the C ABI) with the CPU checker."""
+"""Parity of the CUDA path (through the C ABI) with the oracle."""
 from __future__ import annotations
 
 import numpy as np

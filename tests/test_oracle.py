@@ -1,4 +1,4 @@
-"""The CPU checker against known answers, invariants and golden MINPACK vectors.
+"""The oracle against known answers, invariants and golden MINPACK vectors.
 
 The reference ships no tests or fixtures; these pin the restatement instead (analytic
 results of the algebra it implements, the reference's own runtime invariants, and
@@ -229,7 +229,7 @@ def test_lm_matches_scipy_minpack_bitwise():
 
 def test_contact_golden_vectors():
     """Committed scipy/MINPACK solutions (numpy residual and Jacobian written
-    independently of the checker)."""
+    independently of the oracle)."""
     data = json.load(open(os.path.join(HERE, "golden", "lm_contact.json")))
     L = po.lib()
     L.orc_contact_lm.restype = C.c_int32

@@ -1,7 +1,7 @@
-"""Statistics beside the step on the device against the CPU checker.
+"""Statistics beside the step on the device against the oracle.
 
 STAT_PARTFLUID: the device sums each of the 35 quantities per polydisperse index over
-the class's particles.  The checker sums the same quantities in particle order from
+the class's particles.  The oracle sums the same quantities in particle order from
 the per-particle shape and density, while the device recovers APR, PMASS and RHOP from
 the pool's derived constants to a few units in the last place, and FP64 pow/atan/log
 differ in the last place between the device and the host.  So each sum must agree to
@@ -28,7 +28,7 @@ pytestmark = pytest.mark.gpu
 
 
 def _per_particle(ens, setup):
-    """[n, 36] per-particle STAT_PARTFLUID quantities from the checker."""
+    """[n, 36] per-particle STAT_PARTFLUID quantities from the oracle."""
     s = po.make_setup(setup)
     out = np.zeros((ens.n, 36))
     a = ens.a
@@ -45,7 +45,7 @@ def _per_particle(ens, setup):
 
 
 @pytest.mark.parametrize("name", ["c1", "poly"])
-def test_stat_partfluid_matches_checker(name):
+def test_stat_partfluid_matches_oracle(name):
     setup, fn, refs, st = case(name)
     n = st["x"].size
     idp = (np.arange(n) % 3 + 1).astype(np.int32)
@@ -86,7 +86,7 @@ def test_stat_partfluid_matches_checker(name):
 
 
 @pytest.mark.parametrize("name", ["dense", "poly"])
-def test_collision_stats_match_checker(name):
+def test_collision_stats_match_oracle(name):
     setup, fn, refs, st = case(name)
     n = st["x"].size
     idp = (np.arange(n) % 2 + 1).astype(np.int32)
