@@ -595,7 +595,7 @@ __global__ void __launch_bounds__(kMatchThreads) k_match(const CollRec *__restri
   for (int64_t e = threadIdx.x; e < nc; e += kMatchThreads) state[e] = 0;
   __syncthreads();
   bool done = (nc == 0);
-  int64_t round = 0;
+  int64_t pass = 0;
   while (!done) {
     for (int64_t e = threadIdx.x; e < nc; e += kMatchThreads) {
       if (state[e] != 0) continue;
@@ -615,7 +615,7 @@ __global__ void __launch_bounds__(kMatchThreads) k_match(const CollRec *__restri
       if (state[e] != 0) continue;
       const CollRec &r = coll[e];
       if (best1[r.home] == r.k1 && best2[r.home] == r.k2 && best1[r.near] == r.k1 && best2[r.near] == r.k2) {
-        state[e] = 3;   // accepted in this round
+        state[e] = 3;   // accepted in this pass
         matched[r.home] = 1;
         matched[r.near] = 1;
       }
@@ -646,10 +646,10 @@ __global__ void __launch_bounds__(kMatchThreads) k_match(const CollRec *__restri
       remaining = t;
     }
     __syncthreads();
-    ++round;
+    ++pass;
     done = (remaining == 0);
-    if (!done && round > nc + 1) {   // every round accepts at least one pair; cannot happen
-      if (threadIdx.x == 0) set_error(st, GP_ETIMEOUT, round);
+    if (!done && pass > nc + 1) {   // every pass accepts at least one pair; cannot happen
+      if (threadIdx.x == 0) set_error(st, GP_ETIMEOUT, pass);
       done = true;
     }
   }
