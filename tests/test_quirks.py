@@ -1,0 +1,127 @@
+"""Reference quirks that the oracle reproduces, one test each where the quirk can be
+isolated on the CPU.  The GPU parity tests hold the device path to the oracle bit for
+bit, so these behaviours carry over to it.
+
+Quirks covered elsewhere:
+- Q5 (DX = L/(N-1), index period N): test_oracle.test_interp_at_nodes_is_exact.
+- Q6 (vorticity ghosts read zero): test_host.test_reference_layout_ghosts.
+- Q7 (zero relative speed): test_oracle.test_force_guard_and_drag_direction.
+- Q13 (greedy COLOR order): test_oracle.test_serial_and_parallel_collision_agree.
+- Q16 (param.in against the reader): test_files.
+- Q18 (mirror boundary): test_oracle.test_frozen_interp_mirror_matches_interior."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+import pyoracle as po
+from gazpart_b200 import config, field
+
+L = 2.0 * np.pi
+
+
+def _quiet_field(s):
+    """Reference-layout arrays of a fluid at rest, for single-particle steps."""
+    z = torch.zeros(s.nz, s.ny, s.nx, dtype=torch.float64)
+    return [field.reference_layout(z, "periodic" if c < 3 else "zero").numpy().copy() for c in range(6)]
+
+
+def _one(s, emaj, apr, x, u, om, q=(1.0, 0.0, 0.0, 0.0), rhop=1000.0):
+    """A one-particle ensemble with the reference's per-particle constants."""
+    from gazpart_b200 import particles
+    st = particles.draw(config.ParticleSpec(n=1, ar=apr, b=emaj / apr, st=1.0, seed=3), s)
+    st["x"][0], st["y"][0], st["z"][0] = x
+    st["u"][0], st["v"][0], st["w"][0] = u
+    st["ox"][0], st["oy"][0], st["oz"][0] = om
+    st["qa"][0], st["qb"][0], st["qc"][0], st["qd"][0] = q
+    return po.Ensemble(s, st)
+
+
+def test_q1_wall_test_runs_in_a_periodic_box():
+    """Q1 (adv_particle_new.f90:331-336,555-560): the x = 0 and x = L planes are tested
+    even with PERIODICITY, so a particle closing on x = 0 rebounds instead of wrapping."""
+    s = config.Setup(nx=16, ny=16, nz=16, visc=0.05, dtime=1e-3, periodicity=True)
+    ens = _one(s, 0.05, 1.5, (0.0504, 3.0, 3.0), (-0.8, 0.0, 0.0), (0.0, 0.0, 0.0))
+    # the symmetry axis lies along x (q = 1), so the x extent is the major semi-axis and
+    # the predictor position crosses x = 0
+    assert 0.0504 - 1e-3 * 0.8 < ens.a["emaj"][0]
+    assert ens.advance(_quiet_field(s)) == 0
+    assert ens.a["u"][0] > 0.0                             # rebounded
+    assert 0.0 < ens.a["x"][0] < 1.0                       # not wrapped to x near L
+
+
+def _angle(q0, q1):
+    d = abs(float(np.dot(q0, q1)) / (np.linalg.norm(q0) * np.linalg.norm(q1)))
+    return 2.0 * np.arccos(min(d, 1.0))
+
+
+def test_q2_quaternion_advanced_twice_per_step():
+    """Q2 (adv_particle_new.f90:323-325,580-582,630-632): without a rebound the step
+    updates q with omega_1 after the predictor and again with omega_{n+1} from the
+    predicted q, so one step turns a spinning sphere by about 2 |omega| dt."""
+    s = config.Setup(nx=16, ny=16, nz=16, visc=0.05, dtime=1e-4)
+    om = np.array([0.0, 0.0, 40.0])
+    ens = _one(s, 0.05, 1.0, (3.0, 3.0, 3.0), (1e-3, 0.0, 0.0), om)
+    q0 = np.array([ens.a[k][0] for k in ("qa", "qb", "qc", "qd")])
+    assert ens.advance(_quiet_field(s)) == 0
+    q1 = np.array([ens.a[k][0] for k in ("qa", "qb", "qc", "qd")])
+    ratio = _angle(q0, q1) / (np.linalg.norm(om) * s.dtime)
+    assert abs(ratio - 2.0) < 0.01, ratio
+
+
+def test_q9_energy_check_stops_inelastic_collisions():
+    """Q9 (collision_response.f90:408-436): the response checks that kinetic energy is
+    conserved to 1e-9 %, so any restitution below 1 stops the run (GP_EENERGY)."""
+    ip = (1e-3, 1e-3, 1e-3)
+    q = np.array([1.0, 0.0, 0.0, 0.0])
+    n = np.array([1.0, 0.0, 0.0])
+    args = (ip, [1.0, 0, 0], [0, 0, 0], q, [-1.0, 0, 0], [0, 0, 0], q, [0.1, 0, 0], [-0.1, 0, 0], n)
+    elastic = config.Setup(nx=16, ny=16, nz=16, ecp=1.0, mup=0.0)
+    rc, u1, _, u2, _ = po.collision_response(elastic, *args)
+    assert rc == 0
+    assert np.allclose(u1, [-1.0, 0, 0]) and np.allclose(u2, [1.0, 0, 0])   # equal masses swap
+    inelastic = config.Setup(nx=16, ny=16, nz=16, ecp=0.9, mup=0.0)
+    rc, *_ = po.collision_response(inelastic, *args)
+    assert rc == 3                                          # GP_EENERGY
+
+
+def test_q10_box_edge_from_the_major_semi_axis():
+    """Q10 (collision_initiation.f90:50,69-75): DPMAX = 2 EMAJ and DXBOX =
+    L / int(L / (2 DPMAX)), whatever the aspect ratio, so for oblate particles (APR < 1,
+    b = EMAJ / APR > EMAJ) a box is narrower than two bounding diameters."""
+    s = config.Setup(nx=16, ny=16, nz=16)
+    g = po.OrcBoxGrid()
+    emaj = 0.1
+    po.lib().orc_collision_initiation(C.byref(po.make_setup(s)), C.c_double(emaj), C.byref(g))
+    assert g.nxbox == int(L / (4 * emaj)) == 15
+    assert g.dxbox == L / 15
+    b_oblate = emaj / 0.2
+    assert g.dxbox < 2 * (2 * b_oblate)
+
+
+def test_q15_no_quaternion_renormalisation():
+    """Q15 (adv_quaternion.f90:81): QUATERNION_INTEGRATION multiplies by a unit map
+    quaternion and does not renormalise, so whatever norm q has is kept (the mixed
+    form renormalises; the FP64 path keeps the reference's update)."""
+    q = np.array([0.6, 0.48, 0.64, 0.0])
+    q *= 1.1 / np.linalg.norm(q)
+    om = np.array([3.1, -7.3, 11.9])
+    for _ in range(100):
+        q = po.quaternion_integration(q, om, 1.7e-3)
+    assert abs(np.linalg.norm(q) - 1.1) < 1e-13
+
+
+def test_q19_x_equal_to_l_is_outside_the_box_grid():
+    """Q19 (boundary_particle.f90:50; collision_detection_connectivity.f90:81-89): the
+    wrap tests x > L strictly, so x == L stays, and its box index int(x / DXBOX) + 1 is
+    NXBOX + 1: out of the grid."""
+    s = config.Setup(nx=16, ny=16, nz=16)
+    st = {k: np.zeros(2) for k in po.STATE_KEYS + po.PROP_KEYS}
+    st["emaj"][:] = 0.05
+    st["apr"][:] = 1.0
+    ens = po.Ensemble(s, st)
+    g = ens.boxgrid()
+    rc, ijk = po.box_index(ens, g, x=[np.nextafter(L, 0.0), L], y=[1.0, 1.0], z=[1.0, 1.0])
+    assert rc == 6 and ijk[0] > 0 and ijk[1] == 0          # ORC_EOUT_OF_GRID for x == L
