@@ -101,6 +101,29 @@ def test_q10_box_edge_from_the_major_semi_axis():
     assert g.dxbox < 2 * (2 * b_oblate)
 
 
+def test_q14_nan_starting_angle_reports_no_contact():
+    """Q14 (ellipsoid_contact_detection.f90:77-87): the starting angles are
+    asin(n_z) and acos(n_x / cos(asin(n_z))).  For a centre line in the x-z plane
+    (n_y = 0) the ratio can round just above 1, acos gives NaN, every LM iterate stays
+    NaN until maxfev, and the pair is not in contact, however deep the overlap.  Just
+    out of that plane the same pairs are found in contact."""
+    q1 = np.array([1.0, 0.0, 0.0, 0.0])
+    q2 = np.array([0.9, 0.3, 0.2, 0.1])
+    q2 /= np.linalg.norm(q2)
+    nan_hits = 0
+    for t in np.linspace(0.05, 1.5, 200):
+        n = np.array([np.cos(t), 0.0, np.sin(t)])
+        r = po.contact_detection(0.05, 1.5, 0.05, 1.5, np.zeros(3), q1, -0.05 * n, q2)
+        if np.isnan(r["x"][0]):
+            nan_hits += 1
+            assert (r["flag"], r["info"], r["nfev"]) == (0, 5, 300)
+            m = np.array([np.cos(t), 1e-3, np.sin(t)])
+            m /= np.linalg.norm(m)
+            r2 = po.contact_detection(0.05, 1.5, 0.05, 1.5, np.zeros(3), q1, -0.05 * m, q2)
+            assert r2["flag"] == 1 and not np.isnan(r2["x"][0])
+    assert nan_hits > 10
+
+
 def test_q15_no_quaternion_renormalisation():
     """Q15 (adv_quaternion.f90:81): QUATERNION_INTEGRATION multiplies by a unit map
     quaternion and does not renormalise, so whatever norm q has is kept (the mixed
