@@ -71,6 +71,59 @@ def test_q2_quaternion_advanced_twice_per_step():
     assert abs(ratio - 2.0) < 0.01, ratio
 
 
+def _pair(s, dx):
+    """Two spheroids of different size (so different inertia) closing on each other."""
+    from gazpart_b200 import particles
+    a = particles.draw(config.ParticleSpec(n=1, ar=1.5, b=0.05 / 1.5, st=1.0, seed=3), s)
+    b = particles.draw(config.ParticleSpec(n=1, ar=2.0, b=0.08 / 2.0, st=1.0, seed=4), s)
+    st = {k: np.concatenate([a[k], b[k]]) for k in a}
+    st["x"][:] = [1.0, 1.0 + dx]
+    st["y"][:] = [1.0, 1.02]
+    st["z"][:] = [1.0, 1.01]
+    st["u"][:] = [0.5, -0.5]
+    st["v"][:] = 0.0
+    st["w"][:] = 0.0
+    for k in ("ox", "oy", "oz"):
+        st[k][:] = [0.3, -0.2]
+    q = np.array([[0.9, 0.3, 0.2, 0.1], [0.7, -0.1, 0.5, 0.3]])
+    q /= np.linalg.norm(q, axis=1)[:, None]
+    for c, k in enumerate(("qa", "qb", "qc", "qd")):
+        st[k][:] = q[:, c]
+    return st
+
+
+def test_q8_first_particles_inertia_for_both():
+    """Q8 (collision_response.f90:140-145): COLLISION_RESPONSE rotates particle 1's
+    principal moments for both bodies, so the collision of a small and a large spheroid
+    gives exactly the response computed with the home particle's inertia, not the
+    other's."""
+    s = config.Setup(nx=16, ny=16, nz=16, visc=0.05, dtime=1e-3)
+    ens = po.Ensemble(s, _pair(s, 0.06))
+    a = {k: v.copy() for k, v in ens.a.items()}
+    e1, e2, cn, r1, r2 = (np.zeros(3) for _ in range(5))
+    fl = C.c_int32()
+    hit = po.lib().orc_pair_eval(C.byref(po.make_setup(s)), C.byref(ens.props()), C.byref(ens.state()),
+                                 C.c_int64(0), C.c_int64(1), po.dptr(e1), po.dptr(e2), po.dptr(cn),
+                                 po.dptr(r1), po.dptr(r2), C.byref(fl))
+    assert hit == 1 and fl.value == 1
+    res = ens.collide(prefilter=True)
+    assert res["rc"] == 0 and list(res["home"]) == [0] and list(res["near"]) == [1]
+
+    def response(i):
+        ip = (a["ipxx"][i], a["ipyy"][i], a["ipzz"][i])
+        q = [np.array([a[k][j] for k in ("qa", "qb", "qc", "qd")]) for j in (0, 1)]
+        u = [np.array([a[k][j] for k in ("u", "v", "w")]) for j in (0, 1)]
+        o = [np.array([a[k][j] for k in ("ox", "oy", "oz")]) for j in (0, 1)]
+        return po.collision_response(s, ip, u[0], o[0], q[0], u[1], o[1], q[1], r1, r2, cn)
+
+    got = [np.array([ens.a[k][j] for k in ("u", "v", "w")]) for j in (0, 1)]
+    rc, u1, _, u2, _ = response(0)
+    assert rc == 0 and np.array_equal(got[0], u1) and np.array_equal(got[1], u2)
+    assert a["ipxx"][0] != a["ipxx"][1]
+    rc, v1, _, v2, _ = response(1)
+    assert not (np.array_equal(got[0], v1) and np.array_equal(got[1], v2))
+
+
 def test_q9_energy_check_stops_inelastic_collisions():
     """Q9 (collision_response.f90:408-436): the response checks that kinetic energy is
     conserved to 1e-9 %, so any restitution below 1 stops the run (GP_EENERGY)."""
