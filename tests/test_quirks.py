@@ -28,7 +28,7 @@ def _quiet_field(s):
     return [field.reference_layout(z, "periodic" if c < 3 else "zero").numpy().copy() for c in range(6)]
 
 
-def _one(s, emaj, apr, x, u, om, q=(1.0, 0.0, 0.0, 0.0), rhop=1000.0):
+def _one(s, emaj, apr, x, u, om, q=(1.0, 0.0, 0.0, 0.0)):
     """A one-particle ensemble with the reference's per-particle constants."""
     from gazpart_b200 import particles
     st = particles.draw(config.ParticleSpec(n=1, ar=apr, b=emaj / apr, st=1.0, seed=3), s)
@@ -69,6 +69,80 @@ def test_q2_quaternion_advanced_twice_per_step():
     q1 = np.array([ens.a[k][0] for k in ("qa", "qb", "qc", "qd")])
     ratio = _angle(q0, q1) / (np.linalg.norm(om) * s.dtime)
     assert abs(ratio - 2.0) < 0.01, ratio
+
+
+def _uniform_field(s, c):
+    """Reference-layout arrays of a uniform flow c, with zero vorticity."""
+    out = []
+    for k in range(6):
+        z = torch.full((s.nz, s.ny, s.nx), float(c[k]) if k < 3 else 0.0, dtype=torch.float64)
+        out.append(field.reference_layout(z, "periodic" if k < 3 else "zero").numpy().copy())
+    return out
+
+
+def test_q3_second_stage_torque_uses_the_old_velocity():
+    """Q3 (fluid_torque_ellipsoid.f90:88-105): in the corrector the force sees the
+    predicted velocity u_1, but the torque reads the particle's velocity from PART, the
+    step's u_n.  Rebuilding the spin update from the force and torque routines matches
+    the step with u_n in the second torque and not with u_1."""
+    s = config.Setup(nx=16, ny=16, nz=16, visc=0.05, dtime=5e-3)
+    un = np.array([0.2, -0.1, 0.05])
+    om = np.array([3.0, -2.0, 5.0])
+    q0 = np.array([0.9, 0.3, 0.2, 0.1])
+    q0 /= np.linalg.norm(q0)
+    ens = _one(s, 0.05, 2.5, (3.0, 3.0, 3.0), un, om, q=tuple(q0))
+    p = {k: ens.a[k][0] for k in ("emaj", "apr", "rhop", "ipxx", "ipyy", "ipzz")}
+    assert ens.advance(_uniform_field(s, (0.7, 0.4, -0.3))) == 0
+    uf = np.array([ens.a[k][0] for k in ("ufap", "vfap", "wfap")])
+    vort = np.zeros(3)
+    got = np.array([ens.a[k][0] for k in ("ox", "oy", "oz")])
+
+    def k_omega(t, o):
+        return np.array([(t[0] + o[1] * o[2] * (p["ipyy"] - p["ipzz"])) / p["ipxx"],
+                         (t[1] + o[2] * o[0] * (p["ipzz"] - p["ipxx"])) / p["ipyy"],
+                         (t[2] + o[0] * o[1] * (p["ipxx"] - p["ipyy"])) / p["ipzz"]])
+
+    def torque(u, o, q):
+        rc, tp, tr = po.fluid_torque(s, p["emaj"], p["apr"], p["rhop"], u, uf, vort, o, q)
+        assert rc == 0
+        return tp + tr
+
+    rc, fd, fl = po.fluid_force(s, p["emaj"], p["apr"], p["rhop"], un, uf, q0)
+    assert rc == 0
+    u1 = un + s.dtime * (fd + fl)
+    k1 = k_omega(torque(un, om, q0), om)
+    o1 = om + s.dtime * k1
+    q1 = po.quaternion_integration(q0, o1, s.dtime)
+    with_un = om + 0.5 * s.dtime * (k1 + k_omega(torque(un, o1, q1), o1))
+    with_u1 = om + 0.5 * s.dtime * (k1 + k_omega(torque(u1, o1, q1), o1))
+    scale = np.linalg.norm(om)
+    assert np.max(np.abs(got - with_un)) < 1e-13 * scale
+    assert np.max(np.abs(got - with_u1)) > 1e-10 * scale
+
+
+def test_q4_no_reinterpolation_at_the_predictor():
+    """Q4 (adv_particle_new.f90:68-72,139-228): the field is sampled once, at x_n, and
+    the corrector reuses it.  A particle whose predicted position crosses into the next
+    cell would read the x plane I0+3 if the field were sampled again there; changing
+    only that plane leaves the step bit for bit unchanged, while a particle already in
+    that cell sees the change."""
+    s = config.Setup(nx=16, ny=16, nz=16, visc=0.05, dtime=1e-3)
+    m = 7
+    x_below = m * s.dx - 1e-4                       # I0 = m; predictor at m*DX + 4e-4
+    base = _uniform_field(s, (0.3, 0.1, -0.2))
+    bumped = [f.copy() for f in base]
+    for c in range(3):
+        bumped[c][:, :, m + 2] += 1.0                # 1-based plane m + 3
+    out = {}
+    for name, fields in (("base", base), ("bumped", bumped)):
+        for tag, x in (("crossing", x_below), ("inside", m * s.dx + 1e-4)):
+            ens = _one(s, 0.05, 2.0, (x, 3.0, 3.0), (0.5, 0.0, 0.0), (1.0, -1.0, 0.5))
+            assert ens.advance(fields) == 0
+            out[name, tag] = {k: ens.a[k].copy() for k in po.STATE_KEYS}
+    assert out["base", "crossing"]["x"][0] > m * s.dx                  # the predictor did cross
+    for k in po.STATE_KEYS:
+        assert np.array_equal(out["base", "crossing"][k], out["bumped", "crossing"][k]), k
+    assert not np.array_equal(out["base", "inside"]["u"], out["bumped", "inside"]["u"])
 
 
 def _pair(s, dx):
