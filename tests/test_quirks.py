@@ -263,6 +263,24 @@ def test_q15_no_quaternion_renormalisation():
     assert abs(np.linalg.norm(q) - 1.1) < 1e-13
 
 
+def test_q17_random_field_mode_takes_the_frozen_flow_2_boundary():
+    """Q17 (adv_particle_new.f90:685-686): only FROZEN_FLOW 1-3 reach a boundary call,
+    so the random-field mode runs as FROZEN_FLOW = 2, whose BOUNDARY_PARTICLE wraps
+    every direction; the C ABI refuses FROZEN_FLOW 4 and above (it checks its arguments
+    before it touches the device)."""
+    import pytest
+    from gazpart_b200 import api
+    s = config.Setup(nx=16, ny=16, nz=16, visc=0.05, dtime=1e-3)
+    assert s.frozen_flow == 2
+    ens = _one(s, 0.02, 1.5, (3.0, 3.0, L - 1e-4), (0.0, 0.0, 0.5), (0.0, 0.0, 0.0))
+    assert ens.advance(_quiet_field(s)) == 0
+    assert 0.0 < ens.a["z"][0] < 1e-3                      # wrapped through z = L
+    for bad in (0, 4):
+        with pytest.raises(api.GPError) as e:
+            api.Context(config.Setup(nx=16, ny=16, nz=16, frozen_flow=bad))
+        assert e.value.code == 9                           # GP_EBADARG
+
+
 def test_q19_x_equal_to_l_is_outside_the_box_grid():
     """Q19 (boundary_particle.f90:50; collision_detection_connectivity.f90:81-89): the
     wrap tests x > L strictly, so x == L stays, and its box index int(x / DXBOX) + 1 is
