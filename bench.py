@@ -58,6 +58,13 @@ def parse():
 # ---------------------------------------------------------------------------
 # workload construction
 # ---------------------------------------------------------------------------
+# steps the autotuner moves the particles before it restores them (gp_autotune): one-step
+# graphs for each of the 4 launch grids at 5 sizes, 3 each; then eight-step graphs, 3 each,
+# for up to 5 overlap choices (none; the gather at two grids; the gather and the
+# speculative integrate at two grids)
+AUTOTUNE_STEPS = 4 * 5 * 3 + 5 * 3 * 8
+
+
 def x_margin_for(w, steps: int) -> float:
     """Distance from the x planes at which the run's particles start.
 
@@ -373,7 +380,8 @@ def run_serving(args, rank: int, world: int, local: int):
         with api.Context(setup, "mixed") as tmp:
             tmp.set_fields({k: fields[fid][k].contiguous() for k in api.FIELD_KEYS})
             for t, spec, steps in mine:
-                m = min(setup.lx / 4.0, 1.1 * 6.0 * w.dtime * steps)
+                # the largest job also carries the autotuner's trials before it leaves
+                m = min(setup.lx / 4.0, 1.1 * 6.0 * w.dtime * max(steps, AUTOTUNE_STEPS + 6))
                 st = particles.draw(dataclasses.replace(spec, x_margin=m), setup)
                 xs = [torch.from_numpy(st[k]).to(device) for k in ("x", "y", "z")]
                 g = [tmp.interp_lag3(c, *xs).cpu().numpy() for c in range(6)]
@@ -494,9 +502,10 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device(device))
 
-    # the autotuner's trials (60 one-step and 72 graph steps) and the three one-step graphs also
-    # move the particles before the state is restored, and the statistics timing adds 24 steps
-    run_steps = args.warmup + args.steps + args.e2e_steps + 138 + 28
+    # the autotuner's trials (4 launches x 5 grids x 3 one-step graphs, then up to 5 overlap
+    # choices x 3 eight-step graphs) and the three one-step graphs also move the particles
+    # before the state is restored, and the statistics timing adds 24 steps
+    run_steps = args.warmup + args.steps + args.e2e_steps + AUTOTUNE_STEPS + 6 + 28
     setup, f, st = build_inputs(w, device, precision, run_steps, rank, world)
     batched = isinstance(st, list)
     max_emaj = float(st["emaj"].max()) if not batched else None
