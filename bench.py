@@ -65,6 +65,16 @@ def parse():
 AUTOTUNE_STEPS = 4 * 5 * 3 + 5 * 3 * 8
 
 
+def volume_fraction(states, setup) -> float:
+    """Solid volume fraction of the drawn particles: each spheroid has the semi-axis EMAJ
+    along its axis and EMAJ / APR across it (calculate_ellipsoid_matrix.f90), so its
+    volume is (4/3) pi EMAJ (EMAJ / APR)^2; the sum over the box volume."""
+    import numpy as np
+    sts = states if isinstance(states, list) else [states]
+    v = sum(float(np.sum(4.0 / 3.0 * np.pi * s["emaj"] * (s["emaj"] / s["apr"]) ** 2)) for s in sts)
+    return v / (setup.lx * setup.ly * setup.lz)
+
+
 def x_margin_for(w, steps: int) -> float:
     """Distance from the x planes at which the run's particles start.
 
@@ -647,6 +657,7 @@ def main():
                                            else f"replicas x{world}"),
                            "l2": "inputs larger than L2 (state+field > 5 GB)",
                            "x_margin": x_margin_for(w, run_steps), "launch_grids": tune,
+                           "volume_fraction": None if (batched and world > 1) else volume_fraction(st, setup),
                            "classes": len(st) if batched else 1},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": kps * args.steps,
                 "kernels_per_step": kps, "phase_ms": phases,

@@ -235,3 +235,16 @@ def test_launch_choices_map_to_the_abi(monkeypatch, choice):
     # the speculative integrate implies the overlap
     ctx.set_launch({"gather": 148, "integrate": 148, "bin": 148, "search": 148, "speculative_integrate": True})
     assert fake.seen[-1] == 2
+
+
+def test_volume_fraction_known_answers():
+    """bench.volume_fraction: a sphere and a prolate and an oblate spheroid (semi-axes
+    EMAJ along the axis, EMAJ/APR across) in a unit box, and a list of classes."""
+    import bench
+    s = config.Setup(nx=8, ny=8, nz=8, lx=1.0, ly=1.0, lz=1.0)
+    one = {"emaj": np.array([0.1]), "apr": np.array([1.0])}
+    assert abs(bench.volume_fraction(one, s) - 4.0 / 3.0 * math.pi * 1e-3) < 1e-15
+    pro = {"emaj": np.array([0.2]), "apr": np.array([2.0])}       # semi-axes 0.2, 0.1, 0.1
+    obl = {"emaj": np.array([0.05]), "apr": np.array([0.5])}      # semi-axes 0.05, 0.1, 0.1
+    v = 4.0 / 3.0 * math.pi * (0.2 * 0.01 + 0.05 * 0.01)
+    assert abs(bench.volume_fraction([pro, obl], s) - v) < 1e-15
