@@ -515,7 +515,7 @@ def main():
     # the autotuner's trials (4 launches x 5 grids x 3 one-step graphs, then up to 5 overlap
     # choices x 3 eight-step graphs) and the three one-step graphs also move the particles
     # before the state is restored, and the statistics timing adds 24 steps
-    run_steps = args.warmup + args.steps + args.e2e_steps + AUTOTUNE_STEPS + 6 + 28
+    run_steps = args.warmup + args.steps + 2 * (args.e2e_steps + 1) + AUTOTUNE_STEPS + 6 + 28
     setup, f, st = build_inputs(w, device, precision, run_steps, rank, world)
     batched = isinstance(st, list)
     max_emaj = float(st["emaj"].max()) if not batched else None
@@ -601,9 +601,21 @@ def main():
     e2e_s = (time.perf_counter() - t0) / args.e2e_steps
     ctx.raise_status("e2e steps")
     bytes_state = 13 * 8 * n
+    serial = {"value": n / e2e_s, "unit": "particle-steps/s", "h2d_bytes_per_step": bytes_state,
+              "d2h_bytes_per_step": bytes_state, "ms_per_step": 1e3 * e2e_s,
+              "ms_parts": {k: 1e3 * v / args.e2e_steps for k, v in parts.items()},
+              "api": "gp_put_state + gp_step(1) + gp_download_state"}
+    # the same step as one call (gp_step_host): the copies overlap the step where the data
+    # allow; same bytes each way, same results bit for bit
+    ctx.step_host(pinned)
+    ctx.sync()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        ctx.step_host(pinned)
+    e2e_s = (time.perf_counter() - t0) / args.e2e_steps
+    ctx.raise_status("e2e one-call steps")
     e2e = {"value": n / e2e_s, "unit": "particle-steps/s", "h2d_bytes_per_step": bytes_state,
-           "d2h_bytes_per_step": bytes_state, "ms_per_step": 1e3 * e2e_s,
-           "ms_parts": {k: 1e3 * v / args.e2e_steps for k, v in parts.items()}}
+           "d2h_bytes_per_step": bytes_state, "ms_per_step": 1e3 * e2e_s, "api": "gp_step_host"}
 
     restart_io = None
     if rank == 0 and not batched and not args.no_io:
@@ -659,7 +671,8 @@ def main():
                            "x_margin": x_margin_for(w, run_steps), "launch_grids": tune,
                            "volume_fraction": None if (batched and world > 1) else volume_fraction(st, setup),
                            "classes": len(st) if batched else 1},
-                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": kps * args.steps,
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "e2e_put_step_download": serial,
+                "gpu_launches": kps * args.steps,
                 "kernels_per_step": kps, "phase_ms": phases,
                 "phase_note": phase_note(tune),
                 "phase_ms_one_step_graphs": phases_alone,

@@ -90,6 +90,7 @@ SIGNATURES = {
     "gp_upload_state": [_ctx, C.c_int64, C.POINTER(_vp), C.POINTER(_vp), C.c_int32],
     "gp_download_state": [_ctx, C.c_int64, C.POINTER(_vp), C.POINTER(_vp), C.c_int32],
     "gp_put_state": [_ctx, C.c_int64, C.POINTER(_vp), C.c_int32],
+    "gp_step_host": [_ctx, C.c_int64, C.POINTER(_vp), C.POINTER(_vp)],
     "gp_upload_classes": [_ctx, C.c_int32, _i64p, C.POINTER(_vp), C.POINTER(_vp), C.c_int32],
     "gp_autotune": [_ctx, _ip],
     "gp_set_launch": [_ctx, _ip],

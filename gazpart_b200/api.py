@@ -289,6 +289,24 @@ class Context:
             dev = d
         check(_lib.lib().gp_put_state(self._h, self.n, cols, dev), "gp_put_state")
 
+    def step_host(self, state: Dict[str, np.ndarray], out: Optional[Dict[str, np.ndarray]] = None
+                  ) -> Dict[str, np.ndarray]:
+        """One step of a host-resident ensemble (gp_step_host): the 13 state columns in
+        (caller order), one step, the state out into `out` (default: `state` itself), with
+        the copies overlapped with the step.  Arrays must be float64 and contiguous; pinned
+        memory lets the copies run asynchronously."""
+        out = state if out is None else out
+        for d in (state, out):
+            for k in STATE_KEYS:
+                a = d[k]
+                if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.c_contiguous
+                        and a.shape == (self.n,)):
+                    raise ValueError(f"{k}: expected a contiguous float64 array of {self.n} values")
+        cin = (C.c_void_p * 13)(*[C.c_void_p(state[k].ctypes.data) for k in STATE_KEYS])
+        cout = (C.c_void_p * 13)(*[C.c_void_p(out[k].ctypes.data) for k in STATE_KEYS])
+        check(_lib.lib().gp_step_host(self._h, self.n, cin, cout), "gp_step_host")
+        return out
+
     def download_into(self, out: Dict[str, np.ndarray]) -> None:
         """Download the state columns into preallocated (e.g. pinned) float64 arrays."""
         cols = (C.c_void_p * 13)(*[C.c_void_p(out[k].ctypes.data) for k in STATE_KEYS])

@@ -89,6 +89,8 @@ struct gp_ctx {
   // while the collision phase finishes on `stream`.
   cudaStream_t side = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // gp_step_host's copy/compute hand-offs (created on first use)
+  cudaEvent_t ev_host[5] = {};
   // phase begin/end timestamps of the step being captured by gp_step_timed
   // ([2p] begin, [2p+1] end of phase p; null otherwise)
   cudaEvent_t *marks = nullptr;
@@ -651,6 +653,8 @@ int gp_ctx_destroy(gp_ctx *c) {
   dfree(c->d_status); dfree(c->d_scratch);
   if (c->ev_fork) cudaEventDestroy(c->ev_fork);
   if (c->ev_join) cudaEventDestroy(c->ev_join);
+  for (auto &e : c->ev_host)
+    if (e) cudaEventDestroy(e);
   if (c->side) cudaStreamDestroy(c->side);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -1128,6 +1132,61 @@ int gp_put_state(gp_ctx *c, int64_t n, const double *const *cols, int32_t on_dev
   GP_CK(cudaGetLastError());
   GP_CK(cudaStreamSynchronize(c->stream));
   c->fluid_ok = false;
+  return GP_OK;
+}
+
+// One step of an ensemble held in host arrays: put the state, one step (ADV_PARTICLE_ELLP
+// + COLLISION, as gp_step(ctx, 1)), download it, with the copies overlapped with the
+// step where the data allow.  The gather reads only positions, so it starts once those
+// three columns are in; positions and quaternions are final after the integrate (the
+// response changes velocities and spins only), so they go out while the collision phase
+// runs.  The kernels and their order are those of put, step and download, so the
+// results are identical.  in_cols and out_cols may be the same arrays: every column is
+// in before any goes out.
+int gp_step_host(gp_ctx *c, int64_t n, const double *const *in_cols, double *const *out_cols) {
+  if (!c || !in_cols || !out_cols || n <= 0 || n != c->n || !c->grid_ready) return GP_EBADARG;
+  for (int k = 0; k < kNState; ++k)
+    if (!in_cols[k] || !out_cols[k]) return GP_EBADARG;
+  GP_TRY(ensure_scratch(c, (size_t)kNState * n));
+  for (auto &e : c->ev_host)
+    if (!e) GP_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  double *tmp = c->d_scratch;
+  const size_t bytes = (size_t)n * sizeof(double);
+  cudaEvent_t *ev = c->ev_host;
+  // the copies wait for whatever the stream still does with the scratch buffer
+  GP_CK(cudaEventRecord(ev[0], c->stream));
+  GP_CK(cudaStreamWaitEvent(c->side, ev[0], 0));
+  for (int k = 0; k < kNState; ++k) {
+    GP_CK(cudaMemcpyAsync(tmp + (size_t)k * n, in_cols[k], bytes, cudaMemcpyHostToDevice, c->side));
+    if (k == 2) GP_CK(cudaEventRecord(ev[1], c->side));   // x, y, z are in
+  }
+  GP_CK(cudaEventRecord(ev[2], c->side));                 // every column is in
+  GP_CK(cudaStreamWaitEvent(c->stream, ev[1], 0));
+  launch_scatter_state(c->d_inst, c->d_pv, c->n_slots, tmp, n, c->stream, kColsPos);
+  GP_CK(cudaGetLastError());
+  GP_TRY(enqueue_gather(c, c->stream));
+  GP_CK(cudaStreamWaitEvent(c->stream, ev[2], 0));
+  launch_scatter_state(c->d_inst, c->d_pv, c->n_slots, tmp, n, c->stream, kAllStateCols & ~kColsPos);
+  GP_CK(cudaGetLastError());
+  GP_TRY(enqueue_integrate(c));
+  launch_gather_state(c->d_inst, c->d_pv, c->n_slots, -1, tmp, c->d_fluid_cols, nullptr, n, c->stream,
+                      kColsPosQuat);
+  GP_CK(cudaGetLastError());
+  GP_CK(cudaEventRecord(ev[3], c->stream));
+  GP_TRY(enqueue_collision(c));
+  launch_gather_state(c->d_inst, c->d_pv, c->n_slots, -1, tmp, c->d_fluid_cols, nullptr, n, c->stream,
+                      kColsVelSpin);
+  GP_CK(cudaGetLastError());
+  GP_CK(cudaEventRecord(ev[4], c->stream));
+  GP_CK(cudaStreamWaitEvent(c->side, ev[3], 0));
+  for (int k = 0; k < kNState; ++k)
+    if ((kColsPosQuat >> k) & 1u)
+      GP_CK(cudaMemcpyAsync(out_cols[k], tmp + (size_t)k * n, bytes, cudaMemcpyDeviceToHost, c->side));
+  GP_CK(cudaStreamWaitEvent(c->side, ev[4], 0));
+  for (int k = 0; k < kNState; ++k)
+    if ((kColsVelSpin >> k) & 1u)
+      GP_CK(cudaMemcpyAsync(out_cols[k], tmp + (size_t)k * n, bytes, cudaMemcpyDeviceToHost, c->side));
+  GP_CK(cudaStreamSynchronize(c->side));
   return GP_OK;
 }
 

@@ -88,11 +88,17 @@ void launch_match(const CollRec *coll, const unsigned long long *ncoll, int64_t 
                   unsigned long long *best2, int8_t *matched, int8_t *state, Status *st, cudaStream_t s);
 void launch_field_layout(void *dst, int prec, int nx, int ny, int nz, int ncomp, int comp, const double *src,
                          int src_layout, int ghost_mode, cudaStream_t s);
+// state columns as bits (x y z u v w qa qb qc qd ox oy oz = bits 0..12)
+constexpr unsigned kAllStateCols = (1u << kNState) - 1u;
+constexpr unsigned kColsPosQuat = 0x3C7u;    // x y z qa qb qc qd: final once the integrate is done
+constexpr unsigned kColsVelSpin = 0x1C38u;   // u v w ox oy oz: the response may still change them
+constexpr unsigned kColsPos = 0x7u;          // x y z: all the gather reads
 void launch_gather_state(const InstDev *insts, const PoolView *pv, int64_t n, int only, double *out,
-                         double *const *fluid_cols, double *fluid_out, int64_t count, cudaStream_t s);
+                         double *const *fluid_cols, double *fluid_out, int64_t count, cudaStream_t s,
+                         unsigned cols = kAllStateCols);
 void launch_retire(const PoolView *pv, int64_t n, int inst, cudaStream_t s);
 void launch_scatter_state(const InstDev *insts, const PoolView *pv, int64_t n, const double *cols,
-                          int64_t count, cudaStream_t s);
+                          int64_t count, cudaStream_t s, unsigned mask = kAllStateCols);
 void launch_init_pool(const PoolView *pv, int64_t begin, int64_t n, int inst, const double *cols,
                       const double *pcs, int64_t ld, int64_t src, cudaStream_t s);
 void launch_connectivity(int nxb, int nyb, int nzb, int periodicity, int32_t *ncon, int32_t *con, cudaStream_t s);

@@ -710,13 +710,12 @@ void launch_field_layout(void *dst, int prec, int nx, int ny, int nz, int ncomp,
                                                  src_layout, ghost_mode);
 }
 
-// Pool -> caller order for one instance: out[c*count + id] = state column c.
 // Pool -> caller order: out[c*count + begin(class) + id] = state column c, where the
 // caller's arrays hold the classes one after another; with only >= 0, class `only`
-// alone at offset 0.
+// alone at offset 0.  Only the columns whose bit is set in `cols` are written.
 __global__ void k_gather_state(const InstDev *__restrict__ insts, const PoolView *__restrict__ pv, int64_t n,
                                int only, double *__restrict__ out, double *const *fluid, double *__restrict__ fout,
-                               int64_t count) {
+                               int64_t count, unsigned cols) {
   const PoolView P = *pv;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const int inst = P.inst[i];
@@ -724,7 +723,8 @@ __global__ void k_gather_state(const InstDev *__restrict__ insts, const PoolView
     const int64_t id = (only >= 0 ? 0 : insts[inst].begin) + P.id[i];
     if (id < 0 || id >= count) continue;
 #pragma unroll
-    for (int c = 0; c < kNState; ++c) out[c * count + id] = P.st[c][i];
+    for (int c = 0; c < kNState; ++c)
+      if ((cols >> c) & 1u) out[c * count + id] = P.st[c][i];
     if (fout != nullptr && fluid != nullptr) {
 #pragma unroll
       for (int c = 0; c < kNFluid; ++c) fout[c * count + id] = fluid[c][i];
@@ -733,9 +733,10 @@ __global__ void k_gather_state(const InstDev *__restrict__ insts, const PoolView
 }
 
 void launch_gather_state(const InstDev *insts, const PoolView *pv, int64_t n, int only, double *out,
-                         double *const *fluid_cols, double *fluid_out, int64_t count, cudaStream_t s) {
+                         double *const *fluid_cols, double *fluid_out, int64_t count, cudaStream_t s,
+                         unsigned cols) {
   const int grid = 148 * 8;
-  k_gather_state<<<grid, 256, 0, s>>>(insts, pv, n, only, out, fluid_cols, fluid_out, count);
+  k_gather_state<<<grid, 256, 0, s>>>(insts, pv, n, only, out, fluid_cols, fluid_out, count, cols);
 }
 
 // Retires class `inst`: its particles leave the binning, and the next advance drops them.
@@ -749,9 +750,9 @@ void launch_retire(const PoolView *pv, int64_t n, int inst, cudaStream_t s) {
   if (n > 0) k_retire<<<148 * 8, 256, 0, s>>>(pv, n, inst);
 }
 
-// caller order -> pool (state columns only)
+// caller order -> pool (state columns only; those whose bit is set in `mask`)
 __global__ void k_scatter_state(const InstDev *__restrict__ insts, const PoolView *__restrict__ pv, int64_t n,
-                                const double *__restrict__ cols, int64_t count) {
+                                const double *__restrict__ cols, int64_t count, unsigned mask) {
   const PoolView P = *pv;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const int inst = P.inst[i];
@@ -759,13 +760,14 @@ __global__ void k_scatter_state(const InstDev *__restrict__ insts, const PoolVie
     const int64_t id = insts[inst].begin + P.id[i];
     if (id < 0 || id >= count) continue;
 #pragma unroll
-    for (int c = 0; c < kNState; ++c) P.st[c][i] = cols[c * count + id];
+    for (int c = 0; c < kNState; ++c)
+      if ((mask >> c) & 1u) P.st[c][i] = cols[c * count + id];
   }
 }
 
 void launch_scatter_state(const InstDev *insts, const PoolView *pv, int64_t n, const double *cols, int64_t count,
-                          cudaStream_t s) {
-  k_scatter_state<<<148 * 8, 256, 0, s>>>(insts, pv, n, cols, count);
+                          cudaStream_t s, unsigned mask) {
+  k_scatter_state<<<148 * 8, 256, 0, s>>>(insts, pv, n, cols, count, mask);
 }
 
 // One class into pool slots [begin, begin+n): particle k of the class is column entry

@@ -248,6 +248,16 @@ int gp_serve(gp_ctx *ctx, gp_job *jobs, int32_t njobs, double hbm_budget, double
  * order.  The drop-in form of handing PART back to the device after host-side edits. */
 int gp_put_state(gp_ctx *ctx, int64_t n, const double *const *cols, int32_t on_device);
 
+/* One time step of an ensemble held in host memory, in one call: in_cols (the 13 state
+ * columns, caller order) in, one ADV_PARTICLE_ELLP + COLLISION as gp_step(ctx, 1), the
+ * state out to out_cols.  The results are those of gp_put_state, gp_step(ctx, 1) and
+ * gp_download_state in turn, bit for bit; the copies overlap the step where the data
+ * allow (the gather starts once the positions are in; positions and quaternions go out
+ * during the collision phase).  in_cols and out_cols may be the same arrays.  The
+ * reference's main loop with PART on the host (main.f90:496-509) maps to one call per
+ * cycle. */
+int gp_step_host(gp_ctx *ctx, int64_t n, const double *const *in_cols, double *const *out_cols);
+
 /* ---------------------------------------------------------------- hot path ---- */
 /* ADV_PARTICLE_ELLP(NCYCLE)  adv_particle_new.f90:7-704: interpolation of the six
  * fields at x_n, RK2 predictor/corrector with wall handling, BOUNDARY_PARTICLE's
