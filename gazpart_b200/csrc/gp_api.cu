@@ -475,7 +475,7 @@ int enqueue_contact_response(gp_ctx *c) {
                  c->cap_coll, c->d_counters + 3, cst, c->d_counters + 4, c->cap_cst, tail, c->d_counters + 5,
                  c->cap_tail, c->tail_budget, c->d_status, c->contact_grid, c->stream);
   if (tail)
-    launch_contact_tail(c->d_pv, c->d_pairs, tail, c->d_counters + 5, c->cap_tail, c->d_coll, c->d_counters + 1,
+    launch_contact_tail(c->d_inst, c->d_pv, c->d_pairs, tail, c->d_counters + 5, c->cap_tail, c->d_coll, c->d_counters + 1,
                         c->cap_coll, cst, c->d_counters + 4, c->cap_cst, c->d_status, c->stream);
   GP_TRY(mark(c, 2 * GP_PHASE_CONTACT + 1, c->stream));
   GP_TRY(mark(c, 2 * GP_PHASE_RESPONSE, c->stream));

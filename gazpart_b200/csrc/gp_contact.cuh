@@ -1,35 +1,67 @@
-// gp_contact.cuh -- what follows a finished contact solve (collision_interaction.f90:
-// 240-348), shared by the persistent contact kernel and the kernel that finishes the
-// long solves it hands over.
+// gp_contact.cuh -- one candidate pair of collision_interaction.f90:216-348: its
+// geometry, and what follows a finished contact solve.  Shared by the persistent contact
+// kernel and the kernel that finishes the long solves it hands over.
 #pragma once
 
 #include "gp_lm.cuh"
 
 namespace gp {
 
-// A solve handed from k_contact to k_contact_tail: the pair, its problem and the
-// solver's state between two lm_step calls.
+// A solve handed from k_contact to k_contact_tail: the pair and the solver's state
+// between two lm_step calls (the problem itself is rebuilt from the pool).
 struct TailRec {
   int64_t e;                 // index of the pair in the candidate list
-  ContactProb CP;
   LmState S;
+};
+
+// The pair's bodies as the contact test sees them (collision_interaction.f90:216-249):
+// HOME at its position, NEAR at the minimum image, orientations and semi-axes.
+struct PairBodies {
+  double c1[3], c2[3];
   Quat q1, q2;
   double a1, b1, a2, b2;
 };
 
-// The solve of pair e has returned: contact test, contact-point velocities, NVREL,
-// the contact record for the statistics and the colliding-pair record.
-__device__ __forceinline__ void finish_pair(const PoolView &P, const PairRec *__restrict__ pairs, int64_t e,
-                                            const ContactProb &CP, const LmState &S, const Quat &q1,
-                                            const Quat &q2, double a1, double b1, double a2, double b2,
-                                            CollRec *__restrict__ coll, unsigned long long *ncoll,
-                                            int64_t cap_coll, ContactStatRec *__restrict__ cst,
-                                            unsigned long long *ncst, int64_t cap_cst, Status *st) {
+__device__ __forceinline__ void pair_bodies(const InstDev *__restrict__ insts, const PoolView &P, int i1, int i2,
+                                            PairBodies &B) {
+  const InstDev &I = insts[P.inst[i1]];
+  const double x1 = P.st[0][i1], y1 = P.st[1][i1], z1 = P.st[2][i1];
+  double vkx = P.st[0][i2] - x1, vky = P.st[1][i2] - y1, vkz = P.st[2][i2] - z1;
+  if ((fabs(vkx) > I.lx / 2) && I.periodicity) vkx = vkx - copysign(I.lx, vkx);
+  if (fabs(vky) > I.ly / 2.) vky = vky - copysign(I.ly, vky);
+  if (fabs(vkz) > I.lz / 2.) vkz = vkz - copysign(I.lz, vkz);
+  B.c1[0] = x1; B.c1[1] = y1; B.c1[2] = z1;
+  B.c2[0] = x1 + vkx; B.c2[1] = y1 + vky; B.c2[2] = z1 + vkz;
+  B.q1 = {P.st[6][i1], P.st[7][i1], P.st[8][i1], P.st[9][i1]};
+  B.q2 = {P.st[6][i2], P.st[7][i2], P.st[8][i2], P.st[9][i2]};
+  B.a1 = P.pc[0][i1]; B.b1 = P.pc[1][i1]; B.a2 = P.pc[0][i2]; B.b2 = P.pc[1][i2];
+}
+
+// The solve of pair e has returned at angles (x0, x1) after nfev evaluations: contact
+// test, contact-point velocities, NVREL, the contact record for the statistics and the
+// colliding-pair record.  Out of line and given only the pair index and the solver's
+// result, so that the solving loop never passes its state by address: the problem is
+// rebuilt from the pool, which the contact phase does not change, by the same set-up
+// (hence to the same values).
+static __device__ __noinline__ void finish_pair(const InstDev *__restrict__ insts, const PoolView *__restrict__ pv,
+                                         const PairRec *__restrict__ pairs, int64_t e, double x0, double x1,
+                                         int nfev, CollRec *__restrict__ coll, unsigned long long *ncoll,
+                                         int64_t cap_coll, ContactStatRec *__restrict__ cst,
+                                         unsigned long long *ncst, int64_t cap_cst, Status *st) {
+  const PoolView P = *pv;
   atomicAdd(&st->n_solve, 1ull);
-  atomicAdd(&st->n_eval, (unsigned long long)S.nfev);
-  atomicMax(&st->max_eval, (unsigned long long)S.nfev);
+  atomicAdd(&st->n_eval, (unsigned long long)nfev);
+  atomicMax(&st->max_eval, (unsigned long long)nfev);
+  const PairRec pr = pairs[e];
+  const int i1 = pr.home, i2 = pr.near;
+  PairBodies B;
+  pair_bodies(insts, P, i1, i2, B);
+  ContactProb CP;
+  double xs[2];
+  contact_setup(B.a1, B.b1, B.a2, B.b2, B.c1, B.q1, B.c2, B.q2, CP, xs);
+  const double x[2] = {x0, x1};
   double ept1[3], ept2[3], cn[3];
-  if (!contact_finish(a1, b1, a2, b2, q1, q2, CP, S.x, ept1, ept2, cn)) return;
+  if (!contact_finish(B.a1, B.b1, B.a2, B.b2, B.q1, B.q2, CP, x, ept1, ept2, cn)) return;
   atomicAdd(&st->n_contact, 1ull);
   // overlap depth |EPT1 - EPT2| for the collision statistics, while the points are at hand
   double depth = 0.0;
@@ -37,18 +69,16 @@ __device__ __forceinline__ void finish_pair(const PoolView &P, const PairRec *__
     const double v0 = ept1[0] - ept2[0], v1 = ept1[1] - ept2[1], v2 = ept1[2] - ept2[2];
     depth = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
   }
-  const PairRec pr = pairs[e];
-  const int i1 = pr.home, i2 = pr.near;
-  const double x1 = CP.b1[0], y1 = CP.b1[1], z1 = CP.b1[2];
-  double rx1[3] = {(ept1[0] - x1), (ept1[1] - y1), (ept1[2] - z1)};
+  const double xh = CP.b1[0], yh = CP.b1[1], zh = CP.b1[2];
+  double rx1[3] = {(ept1[0] - xh), (ept1[1] - yh), (ept1[2] - zh)};
   double om1[3] = {P.st[10][i1], P.st[11][i1], P.st[12][i1]};
-  rot_vec(q1, om1);
+  rot_vec(B.q1, om1);
   const double up1 = P.st[3][i1] + (om1[1] * rx1[2] - om1[2] * rx1[1]);
   const double vp1 = P.st[4][i1] + (om1[2] * rx1[0] - om1[0] * rx1[2]);
   const double wp1 = P.st[5][i1] + (om1[0] * rx1[1] - om1[1] * rx1[0]);
   double rx2[3] = {(ept2[0] - CP.b2[0]), (ept2[1] - CP.b2[1]), (ept2[2] - CP.b2[2])};
   double om2[3] = {P.st[10][i2], P.st[11][i2], P.st[12][i2]};
-  rot_vec(q2, om2);
+  rot_vec(B.q2, om2);
   const double up2 = P.st[3][i2] + (om2[1] * rx2[2] - om2[2] * rx2[1]);
   const double vp2 = P.st[4][i2] + (om2[2] * rx2[0] - om2[0] * rx2[2]);
   const double wp2 = P.st[5][i2] + (om2[0] * rx2[1] - om2[1] * rx2[0]);

@@ -5,7 +5,7 @@
 #include <math_constants.h>
 
 #include "gp_advance.cuh"
-#include "gp_contact.cuh"
+#include "gp_lm.cuh"
 #include "gp_launch.h"
 
 namespace gp {
@@ -121,127 +121,6 @@ void launch_frozen_interp(const double *xain, const double *yain, const double *
   k_frozen_interp<<<grid, 256, 0, s>>>(xain, yain, zain, nx, ny, nz, uain, n, x, y, z, out, st);
 }
 
-// collision_interaction.f90:216-348 for every candidate pair: minimum image, contact
-// (ellipsoid_contact_detection), contact-point velocities, NVREL.  Colliding pairs
-// (flag && NVREL < ZERO) are appended.  Persistent warps with lane refill: a lane whose
-// Levenberg-Marquardt solve has returned finishes its pair and takes the next one from
-// a global queue, so warps do not idle on their slowest pair.
-#ifndef GP_CONTACT_MIN_BLOCKS
-#ifdef GP_LM_INLINE
-#define GP_CONTACT_MIN_BLOCKS 2
-#else
-#define GP_CONTACT_MIN_BLOCKS 8
-#endif
-#endif
-
-__global__ void __launch_bounds__(128, GP_CONTACT_MIN_BLOCKS) k_contact(const InstDev *__restrict__ insts,
-                                                    const PoolView *__restrict__ pv,
-                                                    const PairRec *__restrict__ pairs,
-                                                    const unsigned long long *__restrict__ npairs, int64_t cap_pairs,
-                                                    CollRec *__restrict__ coll, unsigned long long *ncoll,
-                                                    int64_t cap_coll, unsigned long long *queue,
-                                                    ContactStatRec *__restrict__ cst, unsigned long long *ncst,
-                                                    int64_t cap_cst, TailRec *__restrict__ tail,
-                                                    unsigned long long *ntail, int64_t cap_tail, int tail_budget,
-                                                    Status *st) {
-  const PoolView P = *pv;
-  const int64_t np = (int64_t)min(*npairs, (unsigned long long)cap_pairs);
-  const unsigned lane = threadIdx.x & 31u;
-  constexpr unsigned kFull = 0xffffffffu;
-  bool active = false, exhausted = false;
-  int64_t e = 0;
-  ContactProb CP;
-  LmState S;
-  Quat q1, q2;
-  double a1 = 0, b1 = 0, a2 = 0, b2 = 0;
-  for (;;) {
-    if (!exhausted) {
-      const unsigned want = __ballot_sync(kFull, !active);
-      if (want) {
-        const int leader = __ffs(want) - 1;
-        unsigned long long base = 0;
-        if ((int)lane == leader) base = atomicAdd(queue, (unsigned long long)__popc(want));
-        base = __shfl_sync(kFull, base, leader);
-        if ((int64_t)base >= np) {
-          exhausted = true;
-        } else if (!active) {
-          e = (int64_t)base + __popc(want & ((1u << lane) - 1u));
-          if (e < np) {
-            const PairRec pr = pairs[e];
-            const int i1 = pr.home, i2 = pr.near;
-            const InstDev &I = insts[P.inst[i1]];
-            const double x1 = P.st[0][i1], y1 = P.st[1][i1], z1 = P.st[2][i1];
-            double vkx = P.st[0][i2] - x1, vky = P.st[1][i2] - y1, vkz = P.st[2][i2] - z1;
-            if ((fabs(vkx) > I.lx / 2) && I.periodicity) vkx = vkx - copysign(I.lx, vkx);
-            if (fabs(vky) > I.ly / 2.) vky = vky - copysign(I.ly, vky);
-            if (fabs(vkz) > I.lz / 2.) vkz = vkz - copysign(I.lz, vkz);
-            const double c1[3] = {x1, y1, z1};
-            const double c2[3] = {x1 + vkx, y1 + vky, z1 + vkz};
-            q1 = {P.st[6][i1], P.st[7][i1], P.st[8][i1], P.st[9][i1]};
-            q2 = {P.st[6][i2], P.st[7][i2], P.st[8][i2], P.st[9][i2]};
-            a1 = P.pc[0][i1]; b1 = P.pc[1][i1]; a2 = P.pc[0][i2]; b2 = P.pc[1][i2];
-            // symmetry axes (first columns of R(q)); disjoint bodies need no solve
-            const double e1[3] = {1.0 - 2.0 * (q1.c * q1.c + q1.d * q1.d), 2.0 * (q1.b * q1.c + q1.a * q1.d),
-                                  2.0 * (q1.b * q1.d - q1.a * q1.c)};
-            const double e2[3] = {1.0 - 2.0 * (q2.c * q2.c + q2.d * q2.d), 2.0 * (q2.b * q2.c + q2.a * q2.d),
-                                  2.0 * (q2.b * q2.d - q2.a * q2.c)};
-            const double dd = sqrt(vkx * vkx + vky * vky + vkz * vkz);
-            const bool apart = dd > 0.0 && separated(vkx, vky, vkz, e1, a1 * a1, b1 * b1, e2, a2 * a2, b2 * b2,
-                                                     vkx / dd, vky / dd, vkz / dd);
-            if (!apart && contact_setup(a1, b1, a2, b2, c1, q1, c2, q2, CP, S.x)) {
-              lm_begin(CP, S);
-              active = true;
-            }
-          }
-        }
-      }
-    }
-    if (!__any_sync(kFull, active)) {
-      if (exhausted) break;
-      continue;
-    }
-    if (!active) continue;
-    if (lm_step(CP, S, kContactTol) == 0) {
-      // a long solve goes to k_contact_tail, which finishes it with the solver folded
-      // into one kernel; the lane takes a new pair (if the hand-over buffer is full the
-      // lane keeps the solve)
-      if (tail != nullptr && S.nfev >= tail_budget) {
-        const unsigned long long k = atomicAdd(ntail, 1ull);
-        if ((int64_t)k < cap_tail) {
-          TailRec t;
-          t.e = e; t.CP = CP; t.S = S; t.q1 = q1; t.q2 = q2;
-          t.a1 = a1; t.b1 = b1; t.a2 = a2; t.b2 = b2;
-          tail[k] = t;
-          active = false;
-        }
-      }
-      continue;
-    }
-    active = false;
-    finish_pair(P, pairs, e, CP, S, q1, q2, a1, b1, a2, b2, coll, ncoll, cap_coll, cst, ncst, cap_cst, st);
-  }
-}
-
-// Persistent grid for k_contact: as many blocks as can be resident at once on the
-// current device (looked up once, at context creation, outside any stream capture).
-int contact_grid_blocks() {
-  int per_sm = 0, dev = 0, sms = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_contact, 128, 0) != cudaSuccess ||
-      cudaGetDevice(&dev) != cudaSuccess ||
-      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || per_sm <= 0)
-    return 0;
-  return per_sm * sms;
-}
-
-void launch_contact(const InstDev *insts, const PoolView *pv, const PairRec *pairs, const unsigned long long *npairs,
-                    int64_t cap_pairs, CollRec *coll, unsigned long long *ncoll, int64_t cap_coll,
-                    unsigned long long *queue, ContactStatRec *cst, unsigned long long *ncst, int64_t cap_cst,
-                    TailRec *tail, unsigned long long *ntail, int64_t cap_tail, int tail_budget, Status *st,
-                    int grid, cudaStream_t s) {
-  k_contact<<<grid, 128, 0, s>>>(insts, pv, pairs, npairs, cap_pairs, coll, ncoll, cap_coll, queue, cst, ncst,
-                                 cap_cst, tail, ntail, cap_tail, tail_budget, st);
-}
-
 // COLLISION_RESPONSE (collision_response.f90) for the accepted pairs; each particle is
 // in at most one accepted pair.
 __global__ void k_response(const InstDev *__restrict__ insts, const PoolView *__restrict__ pv,
@@ -334,7 +213,7 @@ __global__ void k_euler_batch(int64_t n, const double *ip, double dt, double *om
   }
 }
 
-__global__ void __launch_bounds__(128, GP_CONTACT_MIN_BLOCKS) k_contact_batch(int64_t n, const double *shapes, const double *centres, const double *quats,
+__global__ void __launch_bounds__(128, 8) k_contact_batch(int64_t n, const double *shapes, const double *centres, const double *quats,
                                 int32_t *flag, double *e1, double *e2, double *cn) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const double *s = shapes + 4 * i, *c = centres + 6 * i, *q = quats + 8 * i;

@@ -32,7 +32,7 @@ void launch_contact(const InstDev *insts, const PoolView *pv, const PairRec *pai
                     TailRec *tail, unsigned long long *ntail, int64_t cap_tail, int tail_budget, Status *st,
                     int grid, cudaStream_t s);
 // --- gp_contact_tail.cu (-fmad=false, solver inlined) ---
-void launch_contact_tail(const PoolView *pv, const PairRec *pairs, const TailRec *tail,
+void launch_contact_tail(const InstDev *insts, const PoolView *pv, const PairRec *pairs, const TailRec *tail,
                          const unsigned long long *ntail, int64_t cap_tail, CollRec *coll, unsigned long long *ncoll,
                          int64_t cap_coll, ContactStatRec *cst, unsigned long long *ncst, int64_t cap_cst,
                          Status *st, cudaStream_t s);

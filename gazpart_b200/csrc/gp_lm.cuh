@@ -27,6 +27,9 @@ namespace gp {
 #endif
 // The pieces of one iteration are folded into the iteration itself.
 #define GP_LM_INNER static __device__ __forceinline__
+// Once per solve (set-up and the final contact test): out of line in every build, so
+// that they do not add to the register pressure of the iteration they bracket.
+#define GP_LM_COLD static __device__ __noinline__
 
 // MINPACK's scaled Euclidean norm (minpack_reduc.f90:180-232): three accumulators
 // for tiny, mid-range and huge components.
@@ -181,72 +184,125 @@ CT_QUAL double ct_acos(double x) { return (1.5707963267948966 - ct_asin(x)) + 6.
 struct ContactProb {
   double e1[9], e2[9];   // R diag(a^2,b^2,b^2) R^T (calculate_ellipsoid_matrix.f90:33-72)
   double b1[3], b2[3];
+  // entry k of body W's matrix, coordinate i of body W's centre
+  template <int W> __device__ __forceinline__ double e(int k) const { return W == 0 ? e1[k] : e2[k]; }
+  template <int W> __device__ __forceinline__ double b(int i) const { return W == 0 ? b1[i] : b2[i]; }
 };
 
-// Support points along +-c(x) (ellipsoid_pair_depth.f90:117-142).
-GP_LM_INNER void support_points(const ContactProb& P, const double x[2], double c1[3], double tmp1[3],
-                                               double tmp2[3], double& l1, double& l2, double pt1[3],
-                                               double pt2[3]) {
-  double s0, k0, s1, k1;
-  ct_sincos(x[0], &s0, &k0);
-  ct_sincos(x[1], &s1, &k1);
-  c1[0] = k0 * k1;
-  c1[1] = s0 * k1;
-  c1[2] = s1;
+// The same problem held in shared memory, one column per lane of a 128-thread block
+// (entry m of the lane's problem at base[m * kProbLanes]; m = 0..8 E1, 9..17 E2,
+// 18..20 b1, 21..23 b2): the solve reads it there and keeps its registers for its state.
+constexpr int kProbLanes = 128;
+constexpr int kProbWords = 24;
+struct SmemProb {
+  double* base;
+  template <int W> __device__ __forceinline__ double e(int k) const { return base[(W * 9 + k) * kProbLanes]; }
+  template <int W> __device__ __forceinline__ double b(int i) const { return base[(18 + W * 3 + i) * kProbLanes]; }
+  __device__ __forceinline__ void store(const ContactProb& P) const {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) { base[k * kProbLanes] = P.e1[k]; base[(9 + k) * kProbLanes] = P.e2[k]; }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) { base[(18 + i) * kProbLanes] = P.b1[i]; base[(21 + i) * kProbLanes] = P.b2[i]; }
+  }
+};
+
+// Everything the residual at x computes that the Jacobian at the same x needs again:
+// the trigonometric values of the two angles, the support-function values lambda_1,
+// lambda_2, the factors 1/(2 lambda_i) and the gap vector (whose squares are the
+// residual).  The Jacobian is only ever taken at a point whose residual was the last
+// one accepted, so keeping these avoids a second evaluation of the same expressions.
+struct SupportEval {
+  double s0, k0, s1, k1;   // sin, cos of x[0] and x[1]
+  double l1, l2, f1, f2;   // lambda_i and 1/(2 lambda_i)
+  double depth[3];         // pt1 - pt2
+};
+
+// E_W v, in matvec's order of terms
+template <int W, class Prob>
+__device__ __forceinline__ void prob_matvec(const Prob& P, const double v[3], double o[3]) {
+  const double t0 = P.template e<W>(0) * v[0] + P.template e<W>(3) * v[1] + P.template e<W>(6) * v[2];
+  const double t1 = P.template e<W>(1) * v[0] + P.template e<W>(4) * v[1] + P.template e<W>(7) * v[2];
+  const double t2 = P.template e<W>(2) * v[0] + P.template e<W>(5) * v[1] + P.template e<W>(8) * v[2];
+  o[0] = t0; o[1] = t1; o[2] = t2;
+}
+
+// Support points along +-c(x) (ellipsoid_pair_depth.f90:117-142): E receives the
+// quantities above, pt1/pt2 the points themselves.
+template <class Prob>
+GP_LM_INNER void support_eval(const Prob& P, const double x[2], SupportEval& E, double pt1[3], double pt2[3]) {
+  ct_sincos(x[0], &E.s0, &E.k0);
+  ct_sincos(x[1], &E.s1, &E.k1);
+  const double c1[3] = {E.k0 * E.k1, E.s0 * E.k1, E.s1};
   const double c2[3] = {-c1[0], -c1[1], -c1[2]};
-  matvec(P.e1, c1, tmp1);
-  matvec(P.e2, c2, tmp2);
-  l1 = sqrt(0.25 * (c1[0] * tmp1[0] + c1[1] * tmp1[1] + c1[2] * tmp1[2]));
-  l2 = sqrt(0.25 * (c2[0] * tmp2[0] + c2[1] * tmp2[1] + c2[2] * tmp2[2]));
-  const double f1 = 1.0 / (2.0 * l1), f2 = 1.0 / (2.0 * l2);
+  double t1[3], t2[3];
+  prob_matvec<0>(P, c1, t1);
+  prob_matvec<1>(P, c2, t2);
+  E.l1 = sqrt(0.25 * (c1[0] * t1[0] + c1[1] * t1[1] + c1[2] * t1[2]));
+  E.l2 = sqrt(0.25 * (c2[0] * t2[0] + c2[1] * t2[1] + c2[2] * t2[2]));
+  E.f1 = 1.0 / (2.0 * E.l1);
+  E.f2 = 1.0 / (2.0 * E.l2);
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
-    pt1[i] = f1 * tmp1[i] + P.b1[i];
-    pt2[i] = f2 * tmp2[i] + P.b2[i];
+    pt1[i] = E.f1 * t1[i] + P.template b<0>(i);
+    pt2[i] = E.f2 * t2[i] + P.template b<1>(i);
+    E.depth[i] = pt1[i] - pt2[i];
   }
 }
 
-// fcn, iflag=1 (ellipsoid_contact_detection.f90:290-295)
-GP_LM_INNER void lm_fcn(const ContactProb& P, const double x[2], double fvec[3]) {
-  double c1[3], t1[3], t2[3], l1, l2, pt1[3], pt2[3];
-  support_points(P, x, c1, t1, t2, l1, l2, pt1, pt2);
-#pragma unroll
-  for (int i = 0; i < 3; ++i) {
-    const double d = pt1[i] - pt2[i];
-    fvec[i] = d * d;
-  }
+// Support points alone (the contact test after the solve).
+template <class Prob>
+GP_LM_INNER void support_points(const Prob& P, const double x[2], double c1[3], double pt1[3], double pt2[3]) {
+  SupportEval E;
+  support_eval(P, x, E, pt1, pt2);
+  c1[0] = E.k0 * E.k1;
+  c1[1] = E.s0 * E.k1;
+  c1[2] = E.s1;
 }
 
-GP_LM_INNER void grad_coeff(const double e[9], const double c[3], double l, double co[9]) {
+// fcn, iflag=1 (ellipsoid_contact_detection.f90:290-295): the squared gap components.
+template <class Prob>
+GP_LM_INNER void lm_fcn(const Prob& P, const double x[2], double fvec[3], SupportEval& E) {
+  double pt1[3], pt2[3];
+  support_eval(P, x, E, pt1, pt2);
+#pragma unroll
+  for (int i = 0; i < 3; ++i) fvec[i] = E.depth[i] * E.depth[i];
+}
+
+// d(support point)/dc = E/(2 lambda) - (E c)(E c)^T / (8 lambda^3), with s = 1/(2 lambda);
+// E (outer) in matmul's order of terms.
+template <int W, class Prob>
+GP_LM_INNER void grad_coeff(const Prob& P, const double c[3], double l, double s, double co[9]) {
   double row[3];
 #pragma unroll
-  for (int j = 0; j < 3; ++j) row[j] = c[0] * e[3 * j] + c[1] * e[1 + 3 * j] + c[2] * e[2 + 3 * j];
+  for (int j = 0; j < 3; ++j)
+    row[j] = c[0] * P.template e<W>(3 * j) + c[1] * P.template e<W>(1 + 3 * j) + c[2] * P.template e<W>(2 + 3 * j);
   double outer[9];
 #pragma unroll
   for (int j = 0; j < 3; ++j)
 #pragma unroll
     for (int i = 0; i < 3; ++i) outer[i + 3 * j] = c[i] * row[j];
   double eo[9];
-  matmul(e, outer, eo);
-  const double s = 1.0 / (2.0 * l), t = 1.0 / (8.0 * (l * l * l));   // lambda**3.0
 #pragma unroll
-  for (int k = 0; k < 9; ++k) co[k] = s * e[k] - t * eo[k];
+  for (int j = 0; j < 3; ++j)
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+      eo[i + 3 * j] = P.template e<W>(i) * outer[3 * j] + P.template e<W>(i + 3) * outer[1 + 3 * j] +
+                      P.template e<W>(i + 6) * outer[2 + 3 * j];
+  const double t = 1.0 / (8.0 * (l * l * l));   // lambda**3.0
+#pragma unroll
+  for (int k = 0; k < 9; ++k) co[k] = s * P.template e<W>(k) - t * eo[k];
 }
 
 // fcn, iflag=2: analytic Jacobian (ellipsoid_contact_detection.f90:296-332), 3x2
-// column-major.
-GP_LM_INNER void lm_jac(const ContactProb& P, const double x[2], double fj[6]) {
-  double c1[3], t1[3], t2[3], l1, l2, pt1[3], pt2[3];
-  support_points(P, x, c1, t1, t2, l1, l2, pt1, pt2);
-  const double depth[3] = {pt1[0] - pt2[0], pt1[1] - pt2[1], pt1[2] - pt2[2]};
-  double s0, k0, s1, k1;
-  ct_sincos(x[0], &s0, &k0);
-  ct_sincos(x[1], &s1, &k1);
-  const double g[6] = {-s0 * k1, k0 * k1, 0.0, -k0 * s1, -s0 * s1, k1};
+// column-major, at the point whose residual produced E.
+template <class Prob>
+GP_LM_INNER void lm_jac(const Prob& P, const SupportEval& E, double fj[6]) {
+  const double g[6] = {-E.s0 * E.k1, E.k0 * E.k1, 0.0, -E.k0 * E.s1, -E.s0 * E.s1, E.k1};
+  const double c1[3] = {E.k0 * E.k1, E.s0 * E.k1, E.s1};
   const double c2[3] = {-c1[0], -c1[1], -c1[2]};
   double co1[9], co2[9];
-  grad_coeff(P.e1, c1, l1, co1);
-  grad_coeff(P.e2, c2, l2, co2);
+  grad_coeff<0>(P, c1, E.l1, E.f1, co1);
+  grad_coeff<1>(P, c2, E.l2, E.f2, co2);
 #pragma unroll
   for (int j = 0; j < 2; ++j) {
     const double gj[3] = {g[3 * j], g[3 * j + 1], g[3 * j + 2]};
@@ -255,30 +311,34 @@ GP_LM_INNER void lm_jac(const ContactProb& P, const double x[2], double fj[6]) {
     matvec(co1, gj, gp1);
     matvec(co2, ng, gp2);
 #pragma unroll
-    for (int i = 0; i < 3; ++i) fj[i + 3 * j] = 2.0 * (depth[i] * (gp1[i] - gp2[i]));
+    for (int i = 0; i < 3; ++i) fj[i + 3 * j] = 2.0 * (E.depth[i] * (gp1[i] - gp2[i]));
   }
 }
 
+// The column pivot of the 3x2 QR is either the identity or the swap; `sw` records the
+// swap (MINPACK's ipvt = (2, 1)).  sel(sw, a, b) is element ipvt[j] of a two-vector
+// (a, b) for j = 0, and sel(!sw, a, b) for j = 1; keeping the pivot as a flag lets every
+// index be a compile-time constant, so the solver's state stays in registers.
+__device__ __forceinline__ double sel(bool sw, double a, double b) { return sw ? b : a; }
+
 // QR with column pivoting (3x2), Householder vectors left in a.
-GP_LM_INNER void lm_qrfac(double a[6], int ipvt[2], double rdiag[2], double acnorm[2]) {
+GP_LM_INNER void lm_qrfac(double a[6], bool& sw, double rdiag[2], double acnorm[2]) {
   double wa[2];
 #pragma unroll
   for (int j = 0; j < 2; ++j) {
     acnorm[j] = lm_enorm<3>(a + 3 * j);
     rdiag[j] = acnorm[j];
     wa[j] = rdiag[j];
-    ipvt[j] = j;
   }
+  sw = false;
 #pragma unroll
   for (int j = 0; j < 2; ++j) {
-    int kmax = j;
-    if (j == 0 && rdiag[1] > rdiag[0]) kmax = 1;
-    if (kmax != j) {
+    if (j == 0 && rdiag[1] > rdiag[0]) {
 #pragma unroll
       for (int i = 0; i < 3; ++i) { const double t = a[i]; a[i] = a[i + 3]; a[i + 3] = t; }
       rdiag[1] = rdiag[0];
       wa[1] = wa[0];
-      const int k = ipvt[0]; ipvt[0] = ipvt[1]; ipvt[1] = k;
+      sw = true;
     }
     double ajnorm = (j == 0) ? lm_enorm<3>(a) : lm_enorm<2>(a + 4);
     if (ajnorm != 0.0) {
@@ -309,8 +369,8 @@ GP_LM_INNER void lm_qrfac(double a[6], int ipvt[2], double rdiag[2], double acno
   }
 }
 
-GP_LM_INNER void lm_qrsolv(double r[6], const int ipvt[2], const double diag[2], const double qtb[2],
-                                          double x[2], double sdiag[2]) {
+GP_LM_INNER void lm_qrsolv(double r[6], bool sw, const double diag[2], const double qtb[2], double x[2],
+                           double sdiag[2]) {
   double wa[2];
 #pragma unroll
   for (int j = 0; j < 2; ++j) {
@@ -321,11 +381,11 @@ GP_LM_INNER void lm_qrsolv(double r[6], const int ipvt[2], const double diag[2],
   }
 #pragma unroll
   for (int j = 0; j < 2; ++j) {
-    const int l = ipvt[j];
-    if (diag[l] != 0.0) {
+    const double dl = (j == 0) ? sel(sw, diag[0], diag[1]) : sel(!sw, diag[0], diag[1]);
+    if (dl != 0.0) {
 #pragma unroll
       for (int k = j; k < 2; ++k) sdiag[k] = 0.0;
-      sdiag[j] = diag[l];
+      sdiag[j] = dl;
       double qtbpj = 0.0;
 #pragma unroll
       for (int k = j; k < 2; ++k) {
@@ -366,12 +426,13 @@ GP_LM_INNER void lm_qrsolv(double r[6], const int ipvt[2], const double diag[2],
     if (nsing >= 2) sum = sum + r[1] * wa[1];
     wa[0] = (wa[0] - sum) / sdiag[0];
   }
-  x[ipvt[0]] = wa[0];
-  x[ipvt[1]] = wa[1];
+  // x[ipvt[j]] = wa[j]
+  x[0] = sel(sw, wa[0], wa[1]);
+  x[1] = sel(sw, wa[1], wa[0]);
 }
 
-GP_LM_INNER void lm_lmpar(double r[6], const int ipvt[2], const double diag[2], const double qtb[2],
-                                         double delta, double& par, double x[2], double sdiag[2]) {
+GP_LM_INNER void lm_lmpar(double r[6], bool sw, const double diag[2], const double qtb[2], double delta,
+                          double& par, double x[2], double sdiag[2]) {
   const double dwarf = DBL_MIN;
   double wa1[2], wa2[2];
   int nsing = 2;
@@ -386,8 +447,8 @@ GP_LM_INNER void lm_lmpar(double r[6], const int ipvt[2], const double diag[2], 
     wa1[0] = wa1[0] - r[3] * wa1[1];
   }
   if (nsing >= 1) wa1[0] = wa1[0] / r[0];
-  x[ipvt[0]] = wa1[0];
-  x[ipvt[1]] = wa1[1];
+  x[0] = sel(sw, wa1[0], wa1[1]);
+  x[1] = sel(sw, wa1[1], wa1[0]);
   wa2[0] = diag[0] * x[0];
   wa2[1] = diag[1] * x[1];
   double dxnorm = lm_enorm<2>(wa2);
@@ -396,10 +457,12 @@ GP_LM_INNER void lm_lmpar(double r[6], const int ipvt[2], const double diag[2], 
     par = 0.0;
     return;
   }
+  // diag and wa2 in pivot order: element ipvt[j] for j = 0, 1
+  const double dp0 = sel(sw, diag[0], diag[1]), dp1 = sel(!sw, diag[0], diag[1]);
   double parl = 0.0;
   if (nsing >= 2) {
-#pragma unroll
-    for (int j = 0; j < 2; ++j) { const int l = ipvt[j]; wa1[j] = diag[l] * (wa2[l] / dxnorm); }
+    wa1[0] = dp0 * (sel(sw, wa2[0], wa2[1]) / dxnorm);
+    wa1[1] = dp1 * (sel(!sw, wa2[0], wa2[1]) / dxnorm);
     wa1[0] = (wa1[0] - 0.0) / r[0];
     wa1[1] = (wa1[1] - (0.0 + r[3] * wa1[0])) / r[4];
     const double temp = lm_enorm<2>(wa1);
@@ -408,8 +471,8 @@ GP_LM_INNER void lm_lmpar(double r[6], const int ipvt[2], const double diag[2], 
   {
     const double s0 = 0.0 + r[0] * qtb[0];
     const double s1 = (0.0 + r[3] * qtb[0]) + r[4] * qtb[1];
-    wa1[0] = s0 / diag[ipvt[0]];
-    wa1[1] = s1 / diag[ipvt[1]];
+    wa1[0] = s0 / dp0;
+    wa1[1] = s1 / dp1;
   }
   const double gnorm = lm_enorm<2>(wa1);
   double paru = gnorm / delta;
@@ -423,15 +486,15 @@ GP_LM_INNER void lm_lmpar(double r[6], const int ipvt[2], const double diag[2], 
     const double sp = sqrt(p);
     wa1[0] = sp * diag[0];
     wa1[1] = sp * diag[1];
-    lm_qrsolv(r, ipvt, wa1, qtb, x, sdiag);
+    lm_qrsolv(r, sw, wa1, qtb, x, sdiag);
     wa2[0] = diag[0] * x[0];
     wa2[1] = diag[1] * x[1];
     dxnorm = lm_enorm<2>(wa2);
     const double told = fp;
     fp = dxnorm - delta;
     if (fabs(fp) <= 0.1 * delta || (parl == 0.0 && fp <= told && told < 0.0) || iter == 10) break;
-#pragma unroll
-    for (int j = 0; j < 2; ++j) { const int l = ipvt[j]; wa1[j] = diag[l] * (wa2[l] / dxnorm); }
+    wa1[0] = dp0 * (sel(sw, wa2[0], wa2[1]) / dxnorm);
+    wa1[1] = dp1 * (sel(!sw, wa2[0], wa2[1]) / dxnorm);
     wa1[0] = wa1[0] / sdiag[0];
     wa1[1] = wa1[1] - r[1] * wa1[0];
     wa1[1] = wa1[1] / sdiag[1];
@@ -453,17 +516,20 @@ GP_LM_INNER void lm_lmpar(double r[6], const int ipvt[2], const double diag[2], 
 // pair is lmder's; the split lets a warp refill a lane with a new pair as soon as its
 // pair converges.
 struct LmState {
-  double x[2], fvec[3], fjac[6], diag[2], qtf[2];
+  double x[2], fjac[6], diag[2], qtf[2];
   double fnorm, xnorm, delta, par, temp, gnorm;
-  int ipvt[2];
+  SupportEval E;   // residual evaluation at x (for the next Jacobian; fvec = E.depth^2)
   int nfev, iter;
+  bool swapped;    // column pivot of the last QR: ipvt = (2, 1)
   bool need_jac;
 };
 
-GP_LM_FN void lm_begin(const ContactProb& P, LmState& S) {
-  lm_fcn(P, S.x, S.fvec);
+template <class Prob>
+GP_LM_FN void lm_begin(const Prob& P, LmState& S) {
+  double fvec[3];
+  lm_fcn(P, S.x, fvec, S.E);
   S.nfev = 1;
-  S.fnorm = lm_enorm<3>(S.fvec);
+  S.fnorm = lm_enorm<3>(fvec);
   S.par = 0.0;
   S.iter = 1;
   S.xnorm = 0.0;
@@ -471,18 +537,18 @@ GP_LM_FN void lm_begin(const ContactProb& P, LmState& S) {
   S.temp = 0.0;
   S.gnorm = 0.0;
   S.diag[0] = S.diag[1] = 0.0;
-  S.ipvt[0] = 0;
-  S.ipvt[1] = 1;
+  S.swapped = false;
   S.need_jac = true;
 }
 
-GP_LM_FN int lm_step(const ContactProb& P, LmState& S, double tol) {
+template <class Prob>
+GP_LM_FN int lm_step(const Prob& P, LmState& S, double tol) {
   constexpr int maxfev = 300;
   const double ftol = tol, xtol = tol;
   double wa1[2], wa2[2], wa3[2], wa4[3];
   if (S.need_jac) {
-    lm_jac(P, S.x, S.fjac);
-    lm_qrfac(S.fjac, S.ipvt, wa1, wa2);
+    lm_jac(P, S.E, S.fjac);
+    lm_qrfac(S.fjac, S.swapped, wa1, wa2);
     if (S.iter == 1) {
 #pragma unroll
       for (int j = 0; j < 2; ++j) { S.diag[j] = wa2[j]; if (wa2[j] == 0.0) S.diag[j] = 1.0; }
@@ -493,7 +559,7 @@ GP_LM_FN int lm_step(const ContactProb& P, LmState& S, double tol) {
       if (S.delta == 0.0) S.delta = 100.0;
     }
 #pragma unroll
-    for (int i = 0; i < 3; ++i) wa4[i] = S.fvec[i];
+    for (int i = 0; i < 3; ++i) wa4[i] = S.E.depth[i] * S.E.depth[i];   // fvec at x
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
       if (S.fjac[j + 3 * j] != 0.0) {
@@ -511,7 +577,8 @@ GP_LM_FN int lm_step(const ContactProb& P, LmState& S, double tol) {
     if (S.fnorm != 0.0) {
 #pragma unroll
       for (int j = 0; j < 2; ++j) {
-        const double acn = (S.ipvt[j] == 0) ? wa2[0] : wa2[1];
+        // acnorm of the original column ipvt[j]
+        const double acn = (j == 0) ? sel(S.swapped, wa2[0], wa2[1]) : sel(!S.swapped, wa2[0], wa2[1]);
         if (acn != 0.0) {
           double sum = 0.0;
 #pragma unroll
@@ -528,7 +595,7 @@ GP_LM_FN int lm_step(const ContactProb& P, LmState& S, double tol) {
     S.need_jac = false;
   }
   // one trial step (the body of lmder's inner loop)
-  lm_lmpar(S.fjac, S.ipvt, S.diag, S.qtf, S.delta, S.par, wa1, wa2);
+  lm_lmpar(S.fjac, S.swapped, S.diag, S.qtf, S.delta, S.par, wa1, wa2);
 #pragma unroll
   for (int j = 0; j < 2; ++j) {
     wa1[j] = -wa1[j];
@@ -537,13 +604,15 @@ GP_LM_FN int lm_step(const ContactProb& P, LmState& S, double tol) {
   }
   const double pnorm = lm_enorm<2>(wa3);
   if (S.iter == 1) S.delta = (S.delta < pnorm) ? S.delta : pnorm;
-  lm_fcn(P, wa2, wa4);
+  SupportEval E2;
+  lm_fcn(P, wa2, wa4, E2);
   ++S.nfev;
   const double fnorm1 = lm_enorm<3>(wa4);
   double actred = -1.0;
   if (0.1 * fnorm1 < S.fnorm) { const double r = fnorm1 / S.fnorm; actred = 1.0 - r * r; }
-  const double p0 = (S.ipvt[0] == 0) ? wa1[0] : wa1[1];
-  const double p1 = (S.ipvt[1] == 0) ? wa1[0] : wa1[1];
+  // wa1 in pivot order: element ipvt[j]
+  const double p0 = sel(S.swapped, wa1[0], wa1[1]);
+  const double p1 = sel(!S.swapped, wa1[0], wa1[1]);
   wa3[0] = 0.0 + S.fjac[0] * p0;
   wa3[1] = 0.0;
   wa3[0] = wa3[0] + S.fjac[3] * p1;
@@ -568,8 +637,7 @@ GP_LM_FN int lm_step(const ContactProb& P, LmState& S, double tol) {
   if (ratio >= 1.0e-4) {
 #pragma unroll
     for (int j = 0; j < 2; ++j) { S.x[j] = wa2[j]; wa2[j] = S.diag[j] * S.x[j]; }
-#pragma unroll
-    for (int i = 0; i < 3; ++i) S.fvec[i] = wa4[i];
+    S.E = E2;
     S.xnorm = lm_enorm<2>(wa2);
     S.fnorm = fnorm1;
     ++S.iter;
@@ -646,7 +714,7 @@ static __device__ __noinline__ bool separated(double dx, double dy, double dz, c
   return false;
 }
 
-GP_LM_FN double fmargin(double a, double b, const double pt[3], const double c[3], const Quat& q) {
+GP_LM_COLD double fmargin(double a, double b, const double pt[3], const double c[3], const Quat& q) {
   double ell[9];
   rot_diag(q, 1.0 / (a * a), 1.0 / (b * b), 1.0 / (b * b), ell);
   const double v[3] = {pt[0] - c[0], pt[1] - c[1], pt[2] - c[2]};
@@ -675,11 +743,11 @@ GP_LM_FN bool contact_setup(double a1, double bb1, double a2, double bb2, const 
 }
 
 // pair_depth at the solution and the contact test (ellipsoid_contact_detection.f90:104-179)
-GP_LM_FN bool contact_finish(double a1, double bb1, double a2, double bb2, const Quat& q1,
+GP_LM_COLD bool contact_finish(double a1, double bb1, double a2, double bb2, const Quat& q1,
                                                    const Quat& q2, const ContactProb& P, const double x[2],
                                                    double ept1[3], double ept2[3], double cn[3]) {
-  double cc[3], t1[3], t2[3], l1, l2, pt1[3], pt2[3];
-  support_points(P, x, cc, t1, t2, l1, l2, pt1, pt2);
+  double cc[3], pt1[3], pt2[3];
+  support_points(P, x, cc, pt1, pt2);
   const double d[3] = {pt1[0] - pt2[0], pt1[1] - pt2[1], pt1[2] - pt2[2]};
   const double contact = d[0] * cc[0] + d[1] * cc[1] + d[2] * cc[2];
 #pragma unroll

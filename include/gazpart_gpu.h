@@ -377,18 +377,19 @@ int gp_ellipsoid_contact_detection_batch(gp_ctx *ctx, int64_t n, const double *s
                                          int32_t *flag, double *ept1, double *ept2,
                                          double *cnormal, int32_t on_device);
 /* No counterpart in the reference.  The batched contact detection above for callers
- * that cannot allocate device memory (a loop running under another library's stream
- * capture, a pool that has filled HBM, a real-time loop that cannot take the device
- * synchronisation of cudaFree).  Same arguments and results as
- * gp_ellipsoid_contact_detection_batch, without a context; `stream` is a cudaStream_t
- * (NULL: the default stream) on the current device.  It calls no allocator: inputs and
- * results pass through one static device array of GP_NOALLOC_MAX_PAIRS pairs
- * (220 bytes per pair), and n above that returns GP_EBADARG without doing any work.
- * The array is shared by all calls on a device and keeps the last call's contents;
- * calls that can overlap on the GPU race on it and must be ordered by the caller.
- * The first call on each device looks up the array with that device current and may
- * load this library's device code: make it before any stream capture starts.
- * Synchronises `stream` before returning. */
+ * that cannot allocate device memory (a solver whose particle pool has filled HBM, a
+ * real-time loop that cannot take the device-wide synchronisation of cudaFree, a host
+ * program whose memory plan forbids allocation after start-up).  Same arguments and
+ * results as gp_ellipsoid_contact_detection_batch, without a context; `stream` is a
+ * cudaStream_t (NULL: the default stream) on the current device.  It calls no
+ * allocator: inputs and results pass through one static device array of
+ * GP_NOALLOC_MAX_PAIRS pairs (220 bytes per pair), and n above that returns GP_EBADARG
+ * without doing any work.  The array is shared by all calls on a device and keeps the
+ * last call's contents; calls that can overlap on the GPU race on it and must be
+ * ordered by the caller.  The first call on each device (and the first after the
+ * device's context is replaced) looks up the array with that device current and may
+ * load this library's device code.  Synchronises `stream` before returning; a stream
+ * that is being captured is refused with GP_EBADARG before any work is enqueued. */
 #define GP_NOALLOC_MAX_PAIRS 32768
 int gp_ellipsoid_contact_detection_batch_noalloc(int64_t n, const double *shapes,
                                                  const double *centres, const double *quats,
