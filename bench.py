@@ -46,6 +46,7 @@ def parse():
     ap.add_argument("--no-io", action="store_true", help="skip the restart-file measurement")
     ap.add_argument("--no-stats", action="store_true", help="skip the statistics measurement")
     ap.add_argument("--no-dns", action="store_true", help="skip the live-fluid measurement")
+    ap.add_argument("--no-forms", action="store_true", help="skip the batched and serving sub-benchmarks")
     ap.add_argument("--contact-tail", type=int, default=None,
                     help="evaluations after which a contact solve moves to the inlined-solver kernel (0: never)")
     ap.add_argument("--grids", default=None,
@@ -281,6 +282,134 @@ def time_cpu(w, steps: int, threads: int, scale: int, max_emaj: float):
             "t_col": t_col / steps, "candidates_per_step": res["n_candidates"], "nbox": g.nbox}
 
 
+def time_cpu_one_thread(w, scale: int, max_emaj: float, fraction: float = 0.01, seed: int = 3):
+    """The same sample on one host thread, as the reference runs per MPI rank: the whole
+    advance, and the collision phase timed on a random `fraction` of the step's candidate
+    pairs (each evaluated as collision_interaction.f90:216-348 does, one Levenberg-Marquardt
+    solve per pair) and scaled to all of them."""
+    import pyoracle as po
+    ens, refs, g = cpu_sample(w, scale, max_emaj)
+    t0 = time.perf_counter()
+    rc = ens.advance(refs, nthreads=1)
+    t_adv = time.perf_counter() - t0
+    if rc:
+        raise RuntimeError(f"oracle advance failed ({rc})")
+    ncon, con = ens.connectivity(g)
+    a = ens.a
+    xyz = [po.dptr(a[k]) for k in ("x", "y", "z")]
+    ncand = po.lib().orc_detect_pairs(po.C.byref(g), po.iptr(ncon), po.iptr(con), po.C.c_int64(ens.n), *xyz,
+                                      po.C.c_int64(0), None, None)
+    home = np.zeros(ncand, dtype=np.int32)
+    near = np.zeros(ncand, dtype=np.int32)
+    po.lib().orc_detect_pairs(po.C.byref(g), po.iptr(ncon), po.iptr(con), po.C.c_int64(ens.n), *xyz,
+                              po.C.c_int64(ncand), po.iptr(home), po.iptr(near))
+    pick = np.random.default_rng(seed).choice(ncand, size=max(1, int(fraction * ncand)), replace=False)
+    s, props, st = po.make_setup(ens.setup), ens.props(), ens.state()
+    out = [np.zeros(3) for _ in range(5)]
+    flag = po.C.c_int32()
+    t0 = time.perf_counter()
+    for e in pick:
+        po.lib().orc_pair_eval(po.C.byref(s), po.C.byref(props), po.C.byref(st), po.C.c_int64(int(home[e])),
+                               po.C.c_int64(int(near[e])), *[po.dptr(o) for o in out], po.C.byref(flag))
+    t_pairs = time.perf_counter() - t0
+    t_col = t_pairs * ncand / pick.size
+    return {"value": ens.n / (t_adv + t_col), "n": ens.n, "t_adv": t_adv, "t_col": t_col,
+            "candidates_per_step": int(ncand), "pairs_timed": int(pick.size)}
+
+
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
+def reference_compilers() -> dict:
+    """Where the reference's own Fortran toolchain is on this host (None: absent)."""
+    import shutil
+    return {t: shutil.which(t) for t in ("gfortran", "mpif90", "ifort", "ifx", "flang")}
+
+
+def compare_mixed_fp64(w, device, steps: int, grids=None) -> dict:
+    """The mixed form against the plain FP64 path on the full workload: both start from
+    the same particles and take `steps` steps; every step the accepted pairs of the two
+    are compared, and at the end the velocity error of the mixed form against the FP64
+    path (which follows the oracle bit for bit up to libm) is reported, over every
+    particle and over those that collided in neither run."""
+    import torch
+    setup, f, st = build_inputs(w, device, "mixed", steps)
+    st64 = {k: np.array(v, copy=True) for k, v in st.items()}
+    cm = make_context(setup, f, st, "mixed", device)
+    cf = make_context(setup, {k: v for k, v in f.items()}, st64, "fp64", device)
+    if grids:
+        cm.set_launch({**grids, "overlap_gather": False, "speculative_integrate": False})
+    n = cm.n
+    collided = np.zeros(n, dtype=bool)
+    flips, accepted, per_step = 0, 0, []
+    for _ in range(steps):
+        cm.step(1)
+        cf.step(1)
+        hm, nm = cm.collision_pairs()
+        hf, nf = cf.collision_pairs()
+        for h, nn in ((hm, nm), (hf, nf)):
+            collided[h] = True
+            collided[nn] = True
+        a = set(zip(hm.tolist(), nm.tolist()))
+        b = set(zip(hf.tolist(), nf.tolist()))
+        flips += len(a ^ b)
+        accepted += len(b)
+        per_step.append(len(a ^ b))
+    cm.raise_status("mixed comparison steps")
+    cf.raise_status("fp64 comparison steps")
+    gm, gf = cm.download(), cf.download()
+    cm.close()
+    cf.close()
+    del cm, cf
+    torch.cuda.empty_cache()
+    du = np.sqrt(sum((gm[k] - gf[k]) ** 2 for k in ("u", "v", "w")))
+    nu = np.sqrt(sum(gf[k] ** 2 for k in ("u", "v", "w")))
+    err = du / (nu + 1e-30)
+    free = err[~collided]
+    dx = np.sqrt(sum((gm[k] - gf[k]) ** 2 for k in ("x", "y", "z")))
+    return {"steps": steps, "particles": n, "velocity_rel_err": {
+                "max_never_collided": float(free.max()), "p99_never_collided": float(np.quantile(free, 0.99)),
+                "median_never_collided": float(np.median(free)), "max_all": float(err.max()),
+                "p99_all": float(np.quantile(err, 0.99)), "median_all": float(np.median(err))},
+            "position_abs_err_max": float(dx.max()),
+            "never_collided": int((~collided).sum()),
+            "pair_flips_total": flips, "pair_flips_per_step": per_step, "accepted_pairs_fp64": accepted,
+            "target": "<= 1e-5 relative velocity error against the FP64 path"}
+
+
+def time_batched(args, device) -> dict:
+    """The batched workload (64 classes on one shared 256^3 field) in the same process
+    after the single-ensemble run: autotuned grids, warm-up, one timed graph."""
+    import torch
+    from gazpart_b200 import config
+    w = config.C4
+    steps = max(5, args.steps // 2)
+    run_steps = args.warmup + steps + AUTOTUNE_STEPS + 6
+    setup, f, st = build_inputs(w, device, "mixed", run_steps)
+    ctx = make_context(setup, f, st, "mixed", device)
+    tune = None if args.no_autotune else ctx.autotune()
+    ctx.step(args.warmup)
+    ctx.sync()
+    torch.cuda.synchronize()
+    total_ms, phases, kps = ctx.step_timed(steps)
+    ctx.raise_status("batched steps")
+    n = ctx.n
+    ctx.close()
+    del ctx
+    torch.cuda.empty_cache()
+    return {"workload": w.name, "value": n * steps / (total_ms / 1e3), "unit": "particle-steps/s",
+            "classes": len(st), "particles": n, "steps": steps, "ms_per_step": total_ms / steps,
+            "phase_ms": phases, "kernels_per_step": kps, "launch_grids": tune}
+
+
 def workload_max_emaj(w) -> float:
     from gazpart_b200 import particles
     st = particles.draw(w.spec, w.setup())
@@ -370,9 +499,10 @@ def time_live_fluid(ctx, setup, f) -> dict:
     return out
 
 
-def run_serving(args, rank: int, world: int, local: int):
+def run_serving(args, rank: int, world: int, local: int, emit: bool = True):
     """Jobs arriving at 20/s for --serve-seconds, each on one of eight resident fields,
-    admitted against the HBM budget and stepped together until all are done."""
+    admitted against the HBM budget and stepped together until all are done.  Prints the
+    serving line (emit) or returns its fields."""
     import dataclasses
     import torch
     from gazpart_b200 import api, config, field, particles, serving
@@ -439,7 +569,14 @@ def run_serving(args, rank: int, world: int, local: int):
                 "e2e": {"value": value, "unit": "particle-steps/s",
                         "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
                         "note": "every job enters from and returns to host arrays"}}
+        if not emit:
+            return {"workload": w.name, "particle_steps_per_s": value,
+                    "latency_p50_s": summary["latency_p50_s"], "latency_p99_s": summary["latency_p99_s"],
+                    "jobs": len(jobs), "particles": total, "window_s": args.serve_seconds,
+                    "arrival_rate_per_s": w.rate_per_s, "hbm_budget_bytes": budget, "launch_grids": tune,
+                    "max_resident_jobs": summary.get("max_resident"), "clocks": clocks}
         print(json.dumps(line), flush=True)
+    return None
 
 
 # ---------------------------------------------------------------------------
@@ -629,23 +766,37 @@ def main():
         live_fluid = time_live_fluid(ctx, setup, f)
 
     plain = None
+    mixed_vs_fp64 = None
     if not args.no_plain and precision == "mixed":
         ctx.close()
         del ctx
         torch.cuda.empty_cache()
+        if rank == 0 and world == 1 and not batched:
+            mixed_vs_fp64 = compare_mixed_fp64(w, device, 10, {k: v for k, v in (tune or {}).items()
+                                                               if k in ("gather", "integrate", "bin", "search")})
         st2 = build_inputs(w, device, "fp64", run_steps)[2]
-        f64 = {k: v for k, v in f.items()}
-        pctx = make_context(setup, f64, st2, "fp64", device)
-        if not args.no_autotune:
-            pctx.autotune()
+        pctx = make_context(setup, {k: v for k, v in f.items()}, st2, "fp64", device)
+        ptune = None if args.no_autotune else pctx.autotune()
         pctx.step(max(1, args.warmup))
         pctx.sync()
-        tms, pph, _ = pctx.step_timed(max(5, args.steps // 5))
+        # the same graph length as the mixed value, so that both include one unoverlapped
+        # first step in the same proportion
+        tms, pph, _ = pctx.step_timed(args.steps)
         pctx.raise_status("fp64 steps")
-        plain = {"value": n * max(5, args.steps // 5) / (tms / 1e3), "phase_ms": pph}
+        plain = {"value": n * args.steps / (tms / 1e3), "steps": args.steps, "ms_per_step": tms / args.steps,
+                 "phase_ms": pph, "launch_grids": ptune}
         pctx.close()
+        del pctx
+        torch.cuda.empty_cache()
     else:
         ctx.close()
+        del ctx
+        torch.cuda.empty_cache()
+
+    batched_line = serving_line = None
+    if rank == 0 and world == 1 and not batched and not args.no_forms:
+        batched_line = time_batched(args, device)
+        serving_line = run_serving(args, 0, 1, local, emit=False)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and not batched:
@@ -653,9 +804,17 @@ def main():
         threads = os.cpu_count() or 1
         scale = 16 if w.grid >= 256 else 1
         r = time_cpu(w, 2, threads, scale, max_emaj)
+        r1 = time_cpu_one_thread(w, scale, max_emaj)
         cpu = {"value": r["value"], "unit": "particle-steps/s", "cores": threads, "kind": "port",
+               "cpu_model": cpu_model(),
                "sample": f"{r['n']} particles at the workload's density in a (L/{scale})^3 periodic box, "
-                         f"{r['candidates_per_step']} LM contact solves/step as the reference does, 2 steps"}
+                         f"{r['candidates_per_step']} LM contact solves/step as the reference does, 2 steps",
+               "one_thread": {"value": r1["value"], "unit": "particle-steps/s", "cores": 1,
+                              "sample": f"the same {r1['n']} particles: the advance timed whole, the collision "
+                                        f"phase timed on {r1['pairs_timed']} random candidate pairs of "
+                                        f"{r1['candidates_per_step']} (one LM solve each) and scaled",
+                              "advance_s": r1["t_adv"], "collision_s": r1["t_col"]},
+               "reference_fortran_toolchain": reference_compilers()}
 
     if rank == 0:
         line = {"metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
@@ -676,8 +835,10 @@ def main():
                 "kernels_per_step": kps, "phase_ms": phases,
                 "phase_note": phase_note(tune),
                 "phase_ms_one_step_graphs": phases_alone,
-                "clocks": clocks, "fp64_plain": plain, "restart_io": restart_io, "stats": stats,
-                "live_fluid": live_fluid}
+                "clocks": clocks, "fp64_plain": plain,
+                "mixed_over_fp64": None if plain is None else value / plain["value"],
+                "mixed_vs_fp64": mixed_vs_fp64, "batched": batched_line, "serving": serving_line,
+                "restart_io": restart_io, "stats": stats, "live_fluid": live_fluid}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

@@ -102,7 +102,9 @@ CT_QUAL double ct_poly_cos(double z) {
 }
 
 /* sin and cos of x: Cody-Waite reduction by pi/2 = P1 + P2 + P3 (33 + 33 + 53 bits, so
- * k*P1 and k*P2 are exact for |k| < 2^20), Taylor polynomials on [-pi/4, pi/4]. */
+ * k*P1 and k*P2 are exact for |k| < 2^20; the three parts are fdlibm's published
+ * pio2_1, pio2_2 and pio2_2t, e_rem_pio2.c), Taylor polynomials (coefficients 1/n!) on
+ * [-pi/4, pi/4]. */
 #ifdef GP_LM_INLINE
 #define CT_SINCOS_QUAL CT_QUAL
 #else

@@ -1075,7 +1075,9 @@ CT_QUAL double ct_poly_cos(double z) {
 }
 
 /* sin and cos of x: Cody-Waite reduction by pi/2 = P1 + P2 + P3 (33 + 33 + 53 bits, so
- * k*P1 and k*P2 are exact for |k| < 2^20), Taylor polynomials on [-pi/4, pi/4]. */
+ * k*P1 and k*P2 are exact for |k| < 2^20; the three parts are fdlibm's published
+ * pio2_1, pio2_2 and pio2_2t, e_rem_pio2.c), Taylor polynomials (coefficients 1/n!) on
+ * [-pi/4, pi/4]. */
 CT_QUAL void ct_sincos(double x, double *s, double *c) {
   if (!(fabs(x) < 1.0e9)) {
     *s = x - x + (0.0 / 0.0 + x * 0.0);
@@ -1148,6 +1150,16 @@ CT_QUAL double ct_asin(double x) {
 }
 
 CT_QUAL double ct_acos(double x) { return (1.5707963267948966 - ct_asin(x)) + 6.123233995736766e-17; }
+
+#ifdef ORC_LIBM_TRIG
+/* The reference's own trigonometry in the contact solve (libm sin, cos, asin, acos;
+ * ellipsoid_contact_detection.f90:77-87,193-334).  Built as a second library, it measures
+ * how often the shared functions above change a contact decision. */
+#define ct_sincos(x, s, c) (*(s) = sin(x), *(c) = cos(x))
+#define ct_cos cos
+#define ct_asin asin
+#define ct_acos acos
+#endif
 
 typedef struct {
     double e1[9], e2[9];     /* rotated ellipsoid matrices (calculate_ellipsoid_matrix.f90) */

@@ -15,6 +15,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libgazpart_oracle.so")
+# the same restatement with libm's sin/cos/asin/acos in the contact solve, as the
+# reference computes them (the default build shares its trigonometry with the device)
+LIB_PATHS = {"shared": LIB_PATH, "libm": os.path.join(HERE, "libgazpart_oracle_libm.so")}
 
 STATE_KEYS = ("x", "y", "z", "u", "v", "w", "qa", "qb", "qc", "qd", "ox", "oy", "oz")
 AUX_KEYS = ("ufap", "vfap", "wfap", "vortx", "vorty", "vortz")
@@ -50,26 +53,28 @@ class OrcBoxGrid(C.Structure):
                 ("delta_coll", C.c_double)]
 
 
-_lib = None
+_libs = {}
 
 
 def build() -> None:
     subprocess.run(["make", "-s", "-C", HERE], check=True)
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        if not os.path.exists(LIB_PATH):
+def lib(variant: str = "shared"):
+    """The oracle library: "shared" (contact-solve trigonometry shared with the device)
+    or "libm" (libm's, as the reference calls it)."""
+    if variant not in _libs:
+        path = LIB_PATHS[variant]
+        if not os.path.exists(path):
             build()
-        L = C.CDLL(LIB_PATH)
+        L = C.CDLL(path)
         L.orc_enorm.restype = C.c_double
         L.orc_fmargin.restype = C.c_double
         L.orc_detect_pairs.restype = C.c_int64
         L.orc_contact_detection.restype = C.c_int32
         L.orc_pair_eval.restype = C.c_int32
-        _lib = L
-    return _lib
+        _libs[variant] = L
+    return _libs[variant]
 
 
 def dptr(a: np.ndarray):
@@ -92,8 +97,9 @@ def make_setup(s) -> OrcSetup:
 class Ensemble:
     """Numpy-backed particle state + properties driven through the oracle."""
 
-    def __init__(self, setup, arrays: Dict[str, np.ndarray]):
+    def __init__(self, setup, arrays: Dict[str, np.ndarray], variant: str = "shared"):
         self.setup = setup
+        self.L = lib(variant)
         self.n = int(arrays["x"].shape[0])
         self.a = {}
         for k in STATE_KEYS + PROP_KEYS:
@@ -114,7 +120,7 @@ class Ensemble:
         s = make_setup(self.setup)
         st = self.state()
         eid = C.c_int64(-1)
-        rc = lib().orc_adv_particle_ellp(C.byref(s), C.byref(self.props()), arr, C.byref(st),
+        rc = self.L.orc_adv_particle_ellp(C.byref(s), C.byref(self.props()), arr, C.byref(st),
                                          C.c_int32(nthreads), C.byref(eid))
         self.last_err_id = eid.value
         return rc
@@ -122,13 +128,13 @@ class Ensemble:
     def boxgrid(self) -> OrcBoxGrid:
         g = OrcBoxGrid()
         s = make_setup(self.setup)
-        lib().orc_collision_initiation(C.byref(s), C.c_double(float(self.a["emaj"].max())), C.byref(g))
+        self.L.orc_collision_initiation(C.byref(s), C.c_double(float(self.a["emaj"].max())), C.byref(g))
         return g
 
     def connectivity(self, g: OrcBoxGrid):
         ncon = np.zeros(g.nbox, dtype=np.int32)
         con = np.zeros(g.nbox * 27, dtype=np.int32)
-        lib().orc_box_connectivity(C.byref(g), C.c_int32(int(bool(self.setup.periodicity))),
+        self.L.orc_box_connectivity(C.byref(g), C.c_int32(int(bool(self.setup.periodicity))),
                                    iptr(ncon), iptr(con))
         return ncon, con
 
@@ -141,7 +147,7 @@ class Ensemble:
         home = np.zeros(cap, dtype=np.int32)
         near = np.zeros(cap, dtype=np.int32)
         ncoll, ncand, ncont, eid = C.c_int64(), C.c_int64(), C.c_int64(), C.c_int64()
-        rc = lib().orc_collision(C.byref(s), C.byref(self.props()), C.byref(g), iptr(ncon), iptr(con),
+        rc = self.L.orc_collision(C.byref(s), C.byref(self.props()), C.byref(g), iptr(ncon), iptr(con),
                                  C.byref(st), C.c_int32(int(prefilter)), C.c_int32(nthreads),
                                  C.c_int64(cap), iptr(home), iptr(near), C.byref(ncoll),
                                  C.byref(ncand), C.byref(ncont), C.byref(eid))
@@ -164,7 +170,7 @@ class Ensemble:
             group = np.ascontiguousarray(group, dtype=np.int32)
             gp = iptr(group)
         ncoll, eid = C.c_int64(), C.c_int64()
-        rc = lib().orc_collision_stats(C.byref(s), C.byref(self.props()), C.byref(g), iptr(ncon), iptr(con),
+        rc = self.L.orc_collision_stats(C.byref(s), C.byref(self.props()), C.byref(g), iptr(ncon), iptr(con),
                                        C.byref(st), C.c_int32(int(prefilter)), gp, C.c_int32(ngroups),
                                        dptr(out), C.byref(ncoll), C.byref(eid))
         return rc, out.reshape(ngroups, ngroups, 8), ncoll.value
@@ -179,7 +185,7 @@ class Ensemble:
         if group is not None:
             group = np.ascontiguousarray(group, dtype=np.int32)
             gp = iptr(group)
-        lib().orc_stat_partfluid(C.byref(s), C.byref(self.props()), C.byref(st), gp, C.c_int32(ngroups), dptr(out))
+        self.L.orc_stat_partfluid(C.byref(s), C.byref(self.props()), C.byref(st), gp, C.c_int32(ngroups), dptr(out))
         return out.reshape(ngroups, 36)
 
 
@@ -251,10 +257,10 @@ def transform_vec(v, q):
     return v
 
 
-def contact_detection(emaj1, apr1, emaj2, apr2, b1, q1, b2, q2):
+def contact_detection(emaj1, apr1, emaj2, apr2, b1, q1, b2, q2, variant: str = "shared"):
     e1, e2, cn, xo = np.zeros(3), np.zeros(3), np.zeros(3), np.zeros(2)
     info, nfev = C.c_int32(), C.c_int32()
-    flag = lib().orc_contact_detection(C.c_double(emaj1), C.c_double(apr1), C.c_double(emaj2),
+    flag = lib(variant).orc_contact_detection(C.c_double(emaj1), C.c_double(apr1), C.c_double(emaj2),
                                        C.c_double(apr2), dptr(_v(b1, 3)), dptr(_v(q1, 4)),
                                        dptr(_v(b2, 3)), dptr(_v(q2, 4)), dptr(e1), dptr(e2),
                                        dptr(cn), dptr(xo), C.byref(info), C.byref(nfev))

@@ -50,12 +50,19 @@ def case(name: str):
         f = field.generate(48, seed=13, device="cpu")
         spec = config.ParticleSpec(n=20000, ar_range=(0.5, 2.0), b=0.02, st=1.0, seed=21)
         big = config.ParticleSpec(n=12, ar_range=(0.4, 3.0), b=0.08, st=1.0, seed=22)
+    elif name == "bimodal_small":
+        # the bimodal mix at a fifth of the small particles: cheap enough for the oracle's
+        # unfiltered pair walk in the CPU suite
+        setup = config.Setup(nx=48, ny=48, nz=48, visc=0.05, dtime=1e-3)
+        f = field.generate(48, seed=13, device="cpu")
+        spec = config.ParticleSpec(n=4000, ar_range=(0.5, 2.0), b=0.03, st=1.0, seed=23)
+        big = config.ParticleSpec(n=6, ar_range=(0.4, 3.0), b=0.08, st=1.0, seed=24)
     else:
         raise KeyError(name)
     fn = {k: v.numpy().copy() for k, v in f.items()}
     refs = field_refs(f)
     st = init_state(setup, spec, f, refs)
-    if name == "bimodal":
+    if name in ("bimodal", "bimodal_small"):
         st_big = init_state(setup, big, f, refs)
         st = {k: np.concatenate([st[k], st_big[k]]) for k in st}
     return setup, fn, refs, st

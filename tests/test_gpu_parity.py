@@ -80,12 +80,18 @@ def test_collision_pairs_bit_exact(name):
 
 @pytest.mark.parametrize("name", ["c1", "poly"])
 def test_hundred_steps(name):
-    """100-step trajectories: <= 1e-12 relative for every particle that has not collided.
+    """100-step trajectories run freely on both sides: <= 1e-12 relative for every
+    particle that has not collided, 1e-9 for all.
 
-    A collision's outcome depends on where the Levenberg-Marquardt solve stops
-    (xtol = sqrt(eps) = 1.5e-8); one-ulp differences between the device's and the host's
-    sin/cos move that point, so collided particles are held to 1e-9 (the pair sets
-    themselves are compared exactly in test_collision_pairs_bit_exact)."""
+    The device's advance differs from the oracle's by a few ulps: the force, torque and
+    quaternion routines call pow, atan, sin and cos, and the device's math library and
+    the host's differ there in the last bit.  The contact solve itself is identical on
+    both sides (shared trigonometry, IEEE operations; test_step_parity checks it bit for
+    bit from the same state), but where a Levenberg-Marquardt solve stops (xtol =
+    sqrt(eps)) moves with its inputs: one ulp of input moves a collided particle by about
+    1e-12 (test_oracle_trig), and along a free trajectory those differences compound
+    from collision to collision.  Pair sets from the same state are compared exactly in
+    test_collision_pairs_bit_exact and, every step, in test_step_parity."""
     setup, fn, refs, st = case(name)
     ens = po.Ensemble(setup, copy_state(st))
     worst_free = worst_all = 0.0
@@ -121,22 +127,52 @@ def test_graph_step_matches_api_calls():
         assert np.array_equal(ga[k], gb[k]), k
 
 
-def test_mixed_precision_error_budget():
-    setup, fn, refs, st = case("poly")
+@pytest.mark.parametrize("name", ["poly", "dense"])
+def test_mixed_precision_error_budget(name):
+    """The mixed form (FP32 field and stencil weights, FP32 drag/lift/torque
+    coefficients, FP64 integration and contact solve) against the FP64 oracle.
+
+    Free run, 50 steps on each side: the velocity of every particle that collided in
+    neither run within 1e-5 relative (the maximum, not a quantile).  Every step the same
+    state is also stepped once by the mixed device and the oracle: their accepted pairs
+    are compared; a pair decided by the last bits of the positions may flip, and the flips
+    are counted and held to 1% of the accepted pairs."""
+    setup, fn, refs, st = case(name)
     ens = po.Ensemble(setup, copy_state(st))
-    with _ctx(setup, fn, st, precision="mixed") as ctx:
+    collided = np.zeros(ens.n, dtype=bool)
+    mism = accepted = 0
+    with _ctx(setup, fn, st, precision="mixed") as free, _ctx(setup, fn, st, precision="mixed") as seeded:
         for step in range(50):
+            s0 = {k: ens.a[k].copy() for k in api.STATE_KEYS}
+            seeded.put_state(s0)
+            seeded.step(1)
+            sh, sn = seeded.collision_pairs()
+            free.step(1)
+            fh, fnr = free.collision_pairs()
+            collided[fh] = True
+            collided[fnr] = True
             assert ens.advance(refs, nthreads=8) == 0
-            assert ens.collide(prefilter=True, nthreads=8)["rc"] == 0
-        ctx.step(50)
-        ctx.raise_status()
-        got = ctx.download()
+            r = ens.collide(prefilter=True, nthreads=8)
+            assert r["rc"] == 0
+            collided[r["home"]] = True
+            collided[r["near"]] = True
+            a = set(zip(sh.tolist(), sn.tolist()))
+            b = set(zip(r["home"].tolist(), r["near"].tolist()))
+            mism += len(a ^ b)
+            accepted += len(b)
+        free.raise_status()
+        seeded.raise_status()
+        got = free.download()
     du = np.sqrt(sum((got[k] - ens.a[k]) ** 2 for k in ("u", "v", "w")))
     nu = np.sqrt(sum(ens.a[k] ** 2 for k in ("u", "v", "w")))
-    # particles that took part in a collision can diverge discretely; compare the rest
     err = du / (nu + 1e-30)
-    assert np.median(err) < 1e-6
-    assert np.quantile(err, 0.99) < 1e-5
+    free_err = float(np.max(err[~collided]))
+    print(f"\n{name}: mixed vs FP64 oracle after 50 steps: max {free_err:.2e} over {int((~collided).sum())} "
+          f"never-collided particles (all: median {np.median(err):.1e}, max {err.max():.1e}); "
+          f"pairs from the same state: {mism} flips in {accepted} accepted")
+    assert free_err < 1e-5
+    assert accepted > 0
+    assert mism <= max(1, accepted // 100)
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
