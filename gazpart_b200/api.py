@@ -374,6 +374,16 @@ class Context:
                                             C.byref(cnt)), "gp_collision_pairs")
         return home[:n], near[:n]
 
+    def set_pair_capacity(self, cap_pairs: int, cap_coll: int) -> None:
+        """Sizes of the candidate-pair and colliding-pair buffers (gp_set_pair_capacity);
+        a step that outgrows them grows them and runs again, with the same results."""
+        check(_lib.lib().gp_set_pair_capacity(self._h, int(cap_pairs), int(cap_coll)), "gp_set_pair_capacity")
+
+    def pair_capacity(self):
+        a, b = C.c_int64(), C.c_int64()
+        check(_lib.lib().gp_pair_capacity(self._h, C.byref(a), C.byref(b)), "gp_pair_capacity")
+        return a.value, b.value
+
     def collision_box_connectivity(self):
         nbox = C.c_int32()
         dims = np.zeros(3, dtype=np.int32)

@@ -557,6 +557,7 @@ __global__ void __launch_bounds__(256, GP_GATHER_MIN_BLOCKS) k_gather(const Inst
                                                 const PoolView* __restrict__ src_pv,
                                                 const int32_t* __restrict__ perm, int64_t n,
                                                 double* const* __restrict__ fluid, Status* st) {
+  if (step_halted(st)) return;
   const int lane = threadIdx.x & 31;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w * 32 < n; w += nwarps) {
@@ -662,6 +663,7 @@ __global__ void __launch_bounds__(128, GP_INTEGRATE_MIN_BLOCKS) k_integrate(cons
                                                                            const int32_t* __restrict__ perm, int64_t n,
                                                                            const double* const* __restrict__ fluid,
                                                                            uint32_t* __restrict__ mark, Status* st) {
+  if (step_halted(st)) return;
   for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
     const int64_t i = perm[j];
     if (mark != nullptr && mark[i] != 0u) {
@@ -685,6 +687,7 @@ __global__ void __launch_bounds__(128, GP_INTEGRATE_MIN_BLOCKS) k_integrate_fix(
                                                                                int64_t cap,
                                                                                const double* const* __restrict__ fluid,
                                                                                uint32_t* __restrict__ mark, Status* st) {
+  if (step_halted(st)) return;
   const int64_t np = (int64_t)min(*npairs, (unsigned long long)cap);
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < 2 * np; e += (int64_t)gridDim.x * blockDim.x) {
     const PairRec& r = pairs[e >> 1];
@@ -694,8 +697,10 @@ __global__ void __launch_bounds__(128, GP_INTEGRATE_MIN_BLOCKS) k_integrate_fix(
   }
 }
 
-// After an advance the destination buffer becomes the current one.
-static __global__ void k_swap_pool(PoolView* a, PoolView* b) {
+// After an advance the destination buffer becomes the current one (not after an advance
+// that a halted step skipped).
+static __global__ void k_swap_pool(PoolView* a, PoolView* b, const Status* st) {
+  if (step_halted(st)) return;
   const PoolView t = *a;
   *a = *b;
   *b = t;

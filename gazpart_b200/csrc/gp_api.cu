@@ -460,8 +460,9 @@ int enqueue_bin_search(gp_ctx *c, bool flag = false) {
   GP_TRY(enqueue_bin(c));
   GP_TRY(mark(c, 2 * GP_PHASE_BIN + 1, c->stream));
   GP_TRY(mark(c, 2 * GP_PHASE_SEARCH, c->stream));
-  launch_search(c->d_inst, c->n, sa, c->d_pairs, c->d_counters + 0, c->cap_pairs, c->d_status,
-                c->tune[GP_TUNE_SEARCH], c->stream);
+  // a step with more candidates than either pair buffer holds halts after the search
+  launch_search(c->d_inst, c->n, sa, c->d_pairs, c->d_counters + 0, std::min(c->cap_pairs, c->cap_coll),
+                c->d_status, c->tune[GP_TUNE_SEARCH], c->stream);
   GP_CK(cudaGetLastError());
   return mark(c, 2 * GP_PHASE_SEARCH + 1, c->stream);
 }
@@ -539,6 +540,60 @@ int enqueue_steps(gp_ctx *c, int nsteps, cudaEvent_t *marks) {
 int read_status(gp_ctx *c, Status *h) {
   GP_CK(cudaMemcpyAsync(h, c->d_status, sizeof(Status), cudaMemcpyDeviceToHost, c->stream));
   GP_CK(cudaStreamSynchronize(c->stream));
+  return GP_OK;
+}
+
+// Pair buffers with room for `pairs` candidate pairs (and as many colliding pairs, so
+// that the colliding-pair buffer cannot fill during the contact solves): grown by at
+// least a quarter, never shrunk.  Captured graphs hold the old buffers and are dropped.
+int size_pairs(gp_ctx *c, int64_t pairs, int64_t coll) {
+  const int64_t np = std::max(c->cap_pairs, pairs), nc = std::max(c->cap_coll, coll);
+  if (np == c->cap_pairs && nc == c->cap_coll) return GP_OK;
+  GP_CK(cudaStreamSynchronize(c->stream));
+  GP_CK(cudaStreamSynchronize(c->side));
+  drop_graph(c);
+  if (np != c->cap_pairs) {
+    dfree(c->d_pairs);
+    c->cap_pairs = 0;
+    GP_TRY(dalloc(&c->d_pairs, np));
+    c->cap_pairs = np;
+    if (c->d_cst) {                    // every candidate pair may be in contact
+      dfree(c->d_cst);
+      c->cap_cst = 0;
+      GP_TRY(dalloc(&c->d_cst, (size_t)np));
+      c->cap_cst = np;
+    }
+  }
+  if (nc != c->cap_coll) {
+    dfree(c->d_coll); dfree(c->d_state); dfree(c->d_acc);
+    c->cap_coll = 0;
+    GP_TRY(dalloc(&c->d_coll, nc));
+    GP_TRY(dalloc(&c->d_state, nc));
+    GP_TRY(dalloc(&c->d_acc, nc));
+    c->cap_coll = nc;
+  }
+  return GP_OK;
+}
+
+// A step whose candidate pairs outgrew the buffers stopped after its advance (every
+// later kernel saw the flag and returned; see Status).  This grows the buffers to the
+// count that step reached, clears the flag (and the status code it set, unless another
+// error came first) and runs that step's collision phase again; the loop ends once a
+// collision phase fits.  *halted: whether h showed a halt.
+int resume_after_halt(gp_ctx *c, Status h, bool *halted) {
+  *halted = h.overflow != 0;
+  for (int attempt = 0; h.overflow; ++attempt) {
+    if (attempt >= 4) return GP_EPAIR_OVERFLOW;
+    const int64_t need = (int64_t)h.pairs_needed;
+    const int64_t grow = std::max<int64_t>(need + need / 4 + 1024, c->cap_pairs + c->cap_pairs / 4);
+    GP_TRY(size_pairs(c, grow, grow));
+    if (h.code == GP_EPAIR_OVERFLOW) { h.code = 0; h.first_id = 0; h.first_inst = 0; }
+    h.overflow = 0;
+    h.pairs_needed = 0;
+    GP_CK(cudaMemcpyAsync(c->d_status, &h, sizeof(Status), cudaMemcpyHostToDevice, c->stream));
+    GP_TRY(enqueue_collision(c));
+    GP_TRY(read_status(c, &h));
+  }
   return GP_OK;
 }
 
@@ -1187,6 +1242,21 @@ int gp_step_host(gp_ctx *c, int64_t n, const double *const *in_cols, double *con
     if ((kColsVelSpin >> k) & 1u)
       GP_CK(cudaMemcpyAsync(out_cols[k], tmp + (size_t)k * n, bytes, cudaMemcpyDeviceToHost, c->side));
   GP_CK(cudaStreamSynchronize(c->side));
+  // a collision phase halted by a pair-buffer overflow sent pre-collision velocities:
+  // it runs again with larger buffers and its velocities and spins go out again
+  Status h;
+  bool halted = false;
+  GP_TRY(read_status(c, &h));
+  GP_TRY(resume_after_halt(c, h, &halted));
+  if (halted) {
+    launch_gather_state(c->d_inst, c->d_pv, c->n_slots, -1, tmp, c->d_fluid_cols, nullptr, n, c->stream,
+                        kColsVelSpin);
+    GP_CK(cudaGetLastError());
+    for (int k = 0; k < kNState; ++k)
+      if ((kColsVelSpin >> k) & 1u)
+        GP_CK(cudaMemcpyAsync(out_cols[k], tmp + (size_t)k * n, bytes, cudaMemcpyDeviceToHost, c->stream));
+    GP_CK(cudaStreamSynchronize(c->stream));
+  }
   return GP_OK;
 }
 
@@ -1200,15 +1270,17 @@ int gp_collision(gp_ctx *c, int32_t /*ncycle*/, double /*time*/, int64_t *n_near
   if (!c || c->n <= 0 || !c->grid_ready) return GP_EBADARG;
   GP_CK(cudaMemsetAsync(&c->d_status->n_near, 0, 8 * sizeof(unsigned long long), c->stream));
   GP_TRY(enqueue_collision(c));
+  Status h;
+  GP_TRY(read_status(c, &h));
+  bool halted = false;
+  GP_TRY(resume_after_halt(c, h, &halted));
   if (n_near || n_contact || n_coll) {
-    Status h;
     GP_TRY(read_status(c, &h));
     unsigned long long cnt[4];
     GP_CK(cudaMemcpy(cnt, c->d_counters, sizeof(cnt), cudaMemcpyDeviceToHost));
     if (n_near) *n_near = (int64_t)h.n_near;
     if (n_contact) *n_contact = (int64_t)h.n_contact;
     if (n_coll) *n_coll = (int64_t)cnt[1];
-    if (h.overflow) return GP_EPAIR_OVERFLOW;
   }
   return GP_OK;
 }
@@ -1229,10 +1301,9 @@ int capture_steps(gp_ctx *c, int nsteps, cudaEvent_t *marks, cudaGraph_t *g) {
   return rc;
 }
 
-int gp_step(gp_ctx *c, int32_t nsteps) {
-  if (!c || c->n <= 0 || !c->grid_ready || nsteps < 0) return GP_EBADARG;
-  if (nsteps == 0) return GP_OK;
-  // one graph per step count in use (the cache is bounded; replays reuse it)
+// Replays `nsteps` steps from the graph cache (one graph per step count in use; the
+// cache is bounded).
+int replay_steps(gp_ctx *c, int nsteps) {
   auto it = c->graphs.find(nsteps);
   if (it == c->graphs.end()) {
     if (c->graphs.size() >= 8) drop_graph(c);
@@ -1246,6 +1317,26 @@ int gp_step(gp_ctx *c, int32_t nsteps) {
   }
   GP_CK(cudaGraphLaunch(it->second, c->stream));
   c->fluid_ok = true;   // a replay samples the fluid as the capture did
+  return GP_OK;
+}
+
+int gp_step(gp_ctx *c, int32_t nsteps) {
+  if (!c || c->n <= 0 || !c->grid_ready || nsteps < 0) return GP_EBADARG;
+  // Steps halted by a pair-buffer overflow: the halted step is finished with larger
+  // buffers (resume_after_halt) and the steps after it are replayed.
+  int remaining = nsteps;
+  for (int attempt = 0; remaining > 0; ++attempt) {
+    if (attempt > 32) return GP_EPAIR_OVERFLOW;
+    GP_CK(cudaMemsetAsync(&c->d_status->steps_done, 0, sizeof(unsigned long long), c->stream));
+    GP_TRY(replay_steps(c, remaining));
+    Status h;
+    GP_TRY(read_status(c, &h));
+    bool halted = false;
+    const int64_t done = (int64_t)h.steps_done;
+    GP_TRY(resume_after_halt(c, h, &halted));
+    if (!halted) break;
+    remaining -= (int)done + 1;
+  }
   return GP_OK;
 }
 
@@ -1275,6 +1366,19 @@ int gp_step_timed(gp_ctx *c, int32_t nsteps, float *total_ms, float *phase_ms_av
   }
   if (!rc && cudaGraphLaunch(ge, c->stream) != cudaSuccess) rc = GP_ECUDA;
   if (!rc && cudaStreamSynchronize(c->stream) != cudaSuccess) rc = GP_ECUDA;
+  if (!rc) {
+    // a graph halted by a pair-buffer overflow timed a short step; its halted step is
+    // finished with larger buffers and the whole measurement is taken again
+    Status h;
+    bool halted = false;
+    rc = read_status(c, &h);
+    if (!rc) rc = resume_after_halt(c, h, &halted);
+    if (!rc && halted) {
+      if (ge) cudaGraphExecDestroy(ge);
+      for (auto &x : ev) cudaEventDestroy(x);
+      return gp_step_timed(c, nsteps, total_ms, phase_ms_avg, kernels_per_step);
+    }
+  }
   if (!rc) {
     double acc[GP_NPHASE] = {};
     float t = 0.f;
@@ -1657,6 +1761,12 @@ int gp_serve(gp_ctx *c, gp_job *jobs, int32_t njobs, double hbm_budget, double b
     Status h;
     rc = read_status(c, &h);
     if (rc) break;
+    if (h.overflow) {
+      bool halted = false;
+      rc = resume_after_halt(c, h, &halted);
+      if (!rc) rc = read_status(c, &h);
+      if (rc) break;
+    }
     for (int j : running) {
       --left[j];
       done_work += jobs[j].n;
@@ -1677,6 +1787,36 @@ int gp_serve(gp_ctx *c, gp_job *jobs, int32_t njobs, double hbm_budget, double b
   }
   if (particle_steps) *particle_steps = done_work;
   return rc;
+}
+
+int gp_set_pair_capacity(gp_ctx *c, int64_t cap_pairs, int64_t cap_coll) {
+  if (!c || cap_pairs < 1 || cap_coll < 1 || !c->d_pairs) return GP_EBADARG;
+  GP_CK(cudaStreamSynchronize(c->stream));
+  GP_CK(cudaStreamSynchronize(c->side));
+  // drop to one slot first so that size_pairs reallocates at exactly these sizes
+  drop_graph(c);
+  dfree(c->d_pairs); dfree(c->d_coll); dfree(c->d_state); dfree(c->d_acc);
+  c->cap_pairs = c->cap_coll = 0;
+  GP_TRY(dalloc(&c->d_pairs, cap_pairs));
+  c->cap_pairs = cap_pairs;
+  GP_TRY(dalloc(&c->d_coll, cap_coll));
+  GP_TRY(dalloc(&c->d_state, cap_coll));
+  GP_TRY(dalloc(&c->d_acc, cap_coll));
+  c->cap_coll = cap_coll;
+  if (c->d_cst) {
+    dfree(c->d_cst);
+    c->cap_cst = 0;
+    GP_TRY(dalloc(&c->d_cst, (size_t)cap_pairs));
+    c->cap_cst = cap_pairs;
+  }
+  return GP_OK;
+}
+
+int gp_pair_capacity(gp_ctx *c, int64_t *cap_pairs, int64_t *cap_coll) {
+  if (!c) return GP_EBADARG;
+  if (cap_pairs) *cap_pairs = c->cap_pairs;
+  if (cap_coll) *cap_coll = c->cap_coll;
+  return GP_OK;
 }
 
 int gp_set_launch(gp_ctx *c, const int32_t *grids) {

@@ -34,6 +34,7 @@ __global__ void __launch_bounds__(128, GP_CONTACT_MIN_BLOCKS) k_contact(const In
                                                     int64_t cap_cst, TailRec *__restrict__ tail,
                                                     unsigned long long *ntail, int64_t cap_tail, int tail_budget,
                                                     Status *st) {
+  if (step_halted(st)) return;
   const int64_t np = (int64_t)min(*npairs, (unsigned long long)cap_pairs);
   const unsigned lane = threadIdx.x & 31u;
   constexpr unsigned kFull = 0xffffffffu;

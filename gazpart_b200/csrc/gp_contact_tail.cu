@@ -24,6 +24,7 @@ __global__ void __launch_bounds__(32, GP_TAIL_MIN_BLOCKS) k_contact_tail(const I
                                int64_t cap_tail, CollRec *__restrict__ coll, unsigned long long *ncoll,
                                int64_t cap_coll, ContactStatRec *__restrict__ cst, unsigned long long *ncst,
                                int64_t cap_cst, Status *st) {
+  if (step_halted(st)) return;
   const int64_t nt = (int64_t)min(*ntail, (unsigned long long)cap_tail);
   // record r = thread * blocks + block: the records go round the SMs first
   for (int64_t r = (int64_t)threadIdx.x * gridDim.x + blockIdx.x; r < nt; r += (int64_t)gridDim.x * blockDim.x) {

@@ -26,14 +26,14 @@ void launch_gather_fp64(const InstDev *insts, const PoolView *pv, const int32_t 
 void launch_integrate_fp64(const InstDev *insts, PoolView *pv, PoolView *pv_alt, const int32_t *perm, int64_t n,
                          double *const *fluid, Status *st, int grid, cudaStream_t s, uint32_t *mark) {
   k_integrate<false><<<grid, 128, 0, s>>>(insts, pv, pv_alt, perm, n, fluid, mark, st);
-  if (mark == nullptr) k_swap_pool<<<1, 1, 0, s>>>(pv, pv_alt);
+  if (mark == nullptr) k_swap_pool<<<1, 1, 0, s>>>(pv, pv_alt, st);
 }
 
 void launch_integrate_fix_fp64(const InstDev *insts, PoolView *pv, PoolView *pv_alt, const PairRec *pairs,
                              const unsigned long long *npairs, int64_t cap_pairs, double *const *fluid,
                              uint32_t *mark, Status *st, int grid, cudaStream_t s) {
   k_integrate_fix<false><<<grid, 128, 0, s>>>(insts, pv, pv_alt, pairs, npairs, cap_pairs, fluid, mark, st);
-  k_swap_pool<<<1, 1, 0, s>>>(pv, pv_alt);
+  k_swap_pool<<<1, 1, 0, s>>>(pv, pv_alt, st);
 }
 
 // INTERP_LAG3 (interp_lag3.f90:11-298) for one component at arbitrary points.
@@ -127,6 +127,8 @@ __global__ void k_response(const InstDev *__restrict__ insts, const PoolView *__
                            const CollRec *__restrict__ coll, const unsigned long long *__restrict__ ncoll,
                            int64_t cap_coll, const int8_t *__restrict__ state, int32_t *acc_list,
                            unsigned long long *nacc, Status *st) {
+  if (step_halted(st)) return;
+  if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&st->steps_done, 1ull);
   const PoolView P = *pv;
   const int64_t nc = (int64_t)min(*ncoll, (unsigned long long)cap_coll);
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nc; e += (int64_t)gridDim.x * blockDim.x) {

@@ -22,14 +22,14 @@ void launch_gather_mixed(const InstDev *insts, const PoolView *pv, const int32_t
 void launch_integrate_mixed(const InstDev *insts, PoolView *pv, PoolView *pv_alt, const int32_t *perm, int64_t n,
                          double *const *fluid, Status *st, int grid, cudaStream_t s, uint32_t *mark) {
   k_integrate<true><<<grid, 128, 0, s>>>(insts, pv, pv_alt, perm, n, fluid, mark, st);
-  if (mark == nullptr) k_swap_pool<<<1, 1, 0, s>>>(pv, pv_alt);
+  if (mark == nullptr) k_swap_pool<<<1, 1, 0, s>>>(pv, pv_alt, st);
 }
 
 void launch_integrate_fix_mixed(const InstDev *insts, PoolView *pv, PoolView *pv_alt, const PairRec *pairs,
                              const unsigned long long *npairs, int64_t cap_pairs, double *const *fluid,
                              uint32_t *mark, Status *st, int grid, cudaStream_t s) {
   k_integrate_fix<true><<<grid, 128, 0, s>>>(insts, pv, pv_alt, pairs, npairs, cap_pairs, fluid, mark, st);
-  k_swap_pool<<<1, 1, 0, s>>>(pv, pv_alt);
+  k_swap_pool<<<1, 1, 0, s>>>(pv, pv_alt, st);
 }
 
 }  // namespace gp

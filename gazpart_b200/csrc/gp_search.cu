@@ -64,7 +64,8 @@ __device__ __forceinline__ int cell_coord(double v, double h, int n) {
 }
 
 __global__ void k_bin_count(const InstDev *__restrict__ insts, const PoolView *__restrict__ pv, int64_t n,
-                            SearchArrays sa) {
+                            SearchArrays sa, const Status *st) {
+  if (step_halted(st)) return;
   const PoolView P = *pv;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   const int64_t nround = (n + stride - 1) / stride * stride;   // whole warps stay in the loop
@@ -89,9 +90,9 @@ __global__ void k_bin_count(const InstDev *__restrict__ insts, const PoolView *_
   }
 }
 
-void launch_bin_count(const InstDev *insts, const PoolView *pv, int64_t n, SearchArrays sa, Status *,
+void launch_bin_count(const InstDev *insts, const PoolView *pv, int64_t n, SearchArrays sa, Status *st,
                       int grid, cudaStream_t s) {
-  k_bin_count<<<grid, 256, 0, s>>>(insts, pv, n, sa);
+  k_bin_count<<<grid, 256, 0, s>>>(insts, pv, n, sa, st);
 }
 
 // ---------------------------------------------------------------------------
@@ -181,6 +182,7 @@ void launch_scan(const int32_t *in, int32_t *out, int64_t n, int32_t *tmp, cudaS
 // ---------------------------------------------------------------------------
 __global__ void k_bin_scatter(const InstDev *__restrict__ insts, const PoolView *__restrict__ pv, int64_t n,
                               SearchArrays sa, Status *st) {
+  if (step_halted(st)) return;
   const PoolView P = *pv;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   const int64_t nround = (n + stride - 1) / stride * stride;
@@ -255,6 +257,7 @@ __device__ __forceinline__ void emit_pair(PairRec *pairs, unsigned long long *np
     }
   } else {
     atomicAdd(&st->overflow, 1ull);
+    atomicMax(&st->pairs_needed, slot + 1ull);
     set_error(st, GP_EPAIR_OVERFLOW, (long long)r.home);
   }
 }
@@ -412,6 +415,10 @@ constexpr int kMaxRanges = 10;   // 5 rows, each at most two contiguous ranges
 __global__ void __launch_bounds__(kSearchThreads, GP_SEARCH_MIN_BLOCKS) k_search(
     const InstDev *__restrict__ insts, int64_t n, SearchArrays sa, PairRec *__restrict__ pairs,
     unsigned long long *npairs, int64_t cap, Status *st) {
+  // no halt test here: this kernel is what raises the flag, and a later block must not
+  // skip its pairs because an earlier one overflowed (the count it leaves in
+  // pairs_needed sizes the buffers).  In a step after a halted one the binning did not
+  // run and every cell is empty (its counts were cleared), so the sweep finds nothing.
   __shared__ HomeRec homes[kSearchThreads];
   __shared__ int32_t rstart[kSearchThreads][kMaxRanges];   // first sorted particle of a range
   __shared__ int32_t rcum[kSearchThreads][kMaxRanges];     // candidates of the home before it
@@ -588,6 +595,7 @@ __global__ void __launch_bounds__(kMatchThreads) k_match(const CollRec *__restri
                                                          const unsigned long long *__restrict__ ncoll, int64_t cap,
                                                          unsigned long long *best1, unsigned long long *best2,
                                                          int8_t *matched, int8_t *state, Status *st) {
+  if (step_halted(st)) return;
   __shared__ int remaining_s[kMatchThreads / 32];
   __shared__ int remaining;
   const int64_t nc = (int64_t)min(*ncoll, (unsigned long long)cap);

@@ -205,7 +205,8 @@ void launch_stat_partfluid(const InstDev *insts, const PoolView *pv, int64_t n, 
 // both particles (best1/best2, reset to all ones afterwards).
 __global__ void k_colour_keys(const CollRec *__restrict__ coll, const unsigned long long *__restrict__ ncoll,
                               int64_t cap, const int8_t *__restrict__ state, unsigned long long *best1,
-                              unsigned long long *best2, int set, unsigned long long *steps) {
+                              unsigned long long *best2, int set, unsigned long long *steps, const Status *st) {
+  if (step_halted(st)) return;
   const int64_t nc = (int64_t)min(*ncoll, (unsigned long long)cap);
   if (steps && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(steps, 1ull);   // one more step in the sums
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nc; e += (int64_t)gridDim.x * blockDim.x) {
@@ -228,6 +229,7 @@ __global__ void k_collision_stats(const ContactStatRec *__restrict__ rec, const 
                                   const int32_t *const *__restrict__ group_tab, const int32_t *__restrict__ ngroups,
                                   const unsigned long long *__restrict__ best1,
                                   const unsigned long long *__restrict__ best2, double *acc, Status *st) {
+  if (step_halted(st)) return;
   const int64_t nr = (int64_t)min(*nrec, (unsigned long long)cap);
   const PoolView *__restrict__ P = pv;
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nr; e += (int64_t)gridDim.x * blockDim.x) {
@@ -258,9 +260,9 @@ void launch_collision_stats(const CollRec *coll, const unsigned long long *ncoll
                             const ContactStatRec *rec, const unsigned long long *nrec, int64_t cap_rec,
                             const PoolView *pv, const int32_t *const *group_tab, const int32_t *ngroups, double *acc,
                             unsigned long long *steps, Status *st, cudaStream_t s) {
-  k_colour_keys<<<148, 256, 0, s>>>(coll, ncoll, cap_coll, state, best1, best2, 1, steps);
+  k_colour_keys<<<148, 256, 0, s>>>(coll, ncoll, cap_coll, state, best1, best2, 1, steps, st);
   k_collision_stats<<<148 * 2, 256, 0, s>>>(rec, nrec, cap_rec, pv, group_tab, ngroups, best1, best2, acc, st);
-  k_colour_keys<<<148, 256, 0, s>>>(coll, ncoll, cap_coll, state, best1, best2, 0, nullptr);
+  k_colour_keys<<<148, 256, 0, s>>>(coll, ncoll, cap_coll, state, best1, best2, 0, nullptr, st);
 }
 
 }  // namespace gp

@@ -56,7 +56,17 @@ struct Status {
   unsigned long long n_solve;     // contact solves run (pairs not proven disjoint)
   unsigned long long n_eval;      // function evaluations of those solves
   unsigned long long max_eval;    // largest evaluation count of one solve
+  // A step whose candidate pairs outgrow the pair buffers sets `overflow` at its search;
+  // from then on every step kernel returns at entry (step_halted), so that step stops
+  // after its advance and later steps of a graph do nothing.  pairs_needed: the largest
+  // candidate count such a step reached.  steps_done: steps whose response ran.
+  unsigned long long pairs_needed;
+  unsigned long long steps_done;
 };
+
+__device__ __forceinline__ bool step_halted(const Status *s) {
+  return *reinterpret_cast<const volatile unsigned long long *>(&s->overflow) != 0ull;
+}
 
 __device__ inline void set_error(Status *s, int code, long long id, int inst = -1) {
   if (atomicCAS(&s->code, 0, code) == 0) {

@@ -311,6 +311,22 @@ int gp_autotune(gp_ctx *ctx, int32_t *grids_out);
  * 4 bytes of device memory per pool slot; without them it returns GP_ENOMEM (and the
  * autotuner does not try it). */
 int gp_set_launch(gp_ctx *ctx, const int32_t *grids);
+/* Pair buffers.  The reference's candidate list is a static array of 1e8 pairs with no
+ * check on it (collision.f90:35-37, collision_detection_connectivity.f90:171,189).  Here
+ * the candidate-pair buffer starts at max(2^20, particle capacity) and the colliding-pair
+ * buffer at a quarter of that.  A step whose candidates outgrow either one stops after
+ * its advance (its search counts how many it needed), every later step of the same
+ * graph does nothing, and the call that ran it grows both buffers to the counted need
+ * plus a quarter, runs that step's collision phase again and carries on with the steps
+ * that remain: gp_step, gp_collision, gp_step_host, gp_step_timed and gp_serve all
+ * finish with the same states and pairs as with large enough buffers from the start.
+ * (gp_collision_counters then counts that step's candidate pairs twice: its halted
+ * search and the one that ran again.)
+ * gp_set_pair_capacity sets both sizes (in pairs) directly, smaller or larger;
+ * gp_pair_capacity reports them (either pointer may be NULL).  No counterpart in the
+ * reference. */
+int gp_set_pair_capacity(gp_ctx *ctx, int64_t cap_pairs, int64_t cap_coll);
+int gp_pair_capacity(gp_ctx *ctx, int64_t *cap_pairs, int64_t *cap_coll);
 /* Last step's accepted collisions as (home, near) original indices, in acceptance
  * (list) order; *count receives the total even if it exceeds cap. */
 int gp_collision_pairs(gp_ctx *ctx, int64_t cap, int32_t *home, int32_t *near, int64_t *count);

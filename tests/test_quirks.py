@@ -52,6 +52,48 @@ def test_q1_wall_test_runs_in_a_periodic_box():
     assert 0.0 < ens.a["x"][0] < 1.0                       # not wrapped to x near L
 
 
+def test_q1_rebound_of_a_slender_spheroid_stops_the_run_at_dt_5e4():
+    """Q1 with the 512^3 / 16.8M workload's viscosity and time step (dt = 5e-4): a slender
+    spheroid of that workload's distribution (AR 4.65, EMAJ 4.1e-3) closing on x = 0 in
+    the periodic box rebounds off the plane (adv_particle_new.f90:331-336), which spins it
+    to about 1.7e3 rad/s.  The explicit RK2 update of its angular velocity
+    (adv_particle_new.f90:278-320,516-632) is then unstable at this time step: |omega|
+    grows about twofold per step until the drag is NaN and the reference stops with 'In
+    Fluid force' (fluid_force_ellipsoid.f90:150-159), 25 steps in.  The same particle in
+    the middle of the box runs on.  This is why the benchmark starts its particles away
+    from the x planes (the x margin of its configuration)."""
+    w = config.C3
+    base = w.setup()
+    s = config.Setup(nx=64, ny=64, nz=64, visc=base.visc, dtime=base.dtime)
+    assert s.dtime == 5e-4
+    f = field.generate(64, seed=0, device="cpu")
+    refs = [field.reference_layout(f[k], "periodic" if k in ("u", "v", "w") else "zero").numpy().copy()
+            for k in field.COMPONENTS_6]
+    one = {"x": 6.549342494148082e-06, "y": 1.4964149544965306, "z": 2.1935648850209564,
+           "u": -3.0960604761170893, "v": 1.2298512984753176, "w": -0.921259617618018,
+           "qa": -0.9623316742411799, "qb": 0.0795140439437744, "qc": -0.16238840459726478,
+           "qd": -0.20304007392687276, "ox": -3.2352054866547233, "oy": 3.9569619383875083,
+           "oz": -4.520435237028644, "emaj": 0.004110331918409437, "apr": 4.651382660313813,
+           "rhop": 3309.8084025581375, "ipxx": 3.123558465370345e-07, "ipyy": 3.535143619167598e-06,
+           "ipzz": 3.535143619167598e-06}
+    ens = po.Ensemble(s, {k: np.array([v]) for k, v in one.items()})
+    spins = []
+    rc = 0
+    for step in range(40):
+        rc = ens.advance(refs)
+        if rc:
+            break
+        spins.append(float(np.sqrt(ens.a["ox"][0] ** 2 + ens.a["oy"][0] ** 2 + ens.a["oz"][0] ** 2)))
+    assert rc == 1 and step == 25                          # GP_ENAN_FORCE: 'In Fluid force'
+    assert 1e3 < spins[0] < 3e3                            # the rebound's spin
+    growth = [spins[k + 1] / spins[k] for k in range(4, 14)]
+    assert min(growth) > 1.3                               # the RK2 spin update diverges
+    mid = {k: np.array([v]) for k, v in one.items()}
+    mid["x"] = np.array([s.lx / 2.0])
+    e2 = po.Ensemble(s, mid)
+    assert all(e2.advance(refs) == 0 for _ in range(60))
+
+
 def _angle(q0, q1):
     d = abs(float(np.dot(q0, q1)) / (np.linalg.norm(q0) * np.linalg.norm(q1)))
     return 2.0 * np.arccos(min(d, 1.0))
