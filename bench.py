@@ -215,14 +215,12 @@ def gather_bytes_per_particle(components: int, field_bytes: int) -> int:
 
 
 # DRAM bytes (read + write) per particle of one k_gather launch, from ncu
-# (dram__bytes_read.sum + dram__bytes_write.sum) on the steady-state step; the file
-# under profiles/ named in the value gives the command and the capture.
-# DRAM bytes per particle of one gather launch, from ncu, by workload, precision and the
-# gather's grid (the L2 reuse between neighbouring stencils depends on how many blocks
-# run at once)
+# (dram__bytes_read.sum + dram__bytes_write.sum) on the steady-state step; the file under
+# profiles/ named in the value gives the command and the capture.  The gather's warps
+# take consecutive runs of the cell order from one counter, so the figure does not
+# depend on the gather's grid.
 GATHER_TRAFFIC = {
-    ("c3_512cube_n16777216_fp32field", "mixed", 296): (375.5, "profiles/k_gather_k_integrate_c3_dram.md"),
-    ("c3_512cube_n16777216_fp32field", "mixed", 2368): (602.2, "profiles/k_gather_k_integrate_c3_dram.md"),
+    ("c3_512cube_n16777216_fp32field", "mixed"): (286.2, "profiles/k_gather_k_integrate_c3_dram.md"),
 }
 
 
@@ -707,12 +705,13 @@ def main():
     bpp = gather_bytes_per_particle(6, fbytes)
     peak, peak_kind = hbm_peak()
     achieved = bpp * n / (alone / 1e3) / 1e9
-    tr = GATHER_TRAFFIC.get((w.name, precision, (tune or {}).get("gather", 148 * 8)))
+    tr = GATHER_TRAFFIC.get((w.name, precision))
     roofline = {"bound": "hbm", "kernel": "k_gather", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": peak_kind,
                 "bytes_per_launch": bpp * n, "bytes_per_particle": bpp, "kernel_ms": alone,
                 "kernel_ms_source": "median of three one-step graphs run right after the timed region",
-                "traffic": None if tr is None else tr[0] * n, "traffic_source": None if tr is None else tr[1]}
+                "traffic": None if tr is None else tr[0] * n, "traffic_source": None if tr is None else tr[1],
+                "traffic_gbs": None if tr is None else tr[0] * n / (alone / 1e3) / 1e9}
 
     # end to end through the C ABI with host buffers: H2D of the state, one step,
     # D2H of the state, every step

@@ -467,14 +467,6 @@ __device__ __forceinline__ void load_pc(const PoolView& P, int64_t i, PartConst&
   pc.ipxx = P.pc[7][i]; pc.ipyy = P.pc[8][i]; pc.ipzz = P.pc[9][i];
 }
 
-// Kahan step: sum += w*v with the lost low part carried in cmp.
-__device__ __forceinline__ void kahan_fma(float& sum, float& cmp, float w, float v) {
-  const float y = __fmaf_rn(w, v, -cmp);
-  const float t = __fadd_rn(sum, y);
-  cmp = __fsub_rn(__fsub_rn(t, sum), y);
-  sum = t;
-}
-
 __device__ __forceinline__ float pick4(const float f[4], int k) {
   return k == 0 ? f[0] : (k == 1 ? f[1] : (k == 2 ? f[2] : f[3]));
 }
@@ -482,9 +474,15 @@ __device__ __forceinline__ float pick4(const float f[4], int k) {
 // Warp-cooperative FP32 gather for the 32 particles of one warp.  Eight lanes serve one
 // particle: lane t of the group loads float4 (t & 1) of point (t >> 1) of each of the 16
 // stencil rows (one aligned 128-byte row per group and load instruction, instead of 32
-// scattered 8-byte loads), accumulates w_x w_y w_z U with Kahan-compensated FP32 sums,
-// and the four x points are then summed in double across the group.  mode: 0 no gather,
-// 1 cooperative (contiguous row), 2 left to the lane itself.
+// scattered 8-byte loads).  A lane sums its point's column: the four y rows of each z
+// plane weighted by w_y, then the four planes weighted by w_z (FP32 multiply-adds, 4-term
+// sums), then the product with w_x exactly in double; the four x points are summed in
+// double across the group.  (interp_lag3.f90:220-288 nests the same sums with x
+// innermost; the FP64 form keeps that order.)
+// Its rounding error (a few FP32 ulps of sum |w u|) stays far below the FP32 drag
+// correlations' 1e-7, and it takes a quarter of the instructions of a compensated
+// (Kahan) sum of the 64 products.  mode: 0 no gather, 1 cooperative (contiguous row),
+// 2 left to the lane itself.
 __device__ __forceinline__ void gather_warp_fp32(const InstDev* __restrict__ insts, int mode, int inst,
                                                  int64_t b, float al, float be, float ga, int64_t j0,
                                                  double* const* __restrict__ fluid) {
@@ -498,7 +496,8 @@ __device__ __forceinline__ void gather_warp_fp32(const InstDev* __restrict__ ins
     const int io = __shfl_sync(kFull, inst, o);
     const long long bo = __shfl_sync(kFull, (long long)b, o);
     const float alo = __shfl_sync(kFull, al, o), beo = __shfl_sync(kFull, be, o), gao = __shfl_sync(kFull, ga, o);
-    float4 sum = make_float4(0.f, 0.f, 0.f, 0.f), cmp = make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 zs = make_float4(0.f, 0.f, 0.f, 0.f);
+    float wxl = 0.f;
     if (mo == 1) {
       const InstDev& I = insts[io];
       const float* __restrict__ F = static_cast<const float*>(I.field);
@@ -510,19 +509,26 @@ __device__ __forceinline__ void gather_warp_fp32(const InstDev* __restrict__ ins
       const float wx = pick4(fx, k);
       const float* __restrict__ p = F + (bo + k) * kFieldStride + 4 * half;
 #pragma unroll
-      for (int kk = 0; kk < 4; ++kk)
+      for (int kk = 0; kk < 4; ++kk) {
+        float4 ys = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
         for (int jj = 0; jj < 4; ++jj) {
           const float4 v = __ldg(reinterpret_cast<const float4*>(p + (kk * sz + jj * sy) * kFieldStride));
-          const float w = (fz[kk] * fy[jj]) * wx;
-          kahan_fma(sum.x, cmp.x, w, v.x);
-          kahan_fma(sum.y, cmp.y, w, v.y);
-          kahan_fma(sum.z, cmp.z, w, v.z);
-          kahan_fma(sum.w, cmp.w, w, v.w);
+          ys.x = __fmaf_rn(fy[jj], v.x, ys.x);
+          ys.y = __fmaf_rn(fy[jj], v.y, ys.y);
+          ys.z = __fmaf_rn(fy[jj], v.z, ys.z);
+          ys.w = __fmaf_rn(fy[jj], v.w, ys.w);
         }
+        zs.x = __fmaf_rn(fz[kk], ys.x, zs.x);
+        zs.y = __fmaf_rn(fz[kk], ys.y, zs.y);
+        zs.z = __fmaf_rn(fz[kk], ys.z, zs.z);
+        zs.w = __fmaf_rn(fz[kk], ys.w, zs.w);
+      }
+      wxl = wx;
     }
-    double d0 = (double)sum.x - (double)cmp.x, d1 = (double)sum.y - (double)cmp.y;
-    double d2 = (double)sum.z - (double)cmp.z, d3 = (double)sum.w - (double)cmp.w;
+    const double wd = (double)wxl;
+    double d0 = (double)zs.x * wd, d1 = (double)zs.y * wd;
+    double d2 = (double)zs.z * wd, d3 = (double)zs.w * wd;
 #pragma unroll
     for (int m = 2; m <= 4; m <<= 1) {
       d0 += __shfl_xor_sync(kFull, d0, m);
@@ -548,6 +554,10 @@ __device__ __forceinline__ void gather_warp_fp32(const InstDev* __restrict__ ins
 // and id, so it may run while the collision phase updates velocities.  kMixed: every
 // instance holds an FP32 field (warp-cooperative gather); otherwise FP64 fields,
 // gathered per lane in the reference's summation order.
+// Each warp takes the next 32 slots from *ticket (zero at launch), so the slots in
+// flight at any time are one contiguous run of the cell order whatever the grid: the
+// field rows that neighbouring stencils share stay in L2 between their uses, where a
+// grid-stride loop over many blocks spreads the resident warps over the pool.
 // two blocks of 256 per SM: 128 registers, no spills (at three, 80 registers spill)
 #ifndef GP_GATHER_MIN_BLOCKS
 #define GP_GATHER_MIN_BLOCKS 2
@@ -556,11 +566,15 @@ template <bool kMixed>
 __global__ void __launch_bounds__(256, GP_GATHER_MIN_BLOCKS) k_gather(const InstDev* __restrict__ insts,
                                                 const PoolView* __restrict__ src_pv,
                                                 const int32_t* __restrict__ perm, int64_t n,
-                                                double* const* __restrict__ fluid, Status* st) {
+                                                double* const* __restrict__ fluid,
+                                                unsigned long long* __restrict__ ticket, Status* st) {
   if (step_halted(st)) return;
   const int lane = threadIdx.x & 31;
-  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w * 32 < n; w += nwarps) {
+  for (;;) {
+    unsigned long long wt = 0;
+    if (lane == 0) wt = atomicAdd(ticket, 1ull);
+    const int64_t w = (int64_t)__shfl_sync(0xffffffffu, wt, 0);
+    if (w * 32 >= n) break;
     const int64_t j = w * 32 + lane;
     int inst = -1;
     int64_t i = 0;

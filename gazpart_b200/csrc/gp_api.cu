@@ -42,6 +42,9 @@ using namespace gp;
 
 namespace {
 
+constexpr int kPassCounters = 8;   // first contact-pass counter in gp_ctx::d_counters
+constexpr int kMaxPasses = 8;      // contact passes at most (budget 1 takes 7)
+
 template <typename T>
 int dalloc(T **p, size_t count) {
   *p = nullptr;
@@ -136,9 +139,10 @@ struct gp_ctx {
   int64_t cap_pairs = 0;
   CollRec *d_coll = nullptr;
   int64_t cap_coll = 0;
-  unsigned long long *d_counters = nullptr;   // [0] npairs [1] ncoll [2] nacc [3] contact queue [4] contacts kept
-                                              // for the statistics [5] solves handed to the tail kernel
-                                              // [7] collision steps in the statistics
+  unsigned long long *d_counters = nullptr;   // [0] npairs [1] ncoll [2] nacc [4] contacts kept for the
+                                              // statistics [6] the gather's work ticket [7] collision steps
+                                              // in the statistics; from kPassCounters on, per contact pass,
+                                              // its queue and the solves it hands over
   unsigned long long *d_best1 = nullptr, *d_best2 = nullptr;
   int8_t *d_matched = nullptr, *d_state = nullptr;
   int32_t *d_acc = nullptr;
@@ -174,9 +178,10 @@ struct gp_ctx {
   int64_t cap_cst = 0;
   double *d_colacc = nullptr;           // [kMaxClasses][G][G][GP_NSTAT_COLLISION]
   double *d_stat_partial = nullptr, *d_stat_out = nullptr;
-  // contact solves still running after tail_budget evaluations finish in k_contact_tail
-  // (0: no hand-over, the default: with the gather overlapped it did not shorten the step)
-  TailRec *d_tail = nullptr;
+  // contact passes: a solve still running after tail_budget evaluations (0: never) moves
+  // to the next pass of the contact kernel, whose budget is three times larger, until a
+  // last pass without one; the passes hand over through two alternating buffers
+  TailRec *d_tail[2] = {nullptr, nullptr};
   int64_t cap_tail = 0;
   int tail_budget = 0;
 };
@@ -381,10 +386,10 @@ int mark(gp_ctx *c, int slot, cudaStream_t s) {
 int enqueue_gather(gp_ctx *c, cudaStream_t s) {
   GP_TRY(mark(c, 2 * GP_PHASE_GATHER, s));
   if (c->prm.precision == GP_PREC_MIXED)
-    launch_gather_mixed(c->d_inst, c->d_pv, c->sa.sorted, c->n, c->d_fluid_cols, c->d_status,
+    launch_gather_mixed(c->d_inst, c->d_pv, c->sa.sorted, c->n, c->d_fluid_cols, c->d_counters + 6, c->d_status,
                         c->tune[GP_TUNE_GATHER], s);
   else
-    launch_gather_fp64(c->d_inst, c->d_pv, c->sa.sorted, c->n, c->d_fluid_cols, c->d_status,
+    launch_gather_fp64(c->d_inst, c->d_pv, c->sa.sorted, c->n, c->d_fluid_cols, c->d_counters + 6, c->d_status,
                        c->tune[GP_TUNE_GATHER], s);
   GP_CK(cudaGetLastError());
   return mark(c, 2 * GP_PHASE_GATHER + 1, s);
@@ -471,13 +476,23 @@ int enqueue_bin_search(gp_ctx *c, bool flag = false) {
 int enqueue_contact_response(gp_ctx *c) {
   GP_TRY(mark(c, 2 * GP_PHASE_CONTACT, c->stream));
   ContactStatRec *cst = c->colstats ? c->d_cst : nullptr;
-  TailRec *tail = c->tail_budget > 0 ? c->d_tail : nullptr;
-  launch_contact(c->d_inst, c->d_pv, c->d_pairs, c->d_counters + 0, c->cap_pairs, c->d_coll, c->d_counters + 1,
-                 c->cap_coll, c->d_counters + 3, cst, c->d_counters + 4, c->cap_cst, tail, c->d_counters + 5,
-                 c->cap_tail, c->tail_budget, c->d_status, c->contact_grid, c->stream);
-  if (tail)
-    launch_contact_tail(c->d_inst, c->d_pv, c->d_pairs, tail, c->d_counters + 5, c->cap_tail, c->d_coll, c->d_counters + 1,
-                        c->cap_coll, cst, c->d_counters + 4, c->cap_cst, c->d_status, c->stream);
+  // pass p: budget tail_budget * 3^p while below MINPACK's maxfev (300), then a last
+  // pass without one; pass p takes its work from counter kPassCounters + 2p and hands
+  // over through counter kPassCounters + 2p + 1
+  int budget[kMaxPasses], npass = 0;
+  for (int b = c->tail_budget; b > 0 && b < 300 && npass < kMaxPasses - 1; b *= 3) budget[npass++] = b;
+  budget[npass++] = 0;
+  unsigned long long *pc = c->d_counters + kPassCounters;
+  GP_CK(cudaMemsetAsync(pc, 0, 2 * kMaxPasses * sizeof(unsigned long long), c->stream));
+  for (int p = 0; p < npass; ++p) {
+    const bool last = p == npass - 1;
+    const TailRec *in = p > 0 ? c->d_tail[(p - 1) & 1] : nullptr;
+    TailRec *out = last ? nullptr : c->d_tail[p & 1];
+    launch_contact(c->d_inst, c->d_pv, c->d_pairs, c->d_counters + 0, c->cap_pairs, in,
+                   p > 0 ? pc + 2 * (p - 1) + 1 : nullptr, c->cap_tail, c->d_coll, c->d_counters + 1, c->cap_coll,
+                   pc + 2 * p, cst, c->d_counters + 4, c->cap_cst, out, pc + 2 * p + 1, c->cap_tail, budget[p],
+                   c->d_status, c->contact_grid, c->stream);
+  }
   GP_TRY(mark(c, 2 * GP_PHASE_CONTACT + 1, c->stream));
   GP_TRY(mark(c, 2 * GP_PHASE_RESPONSE, c->stream));
   launch_match(c->d_coll, c->d_counters + 1, c->cap_coll, c->d_best1, c->d_best2, c->d_matched, c->d_state,
@@ -654,12 +669,17 @@ int gp_ctx_create(const gp_params *params, gp_ctx **out) {
   if (!rc) rc = dalloc(&c->d_pv, 1);
   if (!rc) rc = dalloc(&c->d_pv_alt, 1);
   if (!rc) rc = dalloc(&c->d_fluid_cols, kNFluid);
-  if (!rc) rc = dalloc(&c->d_counters, 8);
-  if (!rc && cudaMemset(c->d_counters, 0, 8 * sizeof(unsigned long long)) != cudaSuccess) rc = GP_ECUDA;
+  if (!rc) rc = dalloc(&c->d_counters, kPassCounters + 2 * kMaxPasses);
+  if (!rc && cudaMemset(c->d_counters, 0, (kPassCounters + 2 * kMaxPasses) * sizeof(unsigned long long)) !=
+                 cudaSuccess)
+    rc = GP_ECUDA;
   if (!rc) {
-    c->cap_tail = 16384;
-    if (cudaMalloc(reinterpret_cast<void **>(&c->d_tail), (size_t)c->cap_tail * tail_record_bytes()) != cudaSuccess)
-      rc = GP_ENOMEM;
+    // a full buffer only keeps the solve in its lane, so this bounds nothing else
+    c->cap_tail = 65536;
+    for (int k = 0; k < 2 && !rc; ++k)
+      if (cudaMalloc(reinterpret_cast<void **>(&c->d_tail[k]), (size_t)c->cap_tail * tail_record_bytes()) !=
+          cudaSuccess)
+        rc = GP_ENOMEM;
   }
   if (!rc) rc = dalloc(&c->d_group_tab, kMaxClasses);
   if (!rc) rc = dalloc(&c->d_group_n, kMaxClasses);
@@ -704,7 +724,8 @@ int gp_ctx_destroy(gp_ctx *c) {
   for (auto &g : c->group_dev) dfree(g);
   dfree(c->d_group_tab); dfree(c->d_group_n); dfree(c->d_cst); dfree(c->d_colacc);
   dfree(c->d_stat_partial); dfree(c->d_stat_out);
-  if (c->d_tail) cudaFree(c->d_tail);
+  for (TailRec *t : c->d_tail)
+    if (t) cudaFree(t);
   dfree(c->d_status); dfree(c->d_scratch);
   if (c->ev_fork) cudaEventDestroy(c->ev_fork);
   if (c->ev_join) cudaEventDestroy(c->ev_join);

@@ -15,11 +15,33 @@
 
 namespace gp {
 
+// A solve handed over by an earlier pass: its pair and solver state, and the problem
+// rebuilt from the pool by the same set-up (so to the same values).  Out of line: the
+// solving loop only passes the state it already keeps in local memory.
+static __device__ __noinline__ void resume_solve(const InstDev *__restrict__ insts, const PoolView *__restrict__ pv,
+                                                 const PairRec *__restrict__ pairs, const TailRec *__restrict__ rec,
+                                                 int64_t &e, ContactProb &CP, LmState &S) {
+  e = rec->e;
+  S = rec->S;
+  const PairRec pr = pairs[e];
+  PairBodies B;
+  pair_bodies(insts, *pv, pr.home, pr.near, B);
+  double xs[2];
+  contact_setup(B.a1, B.b1, B.a2, B.b2, B.c1, B.q1, B.c2, B.q2, CP, xs);
+}
+
 // collision_interaction.f90:216-348 for every candidate pair: minimum image, contact
 // (ellipsoid_contact_detection), contact-point velocities, NVREL.  Colliding pairs
 // (flag && NVREL < ZERO) are appended.  Persistent warps with lane refill: a lane whose
 // Levenberg-Marquardt solve has returned finishes its pair and takes the next one from
 // a global queue, so warps do not idle on their slowest pair.
+//
+// Passes.  A warp runs as long as its slowest lane, and a C3 step has about one solve per
+// lane of the persistent grid, so refilling cannot even out solves of 3 to 300
+// evaluations.  With `out` set, a solve still running after `budget` evaluations is
+// written there (pair and solver state) and the lane takes other work; a further pass
+// of this kernel (`in` set) resumes those solves with every lane busy, under a larger
+// budget or none.  The iterates are the same operations in the same order.
 #ifndef GP_CONTACT_MIN_BLOCKS
 #define GP_CONTACT_MIN_BLOCKS 8
 #endif
@@ -28,14 +50,17 @@ __global__ void __launch_bounds__(128, GP_CONTACT_MIN_BLOCKS) k_contact(const In
                                                     const PoolView *__restrict__ pv,
                                                     const PairRec *__restrict__ pairs,
                                                     const unsigned long long *__restrict__ npairs, int64_t cap_pairs,
+                                                    const TailRec *__restrict__ in,
+                                                    const unsigned long long *__restrict__ nin, int64_t cap_in,
                                                     CollRec *__restrict__ coll, unsigned long long *ncoll,
                                                     int64_t cap_coll, unsigned long long *queue,
                                                     ContactStatRec *__restrict__ cst, unsigned long long *ncst,
-                                                    int64_t cap_cst, TailRec *__restrict__ tail,
-                                                    unsigned long long *ntail, int64_t cap_tail, int tail_budget,
+                                                    int64_t cap_cst, TailRec *__restrict__ out,
+                                                    unsigned long long *nout, int64_t cap_out, int budget,
                                                     Status *st) {
   if (step_halted(st)) return;
-  const int64_t np = (int64_t)min(*npairs, (unsigned long long)cap_pairs);
+  const int64_t np = in ? (int64_t)min(*nin, (unsigned long long)cap_in)
+                        : (int64_t)min(*npairs, (unsigned long long)cap_pairs);
   const unsigned lane = threadIdx.x & 31u;
   constexpr unsigned kFull = 0xffffffffu;
   bool active = false, exhausted = false;
@@ -53,8 +78,12 @@ __global__ void __launch_bounds__(128, GP_CONTACT_MIN_BLOCKS) k_contact(const In
         if ((int64_t)base >= np) {
           exhausted = true;
         } else if (!active) {
-          e = (int64_t)base + __popc(want & ((1u << lane) - 1u));
-          if (e < np) {
+          const int64_t q = (int64_t)base + __popc(want & ((1u << lane) - 1u));
+          if (q < np && in) {
+            resume_solve(insts, pv, pairs, in + q, e, CP, S);
+            active = true;
+          } else if (q < np) {
+            e = q;
             const PairRec pr = pairs[e];
             PairBodies B;
             pair_bodies(insts, *pv, pr.home, pr.near, B);
@@ -82,14 +111,13 @@ __global__ void __launch_bounds__(128, GP_CONTACT_MIN_BLOCKS) k_contact(const In
     }
     if (!active) continue;
     if (lm_step(CP, S, kContactTol) == 0) {
-      // a long solve goes to k_contact_tail, which finishes it with fewer solves per SM
-      // competing; the lane takes a new pair (if the hand-over buffer is full the lane
-      // keeps the solve)
-      if (tail != nullptr && S.nfev >= tail_budget) {
-        const unsigned long long k = atomicAdd(ntail, 1ull);
-        if ((int64_t)k < cap_tail) {
-          tail[k].e = e;
-          tail[k].S = S;
+      // past the budget the solve moves on to the next pass and the lane takes other
+      // work (with the hand-over buffer full, the lane keeps the solve)
+      if (out != nullptr && S.nfev >= budget) {
+        const unsigned long long k = atomicAdd(nout, 1ull);
+        if ((int64_t)k < cap_out) {
+          out[k].e = e;
+          out[k].S = S;
           active = false;
         }
       }
@@ -112,12 +140,14 @@ int contact_grid_blocks() {
 }
 
 void launch_contact(const InstDev *insts, const PoolView *pv, const PairRec *pairs, const unsigned long long *npairs,
-                    int64_t cap_pairs, CollRec *coll, unsigned long long *ncoll, int64_t cap_coll,
-                    unsigned long long *queue, ContactStatRec *cst, unsigned long long *ncst, int64_t cap_cst,
-                    TailRec *tail, unsigned long long *ntail, int64_t cap_tail, int tail_budget, Status *st,
-                    int grid, cudaStream_t s) {
-  k_contact<<<grid, 128, 0, s>>>(insts, pv, pairs, npairs, cap_pairs, coll, ncoll, cap_coll, queue, cst, ncst,
-                                 cap_cst, tail, ntail, cap_tail, tail_budget, st);
+                    int64_t cap_pairs, const TailRec *in, const unsigned long long *nin, int64_t cap_in,
+                    CollRec *coll, unsigned long long *ncoll, int64_t cap_coll, unsigned long long *queue,
+                    ContactStatRec *cst, unsigned long long *ncst, int64_t cap_cst, TailRec *out,
+                    unsigned long long *nout, int64_t cap_out, int budget, Status *st, int grid, cudaStream_t s) {
+  k_contact<<<grid, 128, 0, s>>>(insts, pv, pairs, npairs, cap_pairs, in, nin, cap_in, coll, ncoll, cap_coll, queue,
+                                 cst, ncst, cap_cst, out, nout, cap_out, budget, st);
 }
+
+size_t tail_record_bytes() { return sizeof(TailRec); }
 
 }  // namespace gp

@@ -1,13 +1,12 @@
 // gp_contact.cuh -- one candidate pair of collision_interaction.f90:216-348: its
-// geometry, and what follows a finished contact solve.  Shared by the persistent contact
-// kernel and the kernel that finishes the long solves it hands over.
+// geometry, and what follows a finished contact solve.
 #pragma once
 
 #include "gp_lm.cuh"
 
 namespace gp {
 
-// A solve handed from k_contact to k_contact_tail: the pair and the solver's state
+// A solve handed from one pass of k_contact to the next: the pair and the solver's state
 // between two lm_step calls (the problem itself is rebuilt from the pool).
 struct TailRec {
   int64_t e;                 // index of the pair in the candidate list

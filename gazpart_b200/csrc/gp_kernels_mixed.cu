@@ -12,11 +12,12 @@ template __global__ void k_integrate_fix<true>(const InstDev *, const PoolView *
                                                 const unsigned long long *, int64_t, const double *const *,
                                                 uint32_t *, Status *);
 template __global__ void k_gather<true>(const InstDev *, const PoolView *, const int32_t *, int64_t,
-                                         double *const *, Status *);
+                                         double *const *, unsigned long long *, Status *);
 
 void launch_gather_mixed(const InstDev *insts, const PoolView *pv, const int32_t *perm, int64_t n,
-                      double *const *fluid, Status *st, int grid, cudaStream_t s) {
-  k_gather<true><<<grid, 256, 0, s>>>(insts, pv, perm, n, fluid, st);
+                      double *const *fluid, unsigned long long *ticket, Status *st, int grid, cudaStream_t s) {
+  cudaMemsetAsync(ticket, 0, sizeof(unsigned long long), s);
+  k_gather<true><<<grid, 256, 0, s>>>(insts, pv, perm, n, fluid, ticket, st);
 }
 
 void launch_integrate_mixed(const InstDev *insts, PoolView *pv, PoolView *pv_alt, const int32_t *perm, int64_t n,

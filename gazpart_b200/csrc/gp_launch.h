@@ -14,7 +14,7 @@ struct TailRec;   // gp_contact.cuh
 // the two views (so *pv is current afterwards).  With mark non-null, the speculative
 // pass: marked particles are left to launch_integrate_fix_*, which also swaps.
 void launch_gather_fp64(const InstDev *insts, const PoolView *pv, const int32_t *perm, int64_t n,
-                      double *const *fluid, Status *st, int grid, cudaStream_t s);
+                      double *const *fluid, unsigned long long *ticket, Status *st, int grid, cudaStream_t s);
 void launch_integrate_fp64(const InstDev *insts, PoolView *pv, PoolView *pv_alt, const int32_t *perm, int64_t n,
                          double *const *fluid, Status *st, int grid, cudaStream_t s, uint32_t *mark = nullptr);
 void launch_integrate_fix_fp64(const InstDev *insts, PoolView *pv, PoolView *pv_alt, const PairRec *pairs,
@@ -27,15 +27,10 @@ void launch_frozen_interp(const double *xain, const double *yain, const double *
                           double *out, Status *st, cudaStream_t s);
 int contact_grid_blocks();
 void launch_contact(const InstDev *insts, const PoolView *pv, const PairRec *pairs, const unsigned long long *npairs,
-                    int64_t cap_pairs, CollRec *coll, unsigned long long *ncoll, int64_t cap_coll,
-                    unsigned long long *queue, ContactStatRec *cst, unsigned long long *ncst, int64_t cap_cst,
-                    TailRec *tail, unsigned long long *ntail, int64_t cap_tail, int tail_budget, Status *st,
-                    int grid, cudaStream_t s);
-// --- gp_contact_tail.cu (-fmad=false, solver inlined) ---
-void launch_contact_tail(const InstDev *insts, const PoolView *pv, const PairRec *pairs, const TailRec *tail,
-                         const unsigned long long *ntail, int64_t cap_tail, CollRec *coll, unsigned long long *ncoll,
-                         int64_t cap_coll, ContactStatRec *cst, unsigned long long *ncst, int64_t cap_cst,
-                         Status *st, cudaStream_t s);
+                    int64_t cap_pairs, const TailRec *in, const unsigned long long *nin, int64_t cap_in,
+                    CollRec *coll, unsigned long long *ncoll, int64_t cap_coll, unsigned long long *queue,
+                    ContactStatRec *cst, unsigned long long *ncst, int64_t cap_cst, TailRec *out,
+                    unsigned long long *nout, int64_t cap_out, int budget, Status *st, int grid, cudaStream_t s);
 size_t tail_record_bytes();
 void launch_response(const InstDev *insts, const PoolView *pv, const CollRec *coll, const unsigned long long *ncoll,
                      int64_t cap_coll, const int8_t *state, int32_t *acc_list, unsigned long long *nacc, Status *st,
@@ -67,7 +62,7 @@ void launch_collision_stats(const CollRec *coll, const unsigned long long *ncoll
 
 // --- gp_kernels_mixed.cu ---
 void launch_gather_mixed(const InstDev *insts, const PoolView *pv, const int32_t *perm, int64_t n,
-                      double *const *fluid, Status *st, int grid, cudaStream_t s);
+                      double *const *fluid, unsigned long long *ticket, Status *st, int grid, cudaStream_t s);
 void launch_integrate_mixed(const InstDev *insts, PoolView *pv, PoolView *pv_alt, const int32_t *perm, int64_t n,
                          double *const *fluid, Status *st, int grid, cudaStream_t s, uint32_t *mark = nullptr);
 void launch_integrate_fix_mixed(const InstDev *insts, PoolView *pv, PoolView *pv_alt, const PairRec *pairs,

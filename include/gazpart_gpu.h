@@ -190,9 +190,10 @@ int gp_upload_classes(gp_ctx *ctx, int32_t nclass, const int64_t *counts, const 
 
 /* ------------------------------------------------ resident fields and jobs ---- */
 /* No counterpart in the reference.  Contact solves still running after `budget`
- * function evaluations are finished by a second kernel with the solver inlined, whose
- * iterations are shorter; the results do not change.  0 (the default) keeps every
- * solve in the persistent contact kernel; at most 300 (MINPACK's maxfev). */
+ * function evaluations are handed to a further pass of the contact kernel, which runs
+ * them with every lane busy, under three times the budget, until a last pass without
+ * one; the results do not change.  0 keeps every solve in one pass; at most 300
+ * (MINPACK's maxfev). */
 int gp_set_contact_tail(gp_ctx *ctx, int32_t budget);
 int gp_get_contact_tail(gp_ctx *ctx, int32_t *budget);
 /* Mesh (nx, ny, nz) of field slot `field`. */

@@ -201,20 +201,20 @@ def test_speculative_integrate_changes_nothing(name, precision):
 
 @pytest.mark.parametrize("name", ["dense", "bimodal"])
 def test_contact_tail_hand_over_changes_nothing(name):
-    """Solves handed from the persistent contact kernel to the inlined-solver kernel
-    (gp_set_contact_tail) run the same iterates: with every solve handed over after its
-    first iteration, with none handed over and with the default, the colliding pairs and
-    the states after a step are identical."""
+    """Solves handed from one pass of the contact kernel to the next (gp_set_contact_tail)
+    run the same iterates: with every solve handed on after 1, 3, 9, ... evaluations
+    (seven passes), after 4, 12, 36, 108, after 64 and 192, and with one pass, the
+    colliding pairs, the counters and the states after a step are identical."""
     setup, fn, refs, st = case(name)
     res = po.Ensemble(setup, copy_state(st)).collide(prefilter=True, nthreads=8)
     out = {}
-    for budget in (0, 1, 64):
+    for budget in (0, 1, 4, 64):
         with _ctx(setup, fn, st) as ctx:
             ctx.set_contact_tail(budget)
             ctx.collision(1, 0.0)
             ctx.raise_status()
             out[budget] = (ctx.collision_pairs(), ctx.download(), ctx.collision_counters())
-    for budget in (0, 1, 64):
+    for budget in (0, 1, 4, 64):
         (home, near), got, cnt = out[budget]
         assert np.array_equal(home, res["home"]) and np.array_equal(near, res["near"]), budget
         for k in api.STATE_KEYS:
