@@ -175,68 +175,79 @@ __device__ __forceinline__ void gather6_fp32(const InstDev& I, const Stencil& s,
 }
 
 // ---------------------------------------------------------------------------
-// Mixed-precision force and torque: relative velocities and frames in FP64, the
+// Mixed-precision force and torque: slip and spin vectors and frames in FP64, the
 // Zastawny correlation coefficients in FP32, forces assembled in FP64.  The FP32
-// coefficients bound the relative error of every force and torque near 1e-7, so the
-// FP64 quotients here use the cheapest forms that stay far inside that: one
-// reciprocal per denominator, per-particle reciprocals of the constants (MixedConst),
-// and the body-frame flow shared by the force and the torque when both see the same
-// particle velocity (the first RK2 stage).
+// coefficients bound the relative error of every force and torque near 1e-7, so every
+// scalar that only scales them -- the magnitudes of the slip, of its transverse part
+// and of the relative spin, their reciprocals, the per-particle constants (MixedConst)
+// -- is formed in FP32 as well, and the body-frame flow is shared by the force and the
+// torque when both see the same particle velocity (the first RK2 stage).  The
+// directions (the body-frame slip and the rotations) stay FP64.
 // ---------------------------------------------------------------------------
 struct MixedConst {
-  double dv;              // deq / visc: particle Reynolds number per unit slip speed
-  double d2v;             // deq^2 / visc: rotational Reynolds number per unit spin
-  double rix, riy, riz;   // 1 / principal moments of inertia
+  float dv;               // deq / visc: particle Reynolds number per unit slip speed
+  float d2v;              // deq^2 / visc: rotational Reynolds number per unit spin
+  double rix, riy, riz;   // 1 / principal moments of inertia (FP32 reciprocals)
 };
 
 __device__ __forceinline__ void mixed_const(const PartConst& pc, double visc, MixedConst& mc) {
-  mc.dv = pc.deq / visc;
-  mc.d2v = (pc.deq * pc.deq) / visc;
-  mc.rix = 1.0 / pc.ipxx;
-  mc.riy = 1.0 / pc.ipyy;
-  mc.riz = 1.0 / pc.ipzz;
+  const float vi = __frcp_rn((float)visc), d = (float)pc.deq;
+  mc.dv = d * vi;
+  mc.d2v = (d * d) * vi;
+  mc.rix = (double)__frcp_rn((float)pc.ipxx);
+  mc.riy = (double)__frcp_rn((float)pc.ipyy);
+  mc.riz = (double)__frcp_rn((float)pc.ipzz);
 }
 
 // Slip velocity u_f - u_p in the body frame (R^T p), its magnitude, the magnitude of its
 // transverse part and the incidence angle phi = |atan(syz / b0)| in [0, pi/2].
 struct RelFlow {
-  double umag, b0, b1, b2, syz, inv_syz;
+  double b0, b1, b2;      // body frame, FP64
+  float umag, syz, inv_syz;
   float lr, sphi, cphi;   // log2 of the particle Reynolds number, sin and cos of phi
 };
 
 static __device__ __forceinline__ void rel_flow(const MixedConst& mc, const double u[3], const double uf[3],
                                                 const double r[9], RelFlow& q) {
   const double p0 = uf[0] - u[0], p1 = uf[1] - u[1], p2 = uf[2] - u[2];
-  q.umag = sqrt(p0 * p0 + p1 * p1 + p2 * p2);
+  const float f0 = (float)p0, f1 = (float)p1, f2 = (float)p2;
+  q.umag = sqrtf(f0 * f0 + f1 * f1 + f2 * f2);
   q.b0 = r[0] * p0 + r[1] * p1 + r[2] * p2;
   q.b1 = r[3] * p0 + r[4] * p1 + r[5] * p2;
   q.b2 = r[6] * p0 + r[7] * p1 + r[8] * p2;
-  q.syz = sqrt(q.b1 * q.b1 + q.b2 * q.b2);
-  q.inv_syz = 1.0 / q.syz;   // used only where syz != 0
+  const float c1 = (float)q.b1, c2 = (float)q.b2;
+  q.syz = sqrtf(c1 * c1 + c2 * c2);
+  q.inv_syz = __frcp_rn(q.syz);   // used only where syz != 0
   // atan2 of the magnitudes is |atan(syz / b0)|, pi/2 where b0 = 0
-  const float phi = atan2f((float)q.syz, fabsf((float)q.b0));
+  const float phi = atan2f(q.syz, fabsf((float)q.b0));
   sincosf(phi, &q.sphi, &q.cphi);
   q.cphi = fmaxf(q.cphi, 0.f);   // float(pi/2) lies above pi/2: keep cos(phi) >= 0 as in FP64
-  q.lr = __log2f((float)(q.umag * mc.dv));
+  q.lr = __log2f(q.umag * mc.dv);
 }
+
+// x^y for x in [0, 1] and y > 0 (sines and cosines of the incidence angle raised to the
+// correlations' exponents) as 2^(y log2 x) with the hardware log2: an absolute error of
+// a few 1e-7 of the result where it is not negligible against the rest of the
+// coefficient, the size of the FP32 correlations' own rounding.  x = 0 gives 0.
+__device__ __forceinline__ float pow_unit(float x, float y) { return exp2f(y * __log2f(x)); }
 
 static __device__ __forceinline__ bool fluid_force_mixed(const PartConst& pc, const RelFlow& q, const double r[9],
                                                          double f[3]) {
   f[0] = f[1] = f[2] = 0.0;
-  if (q.umag == 0.0) return true;
+  if (q.umag == 0.f) return true;
   const float lr = q.lr, sphi = q.sphi, cphi = q.cphi;
   const float cd0 = 18.12f * exp2f(-1.023f * lr) + 4.26f * exp2f(-0.384f * lr);
   const float cd90 = 21.52f * exp2f(-0.990f * lr) + 2.86f * exp2f(-0.260f * lr);
-  const float cdrag = cd0 + (cd90 - cd0) * powf(sphi, 1.95f);
+  const float cdrag = cd0 + (cd90 - cd0) * pow_unit(sphi, 1.95f);
   const float clift = (0.083f * exp2f(0.21f * lr) + 1.582f * exp2f(-0.851f * lr)) *
-                      powf(sphi, 1.842f - 0.802f * exp2f(-0.006f * lr)) *
-                      powf(cphi, 0.874f + 0.009f * exp2f(0.570f * lr));
-  const double kd = pc.cdrag * (double)cdrag * q.umag;
-  const double kl = pc.cdrag * (double)clift * (q.umag * q.umag);
+                      pow_unit(sphi, 1.842f - 0.802f * exp2f(-0.006f * lr)) *
+                      pow_unit(cphi, 0.874f + 0.009f * exp2f(0.570f * lr));
+  const double kd = pc.cdrag * (double)(cdrag * q.umag);
+  const double kl = pc.cdrag * (double)(clift * (q.umag * q.umag));
   double fb0 = kd * q.b0 + kl * (double)sphi * copysign(1.0, -q.b0);
   double fb1 = kd * q.b1, fb2 = kd * q.b2;
-  if (q.syz != 0.0) {
-    const double kc = kl * (double)cphi * q.inv_syz;
+  if (q.syz != 0.f) {
+    const double kc = kl * (double)(cphi * q.inv_syz);
     fb1 += kc * q.b1;
     fb2 += kc * q.b2;
   }
@@ -253,22 +264,23 @@ static __device__ __forceinline__ void fluid_torque_mixed(const PartConst& pc, c
   const double c1 = r[3] * wv[0] + r[4] * wv[1] + r[5] * wv[2];
   const double c2 = r[6] * wv[0] + r[7] * wv[1] + r[8] * wv[2];
   const double o0 = 0.5 * c0 - ox, o1 = 0.5 * c1 - oy, o2 = 0.5 * c2 - oz;
-  const double omag = sqrt(o0 * o0 + o1 * o1 + o2 * o2);
-  const double oyz = sqrt(o2 * o2 + o1 * o1);
+  const float g0 = (float)o0, g1 = (float)o1, g2 = (float)o2;
+  const float omag = sqrtf(g0 * g0 + g1 * g1 + g2 * g2);
+  const double oyz = (double)sqrtf(g2 * g2 + g1 * g1);
   t[0] = t[1] = t[2] = 0.0;
-  if (q.umag != 0.0 && q.syz != 0.0) {
+  if (q.umag != 0.f && q.syz != 0.f) {
     const float lr = q.lr, sphi = q.sphi, cphi = q.cphi;
     const float ctp = (0.935f * exp2f(-0.146f * lr) - 0.469f * exp2f(-0.145f * lr)) *
-                      powf(sphi, 0.116f + 0.748f * exp2f(0.041f * lr)) *
-                      powf(cphi, 0.221f + 0.657f * exp2f(0.044f * lr));
-    const double cp = pc.cpitch * (double)ctp * (q.umag * q.umag) * q.inv_syz;
+                      pow_unit(sphi, 0.116f + 0.748f * exp2f(0.041f * lr)) *
+                      pow_unit(cphi, 0.221f + 0.657f * exp2f(0.044f * lr));
+    const double cp = pc.cpitch * (double)(ctp * (q.umag * q.umag) * q.inv_syz);
     t[1] = cp * fabs(q.b2) * copysign(1.0, q.b0 * q.b2);
     t[2] = cp * fabs(q.b1) * copysign(1.0, q.b0 * q.b1);
   }
-  const double re_r = omag * mc.d2v;
-  if (re_r != 0.0) {
-    const float lr = __log2f((float)re_r);
-    const float ctr = 0.573f * exp2f(-0.154f * lr) + 116.61f / (float)re_r;
+  const float re_r = omag * mc.d2v;
+  if (re_r != 0.f) {
+    const float lr = __log2f(re_r);
+    const float ctr = 0.573f * exp2f(-0.154f * lr) + 116.61f * __frcp_rn(re_r);
     const float ctr2 = 1.244f * exp2f(0.239f * lr) + 378.12f * exp2f(-0.789f * lr);
     const double k = pc.crot * pc.h5;
     t[0] += (double)ctr * k * fabs(o0) * o0;
@@ -300,9 +312,20 @@ struct Forces {
       }
       return ok;
     } else {
+      // one R(q) and, where u and un are the same values, one slip for both routines
+      double rq[9];
+      rotmat(q, rq);
       double fd[3], fl[3], tp[3], tr[3];
-      const bool ok = fluid_force(pc, visc, u[0], u[1], u[2], uf[0], uf[1], uf[2], q, fd, fl);
-      fluid_torque(pc, visc, un[0], un[1], un[2], uf[0], uf[1], uf[2], wv[0], wv[1], wv[2], ox, oy, oz, q, tp, tr);
+      Slip64 sf;
+      slip64(pc, visc, u, uf, rq, sf);
+      const bool ok = fluid_force(pc, sf, rq, fd, fl);
+      if (same_u) {
+        fluid_torque(pc, visc, sf, wv[0], wv[1], wv[2], ox, oy, oz, rq, tp, tr);
+      } else {
+        Slip64 st;
+        slip64(pc, visc, un, uf, rq, st);
+        fluid_torque(pc, visc, st, wv[0], wv[1], wv[2], ox, oy, oz, rq, tp, tr);
+      }
       f[0] = fd[0] + fl[0]; f[1] = fd[1] + fl[1]; f[2] = fd[2] + fl[2];
       t[0] = tp[0] + tr[0]; t[1] = tp[1] + tr[1]; t[2] = tp[2] + tr[2];
       return ok;
@@ -332,15 +355,17 @@ __device__ __forceinline__ void quaternion_step_mixed(Quat& q, const double r[9]
   const double om[3] = {ox, oy, oz};
   double omg[3];
   matvec(r, om, omg);
-  const double n2 = omg[0] * omg[0] + omg[1] * omg[1] + omg[2] * omg[2];
+  const float n2 = (float)(omg[0] * omg[0] + omg[1] * omg[1] + omg[2] * omg[2]);
   Quat map = {1.0, 0.0, 0.0, 0.0};
-  if (n2 != 0.0) {
-    const double inv = rsqrt(n2);
-    const double h = (n2 * inv) * dt * 0.5;
-    double s, c;
-    sincos(h, &s, &c);
-    const double si = s * inv;
-    map = {c, si * omg[0], si * omg[1], si * omg[2]};
+  if (n2 > 0.f) {
+    // the half angle's sine and cosine in FP32: for the small angles of a step the
+    // rotation angle's error is a few 1e-8 of the angle; the axis stays FP64
+    const float inv = rsqrtf(n2);
+    const float h = (n2 * inv) * (float)(dt * 0.5);
+    float s, c;
+    sincosf(h, &s, &c);
+    const double si = (double)(s * inv);
+    map = {(double)c, si * omg[0], si * omg[1], si * omg[2]};
   }
   q = mult_quat(map, q);
   const double inv = rsqrt(q.a * q.a + q.b * q.b + q.c * q.c + q.d * q.d);

@@ -149,85 +149,97 @@ struct PartConst {
   double ipxx, ipyy, ipzz;
 };
 
+// R(q)^T v.  R(conj(q)) is R(q)^T bit for bit (conjugation only flips the signs of
+// exact products), so this is rot_vec(conj(q), v) of transform_basis.f90:77.
+__host__ __device__ inline void matvec_t(const double m[9], const double v[3], double o[3]) {
+  const double t0 = m[0] * v[0] + m[1] * v[1] + m[2] * v[2];
+  const double t1 = m[3] * v[0] + m[4] * v[1] + m[5] * v[2];
+  const double t2 = m[6] * v[0] + m[7] * v[1] + m[8] * v[2];
+  o[0] = t0; o[1] = t1; o[2] = t2;
+}
+
+// The particle's slip through the fluid as fluid_force_ellipsoid.f90:63-90 and
+// fluid_torque_ellipsoid.f90:88-124 both form it, with the same operations: u_f - u_p,
+// its magnitude, the Reynolds number, the slip in the body frame, its transverse part,
+// the incidence angle's sine and cosine.  Formed once where the force and the torque
+// see the same particle velocity.  (rep, umag and the angle are only read when umag0
+// and, for the torque, syz are non-zero, as the reference reads them.)
+struct Slip64 {
+  double p[3];   // body frame
+  double umag0, rep, syz, umag, sphi, cphi;
+};
+
+static __device__ __forceinline__ void slip64(const PartConst& pc, double visc, const double u[3],
+                                              const double uf[3], const double r[9], Slip64& s) {
+  double p[3] = {uf[0] - u[0], uf[1] - u[1], uf[2] - u[2]};
+  s.umag0 = sqrt(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]);
+  s.rep = (s.umag0 * pc.deq) / visc;
+  matvec_t(r, p, s.p);
+  s.syz = sqrt(s.p[1] * s.p[1] + s.p[2] * s.p[2]);
+  const double phi = fabs(atan(s.syz / s.p[0]));
+  s.umag = sqrt(s.p[0] * s.p[0] + s.p[1] * s.p[1] + s.p[2] * s.p[2]);
+  sincos(phi, &s.sphi, &s.cphi);
+}
+
 // fluid_force_ellipsoid.f90:1-161 (guards: zero relative speed -> zero force; zero
 // transverse speed -> zero transverse lift; the reference stops or yields NaN there).
-// Returns false if CDRAG is NaN (the reference's stop at :150-159).
-static __device__ __forceinline__ bool fluid_force(const PartConst& pc, double visc, double up, double vp, double wp,
-                                   double uf, double vf, double wf, const Quat& q, double fd[3], double fl[3]) {
+// Returns false if CDRAG is NaN (the reference's stop at :150-159).  r = R(q).
+static __device__ __forceinline__ bool fluid_force(const PartConst& pc, const Slip64& s, const double r[9],
+                                                   double fd[3], double fl[3]) {
   constexpr double a0 = 1.95, a1 = 18.12, a2 = 1.023, a3 = 4.26, a4 = 0.384;
   constexpr double a5 = 21.52, a6 = 0.990, a7 = 2.86, a8 = 0.260;
   constexpr double b1 = 0.083, b2 = -0.21, b3 = 1.582, b4 = 0.851, b5 = 1.842;
   constexpr double b6 = -0.802, b7 = -0.006, b8 = 0.874, b9 = 0.009, b10 = 0.570;
-  double p[3] = {uf - up, vf - vp, wf - wp};
-  const double umag0 = sqrt(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]);
   fd[0] = fd[1] = fd[2] = 0.0;
   fl[0] = fl[1] = fl[2] = 0.0;
-  if (umag0 == 0.0) return true;
-  const double rep = (umag0 * pc.deq) / visc;
-  rot_vec(conj(q), p);
-  const double syz = sqrt(p[1] * p[1] + p[2] * p[2]);
-  const double phi = fabs(atan(syz / p[0]));
-  const double umag = sqrt(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]);
-  double sphi, cphi;
-  sincos(phi, &sphi, &cphi);
+  if (s.umag0 == 0.0) return true;
+  const double rep = s.rep, sphi = s.sphi, cphi = s.cphi, umag = s.umag;
   const double cd0 = (a1 / pow(rep, a2)) + (a3 / pow(rep, a4));
   const double cd90 = (a5 / pow(rep, a6)) + (a7 / pow(rep, a8));
   const double cdrag = cd0 + (cd90 - cd0) * pow(sphi, a0);
   const double clift = ((b1 / pow(rep, b2)) + (b3 / pow(rep, b4))) * pow(sphi, b5 + b6 * pow(rep, b7)) *
                        pow(cphi, b8 + b9 * pow(rep, b10));
   const double kd = pc.cdrag * cdrag * umag;
-  fd[0] = kd * p[0];
-  fd[1] = kd * p[1];
-  fd[2] = kd * p[2];
+  fd[0] = kd * s.p[0];
+  fd[1] = kd * s.p[1];
+  fd[2] = kd * s.p[2];
   const double kl = pc.cdrag * clift * (umag * umag);
-  fl[0] = kl * sphi * copysign(1.0, -p[0]);
+  fl[0] = kl * sphi * copysign(1.0, -s.p[0]);
   fl[1] = 0.0;
   fl[2] = 0.0;
-  if (syz != 0.0) {
-    fl[1] = kl * cphi * (p[1] / syz);
-    fl[2] = kl * cphi * (p[2] / syz);
+  if (s.syz != 0.0) {
+    fl[1] = kl * cphi * (s.p[1] / s.syz);
+    fl[2] = kl * cphi * (s.p[2] / s.syz);
   }
-  double r[9];
-  rotmat(q, r);
   matvec(r, fd, fd);
   matvec(r, fl, fl);
   return !(cdrag != cdrag);
 }
 
-// fluid_torque_ellipsoid.f90:1-190.  Relative velocity from the particle's stored
-// velocity u_n (:88-105).  Guards as in fluid_force.  Pitching and rotation torques.
-static __device__ __forceinline__ void fluid_torque(const PartConst& pc, double visc, double upn, double vpn, double wpn,
-                                    double uf, double vf, double wf, double wx, double wy, double wz,
-                                    double ox, double oy, double oz, const Quat& q, double tp[3],
-                                    double tr[3]) {
+// fluid_torque_ellipsoid.f90:1-190.  Slip from the particle's stored velocity u_n
+// (:88-105).  Guards as in fluid_force.  Pitching and rotation torques.  r = R(q).
+static __device__ __forceinline__ void fluid_torque(const PartConst& pc, double visc, const Slip64& s,
+                                                    double wx, double wy, double wz, double ox, double oy,
+                                                    double oz, const double r[9], double tp[3], double tr[3]) {
   constexpr double c1 = 0.935, c2 = 0.146, c3 = -0.469, c4 = 0.145, c5 = 0.116;
   constexpr double c6 = 0.748, c7 = 0.041, c8 = 0.221, c9 = 0.657, c10 = 0.044;
   constexpr double r1 = 0.573, r2 = -0.154, r3 = 116.61;
   constexpr double r1_ = 1.244, r2_ = 0.239, r3_ = 378.12, r4_ = 0.789;
-  double rt[9];
-  rotmat(conj(q), rt);
-  double p[3] = {uf - upn, vf - vpn, wf - wpn};
-  const double umag0 = sqrt(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]);
-  matvec(rt, p, p);
-  const double syz = sqrt(p[1] * p[1] + p[2] * p[2]);
-  double curl[3] = {wx, wy, wz};
-  matvec(rt, curl, curl);
+  const double wv[3] = {wx, wy, wz};
+  double curl[3];
+  matvec_t(r, wv, curl);
   const double o0 = 0.5 * curl[0] - ox, o1 = 0.5 * curl[1] - oy, o2 = 0.5 * curl[2] - oz;
   const double omag = sqrt(o0 * o0 + o1 * o1 + o2 * o2);
   const double oyz = sqrt(o2 * o2 + o1 * o1);
   const double re_r = (omag * (pc.deq * pc.deq)) / visc;
   double tp1 = 0.0, tp2 = 0.0, tr0 = 0.0, tr1 = 0.0, tr2 = 0.0;
-  if (umag0 != 0.0 && syz != 0.0) {
-    const double rep = (umag0 * pc.deq) / visc;
-    const double phi = fabs(atan(syz / p[0]));
-    const double umag = sqrt(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]);
-    double sphi, cphi;
-    sincos(phi, &sphi, &cphi);
+  if (s.umag0 != 0.0 && s.syz != 0.0) {
+    const double rep = s.rep, sphi = s.sphi, cphi = s.cphi, umag = s.umag;
     const double ctp = (c1 / pow(rep, c2) + c3 / pow(rep, c4)) * (pow(sphi, c5 + c6 * pow(rep, c7))) *
                        (pow(cphi, c8 + c9 * pow(rep, c10)));
     const double cp = pc.cpitch * ctp * (umag * umag);
-    tp1 = cp * (fabs(p[2]) / syz) * copysign(1.0, p[0] * p[2]);
-    tp2 = cp * (fabs(p[1]) / syz) * copysign(1.0, p[0] * p[1]);
+    tp1 = cp * (fabs(s.p[2]) / s.syz) * copysign(1.0, s.p[0] * s.p[2]);
+    tp2 = cp * (fabs(s.p[1]) / s.syz) * copysign(1.0, s.p[0] * s.p[1]);
   }
   if (re_r != 0.0) {
     const double ctr = r1 * pow(re_r, r2) + r3 / re_r;

@@ -175,10 +175,12 @@ __global__ void k_force_batch(int64_t n, const double *pcs, double visc, const d
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const PartConst pc = pc_from(pcs, i);
     const Quat q = {quat[4 * i], quat[4 * i + 1], quat[4 * i + 2], quat[4 * i + 3]};
+    double r[9];
+    rotmat(q, r);
+    Slip64 sl;
+    slip64(pc, visc, up + 3 * i, uf + 3 * i, r, sl);
     double fd[3], fl[3];
-    if (!fluid_force(pc, visc, up[3 * i], up[3 * i + 1], up[3 * i + 2], uf[3 * i], uf[3 * i + 1], uf[3 * i + 2], q,
-                     fd, fl))
-      set_error(st, GP_ENAN_FORCE, i);
+    if (!fluid_force(pc, sl, r, fd, fl)) set_error(st, GP_ENAN_FORCE, i);
 #pragma unroll
     for (int k = 0; k < 3; ++k) { fdrag[3 * i + k] = fd[k]; flift[3 * i + k] = fl[k]; }
   }
@@ -190,10 +192,13 @@ __global__ void k_torque_batch(int64_t n, const double *pcs, double visc, const 
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const PartConst pc = pc_from(pcs, i);
     const Quat q = {quat[4 * i], quat[4 * i + 1], quat[4 * i + 2], quat[4 * i + 3]};
+    double r[9];
+    rotmat(q, r);
+    Slip64 sl;
+    slip64(pc, visc, pup + 3 * i, pufap + 3 * i, r, sl);
     double a[3], b[3];
-    fluid_torque(pc, visc, pup[3 * i], pup[3 * i + 1], pup[3 * i + 2], pufap[3 * i], pufap[3 * i + 1],
-                 pufap[3 * i + 2], pvort[3 * i], pvort[3 * i + 1], pvort[3 * i + 2], om[3 * i], om[3 * i + 1],
-                 om[3 * i + 2], q, a, b);
+    fluid_torque(pc, visc, sl, pvort[3 * i], pvort[3 * i + 1], pvort[3 * i + 2], om[3 * i], om[3 * i + 1],
+                 om[3 * i + 2], r, a, b);
     if (om[3 * i] != om[3 * i]) set_error(st, GP_ENAN_TORQUE, i);
 #pragma unroll
     for (int k = 0; k < 3; ++k) { tp[3 * i + k] = a[k]; tr[3 * i + k] = b[k]; }
