@@ -262,35 +262,47 @@ __device__ __forceinline__ void emit_pair(PairRec *pairs, unsigned long long *np
   }
 }
 
-// One candidate (s, qs) of the sweep: conservative float test, FP64 bounding-sphere
-// test, centre-line separation test, reference box adjacency, then emission with the
+// A home particle as the conservative float test of its candidates reads it: position,
+// bounding radius, its instance's box lengths and x periodicity (32 bytes).
+struct HomeF {
+  float x, y, z, r, lx, ly, lz;
+  int perx;
+};
+
+__device__ __forceinline__ HomeF home_f(const InstDev &I, double x, double y, double z, double r) {
+  return {(float)x, (float)y, (float)z, (float)r, (float)I.lx, (float)I.ly, (float)I.lz, I.periodicity != 0};
+}
+
+// The conservative float test of candidate qs (sorted position) against a home at sorted
+// position s: |float - double| distance error < 2e-6, slack 1e-5.  Nearly every
+// candidate of the sweep fails it, so it reads only the candidate's float record.
+// kLarge: the home particle is above the cut and sweeps a full stencil; it takes every
+// small candidate and the large ones that follow it in sorted order.  Otherwise the home
+// particle is small, sweeps the half stencil and leaves large candidates to them.
+template <bool kLarge>
+__device__ __forceinline__ bool near_float(const float4 c, int32_t qs, int32_t s, const HomeF &h) {
+  if (c.w < 0.f && (!kLarge || qs <= s)) return false;
+  float fx = c.x - h.x, fy = c.y - h.y, fz = c.z - h.z;
+  if (h.perx && fabsf(fx) > 0.5f * h.lx) fx = fx - copysignf(h.lx, fx);
+  if (fabsf(fy) > 0.5f * h.ly) fy = fy - copysignf(h.ly, fy);
+  if (fabsf(fz) > 0.5f * h.lz) fz = fz - copysignf(h.lz, fz);
+  const float rf = h.r + fabsf(c.w) + 1.0e-5f;
+  return fx * fx + fy * fy + fz * fz <= rf * rf;
+}
+
+// One candidate (s, qs) of the sweep that passed near_float: FP64 bounding-sphere test,
+// centre-line separation test, reference box adjacency, then emission with the
 // reference's ordering keys.
 struct SearchHome {
   double xp, yp, zp, rp;
-  float xpf, ypf, zpf, rpf, lxf, lyf, lzf;
   long long bp;
   int32_t s, pslot, idp;
   bool perx;
 };
 
-// kLarge: the home particle is above the cut and sweeps a full stencil; it takes every
-// small candidate and the large ones that follow it in sorted order.  Otherwise the home
-// particle is small, sweeps the half stencil and leaves large candidates to them.
-template <bool kLarge>
 __device__ __forceinline__ void search_candidate(const InstDev &I, const SearchArrays &sa, const SearchHome &h,
                                                  int32_t qs, PairRec *pairs, unsigned long long *npairs,
                                                  int64_t cap, Status *st) {
-  // conservative float test: |float - double| distance error < 2e-6, slack 1e-5
-  {
-    const float4 c = sa.spk[qs];
-    if (c.w < 0.f && (!kLarge || qs <= h.s)) return;
-    float fx = c.x - h.xpf, fy = c.y - h.ypf, fz = c.z - h.zpf;
-    if (h.perx && fabsf(fx) > 0.5f * h.lxf) fx = fx - copysignf(h.lxf, fx);
-    if (fabsf(fy) > 0.5f * h.lyf) fy = fy - copysignf(h.lyf, fy);
-    if (fabsf(fz) > 0.5f * h.lzf) fz = fz - copysignf(h.lzf, fz);
-    const float rf = h.rpf + fabsf(c.w) + 1.0e-5f;
-    if (fx * fx + fy * fy + fz * fz > rf * rf) return;
-  }
   double dx = sa.sx[qs] - h.xp, dy = sa.sy[qs] - h.yp, dz = sa.sz[qs] - h.zp;
   if (h.perx && fabs(dx) > I.lx / 2) dx = dx - copysign(I.lx, dx);
   if (fabs(dy) > I.ly / 2.) dy = dy - copysign(I.ly, dy);
@@ -420,6 +432,7 @@ __global__ void __launch_bounds__(kSearchThreads, GP_SEARCH_MIN_BLOCKS) k_search
   // pairs_needed sizes the buffers).  In a step after a halted one the binning did not
   // run and every cell is empty (its counts were cleared), so the sweep finds nothing.
   __shared__ HomeRec homes[kSearchThreads];
+  __shared__ HomeF homesf[kSearchThreads];
   __shared__ int32_t rstart[kSearchThreads][kMaxRanges];   // first sorted particle of a range
   __shared__ int32_t rcum[kSearchThreads][kMaxRanges];     // candidates of the home before it
   __shared__ int8_t rnum[kSearchThreads];
@@ -443,6 +456,7 @@ __global__ void __launch_bounds__(kSearchThreads, GP_SEARCH_MIN_BLOCKS) k_search
       hr.pslot = sa.sorted[s];
       hr.idp = sa.sid[s];
       homes[t] = hr;
+      homesf[t] = home_f(I, hr.xp, hr.yp, hr.zp, hr.rp);
       const int nfx = I.nfx, nfy = I.nfy, nfz = I.nfz;
       const bool perx = I.periodicity != 0;
       // the binning pass's own cell of this particle (same inputs, same function)
@@ -536,15 +550,15 @@ __global__ void __launch_bounds__(kSearchThreads, GP_SEARCH_MIN_BLOCKS) k_search
         const int no = rnum[to];
         while (j + 1 < no && rcum[to][j + 1] <= k) ++j;
         const int32_t q = rstart[to][j] + (k - rcum[to][j]);
-        const HomeRec ho = homes[to];
-        const InstDev &I = insts[ho.inst];
-        SearchHome h;
-        h.s = ho.s; h.xp = ho.xp; h.yp = ho.yp; h.zp = ho.zp; h.rp = ho.rp;
-        h.bp = ho.bp; h.pslot = ho.pslot; h.idp = ho.idp;
-        h.perx = I.periodicity != 0;
-        h.xpf = (float)h.xp; h.ypf = (float)h.yp; h.zpf = (float)h.zp; h.rpf = (float)h.rp;
-        h.lxf = (float)I.lx; h.lyf = (float)I.ly; h.lzf = (float)I.lz;
-        search_candidate<false>(I, sa, h, q, pairs, npairs, cap, st);
+        if (near_float<false>(sa.spk[q], q, 0, homesf[to])) {
+          const HomeRec ho = homes[to];
+          const InstDev &I = insts[ho.inst];
+          SearchHome h;
+          h.s = ho.s; h.xp = ho.xp; h.yp = ho.yp; h.zp = ho.zp; h.rp = ho.rp;
+          h.bp = ho.bp; h.pslot = ho.pslot; h.idp = ho.idp;
+          h.perx = I.periodicity != 0;
+          search_candidate(I, sa, h, q, pairs, npairs, cap, st);
+        }
       }
     }
     if (large) {
@@ -555,8 +569,7 @@ __global__ void __launch_bounds__(kSearchThreads, GP_SEARCH_MIN_BLOCKS) k_search
       h.s = hr.s; h.xp = hr.xp; h.yp = hr.yp; h.zp = hr.zp; h.rp = hr.rp;
       h.bp = hr.bp; h.pslot = hr.pslot; h.idp = hr.idp;
       h.perx = I.periodicity != 0;
-      h.xpf = (float)h.xp; h.ypf = (float)h.yp; h.zpf = (float)h.zp; h.rpf = (float)h.rp;
-      h.lxf = (float)I.lx; h.lyf = (float)I.ly; h.lzf = (float)I.lz;
+      const HomeF hf = home_f(I, h.xp, h.yp, h.zp, h.rp);
       const double reach = (h.rp + I.rmax) * (1.0 + 1.0e-6);
       const int rx = (int)ceil(reach / I.hfx), ry = (int)ceil(reach / I.hfy), rz = (int)ceil(reach / I.hfz);
       const bool ally = 2 * ry + 1 >= nfy, allz = 2 * rz + 1 >= nfz;
@@ -570,9 +583,11 @@ __global__ void __launch_bounds__(kSearchThreads, GP_SEARCH_MIN_BLOCKS) k_search
           const int64_t base = I.cell_begin + ((int64_t)wz * nfy + wy) * nfx;
           const RowRanges rr = row_ranges(sa, base, nfx, lo, hi, h.perx || (2 * rx + 1 >= nfx));
           for (int32_t qs = rr.a0; qs < rr.a1; ++qs)
-            if (qs != s) search_candidate<true>(I, sa, h, qs, pairs, npairs, cap, st);
+            if (qs != s && near_float<true>(sa.spk[qs], qs, h.s, hf))
+              search_candidate(I, sa, h, qs, pairs, npairs, cap, st);
           for (int32_t qs = rr.b0; qs < rr.b1; ++qs)
-            if (qs != s) search_candidate<true>(I, sa, h, qs, pairs, npairs, cap, st);
+            if (qs != s && near_float<true>(sa.spk[qs], qs, h.s, hf))
+              search_candidate(I, sa, h, qs, pairs, npairs, cap, st);
         }
       }
     }
