@@ -175,14 +175,14 @@ __device__ __forceinline__ void gather6_fp32(const InstDev& I, const Stencil& s,
 }
 
 // ---------------------------------------------------------------------------
-// Mixed-precision force and torque: slip and spin vectors and frames in FP64, the
-// Zastawny correlation coefficients in FP32, forces assembled in FP64.  The FP32
-// coefficients bound the relative error of every force and torque near 1e-7, so every
-// scalar that only scales them -- the magnitudes of the slip, of its transverse part
-// and of the relative spin, their reciprocals, the per-particle constants (MixedConst)
-// -- is formed in FP32 as well, and the body-frame flow is shared by the force and the
-// torque when both see the same particle velocity (the first RK2 stage).  The
-// directions (the body-frame slip and the rotations) stay FP64.
+// Mixed-precision force and torque.  The Zastawny correlation coefficients are FP32 and
+// bound the relative error of every force and torque near 1e-7, so the rest of the
+// force and torque is formed in FP32 too: the slip u_f - u_p and the spin are taken as
+// FP64 differences of the FP64 state and then rounded, and the rotation R(q), the
+// body-frame slip, its magnitudes and reciprocals, the per-particle constants
+// (MixedConst) and the assembled force and torque are FP32.  The state they advance
+// stays FP64.  The body-frame flow is shared by the force and the torque when both see
+// the same particle velocity (the first RK2 stage).
 // ---------------------------------------------------------------------------
 struct MixedConst {
   float dv;               // deq / visc: particle Reynolds number per unit slip speed
@@ -199,30 +199,50 @@ __device__ __forceinline__ void mixed_const(const PartConst& pc, double visc, Mi
   mc.riz = (double)__frcp_rn((float)pc.ipzz);
 }
 
+// The FP32 arithmetic of the mixed force, torque and rotation increment is written with
+// explicit roundings (__fmaf_rn, __fmul_rn): the plain and the speculative integrate are
+// separate kernels, and a multiply-add that the compiler fused in one and not in the
+// other would make the two give different bits for the same particle.
+__device__ __forceinline__ float dot3f(float a0, float a1, float a2, float b0, float b1, float b2) {
+  return __fmaf_rn(a2, b2, __fmaf_rn(a1, b1, __fmul_rn(a0, b0)));
+}
+
+// R(q) of transform_basis.f90:44-54 in FP32 (same layout as rotmat: r[i + 3j] = R_ij).
+__device__ __forceinline__ void rotmat_f(const Quat& q, float r[9]) {
+  const float q0 = (float)q.a, q1 = (float)q.b, q2 = (float)q.c, q3 = (float)q.d;
+  r[0] = __fsub_rn(1.f, __fmul_rn(2.f, __fmaf_rn(q2, q2, __fmul_rn(q3, q3))));
+  r[3] = __fmul_rn(2.f, __fmaf_rn(q1, q2, -__fmul_rn(q0, q3)));
+  r[6] = __fmul_rn(2.f, __fmaf_rn(q1, q3, __fmul_rn(q0, q2)));
+  r[1] = __fmul_rn(2.f, __fmaf_rn(q1, q2, __fmul_rn(q0, q3)));
+  r[4] = __fsub_rn(1.f, __fmul_rn(2.f, __fmaf_rn(q1, q1, __fmul_rn(q3, q3))));
+  r[7] = __fmul_rn(2.f, __fmaf_rn(q2, q3, -__fmul_rn(q0, q1)));
+  r[2] = __fmul_rn(2.f, __fmaf_rn(q1, q3, -__fmul_rn(q0, q2)));
+  r[5] = __fmul_rn(2.f, __fmaf_rn(q2, q3, __fmul_rn(q0, q1)));
+  r[8] = __fsub_rn(1.f, __fmul_rn(2.f, __fmaf_rn(q1, q1, __fmul_rn(q2, q2))));
+}
+
 // Slip velocity u_f - u_p in the body frame (R^T p), its magnitude, the magnitude of its
 // transverse part and the incidence angle phi = |atan(syz / b0)| in [0, pi/2].
 struct RelFlow {
-  double b0, b1, b2;      // body frame, FP64
+  float b0, b1, b2;       // body frame
   float umag, syz, inv_syz;
   float lr, sphi, cphi;   // log2 of the particle Reynolds number, sin and cos of phi
 };
 
 static __device__ __forceinline__ void rel_flow(const MixedConst& mc, const double u[3], const double uf[3],
-                                                const double r[9], RelFlow& q) {
-  const double p0 = uf[0] - u[0], p1 = uf[1] - u[1], p2 = uf[2] - u[2];
-  const float f0 = (float)p0, f1 = (float)p1, f2 = (float)p2;
-  q.umag = sqrtf(f0 * f0 + f1 * f1 + f2 * f2);
-  q.b0 = r[0] * p0 + r[1] * p1 + r[2] * p2;
-  q.b1 = r[3] * p0 + r[4] * p1 + r[5] * p2;
-  q.b2 = r[6] * p0 + r[7] * p1 + r[8] * p2;
-  const float c1 = (float)q.b1, c2 = (float)q.b2;
-  q.syz = sqrtf(c1 * c1 + c2 * c2);
+                                                const float r[9], RelFlow& q) {
+  const float p0 = (float)(uf[0] - u[0]), p1 = (float)(uf[1] - u[1]), p2 = (float)(uf[2] - u[2]);
+  q.umag = sqrtf(dot3f(p0, p1, p2, p0, p1, p2));
+  q.b0 = dot3f(r[0], r[1], r[2], p0, p1, p2);
+  q.b1 = dot3f(r[3], r[4], r[5], p0, p1, p2);
+  q.b2 = dot3f(r[6], r[7], r[8], p0, p1, p2);
+  q.syz = sqrtf(__fmaf_rn(q.b2, q.b2, __fmul_rn(q.b1, q.b1)));
   q.inv_syz = __frcp_rn(q.syz);   // used only where syz != 0
   // atan2 of the magnitudes is |atan(syz / b0)|, pi/2 where b0 = 0
-  const float phi = atan2f(q.syz, fabsf((float)q.b0));
+  const float phi = atan2f(q.syz, fabsf(q.b0));
   sincosf(phi, &q.sphi, &q.cphi);
   q.cphi = fmaxf(q.cphi, 0.f);   // float(pi/2) lies above pi/2: keep cos(phi) >= 0 as in FP64
-  q.lr = __log2f(q.umag * mc.dv);
+  q.lr = __log2f(__fmul_rn(q.umag, mc.dv));
 }
 
 // x^y for x in [0, 1] and y > 0 (sines and cosines of the incidence angle raised to the
@@ -231,61 +251,64 @@ static __device__ __forceinline__ void rel_flow(const MixedConst& mc, const doub
 // coefficient, the size of the FP32 correlations' own rounding.  x = 0 gives 0.
 __device__ __forceinline__ float pow_unit(float x, float y) { return exp2f(y * __log2f(x)); }
 
-static __device__ __forceinline__ bool fluid_force_mixed(const PartConst& pc, const RelFlow& q, const double r[9],
+static __device__ __forceinline__ bool fluid_force_mixed(const PartConst& pc, const RelFlow& q, const float r[9],
                                                          double f[3]) {
   f[0] = f[1] = f[2] = 0.0;
   if (q.umag == 0.f) return true;
   const float lr = q.lr, sphi = q.sphi, cphi = q.cphi;
-  const float cd0 = 18.12f * exp2f(-1.023f * lr) + 4.26f * exp2f(-0.384f * lr);
-  const float cd90 = 21.52f * exp2f(-0.990f * lr) + 2.86f * exp2f(-0.260f * lr);
-  const float cdrag = cd0 + (cd90 - cd0) * pow_unit(sphi, 1.95f);
-  const float clift = (0.083f * exp2f(0.21f * lr) + 1.582f * exp2f(-0.851f * lr)) *
-                      pow_unit(sphi, 1.842f - 0.802f * exp2f(-0.006f * lr)) *
-                      pow_unit(cphi, 0.874f + 0.009f * exp2f(0.570f * lr));
-  const double kd = pc.cdrag * (double)(cdrag * q.umag);
-  const double kl = pc.cdrag * (double)(clift * (q.umag * q.umag));
-  double fb0 = kd * q.b0 + kl * (double)sphi * copysign(1.0, -q.b0);
-  double fb1 = kd * q.b1, fb2 = kd * q.b2;
+  const float cd0 = __fmaf_rn(18.12f, exp2f(-1.023f * lr), __fmul_rn(4.26f, exp2f(-0.384f * lr)));
+  const float cd90 = __fmaf_rn(21.52f, exp2f(-0.990f * lr), __fmul_rn(2.86f, exp2f(-0.260f * lr)));
+  const float cdrag = __fmaf_rn(__fsub_rn(cd90, cd0), pow_unit(sphi, 1.95f), cd0);
+  const float clift = __fmul_rn(__fmul_rn(__fmaf_rn(0.083f, exp2f(0.21f * lr), __fmul_rn(1.582f, exp2f(-0.851f * lr))),
+                                          pow_unit(sphi, __fmaf_rn(-0.802f, exp2f(-0.006f * lr), 1.842f))),
+                                pow_unit(cphi, __fmaf_rn(0.009f, exp2f(0.570f * lr), 0.874f)));
+  const float cd = (float)pc.cdrag;
+  const float kd = __fmul_rn(__fmul_rn(cd, cdrag), q.umag);
+  const float kl = __fmul_rn(__fmul_rn(cd, clift), __fmul_rn(q.umag, q.umag));
+  const float fb0 = __fmaf_rn(kd, q.b0, __fmul_rn(__fmul_rn(kl, sphi), copysignf(1.f, -q.b0)));
+  float fb1 = __fmul_rn(kd, q.b1), fb2 = __fmul_rn(kd, q.b2);
   if (q.syz != 0.f) {
-    const double kc = kl * (double)(cphi * q.inv_syz);
-    fb1 += kc * q.b1;
-    fb2 += kc * q.b2;
+    const float kc = __fmul_rn(__fmul_rn(kl, cphi), q.inv_syz);
+    fb1 = __fmaf_rn(kc, q.b1, fb1);
+    fb2 = __fmaf_rn(kc, q.b2, fb2);
   }
-  f[0] = r[0] * fb0 + r[3] * fb1 + r[6] * fb2;
-  f[1] = r[1] * fb0 + r[4] * fb1 + r[7] * fb2;
-  f[2] = r[2] * fb0 + r[5] * fb1 + r[8] * fb2;
+  f[0] = (double)dot3f(r[0], r[3], r[6], fb0, fb1, fb2);
+  f[1] = (double)dot3f(r[1], r[4], r[7], fb0, fb1, fb2);
+  f[2] = (double)dot3f(r[2], r[5], r[8], fb0, fb1, fb2);
   return !(cdrag != cdrag) && isfinite(f[0]) && isfinite(f[1]) && isfinite(f[2]);
 }
 
 static __device__ __forceinline__ void fluid_torque_mixed(const PartConst& pc, const MixedConst& mc, const RelFlow& q,
                                                           const double wv[3], double ox, double oy, double oz,
-                                                          const double r[9], double t[3]) {
-  const double c0 = r[0] * wv[0] + r[1] * wv[1] + r[2] * wv[2];
-  const double c1 = r[3] * wv[0] + r[4] * wv[1] + r[5] * wv[2];
-  const double c2 = r[6] * wv[0] + r[7] * wv[1] + r[8] * wv[2];
-  const double o0 = 0.5 * c0 - ox, o1 = 0.5 * c1 - oy, o2 = 0.5 * c2 - oz;
-  const float g0 = (float)o0, g1 = (float)o1, g2 = (float)o2;
-  const float omag = sqrtf(g0 * g0 + g1 * g1 + g2 * g2);
-  const double oyz = (double)sqrtf(g2 * g2 + g1 * g1);
+                                                          const float r[9], double t[3]) {
+  const float w0 = (float)wv[0], w1 = (float)wv[1], w2 = (float)wv[2];
+  const float c0 = dot3f(r[0], r[1], r[2], w0, w1, w2);
+  const float c1 = dot3f(r[3], r[4], r[5], w0, w1, w2);
+  const float c2 = dot3f(r[6], r[7], r[8], w0, w1, w2);
+  const float o0 = __fmaf_rn(0.5f, c0, -(float)ox), o1 = __fmaf_rn(0.5f, c1, -(float)oy);
+  const float o2 = __fmaf_rn(0.5f, c2, -(float)oz);
+  const float omag = sqrtf(dot3f(o0, o1, o2, o0, o1, o2));
+  const float oyz = sqrtf(__fmaf_rn(o2, o2, __fmul_rn(o1, o1)));
   t[0] = t[1] = t[2] = 0.0;
   if (q.umag != 0.f && q.syz != 0.f) {
     const float lr = q.lr, sphi = q.sphi, cphi = q.cphi;
-    const float ctp = (0.935f * exp2f(-0.146f * lr) - 0.469f * exp2f(-0.145f * lr)) *
-                      pow_unit(sphi, 0.116f + 0.748f * exp2f(0.041f * lr)) *
-                      pow_unit(cphi, 0.221f + 0.657f * exp2f(0.044f * lr));
-    const double cp = pc.cpitch * (double)(ctp * (q.umag * q.umag) * q.inv_syz);
-    t[1] = cp * fabs(q.b2) * copysign(1.0, q.b0 * q.b2);
-    t[2] = cp * fabs(q.b1) * copysign(1.0, q.b0 * q.b1);
+    const float ctp =
+        __fmul_rn(__fmul_rn(__fmaf_rn(0.935f, exp2f(-0.146f * lr), __fmul_rn(-0.469f, exp2f(-0.145f * lr))),
+                            pow_unit(sphi, __fmaf_rn(0.748f, exp2f(0.041f * lr), 0.116f))),
+                  pow_unit(cphi, __fmaf_rn(0.657f, exp2f(0.044f * lr), 0.221f)));
+    const float cp = __fmul_rn(__fmul_rn(__fmul_rn((float)pc.cpitch, ctp), __fmul_rn(q.umag, q.umag)), q.inv_syz);
+    t[1] = (double)(cp * fabsf(q.b2) * copysignf(1.f, q.b0 * q.b2));
+    t[2] = (double)(cp * fabsf(q.b1) * copysignf(1.f, q.b0 * q.b1));
   }
-  const float re_r = omag * mc.d2v;
+  const float re_r = __fmul_rn(omag, mc.d2v);
   if (re_r != 0.f) {
     const float lr = __log2f(re_r);
-    const float ctr = 0.573f * exp2f(-0.154f * lr) + 116.61f * __frcp_rn(re_r);
-    const float ctr2 = 1.244f * exp2f(0.239f * lr) + 378.12f * exp2f(-0.789f * lr);
-    const double k = pc.crot * pc.h5;
-    t[0] += (double)ctr * k * fabs(o0) * o0;
-    t[1] += (double)ctr2 * k * oyz * o1;
-    t[2] += (double)ctr2 * k * oyz * o2;
+    const float ctr = __fmaf_rn(0.573f, exp2f(-0.154f * lr), __fmul_rn(116.61f, __frcp_rn(re_r)));
+    const float ctr2 = __fmaf_rn(1.244f, exp2f(0.239f * lr), __fmul_rn(378.12f, exp2f(-0.789f * lr)));
+    const float k = (float)(pc.crot * pc.h5);
+    t[0] += (double)(ctr * k * fabsf(o0) * o0);
+    t[1] += (double)(ctr2 * k * oyz * o1);
+    t[2] += (double)(ctr2 * k * oyz * o2);
   }
 }
 
@@ -293,11 +316,11 @@ template <bool kMixed>
 struct Forces {
   // F (lab frame, per unit mass) and T (body frame) for stage velocities: the force
   // sees the stage velocity u, the torque the velocity un at the start of the step
-  // (same_u: u and un are the same values).  r = R(q) (mixed form only).
+  // (same_u: u and un are the same values).  r = R(q) in FP32 (mixed form only).
   __device__ __forceinline__ static bool eval(const PartConst& pc, double visc, const MixedConst& mc,
                                               const double u[3], const double un[3], bool same_u,
                                               const double uf[3], const double wv[3], double ox, double oy,
-                                              double oz, const Quat& q, const double r[9], double f[3],
+                                              double oz, const Quat& q, const float r[9], double f[3],
                                               double t[3]) {
     if (kMixed) {
       RelFlow qf;
@@ -349,23 +372,25 @@ __device__ __forceinline__ void k_omega(const double t[3], double ox, double oy,
 }
 
 // Quaternion step of adv_quaternion.f90:39-84 followed by renormalisation (mixed form).
-// r = R(q): the body-to-lab rotation that the stage's force evaluation already built.
-__device__ __forceinline__ void quaternion_step_mixed(Quat& q, const double r[9], double ox, double oy, double oz,
+// r = R(q) in FP32: the body-to-lab rotation that the stage's force evaluation already
+// built.  The increment (the spin in the lab frame, the half angle's sine and cosine) is
+// FP32: a relative error of a few 1e-8 of one step's rotation; the product with q and
+// the renormalisation are FP64.
+__device__ __forceinline__ void quaternion_step_mixed(Quat& q, const float r[9], double ox, double oy, double oz,
                                                       double dt) {
-  const double om[3] = {ox, oy, oz};
-  double omg[3];
-  matvec(r, om, omg);
-  const float n2 = (float)(omg[0] * omg[0] + omg[1] * omg[1] + omg[2] * omg[2]);
+  const float w0 = (float)ox, w1 = (float)oy, w2 = (float)oz;
+  const float g0 = dot3f(r[0], r[3], r[6], w0, w1, w2);
+  const float g1 = dot3f(r[1], r[4], r[7], w0, w1, w2);
+  const float g2 = dot3f(r[2], r[5], r[8], w0, w1, w2);
+  const float n2 = dot3f(g0, g1, g2, g0, g1, g2);
   Quat map = {1.0, 0.0, 0.0, 0.0};
   if (n2 > 0.f) {
-    // the half angle's sine and cosine in FP32: for the small angles of a step the
-    // rotation angle's error is a few 1e-8 of the angle; the axis stays FP64
     const float inv = rsqrtf(n2);
-    const float h = (n2 * inv) * (float)(dt * 0.5);
+    const float h = __fmul_rn(__fmul_rn(n2, inv), (float)(dt * 0.5));
     float s, c;
     sincosf(h, &s, &c);
-    const double si = (double)(s * inv);
-    map = {(double)c, si * omg[0], si * omg[1], si * omg[2]};
+    const float si = __fmul_rn(s, inv);
+    map = {(double)c, (double)__fmul_rn(si, g0), (double)__fmul_rn(si, g1), (double)__fmul_rn(si, g2)};
   }
   q = mult_quat(map, q);
   const double inv = rsqrt(q.a * q.a + q.b * q.b + q.c * q.c + q.d * q.d);
@@ -374,7 +399,7 @@ __device__ __forceinline__ void quaternion_step_mixed(Quat& q, const double r[9]
 
 // One quaternion update; r = R(q) is used by the mixed form only.
 template <bool kMixed>
-__device__ __forceinline__ void quat_advance(Quat& q, const double r[9], double ox, double oy, double oz, double dt) {
+__device__ __forceinline__ void quat_advance(Quat& q, const float r[9], double ox, double oy, double oz, double dt) {
   if (kMixed) quaternion_step_mixed(q, r, ox, oy, oz, dt);
   else quaternion_integration(q, ox, oy, oz, dt);
 }
@@ -390,10 +415,10 @@ __device__ __forceinline__ int advance_particle(const InstDev& I, const PartCons
   const double un[3] = {U[0], U[1], U[2]};
   double f[3], t[3];
   MixedConst mc;
-  double r0[9], r1[9];   // R(Q) and R(q1), mixed form only
+  float r0[9], r1[9];   // R(Q) and R(q1) in FP32, mixed form only
   if (kMixed) {
     mixed_const(pc, I.visc, mc);
-    rotmat(Q, r0);
+    rotmat_f(Q, r0);
   }
   int err = 0;
   if (!Forces<kMixed>::eval(pc, I.visc, mc, un, un, true, uf, wv, O[0], O[1], O[2], Q, r0, f, t)) err = GP_ENAN_FORCE;
@@ -429,11 +454,11 @@ __device__ __forceinline__ int advance_particle(const InstDev& I, const PartCons
       o1[i] = O[i] + (dt - delt) * k1o[i];
     }
     q1 = Q;
-    if (kMixed) rotmat(Q, r0);   // rebuilt here, so that R(Q) need not stay live on the common path
+    if (kMixed) rotmat_f(Q, r0);   // rebuilt here, so that R(Q) need not stay live on the common path
     quat_advance<kMixed>(q1, r0, o1[0], o1[1], o1[2], dt - delt);
     rc = wall_rebound(I.ecw, I.muw, pc, u1[0], u1[1], u1[2], o1[0], o1[1], o1[2], q1, arm, wn);
     if (rc && !err) err = rc;
-    if (kMixed) rotmat(q1, r1);
+    if (kMixed) rotmat_f(q1, r1);
     if (!Forces<kMixed>::eval(pc, I.visc, mc, u1, un, false, uf, wv, o1[0], o1[1], o1[2], q1, r1, f, t) && !err)
       err = GP_ENAN_FORCE;
     if (o1[0] != o1[0] && !err) err = GP_ENAN_TORQUE;
@@ -453,7 +478,7 @@ __device__ __forceinline__ int advance_particle(const InstDev& I, const PartCons
     return err;
   }
   // unbounced second stage, adv_particle_new.f90:513-637
-  if (kMixed) rotmat(q1, r1);
+  if (kMixed) rotmat_f(q1, r1);
   if (!Forces<kMixed>::eval(pc, I.visc, mc, u1, un, false, uf, wv, o1[0], o1[1], o1[2], q1, r1, f, t) && !err)
     err = GP_ENAN_FORCE;
   if (o1[0] != o1[0] && !err) err = GP_ENAN_TORQUE;
