@@ -94,9 +94,8 @@ __global__ void __launch_bounds__(128, GP_CONTACT_MIN_BLOCKS) k_contact(const In
                                   2.0 * (q1.b * q1.d - q1.a * q1.c)};
             const double e2[3] = {1.0 - 2.0 * (q2.c * q2.c + q2.d * q2.d), 2.0 * (q2.b * q2.c + q2.a * q2.d),
                                   2.0 * (q2.b * q2.d - q2.a * q2.c)};
-            const double dd = sqrt(vkx * vkx + vky * vky + vkz * vkz);
-            const bool apart = dd > 0.0 && separated(vkx, vky, vkz, e1, B.a1 * B.a1, B.b1 * B.b1, e2,
-                                                     B.a2 * B.a2, B.b2 * B.b2, vkx / dd, vky / dd, vkz / dd);
+            const bool apart =
+                separated(vkx, vky, vkz, e1, B.a1 * B.a1, B.b1 * B.b1, e2, B.a2 * B.a2, B.b2 * B.b2);
             if (!apart && contact_setup(B.a1, B.b1, B.a2, B.b2, B.c1, q1, B.c2, q2, CP, S.x)) {
               lm_begin(CP, S);
               active = true;

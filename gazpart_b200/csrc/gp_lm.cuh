@@ -702,40 +702,54 @@ GP_LM_FN int lm_step(const Prob& P, LmState& S, double tol) {
 // a few projected-gradient steps from the centre line (the best of four step lengths
 // each) find such an n for nearly every disjoint pair.  Disjoint bodies cannot hold
 // each other's support points, so ellipsoid_contact_detection.f90:125 cannot flag the
-// pair; g must exceed 1e-9 of its terms, far above rounding, so a pair is dropped only
-// when it is disjoint.
-static __device__ __forceinline__ double support_gap(const double n[3], double dx, double dy, double dz, const double e1[3],
-                                              double a1, double b1, const double e2[3], double a2, double b2,
-                                              double &h1, double &h2, double &c1, double &c2) {
+// pair.  The test runs in FP32: its rounding moves g by about 1e-6 of its terms (the
+// inputs rounded to FP32, 3-term dot products, square roots, a unit vector normalised
+// to 1e-7), so g must exceed 1e-4 of its terms, and a pair is dropped only when it is
+// disjoint; pairs closer than that to touching are left to the solver, as are pairs
+// whose g turns NaN.  It never decides a contact, so its precision changes which pairs
+// are solved, not a result.
+static __device__ __forceinline__ float support_gap(const float n[3], const float d[3], const float e1[3],
+                                                    float a1, float b1, const float e2[3], float a2, float b2,
+                                                    float &h1, float &h2, float &c1, float &c2) {
   c1 = e1[0] * n[0] + e1[1] * n[1] + e1[2] * n[2];
   c2 = e2[0] * n[0] + e2[1] * n[1] + e2[2] * n[2];
-  h1 = sqrt(fmax(b1 + (a1 - b1) * c1 * c1, 0.0));
-  h2 = sqrt(fmax(b2 + (a2 - b2) * c2 * c2, 0.0));
-  return n[0] * dx + n[1] * dy + n[2] * dz - h1 - h2;
+  h1 = sqrtf(fmaxf(b1 + (a1 - b1) * c1 * c1, 0.f));
+  h2 = sqrtf(fmaxf(b2 + (a2 - b2) * c2 * c2, 0.f));
+  return n[0] * d[0] + n[1] * d[1] + n[2] * d[2] - h1 - h2;
 }
 
-static __device__ __noinline__ bool separated(double dx, double dy, double dz, const double e1[3], double a1, double b1,
-                                       const double e2[3], double a2, double b2, double ux, double uy, double uz) {
-  double n[3] = {ux, uy, uz};
-  const double dist = sqrt(dx * dx + dy * dy + dz * dz);
-  double h1, h2, c1, c2;
-  double g = support_gap(n, dx, dy, dz, e1, a1, b1, e2, a2, b2, h1, h2, c1, c2);
+// (dx, dy, dz): centre of body 2 minus centre of body 1; e1, e2 unit axes; a, b the
+// squared semi-axes along and across the axis.
+static __device__ __noinline__ bool separated(double dx, double dy, double dz, const double e1d[3], double a1d,
+                                              double b1d, const double e2d[3], double a2d, double b2d) {
+  const float d[3] = {(float)dx, (float)dy, (float)dz};
+  const float e1[3] = {(float)e1d[0], (float)e1d[1], (float)e1d[2]};
+  const float e2[3] = {(float)e2d[0], (float)e2d[1], (float)e2d[2]};
+  const float a1 = (float)a1d, b1 = (float)b1d, a2 = (float)a2d, b2 = (float)b2d;
+  const float dist = sqrtf(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+  if (!(dist > 0.f)) return false;
+  const float idist = __frcp_rn(dist);
+  float n[3] = {d[0] * idist, d[1] * idist, d[2] * idist};
+  float h1, h2, c1, c2;
+  float g = support_gap(n, d, e1, a1, b1, e2, a2, b2, h1, h2, c1, c2);
   for (int it = 0; it < 4; ++it) {
     // gradient of g: d - E1 n / h1 - E2 n / h2, with E n = b^2 n + (a^2 - b^2)(e.n) e
-    double gr[3];
-    for (int k = 0; k < 3; ++k) {
-      const double d_k = k == 0 ? dx : (k == 1 ? dy : dz);
-      gr[k] = d_k - (b1 * n[k] + (a1 - b1) * c1 * e1[k]) / h1 - (b2 * n[k] + (a2 - b2) * c2 * e2[k]) / h2;
-    }
-    const double gn = gr[0] * n[0] + gr[1] * n[1] + gr[2] * n[2];
-    const double t[3] = {(gr[0] - gn * n[0]) / dist, (gr[1] - gn * n[1]) / dist, (gr[2] - gn * n[2]) / dist};
-    double best = -1e300, bn[3] = {n[0], n[1], n[2]}, bh1 = h1, bh2 = h2, bc1 = c1, bc2 = c2;
-    for (double alpha = 0.25; alpha <= 2.0; alpha *= 2.0) {
-      double m[3] = {n[0] + alpha * t[0], n[1] + alpha * t[1], n[2] + alpha * t[2]};
-      const double inv = 1.0 / sqrt(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
+    const float i1 = __frcp_rn(h1), i2 = __frcp_rn(h2);
+    float gr[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+      gr[k] = d[k] - (b1 * n[k] + (a1 - b1) * c1 * e1[k]) * i1 - (b2 * n[k] + (a2 - b2) * c2 * e2[k]) * i2;
+    const float gn = gr[0] * n[0] + gr[1] * n[1] + gr[2] * n[2];
+    const float t[3] = {(gr[0] - gn * n[0]) * idist, (gr[1] - gn * n[1]) * idist, (gr[2] - gn * n[2]) * idist};
+    float best = -3.0e38f, bn[3] = {n[0], n[1], n[2]}, bh1 = h1, bh2 = h2, bc1 = c1, bc2 = c2;
+#pragma unroll
+    for (int ka = 0; ka < 4; ++ka) {
+      const float alpha = 0.25f * (float)(1 << ka);
+      float m[3] = {n[0] + alpha * t[0], n[1] + alpha * t[1], n[2] + alpha * t[2]};
+      const float inv = rsqrtf(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
       m[0] *= inv; m[1] *= inv; m[2] *= inv;
-      double mh1, mh2, mc1, mc2;
-      const double gm = support_gap(m, dx, dy, dz, e1, a1, b1, e2, a2, b2, mh1, mh2, mc1, mc2);
+      float mh1, mh2, mc1, mc2;
+      const float gm = support_gap(m, d, e1, a1, b1, e2, a2, b2, mh1, mh2, mc1, mc2);
       if (gm > best) {
         best = gm;
         bn[0] = m[0]; bn[1] = m[1]; bn[2] = m[2];
@@ -746,8 +760,8 @@ static __device__ __noinline__ bool separated(double dx, double dy, double dz, c
     n[0] = bn[0]; n[1] = bn[1]; n[2] = bn[2];
     h1 = bh1; h2 = bh2; c1 = bc1; c2 = bc2;
     g = best;
-    const double scale = fabs(n[0] * dx + n[1] * dy + n[2] * dz) + h1 + h2;
-    if (g > 1e-9 * scale) return true;
+    const float scale = fabsf(n[0] * d[0] + n[1] * d[1] + n[2] * d[2]) + h1 + h2;
+    if (g > 1.0e-4f * scale) return true;
   }
   return false;
 }
