@@ -144,6 +144,16 @@ class Context:
         check(_lib.lib().gp_get_contact_tail(self._h, C.byref(b)), "gp_get_contact_tail")
         return b.value
 
+    def set_contact_order(self, on: bool) -> None:
+        """Hand the contact solves to the lanes in decreasing predicted length (the
+        default) or in candidate-list order; results are unchanged."""
+        check(_lib.lib().gp_set_contact_order(self._h, 1 if on else 0), "gp_set_contact_order")
+
+    def contact_order(self) -> bool:
+        v = C.c_int32()
+        check(_lib.lib().gp_get_contact_order(self._h, C.byref(v)), "gp_get_contact_order")
+        return bool(v.value)
+
     def enable_collision_stats(self, on: bool = True) -> None:
         check(_lib.lib().gp_collision_stats_enable(self._h, 1 if on else 0), "gp_collision_stats_enable")
 

@@ -184,6 +184,16 @@ struct gp_ctx {
   TailRec *d_tail[2] = {nullptr, nullptr};
   int64_t cap_tail = 0;
   int tail_budget = 0;
+  // contact queue order (gp_contact.cu): what each particle's solves took in the last
+  // collision phase (d_evhist, by instance begin + id), each candidate pair's bin and the
+  // pairs in decreasing predicted length.  Optional: where there is no room it stays off.
+  bool qorder_on = true;
+  uint32_t *d_evhist = nullptr;
+  int64_t cap_evhist = 0;
+  uint32_t *d_qorder = nullptr;
+  uint8_t *d_qkey = nullptr;
+  int64_t cap_qorder = 0;
+  uint32_t *d_qbins = nullptr;   // 2 * kQueueBins
 };
 
 namespace {
@@ -247,7 +257,36 @@ void free_pool(gp_ctx *c) {
   dfree(c->d_pairs); dfree(c->d_coll); dfree(c->d_state); dfree(c->d_acc);
   dfree(c->d_mark);
   c->cap_mark = 0;
+  dfree(c->d_evhist); dfree(c->d_qorder); dfree(c->d_qkey);
+  c->cap_evhist = 0;
+  c->cap_qorder = 0;
   c->cap = 0;
+}
+
+// The contact queue's order buffers: the particles' record (zero) for `cap` particles,
+// and the order and bin of each of `cap_pairs` pairs.  The order is optional: where
+// there is no room it stays off, and a failed allocation's error is cleared so that later
+// launch checks do not read it.
+void try_qorder(gp_ctx *c) {
+  if (c->cap_evhist < c->cap) {
+    dfree(c->d_evhist);
+    c->cap_evhist = 0;
+    if (dalloc(&c->d_evhist, (size_t)c->cap) == GP_OK &&
+        cudaMemsetAsync(c->d_evhist, 0, (size_t)c->cap * sizeof(uint32_t), c->stream) == cudaSuccess)
+      c->cap_evhist = c->cap;
+  }
+  if (c->cap_qorder < c->cap_pairs) {
+    dfree(c->d_qorder); dfree(c->d_qkey);
+    c->cap_qorder = 0;
+    if (dalloc(&c->d_qorder, (size_t)c->cap_pairs) == GP_OK && dalloc(&c->d_qkey, (size_t)c->cap_pairs) == GP_OK)
+      c->cap_qorder = c->cap_pairs;
+  }
+  cudaGetLastError();
+}
+
+bool qorder_ready(const gp_ctx *c) {
+  return c->qorder_on && c->d_qbins && c->cap_evhist >= c->cap && c->cap_evhist >= c->n_slots &&
+         c->cap_qorder >= c->cap_pairs;
 }
 
 // The speculative integrate's marks, one per pool slot, all zero.
@@ -315,6 +354,7 @@ int alloc_pool(gp_ctx *c, int64_t cap) {
     c->cap_cst = c->cap_pairs;
   }
   if (c->spec && !try_mark(c)) c->spec = false;
+  try_qorder(c);
   return GP_OK;
 }
 
@@ -468,6 +508,17 @@ int enqueue_bin_search(gp_ctx *c, bool flag = false) {
   // a step with more candidates than either pair buffer holds halts after the search
   launch_search(c->d_inst, c->n, sa, c->d_pairs, c->d_counters + 0, std::min(c->cap_pairs, c->cap_coll),
                 c->d_status, c->tune[GP_TUNE_SEARCH], c->stream);
+  // The contact queue's order: the pairs in decreasing predicted length, from the
+  // particles' record of the last collision phase, which is then cleared for this one.
+  // It is formed here, before a multi-step graph forks the next gather onto the side
+  // stream, so that the contact kernel is the first work ready after the fork and its
+  // persistent grid takes the SMs before the gather's blocks do.
+  if (qorder_ready(c)) {
+    GP_CK(cudaMemsetAsync(c->d_qbins, 0, 2 * kQueueBins * sizeof(uint32_t), c->stream));
+    launch_queue_order(c->d_inst, c->d_pv, c->d_pairs, c->d_counters + 0, c->cap_pairs, c->d_evhist, c->n_slots,
+                       c->d_qkey, c->d_qbins, c->d_qorder, c->d_status, 148 * 4, c->stream);
+    GP_CK(cudaMemsetAsync(c->d_evhist, 0, (size_t)c->n_slots * sizeof(uint32_t), c->stream));
+  }
   GP_CK(cudaGetLastError());
   return mark(c, 2 * GP_PHASE_SEARCH + 1, c->stream);
 }
@@ -484,6 +535,9 @@ int enqueue_contact_response(gp_ctx *c) {
   budget[npass++] = 0;
   unsigned long long *pc = c->d_counters + kPassCounters;
   GP_CK(cudaMemsetAsync(pc, 0, 2 * kMaxPasses * sizeof(unsigned long long), c->stream));
+  // the first pass takes the pairs in the order enqueue_bin_search formed
+  const bool order = qorder_ready(c);
+  const int64_t nhist = order ? c->n_slots : 0;
   for (int p = 0; p < npass; ++p) {
     const bool last = p == npass - 1;
     const TailRec *in = p > 0 ? c->d_tail[(p - 1) & 1] : nullptr;
@@ -491,6 +545,7 @@ int enqueue_contact_response(gp_ctx *c) {
     launch_contact(c->d_inst, c->d_pv, c->d_pairs, c->d_counters + 0, c->cap_pairs, in,
                    p > 0 ? pc + 2 * (p - 1) + 1 : nullptr, c->cap_tail, c->d_coll, c->d_counters + 1, c->cap_coll,
                    pc + 2 * p, cst, c->d_counters + 4, c->cap_cst, out, pc + 2 * p + 1, c->cap_tail, budget[p],
+                   (order && p == 0) ? c->d_qorder : nullptr, order ? c->d_evhist : nullptr, nhist,
                    c->d_status, c->contact_grid, c->stream);
   }
   GP_TRY(mark(c, 2 * GP_PHASE_CONTACT + 1, c->stream));
@@ -572,6 +627,7 @@ int size_pairs(gp_ctx *c, int64_t pairs, int64_t coll) {
     c->cap_pairs = 0;
     GP_TRY(dalloc(&c->d_pairs, np));
     c->cap_pairs = np;
+    try_qorder(c);
     if (c->d_cst) {                    // every candidate pair may be in contact
       dfree(c->d_cst);
       c->cap_cst = 0;
@@ -681,6 +737,7 @@ int gp_ctx_create(const gp_params *params, gp_ctx **out) {
           cudaSuccess)
         rc = GP_ENOMEM;
   }
+  if (!rc) rc = dalloc(&c->d_qbins, 2 * kQueueBins);
   if (!rc) rc = dalloc(&c->d_group_tab, kMaxClasses);
   if (!rc) rc = dalloc(&c->d_group_n, kMaxClasses);
   if (!rc) {
@@ -723,7 +780,7 @@ int gp_ctx_destroy(gp_ctx *c) {
   dfree(c->d_counters);
   for (auto &g : c->group_dev) dfree(g);
   dfree(c->d_group_tab); dfree(c->d_group_n); dfree(c->d_cst); dfree(c->d_colacc);
-  dfree(c->d_stat_partial); dfree(c->d_stat_out);
+  dfree(c->d_stat_partial); dfree(c->d_stat_out); dfree(c->d_qbins);
   for (TailRec *t : c->d_tail)
     if (t) cudaFree(t);
   dfree(c->d_status); dfree(c->d_scratch);
@@ -1118,6 +1175,23 @@ int gp_set_contact_tail(gp_ctx *c, int32_t budget) {
 int gp_get_contact_tail(gp_ctx *c, int32_t *budget) {
   if (!c || !budget) return GP_EBADARG;
   *budget = c->tail_budget;
+  return GP_OK;
+}
+
+int gp_set_contact_order(gp_ctx *c, int32_t on) {
+  if (!c) return GP_EBADARG;
+  if ((on != 0) == c->qorder_on) return GP_OK;
+  GP_CK(cudaStreamSynchronize(c->stream));
+  c->qorder_on = on != 0;
+  drop_graph(c);
+  if (c->qorder_on && c->d_evhist)   // no record carried over from before it was off
+    GP_CK(cudaMemsetAsync(c->d_evhist, 0, (size_t)c->cap_evhist * sizeof(uint32_t), c->stream));
+  return GP_OK;
+}
+
+int gp_get_contact_order(gp_ctx *c, int32_t *on) {
+  if (!c || !on) return GP_EBADARG;
+  *on = qorder_ready(c) ? 1 : 0;
   return GP_OK;
 }
 

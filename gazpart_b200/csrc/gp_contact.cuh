@@ -41,18 +41,24 @@ __device__ __forceinline__ void pair_bodies(const InstDev *__restrict__ insts, c
 // colliding-pair record.  Out of line and given only the pair index and the solver's
 // result, so that the solving loop never passes its state by address: the problem is
 // rebuilt from the pool, which the contact phase does not change, by the same set-up
-// (hence to the same values).
+// (hence to the same values).  hist (optional): the queue order's record of the solve.
 static __device__ __noinline__ void finish_pair(const InstDev *__restrict__ insts, const PoolView *__restrict__ pv,
                                          const PairRec *__restrict__ pairs, int64_t e, double x0, double x1,
                                          int nfev, CollRec *__restrict__ coll, unsigned long long *ncoll,
                                          int64_t cap_coll, ContactStatRec *__restrict__ cst,
-                                         unsigned long long *ncst, int64_t cap_cst, Status *st) {
+                                         unsigned long long *ncst, int64_t cap_cst, uint32_t *hist,
+                                         int64_t nhist, Status *st) {
   const PoolView P = *pv;
   atomicAdd(&st->n_solve, 1ull);
   atomicAdd(&st->n_eval, (unsigned long long)nfev);
   atomicMax(&st->max_eval, (unsigned long long)nfev);
   const PairRec pr = pairs[e];
   const int i1 = pr.home, i2 = pr.near;
+  if (hist) {   // what this solve took, for the next collision phase's queue order
+    const int64_t k0 = insts[P.inst[i1]].begin, g1 = k0 + P.id[i1], g2 = k0 + P.id[i2];
+    if (g1 < nhist) atomicMax(&hist[g1], (uint32_t)nfev + 1u);
+    if (g2 < nhist) atomicMax(&hist[g2], (uint32_t)nfev + 1u);
+  }
   PairBodies B;
   pair_bodies(insts, P, i1, i2, B);
   ContactProb CP;

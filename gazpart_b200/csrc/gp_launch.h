@@ -30,8 +30,15 @@ void launch_contact(const InstDev *insts, const PoolView *pv, const PairRec *pai
                     int64_t cap_pairs, const TailRec *in, const unsigned long long *nin, int64_t cap_in,
                     CollRec *coll, unsigned long long *ncoll, int64_t cap_coll, unsigned long long *queue,
                     ContactStatRec *cst, unsigned long long *ncst, int64_t cap_cst, TailRec *out,
-                    unsigned long long *nout, int64_t cap_out, int budget, Status *st, int grid, cudaStream_t s);
+                    unsigned long long *nout, int64_t cap_out, int budget, const uint32_t *order,
+                    uint32_t *hist, int64_t nhist, Status *st, int grid, cudaStream_t s);
 size_t tail_record_bytes();
+// The contact queue's order for the candidate pairs (gp_contact.cu): bins holds
+// 2 * kQueueBins counters, zero at the launch; key one byte per pair slot.
+constexpr int kQueueBins = 256;
+void launch_queue_order(const InstDev *insts, const PoolView *pv, const PairRec *pairs,
+                        const unsigned long long *npairs, int64_t cap_pairs, const uint32_t *hist, int64_t nhist,
+                        uint8_t *key, uint32_t *bins, uint32_t *order, const Status *st, int grid, cudaStream_t s);
 void launch_response(const InstDev *insts, const PoolView *pv, const CollRec *coll, const unsigned long long *ncoll,
                      int64_t cap_coll, const int8_t *state, int32_t *acc_list, unsigned long long *nacc, Status *st,
                      int grid, cudaStream_t s);

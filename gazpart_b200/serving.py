@@ -22,8 +22,9 @@ from .api import PROP_KEYS, STATE_KEYS, Context, check
 # Device bytes one resident particle costs: two pool buffers (13 state + 10 constant
 # doubles, id, class), the six interpolated field values, the search arrays (cell,
 # order, position, radius, packed float4, axis, semi-axes, box key, class, id), the
-# matching words and its share of the pair and contact buffers.
-BYTES_PER_PARTICLE = 2 * (23 * 8 + 8) + 6 * 8 + (4 + 4 + 32 + 16 + 24 + 16 + 8 + 8) + 17 + 24 + 26
+# matching words, its share of the pair and contact buffers, and the contact queue's
+# order (the particle's record of its last solves, a pair slot's order and bin).
+BYTES_PER_PARTICLE = 2 * (23 * 8 + 8) + 6 * 8 + (4 + 4 + 32 + 16 + 24 + 16 + 8 + 8) + 17 + 24 + 26 + 4 + 5
 
 
 class GPJob(C.Structure):

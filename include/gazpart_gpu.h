@@ -196,6 +196,13 @@ int gp_upload_classes(gp_ctx *ctx, int32_t nclass, const int64_t *counts, const 
  * (MINPACK's maxfev). */
 int gp_set_contact_tail(gp_ctx *ctx, int32_t budget);
 int gp_get_contact_tail(gp_ctx *ctx, int32_t *budget);
+/* No counterpart in the reference.  With the order on (the default), the contact solves
+ * of a collision phase are handed to the lanes in decreasing predicted length, each pair
+ * predicted from what its particles' solves took in the last collision phase, so that
+ * solves of similar length share a warp; the results do not change.  The getter reports
+ * whether the order is in use (on, with its buffers allocated). */
+int gp_set_contact_order(gp_ctx *ctx, int32_t on);
+int gp_get_contact_order(gp_ctx *ctx, int32_t *on);
 /* Mesh (nx, ny, nz) of field slot `field`. */
 int gp_field_shape(gp_ctx *ctx, int32_t field, int32_t dims[3]);
 /* No counterpart in the reference (serving).  More resident fields beside the one of

@@ -220,3 +220,31 @@ def test_contact_tail_hand_over_changes_nothing(name):
         for k in api.STATE_KEYS:
             assert np.array_equal(got[k], out[0][1][k]), (budget, k)
         assert cnt == out[0][2], budget
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("name", ["dense", "bimodal"])
+def test_contact_order_changes_nothing(name, precision):
+    """The contact queue's order (solves handed out in decreasing predicted length, from
+    what each particle's solves took in the last collision phase) changes only which lane
+    solves a pair: a six-step graph and three single steps after it give the same states,
+    counters and colliding pairs with the order on and off, bit for bit."""
+    setup, fn, refs, st = case(name)
+    grids = {"gather": 296, "integrate": 592, "bin": 592, "search": 592}
+    out = {}
+    for on in (False, True):
+        with _ctx(setup, fn, st, precision) as ctx:
+            ctx.set_launch({**grids, "overlap_gather": True})
+            ctx.set_contact_order(on)
+            assert ctx.contact_order() == on
+            ctx.step(6)
+            for _ in range(3):
+                ctx.step(1)
+            ctx.raise_status()
+            out[on] = (ctx.download(), ctx.collision_counters(), ctx.collision_pairs())
+    assert out[False][1]["accepted"] > 0
+    assert out[True][1] == out[False][1]
+    for a, b in zip(out[True][2], out[False][2]):
+        assert np.array_equal(a, b)
+    for k in api.STATE_KEYS:
+        assert np.array_equal(out[True][0][k], out[False][0][k]), k
