@@ -135,6 +135,8 @@ SIGNATURES = {
     "gp_get_contact_tail": [_ctx, _ip],
     "gp_set_contact_order": [_ctx, C.c_int32],
     "gp_get_contact_order": [_ctx, _ip],
+    "gp_set_gather_staging": [_ctx, C.c_int32],
+    "gp_get_gather_staging": [_ctx, _ip],
     "gp_dns_create": [C.POINTER(GPParams), C.c_int32, C.c_double, C.POINTER(_vp)],
     "gp_dns_destroy": [_vp],
     "gp_dns_set_velocity": [_vp, _vp, _vp, _vp, C.c_int32],

@@ -154,6 +154,16 @@ class Context:
         check(_lib.lib().gp_get_contact_order(self._h, C.byref(v)), "gp_get_contact_order")
         return bool(v.value)
 
+    def set_gather_staging(self, mode: int) -> None:
+        """Mixed gather: 0 stencil rows through L1, 1 each stencil box staged in shared
+        memory by the TMA (one field for every class); results are unchanged."""
+        check(_lib.lib().gp_set_gather_staging(self._h, int(mode)), "gp_set_gather_staging")
+
+    def gather_staging(self) -> int:
+        v = C.c_int32()
+        check(_lib.lib().gp_get_gather_staging(self._h, C.byref(v)), "gp_get_gather_staging")
+        return v.value
+
     def enable_collision_stats(self, on: bool = True) -> None:
         check(_lib.lib().gp_collision_stats_enable(self._h, 1 if on else 0), "gp_collision_stats_enable")
 
@@ -340,6 +350,7 @@ class Context:
         out["overlap_gather"] = bool(g[len(_lib.TUNABLES)])
         out["speculative_integrate"] = g[len(_lib.TUNABLES)] == 2
         out["contact_tail"] = self.contact_tail()
+        out["gather_staging"] = self.gather_staging()
         return out
 
     def set_launch(self, grids: Dict[str, int]) -> None:
@@ -350,6 +361,8 @@ class Context:
         check(_lib.lib().gp_set_launch(self._h, g), "gp_set_launch")
         if "contact_tail" in grids:
             self.set_contact_tail(int(grids["contact_tail"]))
+        if "gather_staging" in grids:
+            self.set_gather_staging(int(grids["gather_staging"]))
 
     def download(self, fluid: bool = False) -> Dict[str, np.ndarray]:
         out = {k: np.empty(self.n) for k in STATE_KEYS}

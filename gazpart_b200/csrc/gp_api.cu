@@ -16,6 +16,7 @@
 #include <utility>
 #include <vector>
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "../../include/gazpart_gpu.h"
@@ -194,6 +195,12 @@ struct gp_ctx {
   uint8_t *d_qkey = nullptr;
   int64_t cap_qorder = 0;
   uint32_t *d_qbins = nullptr;   // 2 * kQueueBins
+  // the mixed gather's staging: 0 stencil rows through L1, 1 each stencil box staged in
+  // shared memory by the TMA (gp_gather_tma.cu), over gmap, the tensor map of gmap_field
+  int gather_staging = 0;
+  CUtensorMap gmap{};
+  const void *gmap_field = nullptr;
+  int gmap_dims[3] = {0, 0, 0};
 };
 
 namespace {
@@ -423,9 +430,46 @@ int mark(gp_ctx *c, int slot, cudaStream_t s) {
 }
 
 // Stencil gather at x_n for the particles in the last binning's order, on stream s.
+// The one field every live class reads (the TMA-staged gather maps a single field), or
+// false when they read several.
+bool single_field(const gp_ctx *c, const InstDev **out) {
+  const InstDev *f = nullptr;
+  if (c->insts.empty()) {
+    f = &c->tmpl;
+  } else {
+    for (size_t k = 0; k < c->insts.size(); ++k) {
+      if (!c->live[k]) continue;
+      const InstDev &I = c->insts[k];
+      if (f && (I.field != f->field || I.nx != f->nx || I.ny != f->ny || I.nz != f->nz)) return false;
+      if (!f) f = &I;
+    }
+  }
+  if (!f || !f->field) return false;
+  *out = f;
+  return true;
+}
+
+// The tensor map of the single field, made again when the field or its mesh changed.
+int ensure_field_map(gp_ctx *c) {
+  const InstDev *f = nullptr;
+  if (c->prm.precision != GP_PREC_MIXED || !single_field(c, &f)) return GP_EBADARG;
+  if (c->gmap_field == f->field && c->gmap_dims[0] == f->nx && c->gmap_dims[1] == f->ny && c->gmap_dims[2] == f->nz)
+    return GP_OK;
+  c->gmap_field = nullptr;
+  GP_TRY(make_field_map(f->field, f->nx, f->ny, f->nz, &c->gmap));
+  c->gmap_field = f->field;
+  c->gmap_dims[0] = f->nx; c->gmap_dims[1] = f->ny; c->gmap_dims[2] = f->nz;
+  return GP_OK;
+}
+
 int enqueue_gather(gp_ctx *c, cudaStream_t s) {
   GP_TRY(mark(c, 2 * GP_PHASE_GATHER, s));
-  if (c->prm.precision == GP_PREC_MIXED)
+  if (c->prm.precision == GP_PREC_MIXED && c->gather_staging == 1 && ensure_field_map(c) == GP_OK)
+    // two blocks of four warps per SM are resident; the warps take their runs from the
+    // ticket, so more blocks would only wait
+    launch_gather_tma(c->gmap, c->d_inst, c->d_pv, c->sa.sorted, c->n, c->d_fluid_cols, c->d_counters + 6,
+                      c->d_status, 148 * 2, s);
+  else if (c->prm.precision == GP_PREC_MIXED)
     launch_gather_mixed(c->d_inst, c->d_pv, c->sa.sorted, c->n, c->d_fluid_cols, c->d_counters + 6, c->d_status,
                         c->tune[GP_TUNE_GATHER], s);
   else
@@ -1195,6 +1239,24 @@ int gp_get_contact_order(gp_ctx *c, int32_t *on) {
   return GP_OK;
 }
 
+int gp_set_gather_staging(gp_ctx *c, int32_t mode) {
+  if (!c || mode < 0 || mode > 1) return GP_EBADARG;
+  if (mode == 1) {
+    GP_TRY(ensure_field_map(c));
+    GP_TRY(gather_tma_prepare());
+  }
+  c->gather_staging = mode;
+  drop_graph(c);
+  return GP_OK;
+}
+
+int gp_get_gather_staging(gp_ctx *c, int32_t *mode) {
+  if (!c || !mode) return GP_EBADARG;
+  const InstDev *f = nullptr;
+  *mode = (c->gather_staging == 1 && c->prm.precision == GP_PREC_MIXED && single_field(c, &f)) ? 1 : 0;
+  return GP_OK;
+}
+
 int gp_collision_stats_enable(gp_ctx *c, int32_t on) {
   if (!c) return GP_EBADARG;
   if ((on != 0) == c->colstats) return GP_OK;
@@ -1960,6 +2022,26 @@ int gp_autotune(gp_ctx *c, int32_t *grids_out) {
     }
     c->tune[t] = best;
   }
+  // The mixed gather's staging (stencil rows through L1, or each stencil box staged by
+  // the TMA), by the gather's one-step time, where the classes read one field.
+  if (!rc && c->prm.precision == GP_PREC_MIXED && ensure_field_map(c) == GP_OK && gather_tma_prepare() == GP_OK) {
+    int best = c->gather_staging;
+    float best_ms = 1e30f;
+    for (int m = 0; m < 2 && !rc; ++m) {
+      c->gather_staging = m;
+      drop_graph(c);
+      float ph[GP_NPHASE], trial[3];
+      for (int r = 0; r < 3 && !rc; ++r) {
+        rc = gp_step_timed(c, 1, nullptr, ph, nullptr);
+        trial[r] = ph[GP_PHASE_GATHER];
+      }
+      if (rc) break;
+      std::sort(trial, trial + 3);
+      if (trial[1] < best_ms) { best_ms = trial[1]; best = m; }
+    }
+    c->gather_staging = best;
+  }
+  cudaGetLastError();
   // Overlapped gather (and speculative integrate) or not, timed as eight-step graphs
   // (median of three), closer to the steady state than shorter graphs.  Overlapped work
   // only gets the SMs the contact solves leave, so it is also tried with the gather at

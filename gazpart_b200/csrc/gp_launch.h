@@ -1,6 +1,7 @@
 // gp_launch.h -- host-side launchers of the device kernels (one per translation unit
 // so that the FP64 path can be compiled without FMA contraction).
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "gp_types.h"
@@ -56,6 +57,18 @@ void launch_contact_batch(int64_t n, const double *shapes /*n*4: a1 b1 a2 b2*/, 
 void launch_response_batch(int64_t n, double ecp, double mup, const double *ip /*n*3*/, double *p1 /*n*10*/,
                            double *p2, const double *r1, const double *r2, const double *nrm, Status *st,
                            cudaStream_t s);
+
+// --- gp_gather_tma.cu: the FP32 gather with each stencil box staged by the TMA ---
+// make_field_map: tensor map over one FP32 field slot ([z][y][x][8], the interior sizes
+// given); gather_tma_prepare: the kernel's shared-memory limit, once, outside any stream
+// capture; launch_gather_tma: as launch_gather_mixed, for instances that all read the
+// mapped field.
+int make_field_map(const void *field, int nx, int ny, int nz, CUtensorMap *out);
+int gather_tma_prepare();
+size_t gather_tma_smem_bytes();
+void launch_gather_tma(const CUtensorMap &map, const InstDev *insts, const PoolView *pv, const int32_t *perm,
+                       int64_t n, double *const *fluid, unsigned long long *ticket, Status *st, int grid,
+                       cudaStream_t s);
 
 // --- gp_stats.cu (-fmad=false) ---
 void launch_stat_partfluid(const InstDev *insts, const PoolView *pv, int64_t n, int inst, double *const *fluid,

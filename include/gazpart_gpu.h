@@ -203,6 +203,16 @@ int gp_get_contact_tail(gp_ctx *ctx, int32_t *budget);
  * whether the order is in use (on, with its buffers allocated). */
 int gp_set_contact_order(gp_ctx *ctx, int32_t on);
 int gp_get_contact_order(gp_ctx *ctx, int32_t *on);
+/* No counterpart in the reference.  How the mixed form's stencil gather
+ * (interp_lag3.f90:124-288) brings the field in: 0 (the default) loads each particle's
+ * 16 stencil rows through L1; 1 stages each particle's 4x4x4-point box in shared memory
+ * with the tensor-memory accelerator (one cp.async.bulk.tensor request per particle,
+ * several particles in flight per warp).  Both give the same values bit for bit.  1 needs
+ * the mixed precision and every class on one field, GP_EBADARG otherwise; should classes
+ * later read several fields, the gather goes back to rows.  gp_autotune times both and
+ * keeps the faster; the getter reports the staging in use. */
+int gp_set_gather_staging(gp_ctx *ctx, int32_t mode);
+int gp_get_gather_staging(gp_ctx *ctx, int32_t *mode);
 /* Mesh (nx, ny, nz) of field slot `field`. */
 int gp_field_shape(gp_ctx *ctx, int32_t field, int32_t dims[3]);
 /* No counterpart in the reference (serving).  More resident fields beside the one of
@@ -305,7 +315,8 @@ enum {
     GP_NTUNE = 4
 };
 /* Autotuner: for each launch above, in turn, times one-step graphs of the resident
- * ensemble with 148 x {1,2,4,8,16} blocks and keeps the fastest; then times eight-step
+ * ensemble with 148 x {1,2,4,8,16} blocks and keeps the fastest; for the mixed form on
+ * one field, also the gather's staging (gp_set_gather_staging); then times eight-step
  * graphs without and with the next step's gather run on a second stream beside the
  * contact solves, the latter also with the next step's integrate of the particles in
  * no candidate pair following the gather there (each also with the gather at 148 x 16

@@ -122,3 +122,27 @@ def test_channel_steps_match_oracle():
     j = np.arange(40, 60)
     assert np.all(got["z"][j] < 0.01) and np.all(got["y"][j] > L - 0.01)      # y and z wrapped
     assert np.any(got["x"] != x0)
+
+
+@pytest.mark.gpu
+def test_channel_mixed_gather_staging_changes_nothing():
+    """In the channel the stencils next to the walls are mirrored (not four contiguous
+    points), and the TMA-staged mixed gather leaves those to per-lane loads: six steps
+    give the row gather's states and fluid values bit for bit."""
+    s = _setup()
+    x_in, ug, vorty = _profile()
+    f = field.channel(s, x_in, ug, vorty, po.frozen_interp_lag3)
+    fn = {k: v.numpy().copy() for k, v in f.items()}
+    st, refs = _channel_state(s, f)
+    out = {}
+    for mode in (0, 1):
+        with api.Context(s, "mixed", store_fluid=True) as ctx:
+            ctx.set_fields(fn)
+            ctx.upload(st)
+            ctx.set_gather_staging(mode)
+            assert ctx.gather_staging() == mode
+            ctx.step(6)
+            ctx.raise_status()
+            out[mode] = ctx.download(fluid=True)
+    for k in out[0]:
+        assert np.array_equal(out[0][k], out[1][k], equal_nan=True), k

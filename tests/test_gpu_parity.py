@@ -248,3 +248,29 @@ def test_contact_order_changes_nothing(name, precision):
         assert np.array_equal(a, b)
     for k in api.STATE_KEYS:
         assert np.array_equal(out[True][0][k], out[False][0][k]), k
+
+
+@pytest.mark.parametrize("name", ["dense", "poly"])
+def test_gather_staging_changes_nothing(name):
+    """The mixed gather with each particle's stencil box staged in shared memory by the
+    TMA (gp_set_gather_staging(1)) sums the same values in the same order as the gather
+    of stencil rows through L1: the interpolated fluid values and the states after one
+    step and after five more steps with the gather overlapped are the same bit for bit."""
+    setup, fn, refs, st = case(name)
+    out = {}
+    for mode in (0, 1):
+        with _ctx(setup, fn, st, "mixed", store_fluid=True) as ctx:
+            ctx.set_gather_staging(mode)
+            assert ctx.gather_staging() == mode
+            ctx.step(1)
+            first = ctx.download(fluid=True)
+            ctx.set_launch({"gather": 296, "integrate": 592, "bin": 592, "search": 592, "overlap_gather": True})
+            assert ctx.gather_staging() == mode
+            ctx.step(5)
+            ctx.raise_status()
+            out[mode] = (first, ctx.download(fluid=True), ctx.collision_counters())
+    assert np.all(np.isfinite(out[0][0]["ufap"]))
+    for a, b in ((out[0][0], out[1][0]), (out[0][1], out[1][1])):
+        for k in a:
+            assert np.array_equal(a[k], b[k]), k
+    assert out[0][2] == out[1][2]

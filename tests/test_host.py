@@ -217,6 +217,13 @@ class _FakeLaunchLib:
     def gp_get_contact_tail(self, h, b):
         return 0
 
+    def gp_set_gather_staging(self, h, m):
+        self.staging = m
+        return 0
+
+    def gp_get_gather_staging(self, h, m):
+        return 0
+
 
 @pytest.mark.parametrize("choice", [0, 1, 2])
 def test_launch_choices_map_to_the_abi(monkeypatch, choice):
