@@ -236,12 +236,20 @@ static __device__ __forceinline__ void rel_flow(const MixedConst& mc, const doub
   q.b0 = dot3f(r[0], r[1], r[2], p0, p1, p2);
   q.b1 = dot3f(r[3], r[4], r[5], p0, p1, p2);
   q.b2 = dot3f(r[6], r[7], r[8], p0, p1, p2);
-  q.syz = sqrtf(__fmaf_rn(q.b2, q.b2, __fmul_rn(q.b1, q.b1)));
+  const float s2 = __fmaf_rn(q.b2, q.b2, __fmul_rn(q.b1, q.b1));
+  q.syz = sqrtf(s2);
   q.inv_syz = __frcp_rn(q.syz);   // used only where syz != 0
-  // atan2 of the magnitudes is |atan(syz / b0)|, pi/2 where b0 = 0
-  const float phi = atan2f(q.syz, fabsf(q.b0));
-  sincosf(phi, &q.sphi, &q.cphi);
-  q.cphi = fmaxf(q.cphi, 0.f);   // float(pi/2) lies above pi/2: keep cos(phi) >= 0 as in FP64
+  // phi = |atan(syz / b0)| (pi/2 where b0 = 0) has sin(phi) = syz / |b| and
+  // cos(phi) = |b0| / |b|: no angle needs forming (|b| = 0 gives phi = 0)
+  const float bb = __fmaf_rn(q.b0, q.b0, s2);
+  if (bb > 0.f) {
+    const float inv = rsqrtf(bb);
+    q.sphi = fminf(__fmul_rn(q.syz, inv), 1.f);
+    q.cphi = fminf(__fmul_rn(fabsf(q.b0), inv), 1.f);
+  } else {
+    q.sphi = 0.f;
+    q.cphi = 1.f;
+  }
   q.lr = __log2f(__fmul_rn(q.umag, mc.dv));
 }
 
@@ -388,7 +396,25 @@ __device__ __forceinline__ void quaternion_step_mixed(Quat& q, const float r[9],
     const float inv = rsqrtf(n2);
     const float h = __fmul_rn(__fmul_rn(n2, inv), (float)(dt * 0.5));
     float s, c;
-    sincosf(h, &s, &c);
+    if (h <= 0.785f) {
+      // Taylor series of sin and cos about 0, nested in h^2 up to the h^9 and h^10 terms:
+      // sin h = h (1 - h^2/(2.3) (1 - h^2/(4.5) (1 - h^2/(6.7) (1 - h^2/(8.9))))),
+      // cos h = 1 - h^2/(1.2) (1 - h^2/(3.4) (...(1 - h^2/(9.10)))); the first term left
+      // out is below 3e-9 for h <= pi/4, under FP32's rounding
+      const float h2 = __fmul_rn(h, h);
+      float ps = __fmaf_rn(-h2, 1.f / 72.f, 1.f);
+      ps = __fmaf_rn(__fmul_rn(-h2, 1.f / 42.f), ps, 1.f);
+      ps = __fmaf_rn(__fmul_rn(-h2, 1.f / 20.f), ps, 1.f);
+      ps = __fmaf_rn(__fmul_rn(-h2, 1.f / 6.f), ps, 1.f);
+      s = __fmul_rn(h, ps);
+      float pc = __fmaf_rn(-h2, 1.f / 90.f, 1.f);
+      pc = __fmaf_rn(__fmul_rn(-h2, 1.f / 56.f), pc, 1.f);
+      pc = __fmaf_rn(__fmul_rn(-h2, 1.f / 30.f), pc, 1.f);
+      pc = __fmaf_rn(__fmul_rn(-h2, 1.f / 12.f), pc, 1.f);
+      c = __fmaf_rn(__fmul_rn(-h2, 0.5f), pc, 1.f);
+    } else {
+      sincosf(h, &s, &c);
+    }
     const float si = __fmul_rn(s, inv);
     map = {(double)c, (double)__fmul_rn(si, g0), (double)__fmul_rn(si, g1), (double)__fmul_rn(si, g2)};
   }

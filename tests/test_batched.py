@@ -79,8 +79,9 @@ def test_autotune_keeps_the_state_and_the_results():
         for key in api.STATE_KEYS:
             assert np.array_equal(before[key], after[key]), key
         assert set(grids) == {"gather", "integrate", "bin", "search", "overlap_gather", "speculative_integrate",
-                              "contact_tail"}
+                              "contact_tail", "gather_staging"}
         assert grids["contact_tail"] == 0        # the default; the autotuner leaves it
+        assert grids["gather_staging"] == 0      # FP64: rows only
         assert all(grids[k] in (148, 296, 592, 1184, 2368) for k in ("gather", "integrate", "bin", "search"))
         # launch shapes change no result
         a.step(3)
