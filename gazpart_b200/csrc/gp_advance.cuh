@@ -221,6 +221,20 @@ __device__ __forceinline__ void rotmat_f(const Quat& q, float r[9]) {
   r[8] = __fsub_rn(1.f, __fmul_rn(2.f, __fmaf_rn(q1, q1, __fmul_rn(q2, q2))));
 }
 
+// 2^x and the square root as one hardware instruction each (ex2.approx, sqrt.approx):
+// relative errors near 2^-22, below the FP32 correlations' own 1e-7; sqrt(0) = 0 and
+// 2^-inf = 0 as the force and torque need.
+__device__ __forceinline__ float ex2_fast(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float sqrt_fast(float x) {
+  float y;
+  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
 // Slip velocity u_f - u_p in the body frame (R^T p), its magnitude, the magnitude of its
 // transverse part and the incidence angle phi = |atan(syz / b0)| in [0, pi/2].
 struct RelFlow {
@@ -232,12 +246,12 @@ struct RelFlow {
 static __device__ __forceinline__ void rel_flow(const MixedConst& mc, const double u[3], const double uf[3],
                                                 const float r[9], RelFlow& q) {
   const float p0 = (float)(uf[0] - u[0]), p1 = (float)(uf[1] - u[1]), p2 = (float)(uf[2] - u[2]);
-  q.umag = sqrtf(dot3f(p0, p1, p2, p0, p1, p2));
+  q.umag = sqrt_fast(dot3f(p0, p1, p2, p0, p1, p2));
   q.b0 = dot3f(r[0], r[1], r[2], p0, p1, p2);
   q.b1 = dot3f(r[3], r[4], r[5], p0, p1, p2);
   q.b2 = dot3f(r[6], r[7], r[8], p0, p1, p2);
   const float s2 = __fmaf_rn(q.b2, q.b2, __fmul_rn(q.b1, q.b1));
-  q.syz = sqrtf(s2);
+  q.syz = sqrt_fast(s2);
   q.inv_syz = __frcp_rn(q.syz);   // used only where syz != 0
   // phi = |atan(syz / b0)| (pi/2 where b0 = 0) has sin(phi) = syz / |b| and
   // cos(phi) = |b0| / |b|: no angle needs forming (|b| = 0 gives phi = 0)
@@ -254,22 +268,22 @@ static __device__ __forceinline__ void rel_flow(const MixedConst& mc, const doub
 }
 
 // x^y for x in [0, 1] and y > 0 (sines and cosines of the incidence angle raised to the
-// correlations' exponents) as 2^(y log2 x) with the hardware log2: an absolute error of
-// a few 1e-7 of the result where it is not negligible against the rest of the
+// correlations' exponents) as 2^(y log2 x) with the hardware log2 and exp2: an absolute
+// error of a few 1e-7 of the result where it is not negligible against the rest of the
 // coefficient, the size of the FP32 correlations' own rounding.  x = 0 gives 0.
-__device__ __forceinline__ float pow_unit(float x, float y) { return exp2f(y * __log2f(x)); }
+__device__ __forceinline__ float pow_unit(float x, float y) { return ex2_fast(y * __log2f(x)); }
 
 static __device__ __forceinline__ bool fluid_force_mixed(const PartConst& pc, const RelFlow& q, const float r[9],
                                                          double f[3]) {
   f[0] = f[1] = f[2] = 0.0;
   if (q.umag == 0.f) return true;
   const float lr = q.lr, sphi = q.sphi, cphi = q.cphi;
-  const float cd0 = __fmaf_rn(18.12f, exp2f(-1.023f * lr), __fmul_rn(4.26f, exp2f(-0.384f * lr)));
-  const float cd90 = __fmaf_rn(21.52f, exp2f(-0.990f * lr), __fmul_rn(2.86f, exp2f(-0.260f * lr)));
+  const float cd0 = __fmaf_rn(18.12f, ex2_fast(-1.023f * lr), __fmul_rn(4.26f, ex2_fast(-0.384f * lr)));
+  const float cd90 = __fmaf_rn(21.52f, ex2_fast(-0.990f * lr), __fmul_rn(2.86f, ex2_fast(-0.260f * lr)));
   const float cdrag = __fmaf_rn(__fsub_rn(cd90, cd0), pow_unit(sphi, 1.95f), cd0);
-  const float clift = __fmul_rn(__fmul_rn(__fmaf_rn(0.083f, exp2f(0.21f * lr), __fmul_rn(1.582f, exp2f(-0.851f * lr))),
-                                          pow_unit(sphi, __fmaf_rn(-0.802f, exp2f(-0.006f * lr), 1.842f))),
-                                pow_unit(cphi, __fmaf_rn(0.009f, exp2f(0.570f * lr), 0.874f)));
+  const float clift = __fmul_rn(__fmul_rn(__fmaf_rn(0.083f, ex2_fast(0.21f * lr), __fmul_rn(1.582f, ex2_fast(-0.851f * lr))),
+                                          pow_unit(sphi, __fmaf_rn(-0.802f, ex2_fast(-0.006f * lr), 1.842f))),
+                                pow_unit(cphi, __fmaf_rn(0.009f, ex2_fast(0.570f * lr), 0.874f)));
   const float cd = (float)pc.cdrag;
   const float kd = __fmul_rn(__fmul_rn(cd, cdrag), q.umag);
   const float kl = __fmul_rn(__fmul_rn(cd, clift), __fmul_rn(q.umag, q.umag));
@@ -295,15 +309,15 @@ static __device__ __forceinline__ void fluid_torque_mixed(const PartConst& pc, c
   const float c2 = dot3f(r[6], r[7], r[8], w0, w1, w2);
   const float o0 = __fmaf_rn(0.5f, c0, -(float)ox), o1 = __fmaf_rn(0.5f, c1, -(float)oy);
   const float o2 = __fmaf_rn(0.5f, c2, -(float)oz);
-  const float omag = sqrtf(dot3f(o0, o1, o2, o0, o1, o2));
-  const float oyz = sqrtf(__fmaf_rn(o2, o2, __fmul_rn(o1, o1)));
+  const float omag = sqrt_fast(dot3f(o0, o1, o2, o0, o1, o2));
+  const float oyz = sqrt_fast(__fmaf_rn(o2, o2, __fmul_rn(o1, o1)));
   t[0] = t[1] = t[2] = 0.0;
   if (q.umag != 0.f && q.syz != 0.f) {
     const float lr = q.lr, sphi = q.sphi, cphi = q.cphi;
     const float ctp =
-        __fmul_rn(__fmul_rn(__fmaf_rn(0.935f, exp2f(-0.146f * lr), __fmul_rn(-0.469f, exp2f(-0.145f * lr))),
-                            pow_unit(sphi, __fmaf_rn(0.748f, exp2f(0.041f * lr), 0.116f))),
-                  pow_unit(cphi, __fmaf_rn(0.657f, exp2f(0.044f * lr), 0.221f)));
+        __fmul_rn(__fmul_rn(__fmaf_rn(0.935f, ex2_fast(-0.146f * lr), __fmul_rn(-0.469f, ex2_fast(-0.145f * lr))),
+                            pow_unit(sphi, __fmaf_rn(0.748f, ex2_fast(0.041f * lr), 0.116f))),
+                  pow_unit(cphi, __fmaf_rn(0.657f, ex2_fast(0.044f * lr), 0.221f)));
     const float cp = __fmul_rn(__fmul_rn(__fmul_rn((float)pc.cpitch, ctp), __fmul_rn(q.umag, q.umag)), q.inv_syz);
     t[1] = (double)(cp * fabsf(q.b2) * copysignf(1.f, q.b0 * q.b2));
     t[2] = (double)(cp * fabsf(q.b1) * copysignf(1.f, q.b0 * q.b1));
@@ -311,8 +325,8 @@ static __device__ __forceinline__ void fluid_torque_mixed(const PartConst& pc, c
   const float re_r = __fmul_rn(omag, mc.d2v);
   if (re_r != 0.f) {
     const float lr = __log2f(re_r);
-    const float ctr = __fmaf_rn(0.573f, exp2f(-0.154f * lr), __fmul_rn(116.61f, __frcp_rn(re_r)));
-    const float ctr2 = __fmaf_rn(1.244f, exp2f(0.239f * lr), __fmul_rn(378.12f, exp2f(-0.789f * lr)));
+    const float ctr = __fmaf_rn(0.573f, ex2_fast(-0.154f * lr), __fmul_rn(116.61f, __frcp_rn(re_r)));
+    const float ctr2 = __fmaf_rn(1.244f, ex2_fast(0.239f * lr), __fmul_rn(378.12f, ex2_fast(-0.789f * lr)));
     const float k = (float)(pc.crot * pc.h5);
     t[0] += (double)(ctr * k * fabsf(o0) * o0);
     t[1] += (double)(ctr2 * k * oyz * o1);
