@@ -409,3 +409,44 @@ def test_stat_partfluid_known_values():
     assert v[6] == 0.0 or np.isnan(v[7])                           # no transverse lift (0/0 there)
     assert abs(v[22] - (2.0 / 9.0) * rhop * a * a / (s.rhof * s.visc)) < 1e-12 * v[22]
     assert v[35] == 1.0 and v[29] == 0.0
+
+
+def test_solve_lengths_persist_between_steps():
+    """The contact queue's premise, on the oracle: at the 512^3 workload's particle density
+    and sizes (a periodic sample of 4,096 spheroids), nearly every pair whose bounding
+    spheres overlap in a step overlapped in the step before, and the Levenberg-Marquardt
+    evaluation counts of the same pair in two consecutive steps correlate strongly."""
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+    w = config.WORKLOADS["c3_512cube_n16777216_fp32field"]
+    ens, refs, g = bench.cpu_sample(w, 16, bench.workload_max_emaj(w))
+    L = ens.setup.lx
+
+    def solve_lengths():
+        a = ens.a
+        home, near = po.detect_pairs(ens)
+        d = np.stack([a[k][near] - a[k][home] for k in ("x", "y", "z")], 1)
+        d -= L * np.round(d / L)
+        rb = lambda i: np.maximum(a["emaj"][i], a["emaj"][i] / a["apr"][i])   # noqa: E731
+        ok = (d * d).sum(1) <= (rb(home) + rb(near)) ** 2
+        out = {}
+        for e in np.flatnonzero(ok):
+            i1, i2 = int(home[e]), int(near[e])
+            b1 = np.array([a["x"][i1], a["y"][i1], a["z"][i1]])
+            q = [np.array([a[k][i] for k in ("qa", "qb", "qc", "qd")]) for i in (i1, i2)]
+            r = po.contact_detection(a["emaj"][i1], a["apr"][i1], a["emaj"][i2], a["apr"][i2],
+                                     b1, q[0], b1 + d[e], q[1])
+            out[(i1, i2)] = r["nfev"]
+        return out
+
+    first = solve_lengths()
+    assert ens.advance(refs, nthreads=4) == 0
+    assert ens.collide(prefilter=True, nthreads=4, grid=g)["rc"] == 0
+    second = solve_lengths()
+    both = [k for k in second if k in first]
+    assert len(second) >= 50
+    assert len(both) >= 0.9 * len(second)
+    a = np.array([first[k] for k in both], dtype=float)
+    b = np.array([second[k] for k in both], dtype=float)
+    assert np.corrcoef(a, b)[0, 1] > 0.6
