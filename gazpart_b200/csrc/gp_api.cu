@@ -429,7 +429,6 @@ int mark(gp_ctx *c, int slot, cudaStream_t s) {
   return GP_OK;
 }
 
-// Stencil gather at x_n for the particles in the last binning's order, on stream s.
 // The one field every live class reads (the TMA-staged gather maps a single field), or
 // false when they read several.
 bool single_field(const gp_ctx *c, const InstDev **out) {
@@ -462,6 +461,7 @@ int ensure_field_map(gp_ctx *c) {
   return GP_OK;
 }
 
+// Stencil gather at x_n for the particles in the last binning's order, on stream s.
 int enqueue_gather(gp_ctx *c, cudaStream_t s) {
   GP_TRY(mark(c, 2 * GP_PHASE_GATHER, s));
   if (c->prm.precision == GP_PREC_MIXED && c->gather_staging == 1 && ensure_field_map(c) == GP_OK)
