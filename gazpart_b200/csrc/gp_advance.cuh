@@ -184,19 +184,32 @@ __device__ __forceinline__ void gather6_fp32(const InstDev& I, const Stencil& s,
 // stays FP64.  The body-frame flow is shared by the force and the torque when both see
 // the same particle velocity (the first RK2 stage).
 // ---------------------------------------------------------------------------
+// Everything the mixed form's common path needs of a particle's constants, formed once:
+// the full PartConst is not kept, and the rare wall branches read it again from the pool,
+// so that the integrate holds fewer registers.
 struct MixedConst {
   float dv;               // deq / visc: particle Reynolds number per unit slip speed
   float d2v;              // deq^2 / visc: rotational Reynolds number per unit spin
-  double rix, riy, riz;   // 1 / principal moments of inertia (FP32 reciprocals)
+  float cd, cp, krot;     // cdrag, cpitch and crot * h5 in FP32
+  float rix, riy, riz;    // 1 / principal moments of inertia (FP32 reciprocals)
+  double dyz, dzx, dxy;   // ipyy - ipzz, ipzz - ipxx, ipxx - ipyy
+  double rmax;            // bounding radius max(a, b)
 };
 
 __device__ __forceinline__ void mixed_const(const PartConst& pc, double visc, MixedConst& mc) {
   const float vi = __frcp_rn((float)visc), d = (float)pc.deq;
   mc.dv = d * vi;
   mc.d2v = (d * d) * vi;
-  mc.rix = (double)__frcp_rn((float)pc.ipxx);
-  mc.riy = (double)__frcp_rn((float)pc.ipyy);
-  mc.riz = (double)__frcp_rn((float)pc.ipzz);
+  mc.cd = (float)pc.cdrag;
+  mc.cp = (float)pc.cpitch;
+  mc.krot = (float)(pc.crot * pc.h5);
+  mc.rix = __frcp_rn((float)pc.ipxx);
+  mc.riy = __frcp_rn((float)pc.ipyy);
+  mc.riz = __frcp_rn((float)pc.ipzz);
+  mc.dyz = pc.ipyy - pc.ipzz;
+  mc.dzx = pc.ipzz - pc.ipxx;
+  mc.dxy = pc.ipxx - pc.ipyy;
+  mc.rmax = fmax(pc.a, pc.b);
 }
 
 // The FP32 arithmetic of the mixed force, torque and rotation increment is written with
@@ -273,7 +286,7 @@ static __device__ __forceinline__ void rel_flow(const MixedConst& mc, const doub
 // coefficient, the size of the FP32 correlations' own rounding.  x = 0 gives 0.
 __device__ __forceinline__ float pow_unit(float x, float y) { return ex2_fast(y * __log2f(x)); }
 
-static __device__ __forceinline__ bool fluid_force_mixed(const PartConst& pc, const RelFlow& q, const float r[9],
+static __device__ __forceinline__ bool fluid_force_mixed(const MixedConst& mc, const RelFlow& q, const float r[9],
                                                          double f[3]) {
   f[0] = f[1] = f[2] = 0.0;
   if (q.umag == 0.f) return true;
@@ -284,7 +297,7 @@ static __device__ __forceinline__ bool fluid_force_mixed(const PartConst& pc, co
   const float clift = __fmul_rn(__fmul_rn(__fmaf_rn(0.083f, ex2_fast(0.21f * lr), __fmul_rn(1.582f, ex2_fast(-0.851f * lr))),
                                           pow_unit(sphi, __fmaf_rn(-0.802f, ex2_fast(-0.006f * lr), 1.842f))),
                                 pow_unit(cphi, __fmaf_rn(0.009f, ex2_fast(0.570f * lr), 0.874f)));
-  const float cd = (float)pc.cdrag;
+  const float cd = mc.cd;
   const float kd = __fmul_rn(__fmul_rn(cd, cdrag), q.umag);
   const float kl = __fmul_rn(__fmul_rn(cd, clift), __fmul_rn(q.umag, q.umag));
   const float fb0 = __fmaf_rn(kd, q.b0, __fmul_rn(__fmul_rn(kl, sphi), copysignf(1.f, -q.b0)));
@@ -300,7 +313,7 @@ static __device__ __forceinline__ bool fluid_force_mixed(const PartConst& pc, co
   return !(cdrag != cdrag) && isfinite(f[0]) && isfinite(f[1]) && isfinite(f[2]);
 }
 
-static __device__ __forceinline__ void fluid_torque_mixed(const PartConst& pc, const MixedConst& mc, const RelFlow& q,
+static __device__ __forceinline__ void fluid_torque_mixed(const MixedConst& mc, const RelFlow& q,
                                                           const double wv[3], double ox, double oy, double oz,
                                                           const float r[9], double t[3]) {
   const float w0 = (float)wv[0], w1 = (float)wv[1], w2 = (float)wv[2];
@@ -318,7 +331,7 @@ static __device__ __forceinline__ void fluid_torque_mixed(const PartConst& pc, c
         __fmul_rn(__fmul_rn(__fmaf_rn(0.935f, ex2_fast(-0.146f * lr), __fmul_rn(-0.469f, ex2_fast(-0.145f * lr))),
                             pow_unit(sphi, __fmaf_rn(0.748f, ex2_fast(0.041f * lr), 0.116f))),
                   pow_unit(cphi, __fmaf_rn(0.657f, ex2_fast(0.044f * lr), 0.221f)));
-    const float cp = __fmul_rn(__fmul_rn(__fmul_rn((float)pc.cpitch, ctp), __fmul_rn(q.umag, q.umag)), q.inv_syz);
+    const float cp = __fmul_rn(__fmul_rn(__fmul_rn(mc.cp, ctp), __fmul_rn(q.umag, q.umag)), q.inv_syz);
     t[1] = (double)(cp * fabsf(q.b2) * copysignf(1.f, q.b0 * q.b2));
     t[2] = (double)(cp * fabsf(q.b1) * copysignf(1.f, q.b0 * q.b1));
   }
@@ -327,7 +340,7 @@ static __device__ __forceinline__ void fluid_torque_mixed(const PartConst& pc, c
     const float lr = __log2f(re_r);
     const float ctr = __fmaf_rn(0.573f, ex2_fast(-0.154f * lr), __fmul_rn(116.61f, __frcp_rn(re_r)));
     const float ctr2 = __fmaf_rn(1.244f, ex2_fast(0.239f * lr), __fmul_rn(378.12f, ex2_fast(-0.789f * lr)));
-    const float k = (float)(pc.crot * pc.h5);
+    const float k = mc.krot;
     t[0] += (double)(ctr * k * fabsf(o0) * o0);
     t[1] += (double)(ctr2 * k * oyz * o1);
     t[2] += (double)(ctr2 * k * oyz * o2);
@@ -347,13 +360,13 @@ struct Forces {
     if (kMixed) {
       RelFlow qf;
       rel_flow(mc, u, uf, r, qf);
-      const bool ok = fluid_force_mixed(pc, qf, r, f);
+      const bool ok = fluid_force_mixed(mc, qf, r, f);
       if (same_u) {
-        fluid_torque_mixed(pc, mc, qf, wv, ox, oy, oz, r, t);
+        fluid_torque_mixed(mc, qf, wv, ox, oy, oz, r, t);
       } else {
         RelFlow qt;
         rel_flow(mc, un, uf, r, qt);
-        fluid_torque_mixed(pc, mc, qt, wv, ox, oy, oz, r, t);
+        fluid_torque_mixed(mc, qt, wv, ox, oy, oz, r, t);
       }
       return ok;
     } else {
@@ -383,9 +396,9 @@ template <bool kMixed>
 __device__ __forceinline__ void k_omega(const double t[3], double ox, double oy, double oz, const PartConst& pc,
                                         const MixedConst& mc, double k[3]) {
   if (kMixed) {
-    k[0] = (t[0] + oy * oz * (pc.ipyy - pc.ipzz)) * mc.rix;
-    k[1] = (t[1] + oz * ox * (pc.ipzz - pc.ipxx)) * mc.riy;
-    k[2] = (t[2] + ox * oy * (pc.ipxx - pc.ipyy)) * mc.riz;
+    k[0] = (t[0] + oy * oz * mc.dyz) * (double)mc.rix;
+    k[1] = (t[1] + oz * ox * mc.dzx) * (double)mc.riy;
+    k[2] = (t[2] + ox * oy * mc.dxy) * (double)mc.riz;
   } else {
     k[0] = (t[0] + oy * oz * (pc.ipyy - pc.ipzz)) / pc.ipxx;
     k[1] = (t[1] + oz * ox * (pc.ipzz - pc.ipxx)) / pc.ipyy;
@@ -446,20 +459,50 @@ __device__ __forceinline__ void quat_advance(Quat& q, const float r[9], double o
 
 // One particle of adv_particle_new.f90:268-637.  State in/out in registers.
 // Returns 0 or an error code.
+__device__ __forceinline__ void load_pc(const PoolView& P, int64_t i, PartConst& pc) {
+  pc.a = P.pc[0][i]; pc.b = P.pc[1][i]; pc.deq = P.pc[2][i]; pc.cdrag = P.pc[3][i];
+  pc.cpitch = P.pc[4][i]; pc.crot = P.pc[5][i]; pc.h5 = P.pc[6][i];
+  pc.ipxx = P.pc[7][i]; pc.ipyy = P.pc[8][i]; pc.ipzz = P.pc[9][i];
+}
+
+// wall_test for the advance: the FP64 form has the particle's constants at hand; the
+// mixed form takes wall_test's own early exit (centre farther than 1.5 bounding radii
+// from the chosen plane: no intersection) before it reads them back from the pool.
 template <bool kMixed>
-__device__ __forceinline__ int advance_particle(const InstDev& I, const PartConst& pc, const double uf[3],
+__device__ __forceinline__ int wall_test_adv(double lx, const PartConst& pc, const PoolView& S, int64_t si,
+                                             double rmax, double xp, double yp, double zp, const Quat& q,
+                                             double wn[3], double arm[3], double& delta_x, bool& isect) {
+  if (kMixed) {
+    const double wpos0 = (xp < lx / 2.0) ? 0.0 : lx;
+    if (fabs(xp - wpos0) > 1.5 * rmax) {
+      arm[0] = arm[1] = arm[2] = 0.0;
+      isect = false;
+      wn[0] = (xp < lx / 2.0) ? 1.0 : -1.0;
+      wn[1] = 0.0; wn[2] = 0.0;
+      return 0;
+    }
+    PartConst full;
+    load_pc(S, si, full);
+    return wall_test(lx, full, rmax, xp, yp, zp, q, wn, arm, delta_x, isect);
+  }
+  return wall_test(lx, pc, rmax, xp, yp, zp, q, wn, arm, delta_x, isect);
+}
+
+// One particle of adv_particle_new.f90:268-637.  State in/out in registers.  The FP64
+// form takes the particle's constants in pc; the mixed form takes them formed in mc, and
+// reads them again from the pool (S, slot si) in the rare wall branches.
+// Returns 0 or an error code.
+template <bool kMixed>
+__device__ __forceinline__ int advance_particle(const InstDev& I, const PartConst& pc, const MixedConst& mc,
+                                                const PoolView& S, int64_t si, const double uf[3],
                                                 const double wv[3], double X[3], double U[3], double O[3],
                                                 Quat& Q) {
   const double dt = I.dtime;
-  const double rmax = fmax(pc.a, pc.b);
+  const double rmax = kMixed ? mc.rmax : fmax(pc.a, pc.b);
   const double un[3] = {U[0], U[1], U[2]};
   double f[3], t[3];
-  MixedConst mc;
   float r0[9], r1[9];   // R(Q) and R(q1) in FP32, mixed form only
-  if (kMixed) {
-    mixed_const(pc, I.visc, mc);
-    rotmat_f(Q, r0);
-  }
+  if (kMixed) rotmat_f(Q, r0);
   int err = 0;
   if (!Forces<kMixed>::eval(pc, I.visc, mc, un, un, true, uf, wv, O[0], O[1], O[2], Q, r0, f, t)) err = GP_ENAN_FORCE;
   if (O[0] != O[0] && !err) err = GP_ENAN_TORQUE;
@@ -474,7 +517,7 @@ __device__ __forceinline__ int advance_particle(const InstDev& I, const PartCons
   quat_advance<kMixed>(q1, r0, o1[0], o1[1], o1[2], dt);
   double wn[3], arm[3], delta_x = 0.0;
   bool isect;
-  int rc = wall_test(I.lx, pc, rmax, xp1, yp1, zp1, q1, wn, arm, delta_x, isect);
+  int rc = wall_test_adv<kMixed>(I.lx, pc, S, si, rmax, xp1, yp1, zp1, q1, wn, arm, delta_x, isect);
   if (rc && !err) err = rc;
   if (isect && u1[0] * wn[0] < 0.0) {
     // rebound branch, adv_particle_new.f90:358-511
@@ -496,7 +539,13 @@ __device__ __forceinline__ int advance_particle(const InstDev& I, const PartCons
     q1 = Q;
     if (kMixed) rotmat_f(Q, r0);   // rebuilt here, so that R(Q) need not stay live on the common path
     quat_advance<kMixed>(q1, r0, o1[0], o1[1], o1[2], dt - delt);
-    rc = wall_rebound(I.ecw, I.muw, pc, u1[0], u1[1], u1[2], o1[0], o1[1], o1[2], q1, arm, wn);
+    if (kMixed) {
+      PartConst full;
+      load_pc(S, si, full);
+      rc = wall_rebound(I.ecw, I.muw, full, u1[0], u1[1], u1[2], o1[0], o1[1], o1[2], q1, arm, wn);
+    } else {
+      rc = wall_rebound(I.ecw, I.muw, pc, u1[0], u1[1], u1[2], o1[0], o1[1], o1[2], q1, arm, wn);
+    }
     if (rc && !err) err = rc;
     if (kMixed) rotmat_f(q1, r1);
     if (!Forces<kMixed>::eval(pc, I.visc, mc, u1, un, false, uf, wv, o1[0], o1[1], o1[2], q1, r1, f, t) && !err)
@@ -529,7 +578,7 @@ __device__ __forceinline__ int advance_particle(const InstDev& I, const PartCons
   const double xp2 = X[0] + 0.5 * dt * (k1x[0] + k2x[0]);
   const double yp2 = X[1] + 0.5 * dt * (k1x[1] + k2x[1]);
   const double zp2 = X[2] + 0.5 * dt * (k1x[2] + k2x[2]);
-  rc = wall_test(I.lx, pc, rmax, xp2, yp2, zp2, q1, wn, arm, delta_x, isect);
+  rc = wall_test_adv<kMixed>(I.lx, pc, S, si, rmax, xp2, yp2, zp2, q1, wn, arm, delta_x, isect);
   if (rc && !err) err = rc;
   if (isect) {
 #pragma unroll
@@ -549,12 +598,6 @@ __device__ __forceinline__ int advance_particle(const InstDev& I, const PartCons
   Q = q1;
   quat_advance<kMixed>(Q, r1, O[0], O[1], O[2], dt);
   return err;
-}
-
-__device__ __forceinline__ void load_pc(const PoolView& P, int64_t i, PartConst& pc) {
-  pc.a = P.pc[0][i]; pc.b = P.pc[1][i]; pc.deq = P.pc[2][i]; pc.cdrag = P.pc[3][i];
-  pc.cpitch = P.pc[4][i]; pc.crot = P.pc[5][i]; pc.h5 = P.pc[6][i];
-  pc.ipxx = P.pc[7][i]; pc.ipyy = P.pc[8][i]; pc.ipzz = P.pc[9][i];
 }
 
 __device__ __forceinline__ float pick4(const float f[4], int k) {
@@ -717,6 +760,7 @@ __device__ __forceinline__ void integrate_slot(const InstDev* __restrict__ insts
   load_pc(*S, i, pc);
 #pragma unroll 1
   for (int c = 0; c < kNConst; ++c) D->pc[c][j] = S->pc[c][i];
+  MixedConst mc;
   double X[3] = {S->st[0][i], S->st[1][i], S->st[2][i]};
   double U[3] = {S->st[3][i], S->st[4][i], S->st[5][i]};
   Quat Q = {S->st[6][i], S->st[7][i], S->st[8][i], S->st[9][i]};
@@ -726,7 +770,8 @@ __device__ __forceinline__ void integrate_slot(const InstDev* __restrict__ insts
   // stencil out of range (reported by the gather): carried over unchanged
   if (inst >= 0 && !(uf[0] != uf[0] && wv[0] != wv[0])) {
     const InstDev& I = insts[inst];
-    const int err = advance_particle<kMixed>(I, pc, uf, wv, X, U, O, Q);
+    if (kMixed) mixed_const(pc, I.visc, mc);
+    const int err = advance_particle<kMixed>(I, pc, mc, *S, i, uf, wv, X, U, O, Q);
     if (err) set_error(st, err, (long long)S->id[i], inst);
     // adv_particle_new.f90:685-686: the channel wraps y and z only
     // (boundary_particle_yz.f90:44-70), the others every direction when periodic
