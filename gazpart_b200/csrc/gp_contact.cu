@@ -141,9 +141,9 @@ void launch_queue_order(const InstDev *insts, const PoolView *pv, const PairRec 
 // first pass takes the pairs in that order (the queue order above); hist (optional):
 // each pair's outcome is recorded there for the next collision phase's order.
 //
-// Passes.  A warp runs as long as its slowest lane, and a C3 step has about one solve per
-// lane of the persistent grid, so refilling cannot even out solves of 3 to 300
-// evaluations.  With `out` set, a solve still running after `budget` evaluations is
+// Passes.  A warp runs as long as its slowest lane, and a step at 512^3 with 16.8 M
+// spheroids has about one solve per lane of the persistent grid, so refilling cannot
+// even out solves of 3 to 300 evaluations.  With `out` set, a solve still running after `budget` evaluations is
 // written there (pair and solver state) and the lane takes other work; a further pass
 // of this kernel (`in` set) resumes those solves with every lane busy, under a larger
 // budget or none.  The iterates are the same operations in the same order.

@@ -34,9 +34,10 @@ namespace gp {
 // Correctly rounded FP64 division and square root of the solver, one place for every
 // site of the iteration.  They are in line by default.  Out of line
 // (GP_LM_CALLED_ARITH) each site becomes a call and the iteration's code shrinks by a
-// quarter, but on the B200 the bulk of 150k C3-like solves then took 4.45 ms against
-// 3.72 ms in line: the calls cost more than the smaller code saves once the norm's rare
-// paths are out of line (lm_enorm).
+// quarter, but on the B200 the bulk of 150k solves like those of the 512^3 /
+// 16.8 M-spheroid workload then took 4.45 ms against 3.72 ms in line: the calls cost
+// more than the smaller code saves once the norm's rare paths are out of line
+// (lm_enorm).
 #ifdef GP_LM_CALLED_ARITH
 #define GP_LM_ARITH static __device__ __noinline__
 #else

@@ -31,7 +31,8 @@
 ! Limits of this wrapper (not of the C ABI)
 !  - One context for all classes: GRAVITY, ECP and MUP are taken from class 1, and a run
 !    whose classes differ in them stops at COLLISION_INITIATION.
-!  - NPROC = 1 (one rank, one GPU), as the north star has it.
+!  - NPROC = 1 (one rank, one GPU): the path runs on one GPU, without the MPI domain
+!    decomposition.
 
 module gazpart_gpu
   use iso_c_binding

@@ -158,7 +158,7 @@ def _shard_rank_main(rank, world, port, out):
 
 @pytest.mark.parametrize("world", [2, 3])
 def test_batched_classes_shard_over_ranks(world):
-    """bench.py --gpus N splits C4's 64 classes over the ranks: every class on one rank,
+    """bench.py --gpus N splits the 64 classes of the 256^3 batched workload over the ranks: every class on one rank,
     the particle total summed across ranks equals the workload's, the shares balanced."""
     import torch.multiprocessing as mp
     ctx = mp.get_context("spawn")

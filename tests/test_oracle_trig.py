@@ -5,8 +5,8 @@
    oracle and the device share their own (Cody-Waite reduction by fdlibm's three-part
    pi/2, Taylor polynomials) so that their Levenberg-Marquardt iterates agree bit for
    bit.  The same restatement built with libm's functions (libgazpart_oracle_libm.so)
-   shows what that choice changes: no contact flag on 4,000 C3-like pairs, a few
-   evaluation counts, and no accepted pair over 20 steps of the dense and polydisperse
+   shows what that choice changes: no contact flag on 4,000 pairs like those of the
+   512^3 workload, a few evaluation counts, and no accepted pair over 20 steps of the dense and polydisperse
    cases.
 2. The prefilters.  The reference solves every candidate pair (Q12); the oracle and the
    device first drop pairs whose bodies are provably apart.  On the dense, polydisperse

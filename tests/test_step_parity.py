@@ -18,7 +18,7 @@ Each step n starts both sides from the same state S_n (the oracle's) and checks:
    stopping point (xtol = sqrt(eps)) moves with its inputs; its error is reported and
    bounded separately.
 
-The bars are the north star's: integer outputs and pair sets bit-exact, state 1e-12 per
+The bars: integer outputs and pair sets bit-exact, state 1e-12 per
 step."""
 from __future__ import annotations
 
