@@ -236,15 +236,16 @@ int make_field_map(const void* field, int nx, int ny, int nz, CUtensorMap* out) 
   using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                               const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                               CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-  static Encode encode = nullptr;
-  if (!encode) {
+  // looked up once (a thread-safe static initialisation); null if the driver lacks it
+  static const Encode encode = []() -> Encode {
     void* f = nullptr;
     cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
     if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
-        q != cudaDriverEntryPointSuccess || !f)
-      return GP_ECUDA;
-    encode = reinterpret_cast<Encode>(f);
-  }
+        q != cudaDriverEntryPointSuccess)
+      return nullptr;
+    return reinterpret_cast<Encode>(f);
+  }();
+  if (!encode) return GP_ECUDA;
   if (!field || (reinterpret_cast<uintptr_t>(field) & 15u) != 0) return GP_EBADARG;
   const cuuint64_t row = (cuuint64_t)kFieldStride * sizeof(float);
   const cuuint64_t dims[4] = {(cuuint64_t)kFieldStride, (cuuint64_t)nx + 3, (cuuint64_t)ny + 4, (cuuint64_t)nz + 4};
