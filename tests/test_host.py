@@ -26,6 +26,19 @@ def test_library_exports_every_declared_symbol():
     assert sorted(_lib.SIGNATURES) == names
 
 
+def test_tuning_entry_points_refuse_bad_arguments():
+    """The launch-tuning entry points check their arguments before they touch a device:
+    a null context or output pointer, or an out-of-range choice, is GP_EBADARG."""
+    L = _lib.lib()
+    ebadarg = 9
+    v = C.c_int32()
+    assert L.gp_set_contact_order(None, 1) == ebadarg
+    assert L.gp_get_contact_order(None, C.byref(v)) == ebadarg
+    assert L.gp_set_gather_staging(None, 1) == ebadarg
+    assert L.gp_get_gather_staging(None, C.byref(v)) == ebadarg
+    assert L.gp_set_contact_tail(None, 4) == ebadarg
+
+
 def test_params_struct_matches_header_layout():
     # gp_params: 3 int32, 11 doubles, 6 int32, 1 int64 with natural alignment
     assert C.sizeof(_lib.GPParams) == 3 * 4 + 4 + 11 * 8 + 6 * 4 + 8
