@@ -140,6 +140,18 @@ module gazpart_gpu
        real(c_double), intent(inout) :: part1(10), part2(10)
        real(c_double), intent(in) :: r1(3), r2(3), nrm(3)
      end function
+     ! Launch tuning, optional: a driver may call gp_autotune once after
+     ! COLLISION_INITIATION (it times the launch choices on the resident particles and
+     ! restores their state); no result depends on these choices.
+     integer(c_int) function gp_autotune(ctx, grids) bind(c, name='gp_autotune')
+       import; type(c_ptr), value :: ctx; integer(c_int32_t), intent(out) :: grids(5)
+     end function
+     integer(c_int) function gp_set_contact_order(ctx, on) bind(c, name='gp_set_contact_order')
+       import; type(c_ptr), value :: ctx; integer(c_int32_t), value :: on
+     end function
+     integer(c_int) function gp_set_gather_staging(ctx, mode) bind(c, name='gp_set_gather_staging')
+       import; type(c_ptr), value :: ctx; integer(c_int32_t), value :: mode
+     end function
   end interface
 end module gazpart_gpu
 
